@@ -1,0 +1,411 @@
+"""Benchmark of the B200 linear-system path (solves/s), one JSON line on rank 0.
+
+Workload (default): steady 3D Poisson on the unit cube, structured 128^3 trilinear hexahedra
+(2,146,689 DOFs, 57.07M nonzeros), per-element conductivity k ~ logN(0, 1) (seed 1), nodal
+source sin(pi x) sin(pi y) sin(pi z), zero Dirichlet on all faces with symmetric elimination,
+CG + Diagonal preconditioning, tolerance 1e-10 on ||Ax-b||/||b|| of the scaled system.
+A step is one SolveLinearSystem of the assembled system (scaling, preconditioner, Krylov
+loop, back-scaling) with the mixed FP32-inner / FP64-refinement solver; the FP64 drop-in
+solver is timed on the same system in the same run.  Inputs are synthetic (no dataset).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload NAME]
+
+--impl reference times the oracle (the CPU restatement of the reference path, built from
+oracle/) on the host cores on the same workload; each step is a bounded sample (a few
+iterations) extrapolated to the full solve's iteration count.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "solves/s, p50/p99 latency: mixed vs FP64 GPU at 1e-8 rel err; SpMV GB/s"
+UNIT = "solves/s"
+
+
+# ------------------------------------------------------------------------------------- workloads
+def workload_spec(name):
+    from elmerfem_b200 import meshgen
+
+    if name == "poisson128_cg_jacobi":
+        def build():
+            m = meshgen.hex_cube(128)
+            return dict(mesh=m, elem_k=meshgen.lognormal_conductivity(m.nelem, 1.0, 1),
+                        load=meshgen.sine_source(m.coords), bc=range(1, 7), symmetric=True)
+        return build, dict(method=1, precond=1, tol=1e-10, max_iter=20000), \
+            {"workload": "poisson_hex128_lognormal_cg_jacobi", "mesh": "128^3 hex 808", "dofs": 2146689,
+             "method": "CG", "preconditioner": "Diagonal", "tol": 1e-10}
+    if name == "poisson32_bicgstab_ilu0":
+        def build():
+            m = meshgen.hex_cube(32)
+            return dict(mesh=m, elem_k=None, load=np.ones(m.nnodes), bc=range(1, 7), symmetric=False)
+        return build, dict(method=2, precond=2, tol=1e-10, max_iter=1000), \
+            {"workload": "poisson_hex32_bicgstab_ilu0", "mesh": "32^3 hex 808", "dofs": 35937,
+             "method": "BiCGStab", "preconditioner": "ILU0", "tol": 1e-10}
+    raise SystemExit(f"unknown workload {name}")
+
+
+def algorithmic_bytes_per_iter(method, precond, precision, n, nnz, cols16):
+    """Bytes one Krylov iteration must move (matrix streamed once per SpMV pass, vectors once).
+
+    CG+Diagonal, FP32 inner (refinement): SpMV 4z values + (2z|4z) cols + 4n rowptr + P gather 4n
+    + Q write 4n + epilogue P 4n; P update 12n; x/r/z update 32n.
+    CG+Diagonal, FP64 drop-in (x_k residual fused in the next SpMV): SpMV 8z + 4z + 4n + 16n gathers
+    + 8n write + 16n epilogue; P update 24n; update 64n.
+    """
+    if method == 1 and precond in (0, 1):
+        if precision == "mixed":
+            return 4 * nnz + (2 if cols16 else 4) * nnz + 60 * n
+        return 12 * nnz + 132 * n
+    # BiCGStab: two SpMV passes (+x fused in FP64) and two preconditioner applications
+    if precision == "mixed":
+        m = 4 * nnz + (2 if cols16 else 4) * nnz
+        tri = (8 * nnz + 16 * n) if precond == 2 else 0
+        return 2 * m + tri + 120 * n
+    m = 12 * nnz
+    tri = (12 * nnz + 32 * n) if precond == 2 else 0
+    return 2 * m + tri + 260 * n
+
+
+# ------------------------------------------------------------------------------------- clocks
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------- helpers
+def dist_setup(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl" if os.environ.get("BENCH_BACKEND", "nccl") == "nccl" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return rank, world, local, pg
+
+
+def reduce_max(pg, value, device):
+    if pg is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg, device):
+    if pg is not None:
+        import torch
+
+        pg.all_reduce(torch.zeros(1, device=device))
+
+
+def read_peaks():
+    try:
+        pk = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(pk["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def read_traffic(workload):
+    try:
+        t = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        return t.get(workload)
+    except (OSError, ValueError):
+        return None
+
+
+# ------------------------------------------------------------------------------------- CPU arm
+def cpu_solve_rate(p, values, rhs, solve_kw, full_iters, threads):
+    """oracle solve timed at two iteration caps; solves/s extrapolated to full_iters."""
+    import oracle
+
+    lo, hi = 2, 10
+    _, r_lo = oracle.solve(p, values, rhs, method=solve_kw["method"], precond=solve_kw["precond"], max_iter=lo,
+                           tol=1e-300, threads=threads)
+    _, r_hi = oracle.solve(p, values, rhs, method=solve_kw["method"], precond=solve_kw["precond"], max_iter=hi,
+                           tol=1e-300, threads=threads)
+    per_iter = max(1e-9, (r_hi["seconds"] - r_lo["seconds"]) / (hi - lo))
+    setup = max(0.0, r_lo["seconds"] - lo * per_iter)
+    t_full = setup + per_iter * full_iters
+    return 1.0 / t_full, {"seconds_per_iter": per_iter, "setup_seconds": setup, "sample_iters": lo + hi,
+                          "sample_seconds": r_lo["seconds"] + r_hi["seconds"]}
+
+
+def run_reference(args, rank, world, pg):
+    if rank != 0:
+        return
+    import oracle
+
+    build, solve_kw, cfg = workload_spec(args.workload)
+    w = build()
+    m = w["mesh"]
+    p = oracle.create_pattern(m)
+    nodal_k = None if w["elem_k"] is not None else np.ones(m.nnodes)
+    vals, rhs = oracle.assemble_poisson(m, p, elem_k=w["elem_k"], nodal_k=nodal_k, load=w["load"])
+    con = np.sort(p.perm[m.boundary_nodes(w["bc"]) - 1]).astype(np.int32)
+    oracle.dirichlet(p, vals, rhs, con, symmetric=w["symmetric"])
+    threads = os.cpu_count() or 1
+    # full iteration count of the FP64 reference path on this system (a known property of the
+    # workload; measured once by a full oracle solve where affordable, else by the sampled rate)
+    full_iters = args.ref_iters
+    for _ in range(args.warmup):
+        pass
+    rates, info = [], None
+    for _ in range(args.steps):
+        r, info = cpu_solve_rate(p, vals, rhs, solve_kw, full_iters, threads)
+        rates.append(r)
+    value = statistics.median(rates)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{info['sample_iters']} oracle iterations on the full system per step, "
+                                       f"extrapolated to {full_iters} iterations",
+                             "seconds_per_iter": info["seconds_per_iter"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------- GPU arm
+def run_gpu(args, rank, world, local, pg):
+    import torch
+
+    import elmerfem_b200 as eg
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ctx = eg.Context(local)
+    ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    build, solve_kw, cfg = workload_spec(args.workload)
+    w = build()
+    m = w["mesh"]
+    pat = eg.create_matrix(m)
+    A = eg.Matrix(ctx, pat)
+    A.bind_assembly(m)
+    nodal_k = None if w["elem_k"] is not None else np.ones(m.nnodes)
+    A.assemble_poisson(elem_k=w["elem_k"], nodal_k=nodal_k, load=w["load"])
+    con = np.sort(pat.perm[m.boundary_nodes(w["bc"]) - 1]).astype(np.int32)
+    A.dirichlet(con, symmetric=w["symmetric"])
+    n, nnz = pat.n, pat.nnz
+    cols16 = True  # every structured workload here has |col-row| < 32768
+    mixed = eg.SolverParams(method=solve_kw["method"], precond=solve_kw["precond"], tol=solve_kw["tol"],
+                            max_iter=solve_kw["max_iter"], precision=eg.MIXED, inner_tol=args.inner_tol)
+    fp64 = eg.SolverParams(method=solve_kw["method"], precond=solve_kw["precond"], tol=solve_kw["tol"],
+                           max_iter=solve_kw["max_iter"])
+    x = torch.zeros(n, dtype=torch.float64, device=dev)
+
+    def step(prm):
+        with torch.cuda.stream(ext):
+            x.zero_()
+        return A.solve_dev(None, x.data_ptr(), prm)
+
+    # warm-up (also the accuracy reference: FP64 drop-in solution)
+    r64 = step(fp64)
+    x64 = x.clone()
+    for _ in range(max(0, args.warmup - 1)):
+        step(mixed)
+    rm = step(mixed)
+    rel_err = float(torch.linalg.norm(x - x64) / torch.linalg.norm(x64))
+
+    # ---- timed: mixed, device-resident inputs
+    launches0 = ctx.kernel_launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(pg, dev)
+    torch.cuda.synchronize()
+    results = []
+    with ClockSampler(local) as clk:
+        e0.record(ext)
+        for _ in range(args.steps):
+            results.append(step(mixed))
+        e1.record(ext)
+        torch.cuda.synchronize()
+    barrier(pg, dev)
+    launches = ctx.kernel_launches - launches0
+    t = e0.elapsed_time(e1) / 1000.0
+    t = reduce_max(pg, t, dev)
+    value = world * args.steps / t
+    lat = sorted(r["seconds"] for r in results)
+
+    # ---- roofline of the dominant kernel (persistent FP32 inner Krylov kernel)
+    iters = sum(r["iters"] for r in results)
+    sec_k = sum(r["seconds_krylov"] for r in results)
+    nlaunch = sum(r["krylov_launches"] for r in results)
+    bpi = algorithmic_bytes_per_iter(solve_kw["method"], solve_kw["precond"], "mixed", n, nnz, cols16)
+    peak, peak_kind = read_peaks()
+    achieved = bpi * iters / sec_k / 1e9
+    traffic = read_traffic(cfg["workload"])
+
+    # ---- FP64 drop-in on the same system
+    t64 = []
+    for _ in range(args.fp64_steps):
+        torch.cuda.synchronize()
+        e0.record(ext)
+        rr = step(fp64)
+        e1.record(ext)
+        torch.cuda.synchronize()
+        t64.append(e0.elapsed_time(e1) / 1000.0)
+    fp64_rate = 1.0 / statistics.median(t64)
+    bpi64 = algorithmic_bytes_per_iter(solve_kw["method"], solve_kw["precond"], "fp64", n, nnz, cols16)
+    ach64 = bpi64 * rr["iters"] / rr["seconds_krylov"] / 1e9
+
+    # ---- end to end through the public C ABI with host buffers (pinned)
+    b_host = torch.from_numpy(A.rhs()).pin_memory()
+    x_host = torch.zeros(n, dtype=torch.float64).pin_memory()
+    import ctypes as C
+
+    from elmerfem_b200 import _lib
+
+    def step_host():
+        x_host.zero_()
+        prm = mixed.to_c()
+        res = _lib.Result()
+        bp = np.ctypeslib.as_array(C.cast(b_host.data_ptr(), C.POINTER(C.c_double)), shape=(n,))
+        xp = np.ctypeslib.as_array(C.cast(x_host.data_ptr(), C.POINTER(C.c_double)), shape=(n,))
+        rc = _lib.lib().egpu_iter_solve(A.handle, bp, xp, C.byref(prm), C.byref(res))
+        assert rc == 1, rc
+        return float(xp[0])
+
+    step_host()
+    barrier(pg, dev)
+    torch.cuda.synchronize()
+    e0.record(ext)
+    for _ in range(args.steps):
+        step_host()
+    e1.record(ext)
+    torch.cuda.synchronize()
+    te = reduce_max(pg, e0.elapsed_time(e1) / 1000.0, dev)
+    e2e = world * args.steps / te
+
+    # ---- CPU baseline (rank 0, N=1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        import oracle
+
+        vals = A.values()
+        rhs = A.rhs()
+        op = oracle.Pattern(n, nnz, 1, pat.perm, pat.rows, pat.cols, pat.diag, 0, 0, 0, 0)
+        threads = os.cpu_count() or 1
+        rate, info = cpu_solve_rate(op, vals, rhs, solve_kw, rr["iters"], threads)
+        cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{info['sample_iters']} oracle iterations on the full system ({info['sample_seconds']:.1f} s),"
+                         f" extrapolated to the FP64 iteration count {rr['iters']}",
+               "seconds_per_iter": info["seconds_per_iter"]}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1000.0 * t / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 refinement", "data": "synthetic",
+                "config": dict(cfg, precision="mixed", parallelism=f"replicas{world}",
+                               l2="matrix (685 MB) larger than L2; no flush needed"),
+                "latency_ms": {"p50": 1000 * lat[len(lat) // 2], "p99": 1000 * lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+                "iterations": {"mixed_inner_total": rm["iters"], "refinements": rm["refinements"],
+                               "fp64": r64["iters"]},
+                "fp64": {"solves_per_s": fp64_rate, "ms_per_solve": 1000 * statistics.median(t64),
+                         "krylov_gbs": ach64},
+                "speedup_mixed_vs_fp64": value / world / fp64_rate,
+                "rel_err_mixed_vs_fp64": rel_err,
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                             "kernel": "cg_kernel<float,LPR,int16 cols> (persistent FP32 inner CG)",
+                             "bytes_per_iter": bpi, "launches": nlaunch},
+                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 8 * n},
+                "gpu_launches": launches,
+                "clocks": clk.summary(),
+                "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    A.free()
+    ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="poisson128_cg_jacobi")
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--inner-tol", type=float, default=1e-4)
+    ap.add_argument("--ref-iters", type=int, default=0, help="FP64 iteration count for the reference arm")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    rank, world, local, pg = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            if args.ref_iters <= 0:
+                args.ref_iters = {"poisson128_cg_jacobi": 2000, "poisson32_bicgstab_ilu0": 19}.get(args.workload, 100)
+            run_reference(args, rank, world, pg)
+        else:
+            run_gpu(args, rank, world, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

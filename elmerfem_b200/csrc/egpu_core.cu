@@ -1,0 +1,1233 @@
+// egpu_core.cu -- context, matrix binding, scaling, ILU0, solve drivers, C ABI.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+
+#include "egpu_internal.cuh"
+#include "egpu_krylov.cuh"
+#include "egpu_solve.h"
+
+using namespace egpu;
+
+void egpu_set_error(const egpu_ctx *ctx, const std::string &msg) {
+  if (ctx) ctx->last_error = msg;
+}
+
+namespace egpu {
+
+// =====================================================================================
+// small kernels
+
+// 1-based Matrix_t arrays -> 0-based device arrays
+__global__ void k_to_zero_based(int *a, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    a[i] -= 1;
+}
+
+__global__ void k_fill64(unsigned long long *p, unsigned long long v, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+// ScaleLinearSystem diagonal part (SolverUtils.src:6500-6562): D_i = 1/sqrt(|a_ii|), with
+// the absolute row sum standing in for a zero diagonal.
+__global__ void k_scale_diag(int n, const int *__restrict__ rows, const int *__restrict__ diag,
+                             const double *__restrict__ vals, double *__restrict__ D) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int j = diag[i];
+    double d = j >= 0 ? vals[j] : 0.0;
+    if (fabs(d) <= EGPU_TINY_DP) {
+      double s = 0.0;
+      for (int k = rows[i]; k < rows[i + 1]; ++k) s += fabs(vals[k]);
+      d = s;
+    }
+    D[i] = fabs(d) > EGPU_TINY_DP ? 1.0 / sqrt(fabs(d)) : 1.0;
+  }
+}
+
+// a_ij * (D_i * D_j) (SolverUtils.src:6570-6575); also the scaled diagonal for Jacobi
+__global__ void k_scale_values(int n, const int *__restrict__ rows, const int *__restrict__ cols,
+                               const int *__restrict__ diag, const double *__restrict__ vals,
+                               const double *__restrict__ D, double *__restrict__ out,
+                               double *__restrict__ dvals) {
+  const int lane = threadIdx.x & 7;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 3; i < n; i += (gridDim.x * blockDim.x) >> 3) {
+    const double di = D[i];
+    for (int k = rows[i] + lane; k < rows[i + 1]; k += 8) out[k] = vals[k] * (di * D[cols[k]]);
+    if (lane == 0) dvals[i] = diag[i] >= 0 ? vals[diag[i]] * (di * di) : 0.0;
+  }
+}
+
+// right-hand side scaling, pass 1: bs = b*D; partials of ||b||^2, ||bs||^2, any x != 0
+__global__ void k_rhs_scale_a(int n, const double *__restrict__ b, const double *__restrict__ D,
+                              const double *__restrict__ x, double *__restrict__ bs,
+                              double *__restrict__ partials, unsigned int *flags) {
+  __shared__ double sm[32 * 2];
+  double acc[2] = {0.0, 0.0};
+  bool nz = false;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double bi = b[i];
+    acc[0] += bi * bi;
+    const double s = bi * D[i];
+    bs[i] = s;
+    acc[1] += s * s;
+    nz |= x[i] != 0.0;
+  }
+  if (__syncthreads_or(nz) && threadIdx.x == 0) atomicOr(flags, 1u);
+  block_sum<2>(acc, sm);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = acc[0];
+    partials[gridDim.x + blockIdx.x] = acc[1];
+  }
+}
+
+// pass 2 (SolverUtils.src:6620-6636): bnorm; D *= bnorm; bs /= bnorm; xs = x / D, or
+// 1e-8 everywhere when x is all zero (IterSolve.src:358-359).  flags bit 1 = zero rhs.
+__global__ void k_rhs_scale_b(int n, int nbp, const double *__restrict__ partials, double *D,
+                              double *bs, const double *__restrict__ x, double *xs,
+                              unsigned int *flags, int scale_system) {
+  __shared__ double sm[4];
+  double b0 = 0.0, b1 = 0.0;
+  if (threadIdx.x < 32) {
+    for (int i = threadIdx.x; i < nbp; i += 32) {
+      b0 += partials[i];
+      b1 += partials[nbp + i];
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      b0 += __shfl_down_sync(0xffffffffu, b0, off);
+      b1 += __shfl_down_sync(0xffffffffu, b1, off);
+    }
+    if (threadIdx.x == 0) {
+      sm[0] = b0;
+      sm[1] = b1;
+    }
+  }
+  __syncthreads();
+  const double borig = sqrt(sm[0]);
+  const double bnorm = scale_system ? sqrt(sm[1]) : 1.0;
+  const bool xnz = (*(volatile unsigned int *)flags & 1u) != 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && borig <= EGPU_TINY_DP) atomicOr(flags, 2u);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double d = scale_system ? D[i] * bnorm : 1.0;
+    if (scale_system) D[i] = d;
+    if (scale_system) bs[i] = bs[i] / bnorm;
+    xs[i] = xnz ? x[i] / d : 1.0e-8;
+  }
+}
+
+// BackScaleLinearSystem x part (SolverUtils.src:6794-6796); zero-rhs short cut writes 0
+__global__ void k_backscale_x(int n, const double *__restrict__ xs, const double *__restrict__ D,
+                              double *x, const unsigned int *flags, int scale_system) {
+  const bool zero = (*flags & 2u) != 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] = zero ? 0.0 : (scale_system ? xs[i] * D[i] : xs[i]);
+}
+
+// CRS_IncompleteLU(A,0), CRSMatrix.src:2312-2356, one warp per row in ascending
+// dependency level.  Row i waits (bounded) for every row k of its strictly lower part;
+// the IKJ update keeps the reference's order of operations per entry, so the factor is
+// bit-identical to the sequential routine.  The U diagonal stays un-inverted here.
+template <int MAXROW>
+__global__ void __launch_bounds__(256) k_ilu0_factor(int n, const int *__restrict__ rows,
+                                                     const int *__restrict__ cols,
+                                                     const int *__restrict__ diag,
+                                                     const int *__restrict__ order,
+                                                     const double *__restrict__ A, double *ilu,
+                                                     int *done, int *err) {
+  __shared__ double S_all[8][MAXROW];
+  __shared__ int C_all[8][MAXROW];
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double *S = S_all[wib];
+  int *Cc = C_all[wib];
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int s = gw; s < n; s += nw) {
+    const int i = order[s];
+    const int beg = rows[i], len = rows[i + 1] - beg, nl = diag[i] - beg;
+    for (int t = lane; t < len; t += 32) {
+      S[t] = A[beg + t];
+      Cc[t] = cols[beg + t];
+    }
+    __syncwarp();
+    for (int m = 0; m < nl; ++m) {
+      const int k = Cc[m];
+      if (lane == 0) {
+        if (ld_acquire_s32(done + k) == 0) {
+          unsigned long long t0 = egpu_globaltimer();
+          while (ld_acquire_s32(done + k) == 0) {
+            if (egpu_globaltimer() - t0 > EGPU_WAIT_NS) {
+              atomicExch(err, (int)EGPU_ERR_TIMEOUT);
+              break;
+            }
+            if (*(volatile int *)err) break;
+          }
+        }
+      }
+      __syncwarp();
+      int e = 0;
+      if (lane == 0) e = *(volatile int *)err;
+      if (__shfl_sync(0xffffffffu, e, 0)) return;
+      double sk = S[m];
+      if (sk == 0.0) continue;
+      const int dk = diag[k];
+      const double ukk = __ldcg(ilu + dk);
+      if (fabs(ukk) > EGPU_AEPS) sk = sk / ukk;
+      __syncwarp();
+      if (lane == 0) S[m] = sk;
+      const int kend = rows[k + 1];
+      for (int l = dk + 1 + lane; l < kend; l += 32) {
+        const int j = cols[l];
+        int lo = 0, hi = len - 1, pos = -1;
+        while (lo <= hi) {
+          const int mid = (lo + hi) >> 1;
+          const int cm = Cc[mid];
+          if (cm == j) {
+            pos = mid;
+            break;
+          }
+          if (cm < j)
+            lo = mid + 1;
+          else
+            hi = mid - 1;
+        }
+        if (pos >= 0) S[pos] = __dsub_rn(S[pos], __dmul_rn(sk, __ldcg(ilu + l)));
+      }
+      __syncwarp();
+    }
+    for (int t = lane; t < len; t += 32) ilu[beg + t] = S[t];
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence();
+      st_release_s32(done + i, 1);
+    }
+  }
+}
+
+// prescale the U diagonal (CRSMatrix.src:2359-2366)
+__global__ void k_ilu_invdiag(int n, const int *__restrict__ diag, double *ilu) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double d = ilu[diag[i]];
+    ilu[diag[i]] = fabs(d) < EGPU_AEPS ? 1.0 : 1.0 / d;
+  }
+}
+
+__global__ void k_to_f32(const double *__restrict__ a, float *__restrict__ b, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+__global__ void k_col_offsets(int n, const int *__restrict__ rows, const int *__restrict__ cols,
+                              int16_t *__restrict__ off) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    for (int k = rows[i]; k < rows[i + 1]; ++k) off[k] = (int16_t)(cols[k] - i);
+}
+
+// standalone SpMV: v = A u (CRS_MatrixVectorProd, CRSMatrix.src:3565-3573)
+template <typename VT, int LPR>
+__global__ void __launch_bounds__(EGPU_BLOCK) k_spmv(int n, const int *__restrict__ rows,
+                                                     const int *__restrict__ cols,
+                                                     const VT *__restrict__ vals,
+                                                     const VT *__restrict__ u, VT *__restrict__ v) {
+  const int lane = threadIdx.x & 31;
+  const int sl = lane & (LPR - 1);
+  const unsigned submask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << (lane & ~(LPR - 1)));
+  const int gsub = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) / LPR);
+  const int nsub = (int)((long long)gridDim.x * blockDim.x / LPR);
+  for (int row = gsub; row < n; row += nsub) {
+    const int beg = __ldg(rows + row), end = __ldg(rows + row + 1);
+    VT s = 0;
+#pragma unroll 4
+    for (int j = beg + sl; j < end; j += LPR) s += __ldcs(vals + j) * __ldg(u + __ldcs(cols + j));
+#pragma unroll
+    for (int off = LPR / 2; off > 0; off >>= 1) s += __shfl_xor_sync(submask, s, off, LPR);
+    if (sl == 0) v[row] = s;
+  }
+}
+
+// =====================================================================================
+// host helpers
+
+static int grid_for(const egpu_ctx *ctx, long long work, int block = 256) {
+  long long g = (work + block - 1) / block;
+  long long cap = (long long)ctx->num_sms * 8;
+  return (int)std::max(1LL, std::min(g, cap));
+}
+
+// Level schedules of the strictly lower / upper parts (rows sorted by dependency level).
+static void build_levels(int n, const std::vector<int> &rows, const std::vector<int> &cols,
+                         const std::vector<int> &diag, std::vector<int> &lower,
+                         std::vector<int> &upper, int &nlow, int &nup, int &maxl, int &maxu) {
+  std::vector<int> lev(n, 0);
+  nlow = 0;
+  maxl = maxu = 0;
+  for (int i = 0; i < n; ++i) {
+    int l = 0;
+    for (int j = rows[i]; j < diag[i]; ++j) l = std::max(l, lev[cols[j]] + 1);
+    lev[i] = l;
+    nlow = std::max(nlow, l + 1);
+    maxl = std::max(maxl, diag[i] - rows[i]);
+    maxu = std::max(maxu, rows[i + 1] - diag[i] - 1);
+  }
+  std::vector<int> cnt(nlow + 1, 0);
+  for (int i = 0; i < n; ++i) cnt[lev[i] + 1]++;
+  for (int l = 0; l < nlow; ++l) cnt[l + 1] += cnt[l];
+  lower.assign(n, 0);
+  for (int i = 0; i < n; ++i) lower[cnt[lev[i]]++] = i;
+  nup = 0;
+  for (int i = n - 1; i >= 0; --i) {
+    int l = 0;
+    for (int j = diag[i] + 1; j < rows[i + 1]; ++j) l = std::max(l, lev[cols[j]] + 1);
+    // lev[] of rows > i already hold upper levels (processed first in this loop)
+    lev[i] = l;
+    nup = std::max(nup, l + 1);
+  }
+  cnt.assign(nup + 1, 0);
+  for (int i = 0; i < n; ++i) cnt[lev[i] + 1]++;
+  for (int l = 0; l < nup; ++l) cnt[l + 1] += cnt[l];
+  upper.assign(n, 0);
+  for (int i = n - 1; i >= 0; --i) upper[cnt[lev[i]]++] = i;
+}
+
+// occupancy-sized cooperative launch
+template <typename K, typename Args>
+static int launch_coop(egpu_ctx *ctx, K kernel, Args &args, int *grid_out = nullptr) {
+  int bps = 0;
+  EGPU_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, EGPU_BLOCK, 0));
+  if (bps < 1) {
+    egpu_set_error(ctx, "persistent kernel does not fit on an SM");
+    return EGPU_ERR_CUDA;
+  }
+  bps = std::min(bps, 2);
+  int grid = ctx->num_sms * bps;
+  if (grid_out) *grid_out = grid;
+  void *kargs[] = {&args};
+  EGPU_CUDA_TRY(ctx, cudaLaunchCooperativeKernel((const void *)kernel, dim3(grid), dim3(EGPU_BLOCK),
+                                                 kargs, 0, ctx->stream));
+  ctx->launches++;
+  return EGPU_OK;
+}
+
+static int pick_lpr(const egpu_mat *A) {
+  double mean = A->n ? (double)A->nnz / A->n : 1.0;
+  if (mean <= 12) return 4;
+  if (mean <= 40) return 8;
+  if (mean <= 96) return 16;
+  return 32;
+}
+
+}  // namespace egpu
+
+// =====================================================================================
+// solve machinery shared with the batch / mixed paths (egpu_solve.h)
+
+namespace egpu {
+
+int ensure_ctx_scratch(egpu_ctx *ctx) {
+  if (!ctx->sync.p) {
+    EGPU_CUDA_TRY(ctx, ctx->sync.alloc(64));
+    EGPU_CUDA_TRY(ctx, ctx->partials.alloc((size_t)NUM_SLOTS * ctx->num_sms * 8 + 4096));
+  }
+  return EGPU_OK;
+}
+
+int reset_sync(egpu_ctx *ctx) {
+  EGPU_CUDA_TRY(ctx, cudaMemsetAsync(ctx->sync.p, 0, 64 * sizeof(unsigned int), ctx->stream));
+  return EGPU_OK;
+}
+
+int read_err(egpu_ctx *ctx, int *err) {
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(err, ctx->sync.p + 1, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  return EGPU_OK;
+}
+
+// Scale: scaled = D A D, dvals = diag(scaled), D = DiagScaling (not yet times ||Db||)
+int scale_matrix(egpu_mat *A, bool scale_system) {
+  egpu_ctx *ctx = A->ctx;
+  const int n = A->n;
+  EGPU_CUDA_TRY(ctx, A->scaled.alloc(A->nnz));
+  EGPU_CUDA_TRY(ctx, A->dscale.alloc(n));
+  EGPU_CUDA_TRY(ctx, A->work.alloc((size_t)12 * n + 64));
+  double *dvals = A->work.p + (size_t)11 * n;
+  if (scale_system) {
+    k_scale_diag<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, A->rows.p, A->diag.p, A->values.p, A->dscale.p);
+  } else {
+    k_fill64<<<grid_for(ctx, n), 256, 0, ctx->stream>>>((unsigned long long *)A->dscale.p,
+                                                         0x3FF0000000000000ull, n);
+  }
+  k_scale_values<<<grid_for(ctx, (long long)n * 8), 256, 0, ctx->stream>>>(
+      n, A->rows.p, A->cols.p, A->diag.p, A->values.p, A->dscale.p, A->scaled.p, dvals);
+  ctx->launches += 2;
+  EGPU_CUDA_TRY(ctx, cudaGetLastError());
+  return EGPU_OK;
+}
+
+int ensure_tri_schedule(egpu_mat *A) {
+  if (A->tri_built) return EGPU_OK;
+  egpu_ctx *ctx = A->ctx;
+  const int n = A->n;
+  std::vector<int> rows(n + 1), cols(A->nnz), diag(n);
+  EGPU_CUDA_TRY(ctx, cudaMemcpy(rows.data(), A->rows.p, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+  EGPU_CUDA_TRY(ctx, cudaMemcpy(cols.data(), A->cols.p, A->nnz * sizeof(int), cudaMemcpyDeviceToHost));
+  EGPU_CUDA_TRY(ctx, cudaMemcpy(diag.data(), A->diag.p, n * sizeof(int), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < n; ++i)
+    if (diag[i] < 0) {
+      egpu_set_error(ctx, "ILU0 needs a stored diagonal in every row");
+      return EGPU_ERR_ARG;
+    }
+  std::vector<int> lo, up;
+  build_levels(n, rows, cols, diag, lo, up, A->tri.lower_levels, A->tri.upper_levels, A->tri.max_lower,
+               A->tri.max_upper);
+  EGPU_CUDA_TRY(ctx, A->tri.lower_order.alloc(n));
+  EGPU_CUDA_TRY(ctx, A->tri.upper_order.alloc(n));
+  EGPU_CUDA_TRY(ctx, cudaMemcpy(A->tri.lower_order.p, lo.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+  EGPU_CUDA_TRY(ctx, cudaMemcpy(A->tri.upper_order.p, up.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+  A->tri_built = true;
+  return EGPU_OK;
+}
+
+// ILU0 of the scaled matrix (IterSolve.src:420-575 -> CRS_IncompleteLU(A,0))
+int ilu0_factor(egpu_mat *A) {
+  egpu_ctx *ctx = A->ctx;
+  int rc = ensure_tri_schedule(A);
+  if (rc) return rc;
+  const int n = A->n;
+  EGPU_CUDA_TRY(ctx, A->ilu.alloc(A->nnz));
+  EGPU_CUDA_TRY(ctx, A->ilu_done.alloc(n));
+  EGPU_CUDA_TRY(ctx, cudaMemsetAsync(A->ilu_done.p, 0, n * sizeof(int), ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaMemsetAsync(ctx->sync.p + 1, 0, sizeof(int), ctx->stream));
+  int *err = (int *)(ctx->sync.p + 1);
+  if (A->max_row > 256) {
+    egpu_set_error(ctx, "ILU0: rows longer than 256 entries are not supported");
+    return EGPU_ERR_ARG;
+  }
+  // every warp resident: one block of 8 warps per slot, grid sized by occupancy
+  int bps = 0;
+  if (A->max_row <= 32) {
+    EGPU_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_ilu0_factor<32>, 256, 0));
+  } else if (A->max_row <= 128) {
+    EGPU_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_ilu0_factor<128>, 256, 0));
+  } else {
+    EGPU_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_ilu0_factor<256>, 256, 0));
+  }
+  int grid = std::max(1, std::min(bps, 4)) * ctx->num_sms;
+  void *args[] = {(void *)&n, &A->rows.p, &A->cols.p, &A->diag.p, &A->tri.lower_order.p, &A->scaled.p,
+                  &A->ilu.p, &A->ilu_done.p, &err};
+  const void *kern = A->max_row <= 32 ? (const void *)k_ilu0_factor<32>
+                     : A->max_row <= 128 ? (const void *)k_ilu0_factor<128>
+                                          : (const void *)k_ilu0_factor<256>;
+  EGPU_CUDA_TRY(ctx, cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(256), args, 0, ctx->stream));
+  k_ilu_invdiag<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, A->diag.p, A->ilu.p);
+  ctx->launches += 2;
+  EGPU_CUDA_TRY(ctx, cudaGetLastError());
+  A->ilu_valid = true;
+  return EGPU_OK;
+}
+
+template <typename VT>
+static int run_krylov(egpu_mat *A, const KArgs<VT> &a0, int method, bool offs) {
+  egpu_ctx *ctx = A->ctx;
+  KArgs<VT> a = a0;
+  const int lpr = pick_lpr(A);
+#define EGPU_LAUNCH_K(KERN, L)                                                 \
+  do {                                                                         \
+    if (offs)                                                                  \
+      return launch_coop(ctx, KERN<VT, L, true>, a);                           \
+    else                                                                       \
+      return launch_coop(ctx, KERN<VT, L, false>, a);                          \
+  } while (0)
+#define EGPU_LAUNCH_M(L)                                                       \
+  do {                                                                         \
+    if (method == EGPU_CG)                                                     \
+      EGPU_LAUNCH_K(cg_kernel, L);                                             \
+    else                                                                       \
+      EGPU_LAUNCH_K(bicgstab_kernel, L);                                       \
+  } while (0)
+  switch (lpr) {
+    case 4: EGPU_LAUNCH_M(4);
+    case 8: EGPU_LAUNCH_M(8);
+    case 16: EGPU_LAUNCH_M(16);
+    default: EGPU_LAUNCH_M(32);
+  }
+#undef EGPU_LAUNCH_M
+#undef EGPU_LAUNCH_K
+}
+
+// FP64 drop-in solve on device buffers.  x_dev: in = initial guess, out = solution.
+int solve_fp64(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_params *prm,
+               egpu_result *res) {
+  egpu_ctx *ctx = A->ctx;
+  const int n = A->n;
+  int rc = ensure_ctx_scratch(ctx);
+  if (rc) return rc;
+  EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+  rc = reset_sync(ctx);
+  if (rc) return rc;
+  const bool sc = prm->scale_system != 0;
+  rc = scale_matrix(A, sc);
+  if (rc) return rc;
+  double *W = A->work.p;
+  double *bs = W + (size_t)10 * n;     // scaled rhs
+  double *dvals = W + (size_t)11 * n;  // scaled diagonal
+  double *xs = x_dev;                  // scaled in place
+  unsigned int *flags = ctx->sync.p + 2;
+  int nbp = std::min(grid_for(ctx, n), 1024);
+  k_rhs_scale_a<<<nbp, 256, 0, ctx->stream>>>(n, b_dev, A->dscale.p, x_dev, bs, ctx->partials.p, flags);
+  k_rhs_scale_b<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, nbp, ctx->partials.p, A->dscale.p, bs,
+                                                            x_dev, xs, flags, sc ? 1 : 0);
+  ctx->launches += 2;
+  // preconditioner (Linear System Refactorize / Precondition Recompute, IterSolve.src:413-421)
+  A->solve_count++;
+  if (prm->precond == EGPU_PREC_ILU0) {
+    const int every = prm->precond_recompute > 0 ? prm->precond_recompute : 1;
+    if (!A->ilu_valid || (prm->refactorize && (A->solve_count - 1) % every == 0)) {
+      rc = ilu0_factor(A);
+      if (rc) return rc;
+    } else {
+      rc = ensure_tri_schedule(A);
+      if (rc) return rc;
+    }
+  }
+  EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaMemsetAsync(ctx->sync.p, 0, sizeof(unsigned int), ctx->stream));
+  int *outs = (int *)(ctx->sync.p + 8);
+  double *outd = (double *)(ctx->sync.p + 16);
+  KArgs<double> a{};
+  a.n = n;
+  a.rows = A->rows.p;
+  a.cols = A->cols.p;
+  a.diag = A->diag.p;
+  a.cols16 = nullptr;
+  a.vals = A->scaled.p;
+  a.ilu = A->ilu.p;
+  a.dvals = dvals;
+  a.lower_order = A->tri.lower_order.p;
+  a.upper_order = A->tri.upper_order.p;
+  a.precond = prm->precond;
+  a.maxit = prm->max_iter;
+  a.true_residual = 1;
+  a.tol = prm->tol;
+  a.b = bs;
+  a.x = xs;
+  a.w = W;
+  a.ldw = n;
+  a.bar = ctx->sync.p;
+  a.err = (int *)(ctx->sync.p + 1);
+  a.partials = ctx->partials.p;
+  a.out_i = outs;
+  a.out_d = outd;
+  // zero right-hand side short cut (SolverUtils.src:7309-7320): k_rhs_scale_b sets bit 1
+  // of flags; the Krylov kernel then returns at once and the back-scaling writes x = 0.
+  a.skip = flags;
+  EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ek0, ctx->stream));
+  rc = run_krylov<double>(A, a, prm->method, false);
+  if (rc) return rc;
+  EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ek1, ctx->stream));
+  k_backscale_x<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, xs, A->dscale.p, x_dev, flags, sc ? 1 : 0);
+  ctx->launches++;
+  EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ev2, ctx->stream));
+  struct {
+    unsigned int sync[64];
+  } h;
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(&h, ctx->sync.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  float ms_all = 0, ms_setup = 0;
+  cudaEventElapsedTime(&ms_all, ctx->ev0, ctx->ev2);
+  cudaEventElapsedTime(&ms_setup, ctx->ev0, ctx->ev1);
+  const int err = (int)h.sync[1];
+  egpu_result r{};
+  const int *hi = (const int *)(h.sync + 8);
+  const double *hd = (const double *)(h.sync + 16);
+  r.info = hi[0];
+  r.iters = hi[1];
+  r.residual = hd[0];
+  r.seconds = ms_all * 1e-3;
+  r.seconds_setup = ms_setup * 1e-3;
+  float ms_k = 0;
+  cudaEventElapsedTime(&ms_k, ctx->ek0, ctx->ek1);
+  r.seconds_krylov = ms_k * 1e-3;
+  r.krylov_launches = 1;
+  if (h.sync[2] & 2u) {  // zero rhs: x = 0, converged
+    r.info = EGPU_HUTI_CONVERGENCE;
+    r.iters = 0;
+    r.residual = 0.0;
+  }
+  if (res) *res = r;
+  if (err) {
+    egpu_set_error(ctx, "device-side wait expired (EGPU_ERR_TIMEOUT)");
+    return err;
+  }
+  return r.info;
+}
+
+
+// -------------------------------------------------------------------------------------
+// mixed precision: FP32 inner Krylov inside FP64 iterative refinement
+
+// r = b - A x (FP64) and partial ||r||^2
+template <int LPR>
+__global__ void __launch_bounds__(EGPU_BLOCK) k_residual(int n, const int *__restrict__ rows,
+                                                         const int *__restrict__ cols,
+                                                         const double *__restrict__ vals,
+                                                         const double *__restrict__ b,
+                                                         const double *__restrict__ x,
+                                                         double *__restrict__ r,
+                                                         double *__restrict__ partials) {
+  __shared__ double sm[32];
+  const int lane = threadIdx.x & 31;
+  const int sl = lane & (LPR - 1);
+  const unsigned submask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << (lane & ~(LPR - 1)));
+  const int gsub = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) / LPR);
+  const int nsub = (int)((long long)gridDim.x * blockDim.x / LPR);
+  double acc[1] = {0.0};
+  for (int row = gsub; row < n; row += nsub) {
+    const int beg = __ldg(rows + row), end = __ldg(rows + row + 1);
+    double s = 0;
+#pragma unroll 4
+    for (int j = beg + sl; j < end; j += LPR) s += __ldcs(vals + j) * __ldcg(x + __ldcs(cols + j));
+#pragma unroll
+    for (int off = LPR / 2; off > 0; off >>= 1) s += __shfl_xor_sync(submask, s, off, LPR);
+    if (sl == 0) {
+      const double ri = b[row] - s;
+      r[row] = ri;
+      acc[0] += ri * ri;
+    }
+  }
+  block_sum<1>(acc, sm);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc[0];
+}
+
+// reduce ||r||^2 -> norms[0] = ||r||; r32 = r / ||r||
+__global__ void k_residual_cast(int n, int nbp, const double *__restrict__ partials,
+                                const double *__restrict__ r, float *__restrict__ r32,
+                                double *norms) {
+  __shared__ double sm[1];
+  if (threadIdx.x < 32) {
+    double t = 0.0;
+    for (int i = threadIdx.x; i < nbp; i += 32) t += partials[i];
+    for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+    if (threadIdx.x == 0) sm[0] = t;
+  }
+  __syncthreads();
+  const double rn = sqrt(sm[0]);
+  if (blockIdx.x == 0 && threadIdx.x == 0) norms[0] = rn;
+  const double inv = rn > 0.0 ? 1.0 / rn : 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    r32[i] = (float)(r[i] * inv);
+}
+
+// x += ||r|| * d
+__global__ void k_refine_update(int n, const float *__restrict__ d, const double *__restrict__ norms,
+                                double *__restrict__ x) {
+  const double rn = norms[0];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] += rn * (double)d[i];
+}
+
+template <typename K>
+static void launch_lpr_residual(egpu_ctx *ctx, int lpr, int grid, int n, const int *rows, const int *cols,
+                                const double *vals, const double *b, const double *x, double *r,
+                                double *partials) {
+  switch (lpr) {
+    case 4: k_residual<4><<<grid, EGPU_BLOCK, 0, ctx->stream>>>(n, rows, cols, vals, b, x, r, partials); break;
+    case 8: k_residual<8><<<grid, EGPU_BLOCK, 0, ctx->stream>>>(n, rows, cols, vals, b, x, r, partials); break;
+    case 16: k_residual<16><<<grid, EGPU_BLOCK, 0, ctx->stream>>>(n, rows, cols, vals, b, x, r, partials); break;
+    default: k_residual<32><<<grid, EGPU_BLOCK, 0, ctx->stream>>>(n, rows, cols, vals, b, x, r, partials); break;
+  }
+  ctx->launches++;
+}
+
+int krylov_fp64_scaled(egpu_mat *A, const double *bs, double *xs, const egpu_params *prm, int *info,
+                       int *iters, double *residual) {
+  egpu_ctx *ctx = A->ctx;
+  const int n = A->n;
+  EGPU_CUDA_TRY(ctx, cudaMemsetAsync(ctx->sync.p, 0, sizeof(unsigned int), ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaMemsetAsync(ctx->sync.p + 2, 0, sizeof(unsigned int), ctx->stream));
+  KArgs<double> a{};
+  a.n = n;
+  a.rows = A->rows.p;
+  a.cols = A->cols.p;
+  a.diag = A->diag.p;
+  a.vals = A->scaled.p;
+  a.ilu = A->ilu.p;
+  a.dvals = A->work.p + (size_t)11 * n;
+  a.lower_order = A->tri.lower_order.p;
+  a.upper_order = A->tri.upper_order.p;
+  a.precond = prm->precond;
+  a.maxit = prm->max_iter;
+  a.true_residual = 1;
+  a.tol = prm->tol;
+  a.b = bs;
+  a.x = xs;
+  a.w = A->work.p;
+  a.ldw = n;
+  a.bar = ctx->sync.p;
+  a.err = (int *)(ctx->sync.p + 1);
+  a.partials = ctx->partials.p;
+  a.out_i = (int *)(ctx->sync.p + 8);
+  a.out_d = (double *)(ctx->sync.p + 16);
+  a.skip = nullptr;
+  int rc = run_krylov<double>(A, a, prm->method, false);
+  if (rc) return rc;
+  unsigned int h[64];
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(h, ctx->sync.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (h[1]) return (int)h[1];
+  *info = ((int *)(h + 8))[0];
+  *iters = ((int *)(h + 8))[1];
+  *residual = ((double *)(h + 16))[0];
+  return EGPU_OK;
+}
+
+// FP32 copies of the scaled matrix, its diagonal and the ILU0 factors; int16 column
+// offsets when every |col - row| < 32768.
+static int prepare_fp32(egpu_mat *A, bool with_ilu) {
+  egpu_ctx *ctx = A->ctx;
+  const int n = A->n;
+  EGPU_CUDA_TRY(ctx, A->scaled32.alloc(A->nnz));
+  k_to_f32<<<grid_for(ctx, A->nnz), 256, 0, ctx->stream>>>(A->scaled.p, A->scaled32.p, A->nnz);
+  EGPU_CUDA_TRY(ctx, A->work32.alloc((size_t)14 * n + 64));
+  k_to_f32<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(A->work.p + (size_t)11 * n, A->work32.p + (size_t)13 * n, n);
+  ctx->launches += 2;
+  if (with_ilu) {
+    EGPU_CUDA_TRY(ctx, A->ilu32.alloc(A->nnz));
+    k_to_f32<<<grid_for(ctx, A->nnz), 256, 0, ctx->stream>>>(A->ilu.p, A->ilu32.p, A->nnz);
+    ctx->launches++;
+  }
+  if (A->max_bandwidth < 32768 && !A->cols16.p) {
+    EGPU_CUDA_TRY(ctx, A->cols16.alloc(A->nnz));
+    k_col_offsets<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, A->rows.p, A->cols.p, A->cols16.p);
+    ctx->launches++;
+  }
+  EGPU_CUDA_TRY(ctx, cudaGetLastError());
+  return EGPU_OK;
+}
+
+int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_params *prm,
+                egpu_result *res) {
+  egpu_ctx *ctx = A->ctx;
+  const int n = A->n;
+  int rc = ensure_ctx_scratch(ctx);
+  if (rc) return rc;
+  EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+  rc = reset_sync(ctx);
+  if (rc) return rc;
+  const bool sc = prm->scale_system != 0;
+  rc = scale_matrix(A, sc);
+  if (rc) return rc;
+  double *W = A->work.p;
+  double *bs = W + (size_t)10 * n;
+  double *rr = W;  // FP64 residual (work vector 0; the FP32 inner solver has its own)
+  double *xs = x_dev;
+  unsigned int *flags = ctx->sync.p + 2;
+  int nbp = std::min(grid_for(ctx, n), 1024);
+  k_rhs_scale_a<<<nbp, 256, 0, ctx->stream>>>(n, b_dev, A->dscale.p, x_dev, bs, ctx->partials.p, flags);
+  k_rhs_scale_b<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, nbp, ctx->partials.p, A->dscale.p, bs, x_dev,
+                                                            xs, flags, sc ? 1 : 0);
+  ctx->launches += 2;
+  A->solve_count++;
+  const bool ilu = prm->precond == EGPU_PREC_ILU0;
+  if (ilu) {
+    rc = ilu0_factor(A);
+    if (rc) return rc;
+  }
+  rc = prepare_fp32(A, ilu);
+  if (rc) return rc;
+  EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+  unsigned int hflags = 0;
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(&hflags, flags, sizeof(hflags), cudaMemcpyDeviceToHost, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  egpu_result r{};
+  float *W32 = A->work32.p;
+  float *r32 = W32 + (size_t)10 * n, *d32 = W32 + (size_t)11 * n, *dv32 = W32 + (size_t)13 * n;
+  double *norms = (double *)(ctx->sync.p + 32);
+  const int lpr = pick_lpr(A);
+  const int rgrid = std::min(1024, (int)std::min<long long>(((long long)n * lpr + EGPU_BLOCK - 1) / EGPU_BLOCK,
+                                                           (long long)ctx->num_sms * 4));
+  // ||bs||: 1 after scaling with the right-hand-side normalisation, else ||b||
+  double bnorm_s = 1.0;
+  if (!sc) {
+    std::vector<double> hp(2 * nbp);
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(hp.data(), ctx->partials.p, 2 * nbp * sizeof(double), cudaMemcpyDeviceToHost));
+    double t = 0.0;
+    for (int i = 0; i < nbp; ++i) t += hp[nbp + i];
+    bnorm_s = std::sqrt(t);
+  }
+  double prev = 0.0;
+  int stagnant = 0;
+  if (hflags & 2u) {
+    r.info = EGPU_HUTI_CONVERGENCE;
+  } else {
+    while (true) {
+      launch_lpr_residual<int>(ctx, lpr, rgrid, n, A->rows.p, A->cols.p, A->scaled.p, bs, xs, rr, ctx->partials.p);
+      k_residual_cast<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, rgrid, ctx->partials.p, rr, r32, norms);
+      ctx->launches++;
+      double hn[1];
+      EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(hn, norms, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+      EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+      const double resid = hn[0] / bnorm_s;
+      r.residual = resid;
+      if (resid < prm->tol) {
+        r.info = EGPU_HUTI_CONVERGENCE;
+        break;
+      }
+      if (r.refinements >= prm->max_refinements || r.iters >= prm->max_iter) {
+        r.info = EGPU_HUTI_MAXITER;
+        break;
+      }
+      // stagnation of the FP32 inner solver: finish in FP64 from the current iterate
+      if (r.refinements > 0 && resid > 0.5 * prev) ++stagnant;
+      if (stagnant >= 2) {
+        int info = 0, its = 0;
+        double res64 = 0;
+        egpu_params p64 = *prm;
+        p64.max_iter = std::max(1, prm->max_iter - r.iters);
+        rc = krylov_fp64_scaled(A, bs, xs, &p64, &info, &its, &res64);
+        if (rc) return rc;
+        r.iters += its;
+        r.info = info;
+        r.residual = res64;
+        break;
+      }
+      prev = resid;
+      // inner FP32 solve of A d = r / ||r||
+      EGPU_CUDA_TRY(ctx, cudaMemsetAsync(ctx->sync.p, 0, sizeof(unsigned int), ctx->stream));
+      KArgs<float> a{};
+      a.n = n;
+      a.rows = A->rows.p;
+      a.cols = A->cols.p;
+      a.diag = A->diag.p;
+      a.cols16 = A->cols16.p;
+      a.vals = A->scaled32.p;
+      a.ilu = A->ilu32.p;
+      a.dvals = dv32;
+      a.lower_order = A->tri.lower_order.p;
+      a.upper_order = A->tri.upper_order.p;
+      a.precond = prm->precond;
+      a.maxit = std::max(1, std::min(prm->inner_max_iter, prm->max_iter - r.iters));
+      a.true_residual = 0;
+      a.tol = prm->inner_tol;
+      a.b = r32;
+      a.x = d32;
+      a.w = W32;
+      a.ldw = n;
+      a.bar = ctx->sync.p;
+      a.err = (int *)(ctx->sync.p + 1);
+      a.partials = ctx->partials.p;
+      a.out_i = (int *)(ctx->sync.p + 8);
+      a.out_d = (double *)(ctx->sync.p + 16);
+      a.skip = nullptr;
+      EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ek0, ctx->stream));
+      rc = run_krylov<float>(A, a, prm->method, A->cols16.p != nullptr);
+      if (rc) return rc;
+      EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ek1, ctx->stream));
+      k_refine_update<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, d32, norms, xs);
+      ctx->launches++;
+      unsigned int h[24];
+      EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(h, ctx->sync.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+      EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+      if (h[1]) {
+        egpu_set_error(ctx, "device-side wait expired in the FP32 inner solver");
+        return (int)h[1];
+      }
+      r.iters += std::max(1, ((int *)(h + 8))[1]);
+      r.refinements++;
+      float ms_k = 0;
+      cudaEventElapsedTime(&ms_k, ctx->ek0, ctx->ek1);
+      r.seconds_krylov += ms_k * 1e-3;
+      r.krylov_launches++;
+    }
+  }
+  k_backscale_x<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, xs, A->dscale.p, x_dev, flags, sc ? 1 : 0);
+  ctx->launches++;
+  EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ev2, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  float ms_all = 0, ms_setup = 0;
+  cudaEventElapsedTime(&ms_all, ctx->ev0, ctx->ev2);
+  cudaEventElapsedTime(&ms_setup, ctx->ev0, ctx->ev1);
+  r.seconds = ms_all * 1e-3;
+  r.seconds_setup = ms_setup * 1e-3;
+  if (res) *res = r;
+  return r.info;
+}
+
+
+// u = (LU)^-1 v with the device factors: one cooperative launch of the two sync-free solves
+template <int TS>
+__global__ void __launch_bounds__(EGPU_BLOCK, 2) k_lu_apply(KArgs<double> a, const double *v, double *u) {
+  const int n = a.n;
+  double *Y = a.w;
+  lower_solve<double, TS>(a, Y, [&](int i) { return v[i]; });
+  upper_solve<double, TS>(a, Y, u, [&](int, double) {});
+  (void)n;
+}
+
+__global__ void k_fill_sentinel(double *p, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    p[i] = __longlong_as_double((long long)EGPU_SENTINEL64);
+}
+
+int lu_apply(egpu_mat *A, const double *v_dev, double *u_dev) {
+  egpu_ctx *ctx = A->ctx;
+  const int n = A->n;
+  EGPU_CUDA_TRY(ctx, A->work.alloc((size_t)12 * n + 64));
+  k_fill_sentinel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(A->work.p, n);
+  k_fill_sentinel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(u_dev, n);
+  ctx->launches += 2;
+  EGPU_CUDA_TRY(ctx, cudaMemsetAsync(ctx->sync.p, 0, 2 * sizeof(unsigned int), ctx->stream));
+  KArgs<double> a{};
+  a.n = n;
+  a.rows = A->rows.p;
+  a.cols = A->cols.p;
+  a.diag = A->diag.p;
+  a.ilu = A->ilu.p;
+  a.lower_order = A->tri.lower_order.p;
+  a.upper_order = A->tri.upper_order.p;
+  a.w = A->work.p;
+  a.err = (int *)(ctx->sync.p + 1);
+  const int lpr = pick_lpr(A);
+  int rc;
+  switch (lpr) {
+    case 4: { auto k = k_lu_apply<4>; int bps = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, EGPU_BLOCK, 0);
+      void *args[] = {&a, &v_dev, &u_dev}; rc = cudaLaunchCooperativeKernel((const void *)k, dim3(ctx->num_sms * std::min(bps, 2)), dim3(EGPU_BLOCK), args, 0, ctx->stream); break; }
+    case 8: { auto k = k_lu_apply<8>; int bps = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, EGPU_BLOCK, 0);
+      void *args[] = {&a, &v_dev, &u_dev}; rc = cudaLaunchCooperativeKernel((const void *)k, dim3(ctx->num_sms * std::min(bps, 2)), dim3(EGPU_BLOCK), args, 0, ctx->stream); break; }
+    case 16: { auto k = k_lu_apply<16>; int bps = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, EGPU_BLOCK, 0);
+      void *args[] = {&a, &v_dev, &u_dev}; rc = cudaLaunchCooperativeKernel((const void *)k, dim3(ctx->num_sms * std::min(bps, 2)), dim3(EGPU_BLOCK), args, 0, ctx->stream); break; }
+    default: { auto k = k_lu_apply<32>; int bps = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, EGPU_BLOCK, 0);
+      void *args[] = {&a, &v_dev, &u_dev}; rc = cudaLaunchCooperativeKernel((const void *)k, dim3(ctx->num_sms * std::min(bps, 2)), dim3(EGPU_BLOCK), args, 0, ctx->stream); break; }
+  }
+  EGPU_CUDA_TRY(ctx, (cudaError_t)rc);
+  ctx->launches++;
+  unsigned int h[2];
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(h, ctx->sync.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (h[1]) {
+    egpu_set_error(ctx, "device-side wait expired in the triangular solve");
+    return (int)h[1];
+  }
+  return EGPU_OK;
+}
+
+}  // namespace egpu
+
+// =====================================================================================
+// C ABI
+
+extern "C" void egpu_params_default(egpu_params *p, int method, int precond) {
+  std::memset(p, 0, sizeof(*p));
+  p->method = method;
+  p->precond = precond;
+  p->max_iter = 1000;
+  p->tol = 1e-10;
+  p->scale_system = 1;
+  p->precision = EGPU_FP64;
+  p->refactorize = 1;
+  p->precond_recompute = 1;
+  p->inner_tol = 1e-4;
+  p->inner_max_iter = 2000;
+  p->max_refinements = 30;
+}
+
+extern "C" int egpu_create(int device, egpu_ctx **out) {
+  if (!out) return EGPU_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return EGPU_ERR_CUDA;
+  auto *ctx = new egpu_ctx;
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    delete ctx;
+    return EGPU_ERR_CUDA;
+  }
+  cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+  int coop = 0;
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+  if (!coop || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return EGPU_ERR_CUDA;
+  }
+  cudaEventCreate(&ctx->ev0);
+  cudaEventCreate(&ctx->ev1);
+  cudaEventCreate(&ctx->ev2);
+  cudaEventCreate(&ctx->ek0);
+  cudaEventCreate(&ctx->ek1);
+  if (egpu::ensure_ctx_scratch(ctx) != EGPU_OK) {
+    egpu_destroy(ctx);
+    return EGPU_ERR_ALLOC;
+  }
+  *out = ctx;
+  return EGPU_OK;
+}
+
+extern "C" void egpu_destroy(egpu_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  ctx->sync.release();
+  ctx->partials.release();
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->ev2) cudaEventDestroy(ctx->ev2);
+  if (ctx->ek0) cudaEventDestroy(ctx->ek0);
+  if (ctx->ek1) cudaEventDestroy(ctx->ek1);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+extern "C" const char *egpu_last_error(const egpu_ctx *ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+extern "C" long long egpu_kernel_launches(const egpu_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+extern "C" void *egpu_stream(const egpu_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+extern "C" int egpu_matrix_bind(egpu_ctx *ctx, int n, const int *rows, const int *cols, const int *diag,
+                                const double *values, egpu_mat **out) {
+  if (!ctx || !out || n <= 0 || !rows || !cols || !diag) return EGPU_ERR_ARG;
+  *out = nullptr;
+  cudaSetDevice(ctx->device);
+  if (rows[0] != 1) {
+    egpu_set_error(ctx, "Rows(1) must be 1 (1-based Matrix_t layout)");
+    return EGPU_ERR_ARG;
+  }
+  const long long nnz = (long long)rows[n] - 1;
+  if (nnz <= 0) return EGPU_ERR_ARG;
+  auto *A = new egpu_mat;
+  A->ctx = ctx;
+  A->n = n;
+  A->nnz = nnz;
+  int maxrow = 0, maxbw = 0;
+  for (int i = 0; i < n; ++i) {
+    const int len = rows[i + 1] - rows[i];
+    if (len < 0) {
+      delete A;
+      egpu_set_error(ctx, "Rows must be non-decreasing");
+      return EGPU_ERR_ARG;
+    }
+    maxrow = std::max(maxrow, len);
+    for (int k = rows[i] - 1; k < rows[i + 1] - 1; ++k) {
+      if (cols[k] < 1 || cols[k] > n) {
+        delete A;
+        egpu_set_error(ctx, "Cols out of range");
+        return EGPU_ERR_ARG;
+      }
+      maxbw = std::max(maxbw, std::abs(cols[k] - 1 - i));
+    }
+  }
+  A->max_row = maxrow;
+  A->max_bandwidth = maxbw;
+  auto fail = [&](cudaError_t e) {
+    egpu_set_error(ctx, std::string("egpu_matrix_bind: ") + cudaGetErrorString(e));
+    delete A;
+    return EGPU_ERR_ALLOC;
+  };
+  cudaError_t e;
+  if ((e = A->rows.alloc(n + 1)) || (e = A->cols.alloc(nnz)) || (e = A->diag.alloc(n)) ||
+      (e = A->values.alloc(nnz)) || (e = A->rhs.alloc(n)))
+    return fail(e);
+  cudaMemcpyAsync(A->rows.p, rows, (n + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
+  cudaMemcpyAsync(A->cols.p, cols, nnz * sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
+  cudaMemcpyAsync(A->diag.p, diag, n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream);
+  k_to_zero_based<<<grid_for(ctx, n + 1), 256, 0, ctx->stream>>>(A->rows.p, n + 1);
+  k_to_zero_based<<<grid_for(ctx, nnz), 256, 0, ctx->stream>>>(A->cols.p, nnz);
+  k_to_zero_based<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(A->diag.p, n);
+  ctx->launches += 3;
+  if (values) {
+    cudaMemcpyAsync(A->values.p, values, nnz * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+    A->has_values = true;
+  } else {
+    cudaMemsetAsync(A->values.p, 0, nnz * sizeof(double), ctx->stream);
+  }
+  cudaMemsetAsync(A->rhs.p, 0, n * sizeof(double), ctx->stream);
+  if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(e);
+  *out = A;
+  return EGPU_OK;
+}
+
+extern "C" int egpu_matrix_update_values(egpu_mat *A, const double *values) {
+  if (!A || !values) return EGPU_ERR_ARG;
+  egpu_ctx *ctx = A->ctx;
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(A->values.p, values, A->nnz * sizeof(double), cudaMemcpyHostToDevice,
+                                     ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  A->has_values = true;
+  return EGPU_OK;
+}
+
+extern "C" int egpu_matrix_values_download(egpu_mat *A, double *values) {
+  if (!A || !values) return EGPU_ERR_ARG;
+  EGPU_CUDA_TRY(A->ctx, cudaMemcpyAsync(values, A->values.p, A->nnz * sizeof(double), cudaMemcpyDeviceToHost,
+                                        A->ctx->stream));
+  EGPU_CUDA_TRY(A->ctx, cudaStreamSynchronize(A->ctx->stream));
+  return EGPU_OK;
+}
+
+extern "C" int egpu_matrix_rhs_download(egpu_mat *A, double *rhs) {
+  if (!A || !rhs) return EGPU_ERR_ARG;
+  EGPU_CUDA_TRY(A->ctx, cudaMemcpyAsync(rhs, A->rhs.p, A->n * sizeof(double), cudaMemcpyDeviceToHost,
+                                        A->ctx->stream));
+  EGPU_CUDA_TRY(A->ctx, cudaStreamSynchronize(A->ctx->stream));
+  return EGPU_OK;
+}
+
+extern "C" void egpu_matrix_free(egpu_mat *A) {
+  if (!A) return;
+  cudaSetDevice(A->ctx->device);
+  cudaStreamSynchronize(A->ctx->stream);
+  delete A;
+}
+
+static int check_params(const egpu_params *p) {
+  if (!p) return EGPU_ERR_ARG;
+  if (p->method != EGPU_CG && p->method != EGPU_BICGSTAB) return EGPU_ERR_ARG;
+  if (p->precond < EGPU_PREC_NONE || p->precond > EGPU_PREC_ILU0) return EGPU_ERR_ARG;
+  if (p->max_iter < 1) return EGPU_ERR_ARG;
+  if (p->precision != EGPU_FP64 && p->precision != EGPU_MIXED) return EGPU_ERR_ARG;
+  return EGPU_OK;
+}
+
+extern "C" int egpu_iter_solve_dev(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_params *prm,
+                                   egpu_result *res) {
+  if (!A || !x_dev || check_params(prm)) return EGPU_ERR_ARG;
+  if (!A->has_values) {
+    egpu_set_error(A->ctx, "matrix has no values (bind values or assemble first)");
+    return EGPU_ERR_STATE;
+  }
+  cudaSetDevice(A->ctx->device);
+  if (!b_dev) b_dev = A->rhs.p;
+  if (prm->precision == EGPU_MIXED) return egpu::solve_mixed(A, b_dev, x_dev, prm, res);
+  return egpu::solve_fp64(A, b_dev, x_dev, prm, res);
+}
+
+extern "C" int egpu_iter_solve(egpu_mat *A, const double *b, double *x, const egpu_params *prm,
+                               egpu_result *res) {
+  if (!A || !b || !x || check_params(prm)) return EGPU_ERR_ARG;
+  egpu_ctx *ctx = A->ctx;
+  cudaSetDevice(ctx->device);
+  const int n = A->n;
+  EGPU_CUDA_TRY(ctx, A->bx.alloc((size_t)2 * n));
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(A->bx.p, b, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(A->bx.p + n, x, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  int rc = egpu_iter_solve_dev(A, A->bx.p, A->bx.p + n, prm, res);
+  if (rc < 0) return rc;
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(x, A->bx.p + n, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return rc;
+}
+
+extern "C" int egpu_mv_dev(egpu_mat *A, const double *u_dev, double *v_dev) {
+  if (!A || !u_dev || !v_dev) return EGPU_ERR_ARG;
+  egpu_ctx *ctx = A->ctx;
+  const int n = A->n;
+  const int lpr = egpu::pick_lpr(A);
+  const long long threads = (long long)n * lpr;
+  int grid = (int)std::min<long long>((threads + EGPU_BLOCK - 1) / EGPU_BLOCK, (long long)ctx->num_sms * 16);
+  switch (lpr) {
+    case 4: egpu::k_spmv<double, 4><<<grid, EGPU_BLOCK, 0, ctx->stream>>>(n, A->rows.p, A->cols.p, A->values.p, u_dev, v_dev); break;
+    case 8: egpu::k_spmv<double, 8><<<grid, EGPU_BLOCK, 0, ctx->stream>>>(n, A->rows.p, A->cols.p, A->values.p, u_dev, v_dev); break;
+    case 16: egpu::k_spmv<double, 16><<<grid, EGPU_BLOCK, 0, ctx->stream>>>(n, A->rows.p, A->cols.p, A->values.p, u_dev, v_dev); break;
+    default: egpu::k_spmv<double, 32><<<grid, EGPU_BLOCK, 0, ctx->stream>>>(n, A->rows.p, A->cols.p, A->values.p, u_dev, v_dev); break;
+  }
+  ctx->launches++;
+  EGPU_CUDA_TRY(ctx, cudaGetLastError());
+  return EGPU_OK;
+}
+
+extern "C" int egpu_mv(egpu_mat *A, const double *u, double *v) {
+  if (!A || !u || !v) return EGPU_ERR_ARG;
+  egpu_ctx *ctx = A->ctx;
+  cudaSetDevice(ctx->device);
+  const int n = A->n;
+  EGPU_CUDA_TRY(ctx, A->bx.alloc((size_t)2 * n));
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(A->bx.p, u, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  int rc = egpu_mv_dev(A, A->bx.p, A->bx.p + n);
+  if (rc) return rc;
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(v, A->bx.p + n, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return EGPU_OK;
+}
+
+// Matrix Vector Proc hook (Load.c:734-747, called from CRSMatrix.src:3555-3559 with a
+// literal 0 for reinit, which therefore is only read).  The handle slot A%SpMV keeps the
+// bound pattern; Values are uploaded on every call because the caller scales and
+// back-scales them in place between calls.  One process-wide context serves the hook.
+static egpu_ctx *g_hook_ctx = nullptr;
+static std::mutex g_hook_mu;
+
+extern "C" void egpu_matvec_subr(void **spmv, int *n, int *rows, int *cols, double *values, double *u,
+                                 double *v, int *reinit) {
+  std::lock_guard<std::mutex> lk(g_hook_mu);
+  if (!g_hook_ctx && egpu_create(0, &g_hook_ctx) != EGPU_OK) return;
+  egpu_mat *A = (egpu_mat *)*spmv;
+  if (A && ((reinit && *reinit) || A->n != *n)) {
+    egpu_matrix_free(A);
+    A = nullptr;
+    *spmv = nullptr;
+  }
+  if (!A) {
+    std::vector<int> diag(*n, 0);
+    for (int i = 0; i < *n; ++i)
+      for (int k = rows[i]; k < rows[i + 1]; ++k)
+        if (cols[k - 1] == i + 1) {
+          diag[i] = k;
+          break;
+        }
+    if (egpu_matrix_bind(g_hook_ctx, *n, rows, cols, diag.data(), values, &A) != EGPU_OK) return;
+    *spmv = A;
+  } else if (egpu_matrix_update_values(A, values) != EGPU_OK) {
+    return;
+  }
+  egpu_mv(A, u, v);
+}
+
+extern "C" int egpu_ilu0_build(egpu_mat *A, int scale_system) {
+  if (!A || !A->has_values) return EGPU_ERR_STATE;
+  egpu_ctx *ctx = A->ctx;
+  cudaSetDevice(ctx->device);
+  int rc = egpu::reset_sync(ctx);
+  if (rc) return rc;
+  rc = egpu::scale_matrix(A, scale_system != 0);
+  if (rc) return rc;
+  rc = egpu::ilu0_factor(A);
+  if (rc) return rc;
+  unsigned int h[2];
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(h, ctx->sync.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (h[1]) {
+    egpu_set_error(ctx, "device-side wait expired in the ILU0 factorisation");
+    return (int)h[1];
+  }
+  return EGPU_OK;
+}
+
+extern "C" int egpu_ilu0_download(egpu_mat *A, double *ilu_values, double *diag_scaling) {
+  if (!A || !A->ilu_valid) return EGPU_ERR_STATE;
+  egpu_ctx *ctx = A->ctx;
+  if (ilu_values)
+    EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(ilu_values, A->ilu.p, A->nnz * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  if (diag_scaling)
+    EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(diag_scaling, A->dscale.p, A->n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return EGPU_OK;
+}
+
+extern "C" int egpu_lu_precondition(egpu_mat *A, const double *v, double *u) {
+  if (!A || !A->ilu_valid || !v || !u) return EGPU_ERR_STATE;
+  egpu_ctx *ctx = A->ctx;
+  cudaSetDevice(ctx->device);
+  const int n = A->n;
+  EGPU_CUDA_TRY(ctx, A->bx.alloc((size_t)2 * n));
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(A->bx.p, v, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  int rc = egpu::lu_apply(A, A->bx.p, A->bx.p + n);
+  if (rc) return rc;
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(u, A->bx.p + n, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return EGPU_OK;
+}

@@ -1,0 +1,300 @@
+// egpu_internal.cuh -- shared device helpers and host-side object layouts.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/elmergpu.h"
+
+// ------------------------------------------------------------------------------------
+// constants
+
+// AEPS = 10*EPSILON(1.0_dp), fem/src/Types.src:64
+#define EGPU_AEPS (10.0 * 2.220446049250313e-16)
+#define EGPU_TINY_DP 2.2250738585072014e-308
+#define EGPU_HUTI_EPSILON 1.17549435E-38
+
+// Upper bound on any device-side spin (grid barrier, sync-free dependency wait):
+// after this many nanoseconds the waiting thread records EGPU_ERR_TIMEOUT and the
+// kernel unwinds.
+#define EGPU_WAIT_NS 2000000000ull
+
+// Bit patterns that mark "not yet produced" in the sync-free triangular solves and the
+// ILU factorisation.  They are NaNs with a payload that arithmetic never produces
+// (hardware NaNs are the canonical 0x7FF8... / 0x7FC0... patterns).
+#define EGPU_SENTINEL64 0x7FF4DEAD5EED0001ull
+#define EGPU_SENTINEL32 0x7FA5EED1u
+
+#define EGPU_BLOCK 512
+
+// ------------------------------------------------------------------------------------
+// error plumbing
+
+#define EGPU_CUDA_TRY(ctx, expr)                                                   \
+  do {                                                                             \
+    cudaError_t e_ = (expr);                                                       \
+    if (e_ != cudaSuccess) {                                                       \
+      egpu_set_error((ctx), std::string(#expr) + ": " + cudaGetErrorString(e_));   \
+      return EGPU_ERR_CUDA;                                                        \
+    }                                                                              \
+  } while (0)
+
+struct egpu_ctx;
+void egpu_set_error(const egpu_ctx *ctx, const std::string &msg);
+
+// ------------------------------------------------------------------------------------
+// device memory owner
+
+template <typename T>
+struct DevBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    if (count == n && p) return cudaSuccess;
+    release();
+    if (count == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e == cudaSuccess) n = count;
+    return e;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// ------------------------------------------------------------------------------------
+// host objects
+
+struct egpu_ctx {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ek0 = nullptr, ek1 = nullptr;
+  mutable std::string last_error;
+  long long launches = 0;
+  // scratch reused by solves on this context
+  DevBuf<unsigned int> sync;    // [0] barrier counter, [1] error flag, [2..] misc
+  DevBuf<double> partials;      // per-block partial sums
+  unsigned int *sync_host_err = nullptr;
+};
+
+struct TriSchedule {
+  // rows in the order the sync-free solve processes them (ascending dependency level)
+  DevBuf<int> lower_order, upper_order;
+  int lower_levels = 0, upper_levels = 0;
+  int max_lower = 0, max_upper = 0;  // longest strictly-lower / strictly-upper row part
+};
+
+struct AssemblyData {
+  int nnodes = 0, nelem = 0, nen = 0, code = 0, dofs = 1, cdim = 3;
+  DevBuf<double> xyz;        // nnodes*3
+  DevBuf<int> elem_nodes;    // nelem*nen, 0-based node ids, element order
+  DevBuf<int> perm;          // nnodes, 0-based row block or -1
+  DevBuf<int> color_elems;   // elements grouped by colour
+  std::vector<int> color_ptr;
+  DevBuf<int> slots;         // per element (nen*dofs)^2 CRS positions (0-based), element order
+  bool bound = false;
+};
+
+struct egpu_mat {
+  egpu_ctx *ctx = nullptr;
+  int n = 0;
+  long long nnz = 0;
+  DevBuf<int> rows, cols, diag;  // 0-based
+  DevBuf<double> values;         // as bound / assembled (unscaled)
+  DevBuf<double> rhs;            // assembled right-hand side
+  bool has_values = false, has_rhs = false;
+  int max_row = 0;               // longest row
+  int max_bandwidth = 0;         // max |col - row|
+  // solve state
+  DevBuf<double> scaled;         // D A D
+  DevBuf<double> dscale;         // DiagScaling (times the rhs norm during a solve)
+  DevBuf<double> ilu;            // ILU0 values on the scaled matrix, inverted U diagonal
+  DevBuf<float> scaled32, ilu32; // FP32 copies for the mixed-precision inner solver
+  DevBuf<int16_t> cols16;        // column offsets (col - row) when |col-row| < 32768
+  DevBuf<int> ilu_done;          // factorisation completion flags
+  TriSchedule tri;
+  bool tri_built = false;
+  int solve_count = 0;
+  bool ilu_valid = false;
+  DevBuf<double> work;           // Krylov work vectors
+  DevBuf<float> work32;
+  DevBuf<double> bx;             // scratch b/x for host-pointer entry points
+  AssemblyData asmb;
+};
+
+// ------------------------------------------------------------------------------------
+// device helpers
+
+__device__ __forceinline__ unsigned long long egpu_globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ int ld_acquire_s32(const int *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release_s32(int *p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void red_release_add_u32(unsigned int *p, unsigned int v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const void *p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned int ld_relaxed_u32(const void *p) {
+  unsigned int v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(void *p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed_u32(void *p, unsigned int v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// value type traits for the sync-free solves
+template <typename T>
+struct Sentinel;
+template <>
+struct Sentinel<double> {
+  __device__ __forceinline__ static double value() { return __longlong_as_double((long long)EGPU_SENTINEL64); }
+  __device__ __forceinline__ static bool is(double v) {
+    return (unsigned long long)__double_as_longlong(v) == EGPU_SENTINEL64;
+  }
+  // bounded wait until p holds a produced value; returns it (or the sentinel on timeout)
+  __device__ __forceinline__ static double wait(const double *p, int *err) {
+    unsigned long long v = ld_relaxed_u64(p);
+    if (v != EGPU_SENTINEL64) return __longlong_as_double((long long)v);
+    unsigned long long t0 = egpu_globaltimer();
+    while (true) {
+      v = ld_relaxed_u64(p);
+      if (v != EGPU_SENTINEL64) break;
+      if (egpu_globaltimer() - t0 > EGPU_WAIT_NS) {
+        atomicExch(err, (int)EGPU_ERR_TIMEOUT);
+        break;
+      }
+      if (*(volatile int *)err) break;
+    }
+    return __longlong_as_double((long long)v);
+  }
+  __device__ __forceinline__ static void publish(double *p, double v) {
+    st_relaxed_u64(p, (unsigned long long)__double_as_longlong(v));
+  }
+};
+template <>
+struct Sentinel<float> {
+  __device__ __forceinline__ static float value() { return __uint_as_float(EGPU_SENTINEL32); }
+  __device__ __forceinline__ static bool is(float v) { return __float_as_uint(v) == EGPU_SENTINEL32; }
+  __device__ __forceinline__ static float wait(const float *p, int *err) {
+    unsigned int v = ld_relaxed_u32(p);
+    if (v != EGPU_SENTINEL32) return __uint_as_float(v);
+    unsigned long long t0 = egpu_globaltimer();
+    while (true) {
+      v = ld_relaxed_u32(p);
+      if (v != EGPU_SENTINEL32) break;
+      if (egpu_globaltimer() - t0 > EGPU_WAIT_NS) {
+        atomicExch(err, (int)EGPU_ERR_TIMEOUT);
+        break;
+      }
+      if (*(volatile int *)err) break;
+    }
+    return __uint_as_float(v);
+  }
+  __device__ __forceinline__ static void publish(float *p, float v) { st_relaxed_u32(p, __float_as_uint(v)); }
+};
+
+// Grid-wide barrier for a cooperative (co-resident) launch.  count is a monotonically
+// increasing arrival counter reset to 0 before the launch; epoch is the per-block count
+// of barriers passed.  The wait is bounded by EGPU_WAIT_NS; on expiry the error flag is
+// set.  Returns false when the kernel must unwind (error flag set by anyone).
+__device__ __forceinline__ bool grid_barrier(unsigned int *count, int *err, unsigned int &epoch) {
+  __syncthreads();
+  epoch += 1;
+  if (threadIdx.x == 0) {
+    const unsigned int target = epoch * gridDim.x;
+    red_release_add_u32(count, 1u);
+    if (ld_acquire_u32(count) < target) {
+      unsigned long long t0 = egpu_globaltimer();
+      unsigned int spins = 0;
+      while (ld_acquire_u32(count) < target) {
+        if ((++spins & 63u) == 0) {
+          if (*(volatile int *)err) break;
+          if (egpu_globaltimer() - t0 > EGPU_WAIT_NS) {
+            atomicExch(err, (int)EGPU_ERR_TIMEOUT);
+            break;
+          }
+        }
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return *(volatile int *)err == 0;
+}
+
+// Deterministic block sum of NV values per thread (fixed shuffle tree, fixed warp order).
+// Result valid in every thread.
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double *smem /* >= 32*NV */) {
+#pragma unroll
+  for (int k = 0; k < NV; ++k)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) smem[k * 32 + warp] = v[k];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    double t = lane < nw ? smem[k * 32 + lane] : 0.0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+    v[k] = __shfl_sync(0xffffffffu, t, 0);
+  }
+  __syncthreads();
+}
+
+// Sum of partials[0..nb) read from L2 in a fixed order (same result in every block).
+__device__ __forceinline__ double reduce_partials(const double *partials, int nb, double *smem) {
+  double t = 0.0;
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x < 32) {
+    for (int i = lane; i < nb; i += 32) t += __ldcg(partials + i);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+    if (lane == 0) smem[0] = t;
+  }
+  __syncthreads();
+  t = smem[0];
+  __syncthreads();
+  return t;
+}

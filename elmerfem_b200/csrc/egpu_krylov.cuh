@@ -1,0 +1,526 @@
+// egpu_krylov.cuh -- persistent Krylov kernels (CG, BiCGStab) with Jacobi / ILU0.
+//
+// One cooperative launch runs a whole solve.  Phases are separated by a bounded grid
+// barrier; dot products are block partials reduced in a fixed order (deterministic).
+//
+// FP64 drop-in mode (true_residual = 1) keeps HUTI's operation sequence
+// (hutiter/src/huti_cg_D.F90:158-240, huti_bicgstab_D.F90:171-267) and its stopping
+// test ||A x_k - b|| / ||b|| < tol.  The A x_k product is computed in the same pass
+// over the matrix as the next iteration's first SpMV (two right-hand sides per matrix
+// read), so the decision for iterate k is taken one phase later; x_k is kept
+// untouched until then, which returns the same iterate and HUTI_ITERS as HUTI.
+//
+// FP32 inner mode (true_residual = 0) is the inner solver of the mixed-precision
+// refinement: x0 = 0, stopping on the recursive residual ||r_k|| <= tol * ||r_0||.
+#pragma once
+
+#include "egpu_internal.cuh"
+
+namespace egpu {
+
+enum { SLOT_BB = 0, SLOT_RHO, SLOT_PQ, SLOT_RR, SLOT_SS, SLOT_TS, SLOT_TT, SLOT_RR2, NUM_SLOTS };
+
+template <typename VT>
+struct KArgs {
+  int n;
+  const int *rows, *cols, *diag;  // 0-based CRS
+  const int16_t *cols16;          // col - row offsets (FP32 path, optional)
+  const VT *vals;                 // scaled matrix
+  const VT *ilu;                  // ILU0 factors (inverted U diagonal)
+  const VT *dvals;                // diagonal of the scaled matrix (Jacobi)
+  const int *lower_order, *upper_order;
+  int precond, maxit, true_residual;
+  double tol;
+  const VT *b;
+  VT *x;
+  VT *w;                          // work vectors, stride ldw
+  long long ldw;
+  unsigned int *bar;
+  int *err;
+  double *partials;               // NUM_SLOTS * gridDim.x
+  int *out_i;                     // [0] info [1] iters
+  double *out_d;                  // [0] residual [1] rhsnorm
+  const unsigned int *skip;       // bit 1 set: zero right-hand side, return at once
+};
+
+template <typename VT>
+__device__ __forceinline__ VT ld_stream(const VT *p) {
+  return __ldcs(p);
+}
+template <typename VT>
+__device__ __forceinline__ VT ld_l2(const VT *p) {
+  return __ldcg(p);
+}
+
+// -------------------------------------------------------------------------------------
+// SpMV over all rows, LPR lanes per row.  epi(row, s0, s1) runs on the row's lane 0.
+template <typename VT, int LPR, bool OFFS, bool TWO, typename F>
+__device__ __forceinline__ void spmv_phase(const KArgs<VT> &a, const VT *x0, const VT *x1, F &&epi) {
+  const int lane = threadIdx.x & 31;
+  const int sl = lane & (LPR - 1);
+  const unsigned submask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << (lane & ~(LPR - 1)));
+  const int gsub = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) / LPR);
+  const int nsub = (int)((long long)gridDim.x * blockDim.x / LPR);
+  for (int row = gsub; row < a.n; row += nsub) {
+    const int beg = __ldg(a.rows + row), end = __ldg(a.rows + row + 1);
+    VT s0 = 0, s1 = 0;
+#pragma unroll 4
+    for (int j = beg + sl; j < end; j += LPR) {
+      const VT v = ld_stream(a.vals + j);
+      const int c = OFFS ? row + (int)ld_stream(a.cols16 + j) : ld_stream(a.cols + j);
+      s0 += v * ld_l2(x0 + c);
+      if (TWO) s1 += v * ld_l2(x1 + c);
+    }
+#pragma unroll
+    for (int off = LPR / 2; off > 0; off >>= 1) {
+      s0 += __shfl_xor_sync(submask, s0, off, LPR);
+      if (TWO) s1 += __shfl_xor_sync(submask, s1, off, LPR);
+    }
+    if (sl == 0) epi(row, s0, s1);
+  }
+}
+
+// -------------------------------------------------------------------------------------
+// Sync-free triangular solves.  Rows are taken in ascending dependency level
+// (lower_order / upper_order); slot s is handled by sub-warp s mod nsub in increasing s,
+// so every dependency of a row sits in an earlier slot of a running sub-warp.  Each
+// produced value is published as itself; consumers spin (bounded) until the entry no
+// longer holds the sentinel.
+//
+// lower: y_i = rhs_i - sum_{j<i} L_ij y_j            (CRS_LUSolve forward, CRSMatrix.src:3346-3352)
+// upper: z_i = u_ii^-1 (y_i - sum_{j>i} U_ij z_j)     (backward, :3355-3362)
+template <typename VT, int TS, typename RHS>
+__device__ __forceinline__ void lower_solve(const KArgs<VT> &a, VT *y, RHS &&rhs) {
+  const int lane = threadIdx.x & 31;
+  const int sl = lane & (TS - 1);
+  const unsigned submask = (TS == 32) ? 0xffffffffu : (((1u << TS) - 1u) << (lane & ~(TS - 1)));
+  const int gsub = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) / TS);
+  const int nsub = (int)((long long)gridDim.x * blockDim.x / TS);
+  for (int s = gsub; s < a.n; s += nsub) {
+    const int i = __ldg(a.lower_order + s);
+    const int beg = __ldg(a.rows + i), end = __ldg(a.diag + i);
+    VT acc = 0;
+    for (int j = beg + sl; j < end; j += TS) {
+      const VT l = __ldg(a.ilu + j);
+      const int c = __ldg(a.cols + j);
+      acc += l * Sentinel<VT>::wait(y + c, a.err);
+    }
+#pragma unroll
+    for (int off = TS / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(submask, acc, off, TS);
+    if (sl == 0) Sentinel<VT>::publish(y + i, rhs(i) - acc);
+  }
+}
+
+template <typename VT, int TS, typename OUT>
+__device__ __forceinline__ void upper_solve(const KArgs<VT> &a, const VT *y, VT *z, OUT &&out) {
+  const int lane = threadIdx.x & 31;
+  const int sl = lane & (TS - 1);
+  const unsigned submask = (TS == 32) ? 0xffffffffu : (((1u << TS) - 1u) << (lane & ~(TS - 1)));
+  const int gsub = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) / TS);
+  const int nsub = (int)((long long)gridDim.x * blockDim.x / TS);
+  for (int s = gsub; s < a.n; s += nsub) {
+    const int i = __ldg(a.upper_order + s);
+    const int dg = __ldg(a.diag + i), end = __ldg(a.rows + i + 1);
+    VT acc = 0;
+    for (int j = dg + 1 + sl; j < end; j += TS) {
+      const VT u = __ldg(a.ilu + j);
+      const int c = __ldg(a.cols + j);
+      acc += u * Sentinel<VT>::wait(z + c, a.err);
+    }
+#pragma unroll
+    for (int off = TS / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(submask, acc, off, TS);
+    if (sl == 0) {
+      const VT yi = Sentinel<VT>::wait(y + i, a.err);
+      const VT zi = __ldg(a.ilu + dg) * (yi - acc);
+      Sentinel<VT>::publish(z + i, zi);
+      out(i, zi);
+    }
+  }
+}
+
+// Jacobi: CRS_DiagPrecondition, CRSMatrix.src:1505-1509
+template <typename VT>
+__device__ __forceinline__ VT diag_prec(VT v, VT d) {
+  return fabs((double)d) > EGPU_AEPS ? v / d : v;
+}
+
+template <typename VT>
+__device__ __forceinline__ void store_partials(const KArgs<VT> &a, int slot, double v) {
+  if (threadIdx.x == 0) a.partials[slot * gridDim.x + blockIdx.x] = v;
+}
+
+// =====================================================================================
+// CG  (huti_dcgsolv, hutiter/src/huti_cg_D.F90:84-257)
+//
+// w layout: R Z P Q Y(ILU lower result)
+template <typename VT, int LPR, bool OFFS>
+__global__ void __launch_bounds__(EGPU_BLOCK, 2) cg_kernel(KArgs<VT> a) {
+  if (a.skip && (*a.skip & 2u)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      a.out_i[0] = EGPU_HUTI_CONVERGENCE;
+      a.out_i[1] = 0;
+      a.out_d[0] = 0.0;
+    }
+    return;
+  }
+  __shared__ double sm[32 * 4];
+  unsigned int epoch = 0;
+  const int n = a.n;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  const int nb = gridDim.x;
+  VT *X = a.x, *R = a.w, *Z = a.w + a.ldw, *P = a.w + 2 * a.ldw, *Q = a.w + 3 * a.ldw,
+     *Y = a.w + 4 * a.ldw;
+  const VT *B = a.b;
+  const bool ilu = a.precond == EGPU_PREC_ILU0;
+  const VT SENT = Sentinel<VT>::value();
+
+  // ---- init: R = B - A X  (x0 = 0 in inner mode: R = B)
+  {
+    double acc[1] = {0.0};
+    if (a.true_residual) {
+      spmv_phase<VT, LPR, OFFS, false>(a, X, X, [&](int i, VT s, VT) { R[i] = B[i] - s; });
+    } else {
+      for (int i = tid; i < n; i += nth) {
+        R[i] = B[i];
+        X[i] = 0;
+      }
+    }
+    for (int i = tid; i < n; i += nth) {
+      const double bi = (double)B[i];
+      acc[0] += bi * bi;
+      if (ilu) {
+        Y[i] = SENT;
+        Z[i] = SENT;
+      }
+    }
+    block_sum<1>(acc, sm);
+    store_partials(a, SLOT_BB, acc[0]);
+  }
+  if (!grid_barrier(a.bar, a.err, epoch)) return;
+  const double rhsnorm = sqrt(reduce_partials(a.partials + SLOT_BB * nb, nb, sm));
+
+  // ---- first preconditioning: Z = M^-1 R, partial rho = R.Z
+  {
+    double acc[1] = {0.0};
+    if (ilu) {
+      lower_solve<VT, LPR>(a, Y, [&](int i) { return R[i]; });
+      upper_solve<VT, LPR>(a, Y, Z, [&](int i, VT zi) { acc[0] += (double)R[i] * (double)zi; });
+    } else {
+      for (int i = tid; i < n; i += nth) {
+        const VT z = a.precond == EGPU_PREC_DIAGONAL ? diag_prec(R[i], a.dvals[i]) : R[i];
+        Z[i] = z;
+        acc[0] += (double)R[i] * (double)z;
+      }
+    }
+    block_sum<1>(acc, sm);
+    store_partials(a, SLOT_RHO, acc[0]);
+  }
+  if (!grid_barrier(a.bar, a.err, epoch)) return;
+
+  int k = 1, info = 0, iters = 0;
+  double rho, oldrho = 1.0, residual = 0.0, rr_prev = 0.0;
+  while (true) {
+    rho = reduce_partials(a.partials + SLOT_RHO * nb, nb, sm);
+    if (!a.true_residual && k > 1) {
+      // inner mode: recursive residual of x_{k-1}
+      residual = sqrt(rr_prev) / rhsnorm;
+      if (residual <= a.tol) { info = EGPU_HUTI_CONVERGENCE; iters = k - 1; break; }
+      if (k > a.maxit) { info = EGPU_HUTI_MAXITER; iters = k - 1; break; }
+    }
+    // ---- P = Z (first iteration) or Z + beta P
+    {
+      const VT beta = (VT)(rho / oldrho);
+      for (int i = tid; i < n; i += nth) {
+        const VT z = Z[i];
+        P[i] = (k == 1) ? z : z + beta * P[i];
+        if (ilu) {
+          Z[i] = SENT;
+          Y[i] = SENT;
+        }
+      }
+    }
+    if (!grid_barrier(a.bar, a.err, epoch)) return;
+    // ---- Q = A P  (+ A x_{k-1} for the stopping test of iterate k-1)
+    {
+      double acc[2] = {0.0, 0.0};
+      if (a.true_residual && k > 1) {
+        spmv_phase<VT, LPR, OFFS, true>(a, P, X, [&](int i, VT s0, VT s1) {
+          Q[i] = s0;
+          acc[0] += (double)P[i] * (double)s0;
+          const double r = (double)s1 - (double)B[i];
+          acc[1] += r * r;
+        });
+      } else {
+        spmv_phase<VT, LPR, OFFS, false>(a, P, P, [&](int i, VT s0, VT) {
+          Q[i] = s0;
+          acc[0] += (double)P[i] * (double)s0;
+        });
+      }
+      block_sum<2>(acc, sm);
+      store_partials(a, SLOT_PQ, acc[0]);
+      store_partials(a, SLOT_RR, acc[1]);
+    }
+    if (!grid_barrier(a.bar, a.err, epoch)) return;
+    const double pq = reduce_partials(a.partials + SLOT_PQ * nb, nb, sm);
+    if (a.true_residual && k > 1) {
+      const double rr = reduce_partials(a.partials + SLOT_RR * nb, nb, sm);
+      residual = sqrt(rr) / rhsnorm;
+      if (residual < a.tol) { info = EGPU_HUTI_CONVERGENCE; iters = k - 1; break; }
+      if (k > a.maxit) { info = EGPU_HUTI_MAXITER; iters = k; break; }
+    }
+    if (rho == 0.0) { info = EGPU_HUTI_CG_RHO; iters = k; break; }
+    // ---- X += alpha P; R -= alpha Q; Z = M^-1 R; partial rho_{k+1}
+    {
+      const double alpha_d = rho / pq;
+      const VT alpha = (VT)alpha_d;
+      double acc[2] = {0.0, 0.0};
+      if (ilu) {
+        lower_solve<VT, LPR>(a, Y, [&](int i) { return R[i] - alpha * Q[i]; });
+        upper_solve<VT, LPR>(a, Y, Z, [&](int i, VT zi) {
+          const VT r = R[i] - alpha * Q[i];
+          R[i] = r;
+          X[i] = X[i] + alpha * P[i];
+          acc[0] += (double)r * (double)zi;
+          acc[1] += (double)r * (double)r;
+        });
+      } else {
+        for (int i = tid; i < n; i += nth) {
+          X[i] = X[i] + alpha * P[i];
+          const VT r = R[i] - alpha * Q[i];
+          R[i] = r;
+          const VT z = a.precond == EGPU_PREC_DIAGONAL ? diag_prec(r, a.dvals[i]) : r;
+          Z[i] = z;
+          acc[0] += (double)r * (double)z;
+          acc[1] += (double)r * (double)r;
+        }
+      }
+      block_sum<2>(acc, sm);
+      store_partials(a, SLOT_RHO, acc[0]);
+      store_partials(a, SLOT_RR2, acc[1]);
+    }
+    if (!grid_barrier(a.bar, a.err, epoch)) return;
+    if (!a.true_residual) rr_prev = reduce_partials(a.partials + SLOT_RR2 * nb, nb, sm);
+    oldrho = rho;
+    ++k;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.out_i[0] = info;
+    a.out_i[1] = iters;
+    a.out_d[0] = residual;
+    a.out_d[1] = rhsnorm;
+  }
+}
+
+// =====================================================================================
+// BiCGStab  (huti_dbicgstabsolv, hutiter/src/huti_bicgstab_D.F90:96-284)
+//
+// w layout: R RTLD P V T S T1V T2V Y1 Y2
+template <typename VT, int LPR, bool OFFS>
+__global__ void __launch_bounds__(EGPU_BLOCK, 2) bicgstab_kernel(KArgs<VT> a) {
+  if (a.skip && (*a.skip & 2u)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      a.out_i[0] = EGPU_HUTI_CONVERGENCE;
+      a.out_i[1] = 0;
+      a.out_d[0] = 0.0;
+    }
+    return;
+  }
+  __shared__ double sm[32 * 4];
+  unsigned int epoch = 0;
+  const int n = a.n;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  const int nb = gridDim.x;
+  VT *X = a.x;
+  VT *R = a.w, *RT = a.w + a.ldw, *P = a.w + 2 * a.ldw, *V = a.w + 3 * a.ldw,
+     *T = a.w + 4 * a.ldw, *S = a.w + 5 * a.ldw, *T1 = a.w + 6 * a.ldw, *T2 = a.w + 7 * a.ldw,
+     *Y1 = a.w + 8 * a.ldw, *Y2 = a.w + 9 * a.ldw;
+  const VT *B = a.b;
+  const bool ilu = a.precond == EGPU_PREC_ILU0;
+  const bool jac = a.precond == EGPU_PREC_DIAGONAL;
+  const VT SENT = Sentinel<VT>::value();
+
+  // ---- init: R = B - A X; RTLD = R; P = V = 0
+  {
+    double acc[2] = {0.0, 0.0};
+    if (a.true_residual) {
+      spmv_phase<VT, LPR, OFFS, false>(a, X, X, [&](int i, VT s, VT) {
+        const VT r = B[i] - s;
+        R[i] = r;
+        RT[i] = r;
+        acc[1] += (double)r * (double)r;
+      });
+    } else {
+      for (int i = tid; i < n; i += nth) {
+        const VT r = B[i];
+        X[i] = 0;
+        R[i] = r;
+        RT[i] = r;
+        acc[1] += (double)r * (double)r;
+      }
+    }
+    for (int i = tid; i < n; i += nth) {
+      const double bi = (double)B[i];
+      acc[0] += bi * bi;
+      P[i] = 0;
+      V[i] = 0;
+      if (ilu) {
+        Y1[i] = SENT;
+        Y2[i] = SENT;
+        T1[i] = SENT;
+        T2[i] = SENT;
+      }
+    }
+    block_sum<2>(acc, sm);
+    store_partials(a, SLOT_BB, acc[0]);
+    store_partials(a, SLOT_RHO, acc[1]);
+    store_partials(a, SLOT_RR2, acc[1]);
+  }
+  if (!grid_barrier(a.bar, a.err, epoch)) return;
+  const double rhsnorm = sqrt(reduce_partials(a.partials + SLOT_BB * nb, nb, sm));
+
+  int k = 1, info = 0, iters = 0;
+  double rho, oldrho = 1.0, omega = 1.0, alpha = 0.0, residual = 0.0, r0norm = 0.0;
+  if (!a.true_residual) r0norm = sqrt(reduce_partials(a.partials + SLOT_RR2 * nb, nb, sm));
+  while (true) {
+    rho = reduce_partials(a.partials + SLOT_RHO * nb, nb, sm);
+    if (!a.true_residual && k > 1) {
+      residual = sqrt(reduce_partials(a.partials + SLOT_RR2 * nb, nb, sm)) / r0norm;
+      if (residual <= a.tol) { info = EGPU_HUTI_CONVERGENCE; iters = k - 1; break; }
+      if (omega == 0.0) { info = EGPU_HUTI_BICGSTAB_OMEGA; iters = k - 1; break; }
+      if (k > a.maxit) { info = EGPU_HUTI_MAXITER; iters = k - 1; break; }
+    }
+    const bool rho_zero = rho == 0.0;
+    // ---- P = R + beta (P - omega V); T1V = M^-1 P
+    {
+      const VT beta = (VT)((rho * alpha) / (oldrho * omega));
+      const VT om = (VT)omega;
+      if (ilu) {
+        lower_solve<VT, LPR>(a, Y1, [&](int i) {
+          const VT p = R[i] + beta * (P[i] - om * V[i]);
+          P[i] = p;
+          return p;
+        });
+        upper_solve<VT, LPR>(a, Y1, T1, [&](int, VT) {});
+      } else {
+        for (int i = tid; i < n; i += nth) {
+          const VT p = R[i] + beta * (P[i] - om * V[i]);
+          P[i] = p;
+          T1[i] = jac ? diag_prec(p, a.dvals[i]) : p;
+        }
+      }
+    }
+    if (!grid_barrier(a.bar, a.err, epoch)) return;
+    // ---- V = A T1V (+ A x_{k-1}); partials RTLD.V, ||A x_{k-1} - b||^2
+    {
+      double acc[2] = {0.0, 0.0};
+      if (a.true_residual && k > 1) {
+        spmv_phase<VT, LPR, OFFS, true>(a, T1, X, [&](int i, VT s0, VT s1) {
+          V[i] = s0;
+          acc[0] += (double)RT[i] * (double)s0;
+          const double r = (double)s1 - (double)B[i];
+          acc[1] += r * r;
+        });
+      } else {
+        spmv_phase<VT, LPR, OFFS, false>(a, T1, T1, [&](int i, VT s0, VT) {
+          V[i] = s0;
+          acc[0] += (double)RT[i] * (double)s0;
+        });
+      }
+      block_sum<2>(acc, sm);
+      store_partials(a, SLOT_PQ, acc[0]);
+      store_partials(a, SLOT_RR, acc[1]);
+    }
+    if (!grid_barrier(a.bar, a.err, epoch)) return;
+    const double rv = reduce_partials(a.partials + SLOT_PQ * nb, nb, sm);
+    if (a.true_residual && k > 1) {
+      const double rr = reduce_partials(a.partials + SLOT_RR * nb, nb, sm);
+      residual = sqrt(rr) / rhsnorm;
+      if (residual < a.tol) { info = EGPU_HUTI_CONVERGENCE; iters = k - 1; break; }
+      if (omega == 0.0) { info = EGPU_HUTI_BICGSTAB_OMEGA; iters = k - 1; break; }
+      if (k > a.maxit) { info = EGPU_HUTI_MAXITER; iters = k; break; }
+    }
+    if (rho_zero) { info = EGPU_HUTI_BICGSTAB_RHO; iters = k; break; }
+    alpha = rho / rv;
+    // ---- S = R - alpha V; T2V = M^-1 S; partial ||S||^2
+    {
+      const VT al = (VT)alpha;
+      double acc[1] = {0.0};
+      if (ilu) {
+        lower_solve<VT, LPR>(a, Y2, [&](int i) {
+          const VT s = R[i] - al * V[i];
+          S[i] = s;
+          acc[0] += (double)s * (double)s;
+          return s;
+        });
+        upper_solve<VT, LPR>(a, Y2, T2, [&](int, VT) {});
+      } else {
+        for (int i = tid; i < n; i += nth) {
+          const VT s = R[i] - al * V[i];
+          S[i] = s;
+          acc[0] += (double)s * (double)s;
+          T2[i] = jac ? diag_prec(s, a.dvals[i]) : s;
+        }
+      }
+      block_sum<1>(acc, sm);
+      store_partials(a, SLOT_SS, acc[0]);
+    }
+    if (!grid_barrier(a.bar, a.err, epoch)) return;
+    // ---- T = A T2V; partials T.S, T.T
+    {
+      double acc[2] = {0.0, 0.0};
+      spmv_phase<VT, LPR, OFFS, false>(a, T2, T2, [&](int i, VT s0, VT) {
+        T[i] = s0;
+        acc[0] += (double)s0 * (double)S[i];
+        acc[1] += (double)s0 * (double)s0;
+      });
+      block_sum<2>(acc, sm);
+      store_partials(a, SLOT_TS, acc[0]);
+      store_partials(a, SLOT_TT, acc[1]);
+    }
+    if (!grid_barrier(a.bar, a.err, epoch)) return;
+    const double ss = reduce_partials(a.partials + SLOT_SS * nb, nb, sm);
+    const double ts = reduce_partials(a.partials + SLOT_TS * nb, nb, sm);
+    const double tt = reduce_partials(a.partials + SLOT_TT * nb, nb, sm);
+    if (sqrt(ss) < EGPU_HUTI_EPSILON) {
+      const VT al = (VT)alpha;
+      for (int i = tid; i < n; i += nth) X[i] = X[i] + al * T1[i];
+      residual = sqrt(ss);
+      info = EGPU_HUTI_BICGSTAB_SNORM;
+      iters = k;
+      break;
+    }
+    omega = ts / tt;
+    // ---- X += alpha T1V + omega T2V; R = S - omega T; partial RTLD.R
+    {
+      const VT al = (VT)alpha, om = (VT)omega;
+      double acc[2] = {0.0, 0.0};
+      for (int i = tid; i < n; i += nth) {
+        X[i] = X[i] + al * T1[i] + om * T2[i];
+        const VT r = S[i] - om * T[i];
+        R[i] = r;
+        acc[0] += (double)RT[i] * (double)r;
+        acc[1] += (double)r * (double)r;
+        if (ilu) {
+          T1[i] = SENT;
+          T2[i] = SENT;
+          Y1[i] = SENT;
+          Y2[i] = SENT;
+        }
+      }
+      block_sum<2>(acc, sm);
+      store_partials(a, SLOT_RHO, acc[0]);
+      store_partials(a, SLOT_RR2, acc[1]);
+    }
+    if (!grid_barrier(a.bar, a.err, epoch)) return;
+    oldrho = rho;
+    ++k;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.out_i[0] = info;
+    a.out_i[1] = iters;
+    a.out_d[0] = residual;
+    a.out_d[1] = rhsnorm;
+  }
+}
+
+}  // namespace egpu

@@ -1,0 +1,22 @@
+// egpu_solve.h -- internal solve entry points shared by the translation units.
+#pragma once
+
+#include "egpu_internal.cuh"
+
+namespace egpu {
+
+int ensure_ctx_scratch(egpu_ctx *ctx);
+int reset_sync(egpu_ctx *ctx);
+int scale_matrix(egpu_mat *A, bool scale_system);
+int ensure_tri_schedule(egpu_mat *A);
+int ilu0_factor(egpu_mat *A);
+int solve_fp64(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_params *prm,
+               egpu_result *res);
+int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_params *prm,
+                egpu_result *res);
+// FP64 Krylov continuation on an already scaled system (used by the mixed path's
+// stagnation fallback): xs in/out, bs scaled rhs; preconditioner state must be current.
+int krylov_fp64_scaled(egpu_mat *A, const double *bs, double *xs, const egpu_params *prm, int *info,
+                       int *iters, double *residual);
+
+}  // namespace egpu

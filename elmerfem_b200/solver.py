@@ -1,0 +1,301 @@
+"""Host-side mirror of ElmerSolver's linear-system interface over the C ABI.
+
+Names follow the reference: ``create_matrix`` is CreateMatrix (ElementUtils.src:698),
+``Matrix`` is a device-bound Matrix_t (Types.src:155-228), ``iter_solver`` is IterSolver
+(IterSolve.src:144) with SolveLinearSystem's scaling around it (SolverUtils.src:7151), and
+``SolverParams.from_sif`` reads the same keywords as IterSolver (IterSolve.src:221-420).
+All compute runs in libelmergpu.so on the GPU; nothing here falls back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import BICGSTAB, CG, FP64, MIXED, PREC_DIAGONAL, PREC_ILU0, PREC_NONE, LibError, check, lib
+
+
+class NotConverged(RuntimeError):
+    """Raised like Fatal('IterSolve', ...) when Linear System Abort Not Converged is True."""
+
+
+class Context:
+    """One GPU, one stream (egpu_create)."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        check(lib().egpu_create(device, C.byref(self._h)), None, "egpu_create")
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def stream(self) -> int:
+        """cudaStream_t (as an integer) every call of this context runs on."""
+        return int(lib().egpu_stream(self._h) or 0)
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(lib().egpu_kernel_launches(self._h))
+
+    def close(self):
+        if self._h:
+            lib().egpu_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class CRSPattern:
+    """Rows/Cols/Diag (1-based, as Matrix_t) plus Perm (node -> row block)."""
+
+    n: int
+    nnz: int
+    dofs: int
+    perm: np.ndarray
+    rows: np.ndarray
+    cols: np.ndarray
+    diag: np.ndarray
+
+
+def create_matrix(mesh, dofs: int = 1, optimize_bandwidth: bool = True) -> CRSPattern:
+    """CreateMatrix for a mesh whose nodes are all active (egpu_pattern_create)."""
+    L = lib()
+    el = np.ascontiguousarray(mesh.elements, dtype=np.int32)
+    n, nnz = C.c_int(), C.c_longlong()
+    check(L.egpu_pattern_create(mesh.nnodes, el.shape[0], el.shape[1], el, dofs, int(optimize_bandwidth),
+                                C.byref(n), C.byref(nnz), None, None, None, None), None, "egpu_pattern_create")
+    perm = np.zeros(mesh.nnodes, np.int32)
+    rows = np.zeros(n.value + 1, np.int32)
+    cols = np.zeros(nnz.value, np.int32)
+    diag = np.zeros(n.value, np.int32)
+    check(L.egpu_pattern_create(mesh.nnodes, el.shape[0], el.shape[1], el, dofs, int(optimize_bandwidth),
+                                C.byref(n), C.byref(nnz), perm.ctypes.data, rows.ctypes.data,
+                                cols.ctypes.data, diag.ctypes.data), None, "egpu_pattern_create")
+    return CRSPattern(n.value, nnz.value, dofs, perm, rows, cols, diag)
+
+
+@dataclass
+class SolverParams:
+    method: int = BICGSTAB
+    precond: int = PREC_ILU0
+    max_iter: int = 1000
+    tol: float = 1e-10
+    scale_system: bool = True
+    precision: int = FP64
+    refactorize: bool = True
+    precond_recompute: int = 1
+    inner_tol: float = 1e-4
+    inner_max_iter: int = 2000
+    max_refinements: int = 30
+    abort_not_converged: bool = True
+    symmetric: bool = False
+
+    def to_c(self) -> _lib.Params:
+        return _lib.Params(self.method, self.precond, self.max_iter, self.tol, int(self.scale_system),
+                           self.precision, int(self.refactorize), self.precond_recompute, self.inner_tol,
+                           self.inner_max_iter, self.max_refinements)
+
+    @classmethod
+    def from_sif(cls, keywords) -> "SolverParams":
+        """Build from a Solver section (text or {keyword: value}); IterSolve.src:221-420."""
+        kw = parse_sif_section(keywords) if isinstance(keywords, str) else {k.lower(): v for k, v in keywords.items()}
+        solver = str(kw.get("linear system solver", "iterative")).lower()
+        if solver != "iterative":
+            raise NotImplementedError(f"Linear System Solver = {solver}: only 'iterative' is on this path")
+        meth = str(kw.get("linear system iterative method", "bicgstab")).lower()
+        if meth not in ("bicgstab", "cg"):
+            raise NotImplementedError(f"Linear System Iterative Method = {meth}")
+        prec = str(kw.get("linear system preconditioning", "none")).lower()
+        if prec.startswith("none"):
+            pc = PREC_NONE
+        elif prec.startswith("diagonal"):
+            pc = PREC_DIAGONAL
+        elif prec.startswith("ilu") and not prec.startswith("ilut"):
+            order = kw.get("linear system ilu order")
+            n = int(round(float(order))) if order is not None else (int(prec[3]) if len(prec) > 3 and prec[3].isdigit() else 0)
+            if n != 0:
+                raise NotImplementedError(f"ILU{n}: only ILU0 is on this path")
+            pc = PREC_ILU0
+        else:
+            raise NotImplementedError(f"Linear System Preconditioning = {prec}")
+        if "linear system max iterations" not in kw:
+            raise KeyError("Linear System Max Iterations is required (ListGetInteger without default)")
+        if "linear system convergence tolerance" not in kw:
+            raise KeyError("Linear System Convergence Tolerance is required")
+        p = cls(method=CG if meth == "cg" else BICGSTAB, precond=pc,
+                max_iter=int(kw["linear system max iterations"]),
+                tol=float(kw["linear system convergence tolerance"]),
+                scale_system=_bool(kw.get("linear system scaling", True)),
+                refactorize=_bool(kw.get("linear system refactorize", True)),
+                precond_recompute=max(1, int(kw.get("linear system precondition recompute", 1))),
+                abort_not_converged=_bool(kw.get("linear system abort not converged", True)),
+                symmetric=_bool(kw.get("linear system symmetric", False)))
+        prec_kw = str(kw.get("linear system precision", "double")).lower()
+        if prec_kw in ("mixed", "single-double", "fp32/fp64"):
+            p.precision = MIXED
+        if "linear system inner tolerance" in kw:
+            p.inner_tol = float(kw["linear system inner tolerance"])
+        return p
+
+
+def _bool(v) -> bool:
+    if isinstance(v, str):
+        return v.strip().lower() in ("true", "logical true", "1", "yes")
+    return bool(v)
+
+
+def parse_sif_section(text: str) -> dict:
+    """Keyword = [type] value lines of one .sif section -> {lowercase keyword: value}."""
+    out = {}
+    for line in text.splitlines():
+        line = line.split("!")[0].strip()
+        if "=" not in line:
+            continue
+        key, val = (s.strip() for s in line.split("=", 1))
+        key = re.sub(r"\(\d+\)$", "", key).strip().lower()
+        val = re.sub(r"^(real|integer|logical|string)\s+", "", val, flags=re.I).strip().strip('"')
+        out[key] = val
+    return out
+
+
+class Matrix:
+    """A Matrix_t bound to the GPU (egpu_matrix_bind)."""
+
+    def __init__(self, ctx: Context, pattern: CRSPattern, values=None):
+        self.ctx = ctx
+        self.pattern = pattern
+        self.n = pattern.n
+        self.nnz = pattern.nnz
+        self._h = C.c_void_p()
+        vals = None if values is None else np.ascontiguousarray(values, np.float64)
+        check(lib().egpu_matrix_bind(ctx.handle, pattern.n, pattern.rows, pattern.cols, pattern.diag,
+                                     None if vals is None else vals.ctypes.data, C.byref(self._h)),
+              ctx.handle, "egpu_matrix_bind")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def free(self):
+        if self._h:
+            lib().egpu_matrix_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def update_values(self, values):
+        check(lib().egpu_matrix_update_values(self._h, np.ascontiguousarray(values, np.float64)), self.ctx.handle,
+              "egpu_matrix_update_values")
+
+    def values(self) -> np.ndarray:
+        v = np.zeros(self.nnz)
+        check(lib().egpu_matrix_values_download(self._h, v), self.ctx.handle, "values")
+        return v
+
+    def rhs(self) -> np.ndarray:
+        v = np.zeros(self.n)
+        check(lib().egpu_matrix_rhs_download(self._h, v), self.ctx.handle, "rhs")
+        return v
+
+    def mv(self, u) -> np.ndarray:
+        """Matrix Vector Proc: v = A u on the GPU."""
+        v = np.zeros(self.n)
+        check(lib().egpu_mv(self._h, np.ascontiguousarray(u, np.float64), v), self.ctx.handle, "egpu_mv")
+        return v
+
+    # ---- preconditioner state (A%ILUValues, A%DiagScaling)
+    def ilu0(self, scale_system: bool = True):
+        """Factor ILU0 on the device; returns (ILUValues with inverted U diagonal, DiagScaling)."""
+        check(lib().egpu_ilu0_build(self._h, int(scale_system)), self.ctx.handle, "egpu_ilu0_build")
+        ilu, d = np.zeros(self.nnz), np.zeros(self.n)
+        check(lib().egpu_ilu0_download(self._h, ilu.ctypes.data, d.ctypes.data), self.ctx.handle, "egpu_ilu0_download")
+        return ilu, d
+
+    def lu_precondition(self, v) -> np.ndarray:
+        """CRS_LUPrecondition with the device factors: u = (LU)^-1 v."""
+        u = np.zeros(self.n)
+        check(lib().egpu_lu_precondition(self._h, np.ascontiguousarray(v, np.float64), u), self.ctx.handle,
+              "egpu_lu_precondition")
+        return u
+
+    # ---- assembly seam
+    def bind_assembly(self, mesh, cdim: int | None = None):
+        p = self.pattern
+        if cdim is None:
+            cdim = 2 if mesh.elem_code // 100 <= 4 else 3
+        check(lib().egpu_assembly_bind(self._h, mesh.nnodes, np.ascontiguousarray(mesh.coords, np.float64), cdim,
+                                       mesh.nelem, mesh.elem_code, np.ascontiguousarray(mesh.elements, np.int32),
+                                       p.perm, p.dofs), self.ctx.handle, "egpu_assembly_bind")
+
+    def assemble_poisson(self, elem_k=None, nodal_k=None, load=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float64) for a in (elem_k, nodal_k, load)]
+        check(lib().egpu_assemble_poisson(self._h, *[None if a is None else a.ctypes.data for a in arrs]),
+              self.ctx.handle, "egpu_assemble_poisson")
+
+    def assemble_elastic(self, young: float, poisson: float, body_force):
+        check(lib().egpu_assemble_elastic(self._h, young, poisson, np.asarray(body_force, np.float64)),
+              self.ctx.handle, "egpu_assemble_elastic")
+
+    def dirichlet(self, con_rows, con_vals=None, symmetric: bool = False):
+        r = np.ascontiguousarray(con_rows, np.int32)
+        v = None if con_vals is None else np.ascontiguousarray(con_vals, np.float64)
+        check(lib().egpu_dirichlet(self._h, r.size, r.ctypes.data, None if v is None else v.ctypes.data,
+                                   int(symmetric)), self.ctx.handle, "egpu_dirichlet")
+
+    # ---- solve
+    def solve(self, b=None, x0=None, params: SolverParams | None = None):
+        """IterSolver on host vectors (b None: the assembled RHS).  Returns (x, result dict)."""
+        params = params or SolverParams()
+        x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64)
+        res = _lib.Result()
+        prm = params.to_c()
+        if b is None:
+            b = self.rhs()
+        rc = check(lib().egpu_iter_solve(self._h, np.ascontiguousarray(b, np.float64), x, C.byref(prm), C.byref(res)),
+                   self.ctx.handle, "egpu_iter_solve")
+        out = res.as_dict()
+        out["status"] = _lib.HUTI.get(rc, str(rc))
+        if params.abort_not_converged and rc != 1:
+            raise NotConverged(f"IterSolve: failed convergence tolerances ({out['status']}, iters {out['iters']})")
+        return x, out
+
+    def solve_dev(self, b_ptr: int | None, x_ptr: int, params: SolverParams | None = None) -> dict:
+        """IterSolver on device buffers (raw CUDA pointers; b_ptr None: the assembled RHS)."""
+        params = params or SolverParams()
+        res = _lib.Result()
+        prm = params.to_c()
+        rc = check(lib().egpu_iter_solve_dev(self._h, b_ptr, x_ptr, C.byref(prm), C.byref(res)), self.ctx.handle,
+                   "egpu_iter_solve_dev")
+        out = res.as_dict()
+        out["status"] = _lib.HUTI.get(rc, str(rc))
+        if params.abort_not_converged and rc != 1:
+            raise NotConverged(f"IterSolve: failed convergence tolerances ({out['status']}, iters {out['iters']})")
+        return out
+
+
+def iter_solver(A: Matrix, b, x, params: SolverParams):
+    """IterSolver(A, x, b, Solver): solves in place into x (numpy), returns the result dict."""
+    sol, res = A.solve(b, x, params)
+    x[...] = sol
+    return res
+
+
+def compute_norm(x) -> float:
+    """ComputeNorm default (SolverUtils.src:4983-4988): sqrt(sum(x^2)/n)."""
+    x = np.asarray(x, np.float64)
+    return float(np.sqrt(np.sum(x * x) / x.size))

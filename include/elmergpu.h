@@ -1,0 +1,169 @@
+/*
+ * elmergpu.h -- C ABI of the B200 linear-system path for ElmerSolver.
+ *
+ * Drop-in seam: the library replaces IterSolver (fem/src/IterSolve.src:144-798) for
+ *   Linear System Solver = Iterative
+ *   Linear System Iterative Method = BiCGStab | CG
+ *   Linear System Preconditioning  = ILU0 | Diagonal | None
+ * and the bulk assembly loop of HeatSolve/StressSolve (modules/HeatSolve.src:655-985,
+ * modules/StressSolve.src:815-1072) for linear Poisson and isotropic elasticity.
+ *
+ * Every pointer argument is a plain host pointer unless the name ends in _dev (device
+ * memory on the context's GPU).  CRS arrays use Elmer's Matrix_t convention
+ * (fem/src/Types.src:155-228): Rows(n+1), Cols(nnz), Diag(n), 1-based int32; Values
+ * double.  The library copies what it needs, never frees or keeps caller memory, and
+ * writes only the output arrays named in each call.
+ *
+ * Return values: >0 is a HUTI status (hutiter/src/huti_fdefs.h:18-52; 1 = converged);
+ * 0 is success for calls that do not iterate; <0 is a library error (EGPU_ERR_*).
+ * No exception crosses the ABI.  A context is used by one host thread at a time.
+ */
+#ifndef ELMERGPU_H
+#define ELMERGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------------- */
+#define EGPU_OK 0
+#define EGPU_ERR_ARG (-1)      /* invalid argument */
+#define EGPU_ERR_CUDA (-2)     /* a CUDA runtime call failed */
+#define EGPU_ERR_ALLOC (-3)    /* device allocation failed */
+#define EGPU_ERR_TIMEOUT (-4)  /* a bounded device-side wait expired (kernel returned) */
+#define EGPU_ERR_STATE (-5)    /* call out of order (e.g. solve before values exist) */
+#define EGPU_ERR_BUDGET (-6)   /* admission refused: footprint exceeds the HBM budget */
+
+/* HUTI status values returned by the solve calls (huti_fdefs.h:18-52) */
+#define EGPU_HUTI_CONVERGENCE 1
+#define EGPU_HUTI_MAXITER 2
+#define EGPU_HUTI_CG_RHO 20
+#define EGPU_HUTI_BICGSTAB_RHO 35
+#define EGPU_HUTI_BICGSTAB_SNORM 36
+#define EGPU_HUTI_BICGSTAB_OMEGA 37
+
+/* ---- keyword surface (IterSolve.src:221-420) ------------------------------------ */
+enum { EGPU_CG = 1, EGPU_BICGSTAB = 2 };                           /* Linear System Iterative Method */
+enum { EGPU_PREC_NONE = 0, EGPU_PREC_DIAGONAL = 1, EGPU_PREC_ILU0 = 2 }; /* Linear System Preconditioning */
+enum { EGPU_FP64 = 0, EGPU_MIXED = 1 };  /* FP64 drop-in | FP32 inner Krylov in FP64 refinement */
+
+typedef struct {
+  int method;             /* EGPU_CG | EGPU_BICGSTAB */
+  int precond;            /* EGPU_PREC_* */
+  int max_iter;           /* Linear System Max Iterations (required, >= 1) */
+  double tol;             /* Linear System Convergence Tolerance (true residual / ||b||) */
+  int scale_system;       /* Linear System Scaling (Elmer default 1) */
+  int precision;          /* EGPU_FP64 | EGPU_MIXED */
+  int refactorize;        /* Linear System Refactorize (Elmer default 1) */
+  int precond_recompute;  /* Linear System Precondition Recompute (Elmer default 1) */
+  /* mixed precision only */
+  double inner_tol;       /* relative reduction of the FP32 inner residual per refinement */
+  int inner_max_iter;     /* cap on inner iterations per refinement */
+  int max_refinements;    /* cap on FP64 refinement steps */
+} egpu_params;
+
+typedef struct {
+  int info;               /* HUTI status */
+  int iters;              /* HUTI_ITERS (FP64) / total inner iterations (mixed) */
+  int refinements;        /* FP64 refinement steps (mixed); 0 for FP64 */
+  double residual;        /* last ||A x - b|| / ||b|| of the scaled system */
+  double seconds;         /* device time of the solve, CUDA events */
+  double seconds_setup;   /* scaling + preconditioner construction part of seconds */
+  double seconds_krylov;  /* device time inside the persistent Krylov kernels */
+  int krylov_launches;    /* number of persistent Krylov kernel launches */
+} egpu_result;
+
+/* fills p with Elmer's defaults for the given method/preconditioner */
+void egpu_params_default(egpu_params *p, int method, int precond);
+
+/* ---- context --------------------------------------------------------------------- */
+typedef struct egpu_ctx egpu_ctx;
+typedef struct egpu_mat egpu_mat;
+
+int egpu_create(int device, egpu_ctx **out);
+void egpu_destroy(egpu_ctx *ctx);
+const char *egpu_last_error(const egpu_ctx *ctx);
+/* number of this library's kernel launches since the context was created */
+long long egpu_kernel_launches(const egpu_ctx *ctx);
+/* the cudaStream_t every call of this context runs on (for callers' CUDA events) */
+void *egpu_stream(const egpu_ctx *ctx);
+
+/* ---- sparsity pattern: CreateMatrix (ElementUtils.src:698-930) -------------------
+ * MakeListMatrix + OptimizeBandwidth (BandwidthOptimize.src:108-355) +
+ * CRS_CreateMatrix/InitializeMatrix/CRS_SortMatrix for a mesh whose nodes are all
+ * active.  Two calls: first with rows/cols/diag == NULL to get n and nnz, then with
+ * buffers of those sizes.  perm (nnodes) receives Elmer's Perm (node -> row block). */
+int egpu_pattern_create(int nnodes, int nelem, int nen, const int *elem_nodes, int dofs,
+                        int optimize_bw, int *n_out, long long *nnz_out, int *perm,
+                        int *rows, int *cols, int *diag);
+
+/* ---- matrix binding (replaces the Matrix_t handed to IterSolver) ----------------- */
+int egpu_matrix_bind(egpu_ctx *ctx, int n, const int *rows, const int *cols, const int *diag,
+                     const double *values, egpu_mat **out);
+/* same pattern, new Values (nonlinear / time steps) */
+int egpu_matrix_update_values(egpu_mat *A, const double *values);
+int egpu_matrix_values_download(egpu_mat *A, double *values);
+int egpu_matrix_rhs_download(egpu_mat *A, double *rhs);
+void egpu_matrix_free(egpu_mat *A);
+
+/* ---- IterSolver replacement (SolveLinearSystem semantics, SolverUtils.src:7151-7525):
+ * zero-rhs short cut, symmetric scaling, x = 1e-8 when x is all zero, ILU0 factored on
+ * the scaled matrix, HUTI true-residual stopping test, back-scaling.  b, x host. */
+int egpu_iter_solve(egpu_mat *A, const double *b, double *x, const egpu_params *prm,
+                    egpu_result *res);
+/* same with b_dev, x_dev in device memory; b_dev == NULL uses the assembled RHS */
+int egpu_iter_solve_dev(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_params *prm,
+                        egpu_result *res);
+
+/* ---- preconditioner state (Matrix_t ILUValues, CRSMatrix.src:2157-2388, 3259-3270) ----
+ * egpu_ilu0_build factors ILU0 of the matrix (scaled as SolveLinearSystem scales it when
+ * scale_system != 0) on the device; egpu_ilu0_download copies the factors (same layout as
+ * Values, inverted U diagonal) and the DiagScaling vector (NULL to skip);
+ * egpu_lu_precondition applies u = (LU)^-1 v with the device factors (pcondProc). */
+int egpu_ilu0_build(egpu_mat *A, int scale_system);
+int egpu_ilu0_download(egpu_mat *A, double *ilu_values, double *diag_scaling);
+int egpu_lu_precondition(egpu_mat *A, const double *v, double *u);
+
+/* ---- Matrix Vector Proc hook (CRSMatrix.src:3555-3559, Load.c:734-747) ----------- */
+int egpu_mv(egpu_mat *A, const double *u, double *v);
+int egpu_mv_dev(egpu_mat *A, const double *u_dev, double *v_dev);
+/* exact MatVecSubr signature; *spmv is the per-matrix handle slot A%SpMV; the
+ * matrix is (re)uploaded when *reinit != 0 or *spmv == NULL */
+void egpu_matvec_subr(void **spmv, int *n, int *rows, int *cols, double *values, double *u,
+                      double *v, int *reinit);
+
+/* ---- assembly seam (HeatSolve / StressSolve bulk loops) --------------------------
+ * Binds the mesh to the matrix pattern: coords (nnodes x 3, row-major), element
+ * connectivity (nelem x nen, 1-based), element code (808 | 504 | 303), Perm.
+ * Builds the element colouring and the element -> CRS slot map on the device. */
+int egpu_assembly_bind(egpu_mat *A, int nnodes, const double *xyz, int cdim, int nelem,
+                       int code, const int *elem_nodes, const int *perm, int dofs);
+/* DiffuseConvectiveCompose diffusion branch: conductivity per element (elem_k, nelem)
+ * or per node (nodal_k, nnodes) or 1; nodal heat source*density (load, nnodes) or 0.
+ * Zeroes and fills Values and the RHS on the device. */
+int egpu_assemble_poisson(egpu_mat *A, const double *elem_k, const double *nodal_k,
+                          const double *load);
+/* StressCompose, isotropic 3D (dofs = 3) with a constant body force */
+int egpu_assemble_elastic(egpu_mat *A, double young, double poisson, const double *body_force3);
+/* DefaultDirichletBCs: con_rows 1-based matrix rows, con_vals values (NULL = 0),
+ * symmetric = Linear System Symmetric (CRS_SetSymmDirichlet) */
+int egpu_dirichlet(egpu_mat *A, int ncon, const int *con_rows, const double *con_vals,
+                   int symmetric);
+
+/* ---- batched solve: many independent systems in one persistent launch ------------
+ * Systems are appended with their own CRS/RHS; egpu_batch_solve runs them all with
+ * one cooperative kernel and per-system convergence masks. */
+typedef struct egpu_batch egpu_batch;
+int egpu_batch_create(egpu_ctx *ctx, egpu_batch **out);
+/* returns the system id (>= 0) or an error */
+int egpu_batch_add(egpu_batch *B, int n, const int *rows, const int *cols, const int *diag,
+                   const double *values, const double *rhs);
+int egpu_batch_solve(egpu_batch *B, const egpu_params *prm, egpu_result *per_system);
+int egpu_batch_solution(egpu_batch *B, int sys, double *x);
+int egpu_batch_tune(egpu_batch *B, const egpu_params *prm, int *lanes_per_row_out);
+void egpu_batch_free(egpu_batch *B);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ELMERGPU_H */

@@ -1,0 +1,194 @@
+"""ctypes binding of the CPU oracle (oracle/elmer_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the CPU
+baseline leg of bench.py as the checker.  The product library never loads it.
+All index arrays are 1-based int32, as in Elmer's Matrix_t.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libelmer_oracle.so")
+_lib = None
+
+CG, BICGSTAB = 1, 2
+PREC_NONE, PREC_DIAGONAL, PREC_ILU0 = 0, 1, 2
+
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+
+class _Params(C.Structure):
+    _fields_ = [("method", C.c_int), ("precond", C.c_int), ("max_iter", C.c_int),
+                ("tol", C.c_double), ("scale_system", C.c_int), ("omp_threads", C.c_int)]
+
+
+class _Result(C.Structure):
+    _fields_ = [("info", C.c_int), ("iters", C.c_int), ("residual", C.c_double),
+                ("seconds_solve", C.c_double), ("seconds_precond_setup", C.c_double)]
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        L.orc_pattern_create.restype = C.c_void_p
+        L.orc_pattern_create.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, C.c_int, C.c_int, C.c_int]
+        L.orc_pattern_info.argtypes = [C.c_void_p] + [C.c_void_p] * 6
+        L.orc_pattern_copy.argtypes = [C.c_void_p, _i32p, _i32p, _i32p, _i32p]
+        L.orc_pattern_free.argtypes = [C.c_void_p]
+        L.orc_assemble_poisson.argtypes = [C.c_int, _f64p, C.c_int, C.c_int, C.c_int, _i32p,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, _i32p, C.c_int,
+                                           _i32p, _i32p, _i32p, _f64p, _f64p]
+        L.orc_assemble_elastic.argtypes = [C.c_int, _f64p, C.c_int, C.c_int, _i32p, C.c_double,
+                                           C.c_double, _f64p, _i32p, C.c_int, _i32p, _i32p,
+                                           _i32p, _f64p, _f64p]
+        L.orc_dirichlet.argtypes = [C.c_int, _i32p, _i32p, _i32p, _f64p, _f64p, C.c_int, _i32p,
+                                    _f64p, C.c_int, C.c_int]
+        L.orc_solve.restype = C.c_int
+        L.orc_solve.argtypes = [C.c_int, _i32p, _i32p, _i32p, _f64p, _f64p, _f64p,
+                                C.POINTER(_Params), C.POINTER(_Result)]
+        L.orc_spmv.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int]
+        L.orc_ilu0.argtypes = [C.c_int, _i32p, _i32p, _i32p, _f64p, _f64p]
+        L.orc_lusolve.argtypes = [C.c_int, _i32p, _i32p, _i32p, _f64p, _f64p]
+        L.orc_scale.argtypes = [C.c_int, _i32p, _i32p, _i32p, _f64p, C.c_void_p, C.c_void_p,
+                                _f64p, C.POINTER(C.c_double), C.c_int]
+        L.orc_compute_norm.restype = C.c_double
+        L.orc_compute_norm.argtypes = [C.c_int, _f64p]
+        L.orc_lower_levels.restype = C.c_int
+        L.orc_lower_levels.argtypes = [C.c_int, _i32p, _i32p, _i32p, _i32p]
+        _lib = L
+    return _lib
+
+
+@dataclass
+class Pattern:
+    n: int
+    nnz: int
+    dofs: int
+    perm: np.ndarray
+    rows: np.ndarray
+    cols: np.ndarray
+    diag: np.ndarray
+    hbw_before: int
+    hbw_after: int
+    start_node: int
+    rejected: int
+
+
+def _ptr(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64).ctypes.data
+
+
+def create_pattern(mesh, dofs: int = 1, optimize: bool = True, use_always: bool = False) -> Pattern:
+    L = lib()
+    el = np.ascontiguousarray(mesh.elements, dtype=np.int32)
+    h = L.orc_pattern_create(mesh.nnodes, el.shape[0], el.shape[1], el, dofs, int(optimize), int(use_always))
+    n, nnz = C.c_int(), C.c_longlong()
+    hb, ha, st, rj = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    L.orc_pattern_info(h, C.byref(n), C.byref(nnz), C.byref(hb), C.byref(ha), C.byref(st), C.byref(rj))
+    perm = np.zeros(mesh.nnodes, np.int32)
+    rows = np.zeros(n.value + 1, np.int32)
+    cols = np.zeros(nnz.value, np.int32)
+    diag = np.zeros(n.value, np.int32)
+    L.orc_pattern_copy(h, perm, rows, cols, diag)
+    L.orc_pattern_free(h)
+    return Pattern(n.value, nnz.value, dofs, perm, rows, cols, diag, hb.value, ha.value, st.value, rj.value)
+
+
+def assemble_poisson(mesh, pat: Pattern, elem_k=None, nodal_k=None, load=None, cdim=None):
+    L = lib()
+    values = np.zeros(pat.nnz, np.float64)
+    rhs = np.zeros(pat.n, np.float64)
+    xyz = np.ascontiguousarray(mesh.coords, dtype=np.float64)
+    if cdim is None:
+        cdim = 2 if mesh.elem_code // 100 <= 4 else 3
+    keep = [np.ascontiguousarray(a, dtype=np.float64) if a is not None else None for a in (elem_k, nodal_k, load)]
+    L.orc_assemble_poisson(mesh.nnodes, xyz, cdim, mesh.nelem, mesh.elem_code,
+                           np.ascontiguousarray(mesh.elements, np.int32),
+                           *[None if a is None else a.ctypes.data for a in keep],
+                           pat.perm, pat.n, pat.rows, pat.cols, pat.diag, values, rhs)
+    return values, rhs
+
+
+def assemble_elastic(mesh, pat: Pattern, young: float, poisson: float, body_force):
+    L = lib()
+    values = np.zeros(pat.nnz, np.float64)
+    rhs = np.zeros(pat.n, np.float64)
+    L.orc_assemble_elastic(mesh.nnodes, np.ascontiguousarray(mesh.coords, np.float64), mesh.nelem,
+                           mesh.elem_code, np.ascontiguousarray(mesh.elements, np.int32),
+                           young, poisson, np.asarray(body_force, np.float64), pat.perm, pat.n,
+                           pat.rows, pat.cols, pat.diag, values, rhs)
+    return values, rhs
+
+
+def dirichlet(pat: Pattern, values, rhs, con_rows, con_vals=None, symmetric=False, scale=True):
+    con_rows = np.ascontiguousarray(con_rows, np.int32)
+    if con_vals is None:
+        con_vals = np.zeros(con_rows.size, np.float64)
+    lib().orc_dirichlet(pat.n, pat.rows, pat.cols, pat.diag, values, rhs, con_rows.size, con_rows,
+                        np.ascontiguousarray(con_vals, np.float64), int(symmetric), int(scale))
+
+
+def solve(pat: Pattern, values, b, method=BICGSTAB, precond=PREC_ILU0, max_iter=1000, tol=1e-10,
+          x0=None, scale=True, threads=0):
+    x = np.zeros(pat.n) if x0 is None else np.array(x0, dtype=np.float64)
+    p = _Params(method, precond, max_iter, tol, int(scale), threads)
+    r = _Result()
+    lib().orc_solve(pat.n, pat.rows, pat.cols, pat.diag, np.ascontiguousarray(values, np.float64),
+                    np.ascontiguousarray(b, np.float64), x, C.byref(p), C.byref(r))
+    return x, {"info": r.info, "iters": r.iters, "residual": r.residual,
+               "seconds": r.seconds_solve, "seconds_precond_setup": r.seconds_precond_setup}
+
+
+def spmv(pat: Pattern, values, u, threads=0):
+    v = np.zeros(pat.n)
+    lib().orc_spmv(pat.n, pat.rows, pat.cols, np.ascontiguousarray(values, np.float64),
+                   np.ascontiguousarray(u, np.float64), v, threads)
+    return v
+
+
+def ilu0(pat: Pattern, values):
+    out = np.zeros(pat.nnz)
+    lib().orc_ilu0(pat.n, pat.rows, pat.cols, pat.diag, np.ascontiguousarray(values, np.float64), out)
+    return out
+
+
+def lusolve(pat: Pattern, ilu, b):
+    x = np.array(b, dtype=np.float64)
+    lib().orc_lusolve(pat.n, pat.rows, pat.cols, pat.diag, np.ascontiguousarray(ilu, np.float64), x)
+    return x
+
+
+def scale(pat: Pattern, values, b=None, x=None, rhs_scale=True):
+    """In-place ScaleLinearSystem; returns (DiagScaling, RhsScaling)."""
+    D = np.zeros(pat.n)
+    rs = C.c_double()
+    lib().orc_scale(pat.n, pat.rows, pat.cols, pat.diag, values,
+                    None if b is None else b.ctypes.data, None if x is None else x.ctypes.data,
+                    D, C.byref(rs), int(rhs_scale))
+    return D, rs.value
+
+
+def compute_norm(x):
+    x = np.ascontiguousarray(x, np.float64)
+    return lib().orc_compute_norm(x.size, x)
+
+
+def lower_levels(pat: Pattern):
+    lv = np.zeros(pat.n, np.int32)
+    nl = lib().orc_lower_levels(pat.n, pat.rows, pat.cols, pat.diag, lv)
+    return nl, lv

@@ -1,0 +1,87 @@
+/*
+ * elmer_oracle.h -- CPU restatement of ElmerSolver's linear-system path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker for the GPU library
+ * (elmerfem_b200/libelmergpu.so): it is linked by the tests, by smoke() and by
+ * the CPU-baseline leg of bench.py, never by the product.  Each function restates
+ * the Fortran routine cited beside it, in the same operation order, with
+ * floating-point contraction disabled (-ffp-contract=off).
+ *
+ * Conventions follow Elmer's Matrix_t (fem/src/Types.src:155-228): Rows(n+1),
+ * Cols(nnz), Diag(n) are 1-based int32; Values are double.
+ */
+#ifndef ELMER_ORACLE_H
+#define ELMER_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- sparsity pattern: MakeListMatrix + OptimizeBandwidth + CRS_CreateMatrix/InitializeMatrix */
+typedef struct orc_pattern orc_pattern;
+
+orc_pattern *orc_pattern_create(int nnodes, int nelem, int nen, const int *elem_nodes,
+                                int dofs, int optimize_bw, int use_optimized_always);
+void orc_pattern_info(const orc_pattern *p, int *n, long long *nnz, int *hbw_before,
+                      int *hbw_after, int *start_node, int *rejected);
+void orc_pattern_copy(const orc_pattern *p, int *perm, int *rows, int *cols, int *diag);
+void orc_pattern_free(orc_pattern *p);
+
+/* ---- element assembly (HeatSolve / StressSolve bulk loops) */
+/* elem_k: per-element conductivity (nelem) or NULL for nodal_k; nodal_k: per-node
+ * conductivity or NULL (then k=1); load: per-node heat source * density (or NULL = 0). */
+void orc_assemble_poisson(int nnodes, const double *xyz, int cdim, int nelem, int code,
+                          const int *elem_nodes, const double *elem_k, const double *nodal_k,
+                          const double *load, const int *perm, int n, const int *rows,
+                          const int *cols, const int *diag, double *values, double *rhs);
+void orc_assemble_elastic(int nnodes, const double *xyz, int nelem, int code,
+                          const int *elem_nodes, double young, double poisson,
+                          const double *body_force3, const int *perm, int n, const int *rows,
+                          const int *cols, const int *diag, double *values, double *rhs);
+
+/* ---- Dirichlet conditions (DefaultDirichletBCs): scale(no rhs) -> set rows -> backscale */
+void orc_dirichlet(int n, const int *rows, const int *cols, const int *diag, double *values,
+                   double *rhs, int ncon, const int *con_rows, const double *con_vals,
+                   int symmetric, int scale);
+
+/* ---- linear solve (SolveLinearSystem -> IterSolver -> HUTI) */
+enum { ORC_CG = 1, ORC_BICGSTAB = 2 };
+enum { ORC_PREC_NONE = 0, ORC_PREC_DIAGONAL = 1, ORC_PREC_ILU0 = 2 };
+typedef struct {
+  int method;          /* ORC_CG | ORC_BICGSTAB */
+  int precond;         /* ORC_PREC_* */
+  int max_iter;        /* Linear System Max Iterations */
+  double tol;          /* Linear System Convergence Tolerance */
+  int scale_system;    /* Linear System Scaling (default 1) */
+  int omp_threads;     /* threads for the SpMV loop (CRSMatrix.src:3565), <=0: all */
+} orc_params;
+typedef struct {
+  int info;            /* HUTI status code (huti_fdefs.h) */
+  int iters;
+  double residual;     /* last ||Ax-b||/||b|| on the scaled system */
+  double seconds_solve;/* scale + IterSolver + backscale */
+  double seconds_precond_setup;
+} orc_result;
+
+/* values/b are not modified (the routine works on copies, as the reference's
+ * scaling and back-scaling leave A and b restored). x: in = initial guess, out = solution. */
+int orc_solve(int n, const int *rows, const int *cols, const int *diag, const double *values,
+              const double *b, double *x, const orc_params *prm, orc_result *res);
+
+/* ---- primitives for unit parity */
+void orc_spmv(int n, const int *rows, const int *cols, const double *values, const double *u,
+              double *v, int omp_threads);
+void orc_ilu0(int n, const int *rows, const int *cols, const int *diag, const double *values,
+              double *ilu_values);
+void orc_lusolve(int n, const int *rows, const int *cols, const int *diag,
+                 const double *ilu_values, double *b);
+void orc_scale(int n, const int *rows, const int *cols, const int *diag, double *values,
+               double *b, double *x, double *diag_scaling, double *rhs_scaling, int rhs_scale);
+double orc_compute_norm(int n, const double *x);
+/* dependency levels of the lower-triangular part (row i after every j<i with a_ij != 0) */
+int orc_lower_levels(int n, const int *rows, const int *cols, const int *diag, int *level);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

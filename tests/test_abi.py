@@ -1,0 +1,75 @@
+"""C-ABI surface: the library loads and exports every declared symbol; keyword parsing (CPU)."""
+import ctypes as C
+
+import pytest
+
+import elmerfem_b200 as eg
+from elmerfem_b200 import _lib
+
+
+def test_library_loads_and_exports_declared_symbols():
+    L = _lib.lib()
+    declared = _lib.declared_symbols()
+    assert len(declared) >= 25
+    missing = [s for s in declared if not hasattr(L, s)]
+    assert not missing, missing
+    assert set(declared) == set(_lib.PROTOTYPES), set(declared) ^ set(_lib.PROTOTYPES)
+
+
+def test_params_default_matches_elmer_defaults():
+    p = _lib.Params()
+    _lib.lib().egpu_params_default(C.byref(p), eg.CG, eg.PREC_DIAGONAL)
+    assert (p.method, p.precond, p.scale_system, p.refactorize, p.precond_recompute) == (1, 1, 1, 1, 1)
+
+
+def test_create_on_missing_device_fails_cleanly():
+    h = C.c_void_p()
+    rc = _lib.lib().egpu_create(10_000, C.byref(h))
+    assert rc == -2 and not h.value
+
+
+def test_null_arguments_rejected():
+    raw = C.CDLL(_lib.LIB_PATH)  # untyped view: pass NULLs straight through
+    assert raw.egpu_iter_solve(None, None, None, None, None) == -1
+    assert raw.egpu_iter_solve_dev(None, None, None, None, None) == -1
+    assert raw.egpu_assembly_bind(None, 0, None, 3, 0, 808, None, None, 1) == -1
+    assert raw.egpu_matrix_bind(None, 0, None, None, None, None, None) == -1
+    assert raw.egpu_mv(None, None, None) == -1
+
+
+SIF = """
+Solver 1
+  Equation = "Heat Equation"
+  Linear System Solver = "Iterative"
+  Linear System Iterative Method = "BiCGStab"
+  Linear System Max Iterations = 350
+  Linear System Convergence Tolerance = 1.0e-08
+  Linear System Abort Not Converged = True
+  Linear System Preconditioning = "ILU0"
+  Linear System Residual Output = 1
+End
+"""
+
+
+def test_sif_keywords():
+    p = eg.SolverParams.from_sif(SIF)
+    assert (p.method, p.precond, p.max_iter, p.tol) == (eg.BICGSTAB, eg.PREC_ILU0, 350, 1e-8)
+    assert p.scale_system and p.abort_not_converged
+    q = eg.SolverParams.from_sif({"Linear System Iterative Method": "CG", "Linear System Preconditioning": "Diagonal",
+                                  "Linear System Max Iterations": 10, "Linear System Convergence Tolerance": 1e-6,
+                                  "Linear System Symmetric": True, "Linear System Precision": "mixed"})
+    assert (q.method, q.precond, q.symmetric, q.precision) == (eg.CG, eg.PREC_DIAGONAL, True, eg.MIXED)
+
+
+@pytest.mark.parametrize("bad", [{"Linear System Solver": "Direct"}, {"Linear System Iterative Method": "GMRES"},
+                                 {"Linear System Preconditioning": "ILU1"}])
+def test_sif_outside_the_path(bad):
+    kw = {"Linear System Max Iterations": 10, "Linear System Convergence Tolerance": 1e-6}
+    kw.update(bad)
+    with pytest.raises(NotImplementedError):
+        eg.SolverParams.from_sif(kw)
+
+
+def test_sif_required_keywords():
+    with pytest.raises(KeyError):
+        eg.SolverParams.from_sif({"Linear System Convergence Tolerance": 1e-6})

@@ -1,0 +1,101 @@
+"""The oracle against the reference's own regression targets and internal invariants (CPU)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from elmerfem_b200 import meshgen
+from helpers import poisson_problem
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _heateq():
+    d = np.load(os.path.join(GOLDEN, "heateq_mesh.npz"))
+    return meshgen.Mesh(d["coords"], 303, d["elements"], 202, d["bnd_elements"], d["bnd_ids"], ())
+
+
+def test_golden_targets_present():
+    t = json.load(open(os.path.join(GOLDEN, "targets.json")))
+    assert t["heateq"]["nrm"] == pytest.approx(0.0768016492512, rel=1e-12)
+
+
+@pytest.mark.parametrize("method,prec", [(oracle.BICGSTAB, oracle.PREC_ILU0), (oracle.CG, oracle.PREC_ILU0),
+                                         (oracle.CG, oracle.PREC_DIAGONAL), (oracle.BICGSTAB, oracle.PREC_NONE)])
+@pytest.mark.parametrize("sym", [False, True])
+def test_heateq_nrm(method, prec, sym):
+    """fem/tests/heateq/TempDist.sif: k=1, source 1, T=0 on all boundaries, NRM=0.768016492512E-01
+    (findnorm EPS 1e-5; the restatement reproduces it to ~1e-11)."""
+    t = json.load(open(os.path.join(GOLDEN, "targets.json")))["heateq"]
+    m = _heateq()
+    p, _, _, v, b, _ = poisson_problem(m, sym=sym)
+    x, r = oracle.solve(p, v, b, method=method, precond=prec, max_iter=350, tol=1e-12)
+    assert r["info"] == 1
+    nrm = oracle.compute_norm(x)
+    assert abs(nrm - t["nrm"]) / t["nrm"] < 1e-9
+
+
+@pytest.mark.parametrize("case,method", [(5, oracle.CG), (10, oracle.BICGSTAB)])
+def test_linearsolvers_nrm(case, method):
+    """fem/tests/linearsolvers/TempDist.sif: no source, T=case on all boundaries, ILU0, tol 1e-12 => NRM=case."""
+    m = _heateq()
+    p = oracle.create_pattern(m)
+    vals, _ = oracle.assemble_poisson(m, p, nodal_k=np.ones(m.nnodes), load=None)
+    con = np.sort(p.perm[m.boundary_nodes(range(1, 7)) - 1]).astype(np.int32)
+    b = np.zeros(p.n)
+    oracle.dirichlet(p, vals, b, con, con_vals=np.full(con.size, float(case)))
+    x, r = oracle.solve(p, vals, b, method=method, precond=oracle.PREC_ILU0, max_iter=3500, tol=1e-12)
+    assert r["info"] == 1
+    assert abs(oracle.compute_norm(x) - case) / case < 1e-9
+
+
+def test_bandwidth_optimisation_accepted_on_heateq():
+    m = _heateq()
+    p = oracle.create_pattern(m)
+    assert p.rejected == 0 and p.hbw_after < p.hbw_before
+    assert sorted(p.perm.tolist()) == list(range(1, m.nnodes + 1))
+
+
+def test_bandwidth_optimisation_rejected_on_structured_cube():
+    p = oracle.create_pattern(meshgen.hex_cube(6))
+    assert p.rejected == 1 and np.array_equal(p.perm, np.arange(1, 7 ** 3 + 1))
+
+
+def test_ilu0_lusolve_inverts_tridiagonal_exactly():
+    """ILU0 of a tridiagonal matrix is its exact LU (no fill), so LU-solve inverts it."""
+    n = 50
+    rows = np.arange(1, 3 * n, 3, dtype=np.int32)
+    rows = np.concatenate([[1], np.cumsum([2] + [3] * (n - 2) + [2]) + 1]).astype(np.int32)
+    cols, vals, diag = [], [], []
+    for i in range(n):
+        for j in (i - 1, i, i + 1):
+            if 0 <= j < n:
+                if j == i:
+                    diag.append(len(cols) + 1)
+                cols.append(j + 1)
+                vals.append(4.0 if i == j else -1.0)
+    pat = oracle.Pattern(n, len(cols), 1, np.arange(1, n + 1, dtype=np.int32), rows, np.array(cols, np.int32),
+                         np.array(diag, np.int32), 0, 0, 0, 0)
+    vals = np.array(vals)
+    ilu = oracle.ilu0(pat, vals)
+    rhs = np.random.default_rng(0).random(n)
+    x = oracle.lusolve(pat, ilu, rhs)
+    assert np.allclose(oracle.spmv(pat, vals, x), rhs, rtol=0, atol=1e-13)
+
+
+def test_hex_stiffness_row_sums_vanish():
+    """Constant fields are in the kernel of the Laplacian: interior row sums are ~0."""
+    m = meshgen.hex_cube(4)
+    p = oracle.create_pattern(m)
+    vals, _ = oracle.assemble_poisson(m, p, nodal_k=np.ones(m.nnodes), load=None)
+    s = oracle.spmv(p, vals, np.ones(p.n))
+    assert np.max(np.abs(s)) < 1e-13
+
+
+def test_zero_rhs_short_cut():
+    m = meshgen.hex_cube(3)
+    p, _, _, v, _, _ = poisson_problem(m)
+    x, r = oracle.solve(p, v, np.zeros(p.n), method=oracle.CG, precond=oracle.PREC_DIAGONAL, max_iter=10)
+    assert r["info"] == 1 and not np.any(x)
