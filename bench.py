@@ -45,6 +45,15 @@ def workload_spec(name):
         return build, dict(method=1, precond=1, tol=1e-10, max_iter=20000), \
             {"workload": "poisson_hex128_lognormal_cg_jacobi", "mesh": "128^3 hex 808", "dofs": 2146689,
              "method": "CG", "preconditioner": "Diagonal", "tol": 1e-10}
+    if name == "poisson96_cg_jacobi":
+        # profiling-size variant of the 128^3 workload (matrix 146 MB in FP32: still larger than L2)
+        def build():
+            m = meshgen.hex_cube(96)
+            return dict(mesh=m, elem_k=meshgen.lognormal_conductivity(m.nelem, 1.0, 1),
+                        load=meshgen.sine_source(m.coords), bc=range(1, 7), symmetric=True)
+        return build, dict(method=1, precond=1, tol=1e-10, max_iter=20000), \
+            {"workload": "poisson_hex96_lognormal_cg_jacobi", "mesh": "96^3 hex 808", "dofs": 912673,
+             "method": "CG", "preconditioner": "Diagonal", "tol": 1e-10}
     if name == "poisson32_bicgstab_ilu0":
         def build():
             m = meshgen.hex_cube(32)

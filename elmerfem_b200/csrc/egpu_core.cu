@@ -65,6 +65,26 @@ __global__ void k_scale_values(int n, const int *__restrict__ rows, const int *_
   }
 }
 
+// scaled values in SELL-32 order (thread per row; padding entries 0)
+__global__ void k_sell_scale(int n, int nslices, const int *__restrict__ rows, const int *__restrict__ cols,
+                             const double *__restrict__ vals, const double *__restrict__ D,
+                             const int *__restrict__ sell_ptr, const int *__restrict__ sell_w,
+                             double *__restrict__ out) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nslices * 32; r += gridDim.x * blockDim.x) {
+    const int sl = r >> 5, lane = r & 31;
+    const int w = sell_w[sl];
+    double *o = out + sell_ptr[sl] + lane;
+    int beg = 0, len = 0;
+    double dr = 0.0;
+    if (r < n) {
+      beg = rows[r];
+      len = rows[r + 1] - beg;
+      dr = D[r];
+    }
+    for (int k = 0; k < w; ++k) o[32 * k] = k < len ? vals[beg + k] * (dr * D[cols[beg + k]]) : 0.0;
+  }
+}
+
 // right-hand side scaling, pass 1: bs = b*D; partials of ||b||^2, ||bs||^2, any x != 0
 __global__ void k_rhs_scale_a(int n, const double *__restrict__ b, const double *__restrict__ D,
                               const double *__restrict__ x, double *__restrict__ bs,
@@ -264,7 +284,9 @@ static int grid_for(const egpu_ctx *ctx, long long work, int block = 256) {
 // Level schedules of the strictly lower / upper parts (rows sorted by dependency level).
 static void build_levels(int n, const std::vector<int> &rows, const std::vector<int> &cols,
                          const std::vector<int> &diag, std::vector<int> &lower,
-                         std::vector<int> &upper, int &nlow, int &nup, int &maxl, int &maxu) {
+                         std::vector<int> &upper, int &nlow, int &nup, int &maxl, int &maxu,
+                         int &maxw) {
+  maxw = 0;
   std::vector<int> lev(n, 0);
   nlow = 0;
   maxl = maxu = 0;
@@ -279,6 +301,7 @@ static void build_levels(int n, const std::vector<int> &rows, const std::vector<
   std::vector<int> cnt(nlow + 1, 0);
   for (int i = 0; i < n; ++i) cnt[lev[i] + 1]++;
   for (int l = 0; l < nlow; ++l) cnt[l + 1] += cnt[l];
+  for (int l = 0; l < nlow; ++l) maxw = std::max(maxw, cnt[l + 1] - cnt[l]);
   lower.assign(n, 0);
   for (int i = 0; i < n; ++i) lower[cnt[lev[i]]++] = i;
   nup = 0;
@@ -292,6 +315,7 @@ static void build_levels(int n, const std::vector<int> &rows, const std::vector<
   cnt.assign(nup + 1, 0);
   for (int i = 0; i < n; ++i) cnt[lev[i] + 1]++;
   for (int l = 0; l < nup; ++l) cnt[l + 1] += cnt[l];
+  for (int l = 0; l < nup; ++l) maxw = std::max(maxw, cnt[l + 1] - cnt[l]);
   upper.assign(n, 0);
   for (int i = n - 1; i >= 0; --i) upper[cnt[lev[i]]++] = i;
 }
@@ -354,8 +378,8 @@ int scale_matrix(egpu_mat *A, bool scale_system) {
   const int n = A->n;
   EGPU_CUDA_TRY(ctx, A->scaled.alloc(A->nnz));
   EGPU_CUDA_TRY(ctx, A->dscale.alloc(n));
-  EGPU_CUDA_TRY(ctx, A->work.alloc((size_t)12 * n + 64));
-  double *dvals = A->work.p + (size_t)11 * n;
+  EGPU_CUDA_TRY(ctx, A->work.alloc((size_t)13 * A->ldw));
+  double *dvals = A->work.p + (size_t)11 * A->ldw;
   if (scale_system) {
     k_scale_diag<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, A->rows.p, A->diag.p, A->values.p, A->dscale.p);
   } else {
@@ -364,7 +388,10 @@ int scale_matrix(egpu_mat *A, bool scale_system) {
   }
   k_scale_values<<<grid_for(ctx, (long long)n * 8), 256, 0, ctx->stream>>>(
       n, A->rows.p, A->cols.p, A->diag.p, A->values.p, A->dscale.p, A->scaled.p, dvals);
-  ctx->launches += 2;
+  EGPU_CUDA_TRY(ctx, A->sell_vals.alloc(A->sell_nnz));
+  k_sell_scale<<<grid_for(ctx, (long long)A->nslices * 32), 256, 0, ctx->stream>>>(
+      n, A->nslices, A->rows.p, A->cols.p, A->values.p, A->dscale.p, A->sell_ptr.p, A->sell_w.p, A->sell_vals.p);
+  ctx->launches += 3;
   EGPU_CUDA_TRY(ctx, cudaGetLastError());
   return EGPU_OK;
 }
@@ -384,7 +411,7 @@ int ensure_tri_schedule(egpu_mat *A) {
     }
   std::vector<int> lo, up;
   build_levels(n, rows, cols, diag, lo, up, A->tri.lower_levels, A->tri.upper_levels, A->tri.max_lower,
-               A->tri.max_upper);
+               A->tri.max_upper, A->tri.max_width);
   EGPU_CUDA_TRY(ctx, A->tri.lower_order.alloc(n));
   EGPU_CUDA_TRY(ctx, A->tri.upper_order.alloc(n));
   EGPU_CUDA_TRY(ctx, cudaMemcpy(A->tri.lower_order.p, lo.data(), n * sizeof(int), cudaMemcpyHostToDevice));
@@ -417,7 +444,9 @@ int ilu0_factor(egpu_mat *A) {
   } else {
     EGPU_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_ilu0_factor<256>, 256, 0));
   }
-  int grid = std::max(1, std::min(bps, 4)) * ctx->num_sms;
+  // enough warps for about twice the widest level, never more than fit at once
+  const int want_blocks = (2 * std::max(1, A->tri.max_width) + 7) / 8;
+  int grid = std::max(1, std::min(std::min(bps, 4) * ctx->num_sms, std::max(ctx->num_sms, want_blocks)));
   void *args[] = {(void *)&n, &A->rows.p, &A->cols.p, &A->diag.p, &A->tri.lower_order.p, &A->scaled.p,
                   &A->ilu.p, &A->ilu_done.p, &err};
   const void *kern = A->max_row <= 32 ? (const void *)k_ilu0_factor<32>
@@ -432,10 +461,29 @@ int ilu0_factor(egpu_mat *A) {
 }
 
 template <typename VT>
+static void set_sell(KArgs<VT> &a, const egpu_mat *A, const VT *vals, bool offs) {
+  a.nslices = A->nslices;
+  a.sell_ptr = A->sell_ptr.p;
+  a.sell_w = A->sell_w.p;
+  a.scols = A->sell_cols.p;
+  a.scols16 = offs ? A->sell_c16.p : nullptr;
+  a.svals = vals;
+}
+
+// sub-warps per block for the sync-free solves: about twice the widest level in total,
+// at least one per block
+static int tri_per_block(const egpu_mat *A, int lpr, int grid) {
+  const int per_block_max = EGPU_BLOCK / lpr;
+  const int want = std::max(1, 2 * A->tri.max_width);
+  return std::max(1, std::min(per_block_max, (want + grid - 1) / grid));
+}
+
+template <typename VT>
 static int run_krylov(egpu_mat *A, const KArgs<VT> &a0, int method, bool offs) {
   egpu_ctx *ctx = A->ctx;
   KArgs<VT> a = a0;
   const int lpr = pick_lpr(A);
+  a.tri_per_block = tri_per_block(A, lpr, ctx->num_sms * 2);
 #define EGPU_LAUNCH_K(KERN, L)                                                 \
   do {                                                                         \
     if (offs)                                                                  \
@@ -474,9 +522,10 @@ int solve_fp64(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_param
   rc = scale_matrix(A, sc);
   if (rc) return rc;
   double *W = A->work.p;
-  double *bs = W + (size_t)10 * n;     // scaled rhs
-  double *dvals = W + (size_t)11 * n;  // scaled diagonal
-  double *xs = x_dev;                  // scaled in place
+  const long long ldw = A->ldw;
+  double *bs = W + (size_t)10 * ldw;     // scaled rhs
+  double *dvals = W + (size_t)11 * ldw;  // scaled diagonal
+  double *xs = W + (size_t)12 * ldw;     // scaled solution (aligned, padded copy of x)
   unsigned int *flags = ctx->sync.p + 2;
   int nbp = std::min(grid_for(ctx, n), 1024);
   k_rhs_scale_a<<<nbp, 256, 0, ctx->stream>>>(n, b_dev, A->dscale.p, x_dev, bs, ctx->partials.p, flags);
@@ -506,6 +555,7 @@ int solve_fp64(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_param
   a.diag = A->diag.p;
   a.cols16 = nullptr;
   a.vals = A->scaled.p;
+  set_sell(a, A, A->sell_vals.p, false);
   a.ilu = A->ilu.p;
   a.dvals = dvals;
   a.lower_order = A->tri.lower_order.p;
@@ -517,7 +567,7 @@ int solve_fp64(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_param
   a.b = bs;
   a.x = xs;
   a.w = W;
-  a.ldw = n;
+  a.ldw = ldw;
   a.bar = ctx->sync.p;
   a.err = (int *)(ctx->sync.p + 1);
   a.partials = ctx->partials.p;
@@ -656,8 +706,9 @@ int krylov_fp64_scaled(egpu_mat *A, const double *bs, double *xs, const egpu_par
   a.cols = A->cols.p;
   a.diag = A->diag.p;
   a.vals = A->scaled.p;
+  set_sell(a, A, A->sell_vals.p, false);
   a.ilu = A->ilu.p;
-  a.dvals = A->work.p + (size_t)11 * n;
+  a.dvals = A->work.p + (size_t)11 * A->ldw;
   a.lower_order = A->tri.lower_order.p;
   a.upper_order = A->tri.upper_order.p;
   a.precond = prm->precond;
@@ -667,7 +718,7 @@ int krylov_fp64_scaled(egpu_mat *A, const double *bs, double *xs, const egpu_par
   a.b = bs;
   a.x = xs;
   a.w = A->work.p;
-  a.ldw = n;
+  a.ldw = A->ldw;
   a.bar = ctx->sync.p;
   a.err = (int *)(ctx->sync.p + 1);
   a.partials = ctx->partials.p;
@@ -693,9 +744,12 @@ static int prepare_fp32(egpu_mat *A, bool with_ilu) {
   const int n = A->n;
   EGPU_CUDA_TRY(ctx, A->scaled32.alloc(A->nnz));
   k_to_f32<<<grid_for(ctx, A->nnz), 256, 0, ctx->stream>>>(A->scaled.p, A->scaled32.p, A->nnz);
-  EGPU_CUDA_TRY(ctx, A->work32.alloc((size_t)14 * n + 64));
-  k_to_f32<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(A->work.p + (size_t)11 * n, A->work32.p + (size_t)13 * n, n);
-  ctx->launches += 2;
+  EGPU_CUDA_TRY(ctx, A->work32.alloc((size_t)14 * A->ldw));
+  k_to_f32<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(A->work.p + (size_t)11 * A->ldw,
+                                                       A->work32.p + (size_t)13 * A->ldw, n);
+  EGPU_CUDA_TRY(ctx, A->sell_vals32.alloc(A->sell_nnz));
+  k_to_f32<<<grid_for(ctx, A->sell_nnz), 256, 0, ctx->stream>>>(A->sell_vals.p, A->sell_vals32.p, A->sell_nnz);
+  ctx->launches += 3;
   if (with_ilu) {
     EGPU_CUDA_TRY(ctx, A->ilu32.alloc(A->nnz));
     k_to_f32<<<grid_for(ctx, A->nnz), 256, 0, ctx->stream>>>(A->ilu.p, A->ilu32.p, A->nnz);
@@ -723,9 +777,10 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
   rc = scale_matrix(A, sc);
   if (rc) return rc;
   double *W = A->work.p;
-  double *bs = W + (size_t)10 * n;
+  const long long ldw = A->ldw;
+  double *bs = W + (size_t)10 * ldw;
   double *rr = W;  // FP64 residual (work vector 0; the FP32 inner solver has its own)
-  double *xs = x_dev;
+  double *xs = W + (size_t)12 * ldw;
   unsigned int *flags = ctx->sync.p + 2;
   int nbp = std::min(grid_for(ctx, n), 1024);
   k_rhs_scale_a<<<nbp, 256, 0, ctx->stream>>>(n, b_dev, A->dscale.p, x_dev, bs, ctx->partials.p, flags);
@@ -746,7 +801,7 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
   EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   egpu_result r{};
   float *W32 = A->work32.p;
-  float *r32 = W32 + (size_t)10 * n, *d32 = W32 + (size_t)11 * n, *dv32 = W32 + (size_t)13 * n;
+  float *r32 = W32 + (size_t)10 * ldw, *d32 = W32 + (size_t)11 * ldw, *dv32 = W32 + (size_t)13 * ldw;
   double *norms = (double *)(ctx->sync.p + 32);
   const int lpr = pick_lpr(A);
   const int rgrid = std::min(1024, (int)std::min<long long>(((long long)n * lpr + EGPU_BLOCK - 1) / EGPU_BLOCK,
@@ -806,6 +861,7 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
       a.diag = A->diag.p;
       a.cols16 = A->cols16.p;
       a.vals = A->scaled32.p;
+      set_sell(a, A, A->sell_vals32.p, A->sell_c16.p != nullptr);
       a.ilu = A->ilu32.p;
       a.dvals = dv32;
       a.lower_order = A->tri.lower_order.p;
@@ -817,7 +873,7 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
       a.b = r32;
       a.x = d32;
       a.w = W32;
-      a.ldw = n;
+      a.ldw = ldw;
       a.bar = ctx->sync.p;
       a.err = (int *)(ctx->sync.p + 1);
       a.partials = ctx->partials.p;
@@ -825,7 +881,7 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
       a.out_d = (double *)(ctx->sync.p + 16);
       a.skip = nullptr;
       EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ek0, ctx->stream));
-      rc = run_krylov<float>(A, a, prm->method, A->cols16.p != nullptr);
+      rc = run_krylov<float>(A, a, prm->method, A->sell_c16.p != nullptr);
       if (rc) return rc;
       EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ek1, ctx->stream));
       k_refine_update<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, d32, norms, xs);
@@ -877,7 +933,7 @@ __global__ void k_fill_sentinel(double *p, long long n) {
 int lu_apply(egpu_mat *A, const double *v_dev, double *u_dev) {
   egpu_ctx *ctx = A->ctx;
   const int n = A->n;
-  EGPU_CUDA_TRY(ctx, A->work.alloc((size_t)12 * n + 64));
+  EGPU_CUDA_TRY(ctx, A->work.alloc((size_t)13 * A->ldw));
   k_fill_sentinel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(A->work.p, n);
   k_fill_sentinel<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(u_dev, n);
   ctx->launches += 2;
@@ -893,6 +949,7 @@ int lu_apply(egpu_mat *A, const double *v_dev, double *u_dev) {
   a.w = A->work.p;
   a.err = (int *)(ctx->sync.p + 1);
   const int lpr = pick_lpr(A);
+  a.tri_per_block = tri_per_block(A, lpr, ctx->num_sms * 2);
   int rc;
   switch (lpr) {
     case 4: { auto k = k_lu_apply<4>; int bps = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, EGPU_BLOCK, 0);
@@ -1046,6 +1103,48 @@ extern "C" int egpu_matrix_bind(egpu_ctx *ctx, int n, const int *rows, const int
     cudaMemsetAsync(A->values.p, 0, nnz * sizeof(double), ctx->stream);
   }
   cudaMemsetAsync(A->rhs.p, 0, n * sizeof(double), ctx->stream);
+  // SELL-32 copy of the pattern for the Krylov SpMV
+  {
+    const int ns = (n + 31) / 32;
+    std::vector<int> sp(ns), sw(ns);
+    long long total = 0;
+    for (int sl = 0; sl < ns; ++sl) {
+      int w = 0;
+      for (int r = sl * 32; r < std::min(n, sl * 32 + 32); ++r) w = std::max(w, rows[r + 1] - rows[r]);
+      sp[sl] = (int)total;
+      sw[sl] = w;
+      total += 32LL * w;
+    }
+    if (total >= (1LL << 31)) {
+      egpu_set_error(ctx, "matrix too large for 32-bit SELL offsets");
+      delete A;
+      return EGPU_ERR_ARG;
+    }
+    const bool c16 = maxbw < 32768;
+    std::vector<int> sc(total);
+    std::vector<int16_t> s16(c16 ? total : 0);
+    for (int sl = 0; sl < ns; ++sl)
+      for (int t = 0; t < 32; ++t) {
+        const int r = sl * 32 + t;
+        const int beg = r < n ? rows[r] - 1 : 0, len = r < n ? rows[r + 1] - rows[r] : 0;
+        for (int k = 0; k < sw[sl]; ++k) {
+          const long long e = sp[sl] + 32LL * k + t;
+          const int c = k < len ? cols[beg + k] - 1 : (r < n ? r : 0);
+          sc[e] = c;
+          if (c16) s16[e] = (int16_t)(k < len ? c - r : 0);
+        }
+      }
+    A->nslices = ns;
+    A->sell_nnz = total;
+    A->ldw = ((long long)n + 32 + 63) / 64 * 64;
+    if ((e = A->sell_ptr.alloc(ns)) || (e = A->sell_w.alloc(ns)) || (e = A->sell_cols.alloc(total)) ||
+        (c16 && (e = A->sell_c16.alloc(total))))
+      return fail(e);
+    cudaMemcpy(A->sell_ptr.p, sp.data(), ns * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(A->sell_w.p, sw.data(), ns * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(A->sell_cols.p, sc.data(), total * sizeof(int), cudaMemcpyHostToDevice);
+    if (c16) cudaMemcpy(A->sell_c16.p, s16.data(), total * sizeof(int16_t), cudaMemcpyHostToDevice);
+  }
   if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(e);
   *out = A;
   return EGPU_OK;

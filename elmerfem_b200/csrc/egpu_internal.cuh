@@ -93,6 +93,7 @@ struct TriSchedule {
   DevBuf<int> lower_order, upper_order;
   int lower_levels = 0, upper_levels = 0;
   int max_lower = 0, max_upper = 0;  // longest strictly-lower / strictly-upper row part
+  int max_width = 0;                 // most rows in one level (lower or upper)
 };
 
 struct AssemblyData {
@@ -123,6 +124,15 @@ struct egpu_mat {
   DevBuf<float> scaled32, ilu32; // FP32 copies for the mixed-precision inner solver
   DevBuf<int16_t> cols16;        // column offsets (col - row) when |col-row| < 32768
   DevBuf<int> ilu_done;          // factorisation completion flags
+  // SELL-32 copy of the pattern (slice s = rows 32s..32s+31, entry (k, lane) at
+  // sell_ptr[s] + 32k + lane; rows padded to the slice width with zero values)
+  int nslices = 0;
+  long long sell_nnz = 0;
+  long long ldw = 0;             // stride of the work vectors (>= n + 32, multiple of 64)
+  DevBuf<int> sell_ptr, sell_w, sell_cols;
+  DevBuf<int16_t> sell_c16;      // col - row, when every |col - row| < 32768
+  DevBuf<double> sell_vals;      // scaled values (FP64)
+  DevBuf<float> sell_vals32;     // scaled values (FP32)
   TriSchedule tri;
   bool tri_built = false;
   int solve_count = 0;
@@ -193,14 +203,16 @@ struct Sentinel<double> {
     unsigned long long v = ld_relaxed_u64(p);
     if (v != EGPU_SENTINEL64) return __longlong_as_double((long long)v);
     unsigned long long t0 = egpu_globaltimer();
-    while (true) {
+    for (unsigned int spin = 1;; ++spin) {
       v = ld_relaxed_u64(p);
       if (v != EGPU_SENTINEL64) break;
-      if (egpu_globaltimer() - t0 > EGPU_WAIT_NS) {
-        atomicExch(err, (int)EGPU_ERR_TIMEOUT);
-        break;
+      if ((spin & 31u) == 0) {
+        if (egpu_globaltimer() - t0 > EGPU_WAIT_NS) {
+          atomicExch(err, (int)EGPU_ERR_TIMEOUT);
+          break;
+        }
+        if (*(volatile int *)err) break;
       }
-      if (*(volatile int *)err) break;
     }
     return __longlong_as_double((long long)v);
   }
@@ -216,14 +228,16 @@ struct Sentinel<float> {
     unsigned int v = ld_relaxed_u32(p);
     if (v != EGPU_SENTINEL32) return __uint_as_float(v);
     unsigned long long t0 = egpu_globaltimer();
-    while (true) {
+    for (unsigned int spin = 1;; ++spin) {
       v = ld_relaxed_u32(p);
       if (v != EGPU_SENTINEL32) break;
-      if (egpu_globaltimer() - t0 > EGPU_WAIT_NS) {
-        atomicExch(err, (int)EGPU_ERR_TIMEOUT);
-        break;
+      if ((spin & 31u) == 0) {
+        if (egpu_globaltimer() - t0 > EGPU_WAIT_NS) {
+          atomicExch(err, (int)EGPU_ERR_TIMEOUT);
+          break;
+        }
+        if (*(volatile int *)err) break;
       }
-      if (*(volatile int *)err) break;
     }
     return __uint_as_float(v);
   }

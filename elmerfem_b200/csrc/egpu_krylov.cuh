@@ -41,42 +41,65 @@ struct KArgs {
   int *out_i;                     // [0] info [1] iters
   double *out_d;                  // [0] residual [1] rhsnorm
   const unsigned int *skip;       // bit 1 set: zero right-hand side, return at once
+  int tri_per_block;              // sub-warps per block taking part in the triangular solves
+  // SELL-32 copy of the scaled matrix used by every SpMV of the Krylov loop
+  int nslices;
+  const int *sell_ptr, *sell_w, *scols;
+  const int16_t *scols16;
+  const VT *svals;
 };
+
+// row sum step: FP64 keeps CRS_MatrixVectorProd's rounding (s = s + a*x, two roundings, row
+// order); FP32 uses a fused multiply-add
+__device__ __forceinline__ double row_madd(double s, double a, double x) { return __dadd_rn(s, __dmul_rn(a, x)); }
+__device__ __forceinline__ float row_madd(float s, float a, float x) { return fmaf(a, x, s); }
+
+// Participants of the sync-free solves: the first tri_per_block sub-warps of every block,
+// numbered block-fastest so consecutive slots land on different SMs.
+template <int TS>
+__device__ __forceinline__ bool tri_participant(int per_block, int &id, int &count) {
+  const int local = threadIdx.x / TS;
+  count = per_block * gridDim.x;
+  id = local * gridDim.x + blockIdx.x;
+  return local < per_block;
+}
 
 template <typename VT>
 __device__ __forceinline__ VT ld_stream(const VT *p) {
   return __ldcs(p);
 }
+// Gathers of vectors written earlier in the same launch use plain cache-all loads: every
+// phase starts after grid_barrier, whose acquire fence discards stale L1 lines, and the
+// stencil's reuse of x across neighbouring rows is then served from L1.
 template <typename VT>
 __device__ __forceinline__ VT ld_l2(const VT *p) {
-  return __ldcg(p);
+  return __ldca(p);
 }
 
 // -------------------------------------------------------------------------------------
-// SpMV over all rows, LPR lanes per row.  epi(row, s0, s1) runs on the row's lane 0.
+// SpMV over all rows on the SELL-32 copy: one warp per slice of 32 rows, lane = row, the
+// slice's entries column-major so each step of k is one coalesced 128-byte (FP32) or
+// 256-byte (FP64) warp load; each row sums in entry order.  Padding entries carry value 0
+// and a valid column.  epi(row, s0, s1) runs once per row on its own lane.
 template <typename VT, int LPR, bool OFFS, bool TWO, typename F>
 __device__ __forceinline__ void spmv_phase(const KArgs<VT> &a, const VT *x0, const VT *x1, F &&epi) {
   const int lane = threadIdx.x & 31;
-  const int sl = lane & (LPR - 1);
-  const unsigned submask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << (lane & ~(LPR - 1)));
-  const int gsub = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) / LPR);
-  const int nsub = (int)((long long)gridDim.x * blockDim.x / LPR);
-  for (int row = gsub; row < a.n; row += nsub) {
-    const int beg = __ldg(a.rows + row), end = __ldg(a.rows + row + 1);
+  const int gw = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nw = (int)(((long long)gridDim.x * blockDim.x) >> 5);
+  for (int s = gw; s < a.nslices; s += nw) {
+    const int r = (s << 5) + lane;
+    const int w = __ldg(a.sell_w + s);
+    const int base = __ldg(a.sell_ptr + s) + lane;
     VT s0 = 0, s1 = 0;
-#pragma unroll 4
-    for (int j = beg + sl; j < end; j += LPR) {
-      const VT v = ld_stream(a.vals + j);
-      const int c = OFFS ? row + (int)ld_stream(a.cols16 + j) : ld_stream(a.cols + j);
-      s0 += v * ld_l2(x0 + c);
-      if (TWO) s1 += v * ld_l2(x1 + c);
+#pragma unroll 8
+    for (int k = 0; k < w; ++k) {
+      const int e = base + (k << 5);
+      const VT v = ld_stream(a.svals + e);
+      const int c = OFFS ? r + (int)ld_stream(a.scols16 + e) : ld_stream(a.scols + e);
+      s0 = row_madd(s0, v, ld_l2(x0 + c));
+      if (TWO) s1 = row_madd(s1, v, ld_l2(x1 + c));
     }
-#pragma unroll
-    for (int off = LPR / 2; off > 0; off >>= 1) {
-      s0 += __shfl_xor_sync(submask, s0, off, LPR);
-      if (TWO) s1 += __shfl_xor_sync(submask, s1, off, LPR);
-    }
-    if (sl == 0) epi(row, s0, s1);
+    if (r < a.n) epi(r, s0, s1);
   }
 }
 
@@ -94,11 +117,14 @@ __device__ __forceinline__ void lower_solve(const KArgs<VT> &a, VT *y, RHS &&rhs
   const int lane = threadIdx.x & 31;
   const int sl = lane & (TS - 1);
   const unsigned submask = (TS == 32) ? 0xffffffffu : (((1u << TS) - 1u) << (lane & ~(TS - 1)));
-  const int gsub = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) / TS);
-  const int nsub = (int)((long long)gridDim.x * blockDim.x / TS);
+  int gsub, nsub;
+  if (!tri_participant<TS>(a.tri_per_block, gsub, nsub)) return;
   for (int s = gsub; s < a.n; s += nsub) {
     const int i = __ldg(a.lower_order + s);
     const int beg = __ldg(a.rows + i), end = __ldg(a.diag + i);
+    // the right-hand side does not depend on the solve: form it before waiting
+    VT r = 0;
+    if (sl == 0) r = rhs(i);
     VT acc = 0;
     for (int j = beg + sl; j < end; j += TS) {
       const VT l = __ldg(a.ilu + j);
@@ -107,7 +133,7 @@ __device__ __forceinline__ void lower_solve(const KArgs<VT> &a, VT *y, RHS &&rhs
     }
 #pragma unroll
     for (int off = TS / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(submask, acc, off, TS);
-    if (sl == 0) Sentinel<VT>::publish(y + i, rhs(i) - acc);
+    if (sl == 0) Sentinel<VT>::publish(y + i, r - acc);
   }
 }
 
@@ -116,11 +142,12 @@ __device__ __forceinline__ void upper_solve(const KArgs<VT> &a, const VT *y, VT 
   const int lane = threadIdx.x & 31;
   const int sl = lane & (TS - 1);
   const unsigned submask = (TS == 32) ? 0xffffffffu : (((1u << TS) - 1u) << (lane & ~(TS - 1)));
-  const int gsub = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) / TS);
-  const int nsub = (int)((long long)gridDim.x * blockDim.x / TS);
+  int gsub, nsub;
+  if (!tri_participant<TS>(a.tri_per_block, gsub, nsub)) return;
   for (int s = gsub; s < a.n; s += nsub) {
     const int i = __ldg(a.upper_order + s);
     const int dg = __ldg(a.diag + i), end = __ldg(a.rows + i + 1);
+    const VT dinv = __ldg(a.ilu + dg);
     VT acc = 0;
     for (int j = dg + 1 + sl; j < end; j += TS) {
       const VT u = __ldg(a.ilu + j);
@@ -131,7 +158,7 @@ __device__ __forceinline__ void upper_solve(const KArgs<VT> &a, const VT *y, VT 
     for (int off = TS / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(submask, acc, off, TS);
     if (sl == 0) {
       const VT yi = Sentinel<VT>::wait(y + i, a.err);
-      const VT zi = __ldg(a.ilu + dg) * (yi - acc);
+      const VT zi = dinv * (yi - acc);
       Sentinel<VT>::publish(z + i, zi);
       out(i, zi);
     }

@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import ctypes as C
 import re
+import weakref
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -29,6 +30,7 @@ class Context:
         self._h = C.c_void_p()
         check(lib().egpu_create(device, C.byref(self._h)), None, "egpu_create")
         self.device = device
+        self._children = weakref.WeakSet()  # matrices bound to this context, freed before it
 
     @property
     def handle(self):
@@ -45,6 +47,8 @@ class Context:
 
     def close(self):
         if self._h:
+            for child in list(self._children):
+                child.free()
             lib().egpu_destroy(self._h)
             self._h = C.c_void_p()
 
@@ -182,15 +186,17 @@ class Matrix:
         check(lib().egpu_matrix_bind(ctx.handle, pattern.n, pattern.rows, pattern.cols, pattern.diag,
                                      None if vals is None else vals.ctypes.data, C.byref(self._h)),
               ctx.handle, "egpu_matrix_bind")
+        ctx._children.add(self)
 
     @property
     def handle(self):
         return self._h
 
     def free(self):
-        if self._h:
+        # a matrix must not outlive its context: Context.close() frees its matrices first
+        if self._h and self.ctx._h:
             lib().egpu_matrix_free(self._h)
-            self._h = C.c_void_p()
+        self._h = C.c_void_p()
 
     def __del__(self):
         try:
