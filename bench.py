@@ -399,7 +399,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="poisson128_cg_jacobi")
     ap.add_argument("--fp64-steps", type=int, default=2)
-    ap.add_argument("--inner-tol", type=float, default=1e-4)
+    ap.add_argument("--inner-tol", type=float, default=3e-4)
     ap.add_argument("--ref-iters", type=int, default=0, help="FP64 iteration count for the reference arm")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()

@@ -339,6 +339,7 @@ static int launch_coop(egpu_ctx *ctx, K kernel, Args &args, int *grid_out = null
   return EGPU_OK;
 }
 
+// lanes per row of the standalone CRS SpMV (egpu_mv)
 static int pick_lpr(const egpu_mat *A) {
   double mean = A->n ? (double)A->nnz / A->n : 1.0;
   if (mean <= 12) return 4;
@@ -346,6 +347,7 @@ static int pick_lpr(const egpu_mat *A) {
   if (mean <= 96) return 16;
   return 32;
 }
+
 
 }  // namespace egpu
 
@@ -478,34 +480,22 @@ static int tri_per_block(const egpu_mat *A, int lpr, int grid) {
   return std::max(1, std::min(per_block_max, (want + grid - 1) / grid));
 }
 
+// One warp per row in the sync-free triangular solves: rows that depend on each other
+// never share a warp, so no lane spins while a diverged lane of its own warp has to
+// produce the value it waits for.
+constexpr int TRI_TS = 32;
+
 template <typename VT>
 static int run_krylov(egpu_mat *A, const KArgs<VT> &a0, int method, bool offs) {
   egpu_ctx *ctx = A->ctx;
   KArgs<VT> a = a0;
-  const int lpr = pick_lpr(A);
-  a.tri_per_block = tri_per_block(A, lpr, ctx->num_sms * 2);
-#define EGPU_LAUNCH_K(KERN, L)                                                 \
-  do {                                                                         \
-    if (offs)                                                                  \
-      return launch_coop(ctx, KERN<VT, L, true>, a);                           \
-    else                                                                       \
-      return launch_coop(ctx, KERN<VT, L, false>, a);                          \
-  } while (0)
-#define EGPU_LAUNCH_M(L)                                                       \
-  do {                                                                         \
-    if (method == EGPU_CG)                                                     \
-      EGPU_LAUNCH_K(cg_kernel, L);                                             \
-    else                                                                       \
-      EGPU_LAUNCH_K(bicgstab_kernel, L);                                       \
-  } while (0)
-  switch (lpr) {
-    case 4: EGPU_LAUNCH_M(4);
-    case 8: EGPU_LAUNCH_M(8);
-    case 16: EGPU_LAUNCH_M(16);
-    default: EGPU_LAUNCH_M(32);
+  a.tri_per_block = tri_per_block(A, TRI_TS, ctx->num_sms * 2);
+  if (method == EGPU_CG) {
+    if (offs) return launch_coop(ctx, cg_kernel<VT, TRI_TS, true>, a);
+    return launch_coop(ctx, cg_kernel<VT, TRI_TS, false>, a);
   }
-#undef EGPU_LAUNCH_M
-#undef EGPU_LAUNCH_K
+  if (offs) return launch_coop(ctx, bicgstab_kernel<VT, TRI_TS, true>, a);
+  return launch_coop(ctx, bicgstab_kernel<VT, TRI_TS, false>, a);
 }
 
 // FP64 drop-in solve on device buffers.  x_dev: in = initial guess, out = solution.
@@ -948,18 +938,15 @@ int lu_apply(egpu_mat *A, const double *v_dev, double *u_dev) {
   a.upper_order = A->tri.upper_order.p;
   a.w = A->work.p;
   a.err = (int *)(ctx->sync.p + 1);
-  const int lpr = pick_lpr(A);
-  a.tri_per_block = tri_per_block(A, lpr, ctx->num_sms * 2);
+  a.tri_per_block = tri_per_block(A, TRI_TS, ctx->num_sms * 2);
   int rc;
-  switch (lpr) {
-    case 4: { auto k = k_lu_apply<4>; int bps = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, EGPU_BLOCK, 0);
-      void *args[] = {&a, &v_dev, &u_dev}; rc = cudaLaunchCooperativeKernel((const void *)k, dim3(ctx->num_sms * std::min(bps, 2)), dim3(EGPU_BLOCK), args, 0, ctx->stream); break; }
-    case 8: { auto k = k_lu_apply<8>; int bps = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, EGPU_BLOCK, 0);
-      void *args[] = {&a, &v_dev, &u_dev}; rc = cudaLaunchCooperativeKernel((const void *)k, dim3(ctx->num_sms * std::min(bps, 2)), dim3(EGPU_BLOCK), args, 0, ctx->stream); break; }
-    case 16: { auto k = k_lu_apply<16>; int bps = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, EGPU_BLOCK, 0);
-      void *args[] = {&a, &v_dev, &u_dev}; rc = cudaLaunchCooperativeKernel((const void *)k, dim3(ctx->num_sms * std::min(bps, 2)), dim3(EGPU_BLOCK), args, 0, ctx->stream); break; }
-    default: { auto k = k_lu_apply<32>; int bps = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, EGPU_BLOCK, 0);
-      void *args[] = {&a, &v_dev, &u_dev}; rc = cudaLaunchCooperativeKernel((const void *)k, dim3(ctx->num_sms * std::min(bps, 2)), dim3(EGPU_BLOCK), args, 0, ctx->stream); break; }
+  {
+    auto k = k_lu_apply<TRI_TS>;
+    int bps = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, EGPU_BLOCK, 0);
+    void *args[] = {&a, &v_dev, &u_dev};
+    rc = cudaLaunchCooperativeKernel((const void *)k, dim3(ctx->num_sms * std::max(1, std::min(bps, 2))),
+                                     dim3(EGPU_BLOCK), args, 0, ctx->stream);
   }
   EGPU_CUDA_TRY(ctx, (cudaError_t)rc);
   ctx->launches++;

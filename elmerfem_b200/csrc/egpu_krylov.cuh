@@ -54,6 +54,57 @@ struct KArgs {
 __device__ __forceinline__ double row_madd(double s, double a, double x) { return __dadd_rn(s, __dmul_rn(a, x)); }
 __device__ __forceinline__ float row_madd(float s, float a, float x) { return fmaf(a, x, s); }
 
+// ---- 16-byte vector access for the element-wise phases (all work vectors are 256-byte
+// aligned with a stride that is a multiple of 64 elements)
+template <int W, typename VT>
+__device__ __forceinline__ void vld(const VT *p, int i, VT (&v)[W]) {
+  if constexpr (W == 1) {
+    v[0] = p[i];
+  } else if constexpr (sizeof(VT) == 8) {
+    const double2 t = *reinterpret_cast<const double2 *>(p + i);
+    v[0] = t.x;
+    v[1] = t.y;
+  } else {
+    const float4 t = *reinterpret_cast<const float4 *>(p + i);
+    v[0] = t.x;
+    v[1] = t.y;
+    v[2] = t.z;
+    v[3] = t.w;
+  }
+}
+template <int W, typename VT>
+__device__ __forceinline__ void vst(VT *p, int i, const VT (&v)[W]) {
+  if constexpr (W == 1) {
+    p[i] = v[0];
+  } else if constexpr (sizeof(VT) == 8) {
+    *reinterpret_cast<double2 *>(p + i) = make_double2(v[0], v[1]);
+  } else {
+    *reinterpret_cast<float4 *>(p + i) = make_float4(v[0], v[1], v[2], v[3]);
+  }
+}
+template <int W, typename VT>
+__device__ __forceinline__ void vfill(VT *p, int i, VT x) {
+  VT v[W];
+#pragma unroll
+  for (int k = 0; k < W; ++k) v[k] = x;
+  vst<W>(p, i, v);
+}
+
+template <int W>
+struct VW {
+  static constexpr int value = W;
+};
+
+// f(i, VW<W>) over [0, n): 16-byte chunks, then a scalar tail
+template <typename VT, typename F>
+__device__ __forceinline__ void vec_loop(int n, F &&f) {
+  constexpr int W = 16 / sizeof(VT);
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  const int nv = n / W;
+  for (int q = tid; q < nv; q += nth) f(q * W, VW<W>{});
+  for (int i = nv * W + tid; i < n; i += nth) f(i, VW<1>{});
+}
+
 // Participants of the sync-free solves: the first tri_per_block sub-warps of every block,
 // numbered block-fastest so consecutive slots land on different SMs.
 template <int TS>
@@ -193,7 +244,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) cg_kernel(KArgs<VT> a) {
   __shared__ double sm[32 * 4];
   unsigned int epoch = 0;
   const int n = a.n;
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+
   const int nb = gridDim.x;
   VT *X = a.x, *R = a.w, *Z = a.w + a.ldw, *P = a.w + 2 * a.ldw, *Q = a.w + 3 * a.ldw,
      *Y = a.w + 4 * a.ldw;
@@ -207,19 +258,25 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) cg_kernel(KArgs<VT> a) {
     if (a.true_residual) {
       spmv_phase<VT, LPR, OFFS, false>(a, X, X, [&](int i, VT s, VT) { R[i] = B[i] - s; });
     } else {
-      for (int i = tid; i < n; i += nth) {
-        R[i] = B[i];
-        X[i] = 0;
-      }
+      vec_loop<VT>(n, [&](int i, auto w) {
+        constexpr int W = decltype(w)::value;
+        VT b[W];
+        vld<W>(B, i, b);
+        vst<W>(R, i, b);
+        vfill<W>(X, i, VT(0));
+      });
     }
-    for (int i = tid; i < n; i += nth) {
-      const double bi = (double)B[i];
-      acc[0] += bi * bi;
+    vec_loop<VT>(n, [&](int i, auto w) {
+      constexpr int W = decltype(w)::value;
+      VT b[W];
+      vld<W>(B, i, b);
+#pragma unroll
+      for (int k = 0; k < W; ++k) acc[0] += (double)b[k] * (double)b[k];
       if (ilu) {
-        Y[i] = SENT;
-        Z[i] = SENT;
+        vfill<W>(Y, i, SENT);
+        vfill<W>(Z, i, SENT);
       }
-    }
+    });
     block_sum<1>(acc, sm);
     store_partials(a, SLOT_BB, acc[0]);
   }
@@ -233,11 +290,19 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) cg_kernel(KArgs<VT> a) {
       lower_solve<VT, LPR>(a, Y, [&](int i) { return R[i]; });
       upper_solve<VT, LPR>(a, Y, Z, [&](int i, VT zi) { acc[0] += (double)R[i] * (double)zi; });
     } else {
-      for (int i = tid; i < n; i += nth) {
-        const VT z = a.precond == EGPU_PREC_DIAGONAL ? diag_prec(R[i], a.dvals[i]) : R[i];
-        Z[i] = z;
-        acc[0] += (double)R[i] * (double)z;
-      }
+      const bool jac = a.precond == EGPU_PREC_DIAGONAL;
+      vec_loop<VT>(n, [&](int i, auto w) {
+        constexpr int W = decltype(w)::value;
+        VT r[W], d[W], z[W];
+        vld<W>(R, i, r);
+        if (jac) vld<W>(a.dvals, i, d);
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+          z[k] = jac ? diag_prec(r[k], d[k]) : r[k];
+          acc[0] += (double)r[k] * (double)z[k];
+        }
+        vst<W>(Z, i, z);
+      });
     }
     block_sum<1>(acc, sm);
     store_partials(a, SLOT_RHO, acc[0]);
@@ -257,14 +322,20 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) cg_kernel(KArgs<VT> a) {
     // ---- P = Z (first iteration) or Z + beta P
     {
       const VT beta = (VT)(rho / oldrho);
-      for (int i = tid; i < n; i += nth) {
-        const VT z = Z[i];
-        P[i] = (k == 1) ? z : z + beta * P[i];
+      const bool first = k == 1;
+      vec_loop<VT>(n, [&](int i, auto w) {
+        constexpr int W = decltype(w)::value;
+        VT z[W], p[W];
+        vld<W>(Z, i, z);
+        if (!first) vld<W>(P, i, p);
+#pragma unroll
+        for (int q = 0; q < W; ++q) p[q] = first ? z[q] : z[q] + beta * p[q];
+        vst<W>(P, i, p);
         if (ilu) {
-          Z[i] = SENT;
-          Y[i] = SENT;
+          vfill<W>(Z, i, SENT);
+          vfill<W>(Y, i, SENT);
         }
-      }
+      });
     }
     if (!grid_barrier(a.bar, a.err, epoch)) return;
     // ---- Q = A P  (+ A x_{k-1} for the stopping test of iterate k-1)
@@ -311,15 +382,27 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) cg_kernel(KArgs<VT> a) {
           acc[1] += (double)r * (double)r;
         });
       } else {
-        for (int i = tid; i < n; i += nth) {
-          X[i] = X[i] + alpha * P[i];
-          const VT r = R[i] - alpha * Q[i];
-          R[i] = r;
-          const VT z = a.precond == EGPU_PREC_DIAGONAL ? diag_prec(r, a.dvals[i]) : r;
-          Z[i] = z;
-          acc[0] += (double)r * (double)z;
-          acc[1] += (double)r * (double)r;
-        }
+        const bool jac = a.precond == EGPU_PREC_DIAGONAL;
+        vec_loop<VT>(n, [&](int i, auto w) {
+          constexpr int W = decltype(w)::value;
+          VT x[W], p[W], r[W], q[W], d[W], z[W];
+          vld<W>(X, i, x);
+          vld<W>(P, i, p);
+          vld<W>(R, i, r);
+          vld<W>(Q, i, q);
+          if (jac) vld<W>(a.dvals, i, d);
+#pragma unroll
+          for (int t = 0; t < W; ++t) {
+            x[t] = x[t] + alpha * p[t];
+            r[t] = r[t] - alpha * q[t];
+            z[t] = jac ? diag_prec(r[t], d[t]) : r[t];
+            acc[0] += (double)r[t] * (double)z[t];
+            acc[1] += (double)r[t] * (double)r[t];
+          }
+          vst<W>(X, i, x);
+          vst<W>(R, i, r);
+          vst<W>(Z, i, z);
+        });
       }
       block_sum<2>(acc, sm);
       store_partials(a, SLOT_RHO, acc[0]);
@@ -355,7 +438,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) bicgstab_kernel(KArgs<VT> a) {
   __shared__ double sm[32 * 4];
   unsigned int epoch = 0;
   const int n = a.n;
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+
   const int nb = gridDim.x;
   VT *X = a.x;
   VT *R = a.w, *RT = a.w + a.ldw, *P = a.w + 2 * a.ldw, *V = a.w + 3 * a.ldw,
@@ -377,26 +460,32 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) bicgstab_kernel(KArgs<VT> a) {
         acc[1] += (double)r * (double)r;
       });
     } else {
-      for (int i = tid; i < n; i += nth) {
-        const VT r = B[i];
-        X[i] = 0;
-        R[i] = r;
-        RT[i] = r;
-        acc[1] += (double)r * (double)r;
-      }
+      vec_loop<VT>(n, [&](int i, auto w) {
+        constexpr int W = decltype(w)::value;
+        VT b[W];
+        vld<W>(B, i, b);
+        vfill<W>(X, i, VT(0));
+        vst<W>(R, i, b);
+        vst<W>(RT, i, b);
+#pragma unroll
+        for (int k = 0; k < W; ++k) acc[1] += (double)b[k] * (double)b[k];
+      });
     }
-    for (int i = tid; i < n; i += nth) {
-      const double bi = (double)B[i];
-      acc[0] += bi * bi;
-      P[i] = 0;
-      V[i] = 0;
+    vec_loop<VT>(n, [&](int i, auto w) {
+      constexpr int W = decltype(w)::value;
+      VT b[W];
+      vld<W>(B, i, b);
+#pragma unroll
+      for (int k = 0; k < W; ++k) acc[0] += (double)b[k] * (double)b[k];
+      vfill<W>(P, i, VT(0));
+      vfill<W>(V, i, VT(0));
       if (ilu) {
-        Y1[i] = SENT;
-        Y2[i] = SENT;
-        T1[i] = SENT;
-        T2[i] = SENT;
+        vfill<W>(Y1, i, SENT);
+        vfill<W>(Y2, i, SENT);
+        vfill<W>(T1, i, SENT);
+        vfill<W>(T2, i, SENT);
       }
-    }
+    });
     block_sum<2>(acc, sm);
     store_partials(a, SLOT_BB, acc[0]);
     store_partials(a, SLOT_RHO, acc[1]);
@@ -429,11 +518,21 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) bicgstab_kernel(KArgs<VT> a) {
         });
         upper_solve<VT, LPR>(a, Y1, T1, [&](int, VT) {});
       } else {
-        for (int i = tid; i < n; i += nth) {
-          const VT p = R[i] + beta * (P[i] - om * V[i]);
-          P[i] = p;
-          T1[i] = jac ? diag_prec(p, a.dvals[i]) : p;
-        }
+        vec_loop<VT>(n, [&](int i, auto w) {
+          constexpr int W = decltype(w)::value;
+          VT r[W], p[W], v[W], d[W], t[W];
+          vld<W>(R, i, r);
+          vld<W>(P, i, p);
+          vld<W>(V, i, v);
+          if (jac) vld<W>(a.dvals, i, d);
+#pragma unroll
+          for (int q = 0; q < W; ++q) {
+            p[q] = r[q] + beta * (p[q] - om * v[q]);
+            t[q] = jac ? diag_prec(p[q], d[q]) : p[q];
+          }
+          vst<W>(P, i, p);
+          vst<W>(T1, i, t);
+        });
       }
     }
     if (!grid_barrier(a.bar, a.err, epoch)) return;
@@ -481,12 +580,21 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) bicgstab_kernel(KArgs<VT> a) {
         });
         upper_solve<VT, LPR>(a, Y2, T2, [&](int, VT) {});
       } else {
-        for (int i = tid; i < n; i += nth) {
-          const VT s = R[i] - al * V[i];
-          S[i] = s;
-          acc[0] += (double)s * (double)s;
-          T2[i] = jac ? diag_prec(s, a.dvals[i]) : s;
-        }
+        vec_loop<VT>(n, [&](int i, auto w) {
+          constexpr int W = decltype(w)::value;
+          VT r[W], v[W], d[W], sv[W], t[W];
+          vld<W>(R, i, r);
+          vld<W>(V, i, v);
+          if (jac) vld<W>(a.dvals, i, d);
+#pragma unroll
+          for (int q = 0; q < W; ++q) {
+            sv[q] = r[q] - al * v[q];
+            acc[0] += (double)sv[q] * (double)sv[q];
+            t[q] = jac ? diag_prec(sv[q], d[q]) : sv[q];
+          }
+          vst<W>(S, i, sv);
+          vst<W>(T2, i, t);
+        });
       }
       block_sum<1>(acc, sm);
       store_partials(a, SLOT_SS, acc[0]);
@@ -510,7 +618,15 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) bicgstab_kernel(KArgs<VT> a) {
     const double tt = reduce_partials(a.partials + SLOT_TT * nb, nb, sm);
     if (sqrt(ss) < EGPU_HUTI_EPSILON) {
       const VT al = (VT)alpha;
-      for (int i = tid; i < n; i += nth) X[i] = X[i] + al * T1[i];
+      vec_loop<VT>(n, [&](int i, auto w) {
+        constexpr int W = decltype(w)::value;
+        VT x[W], t[W];
+        vld<W>(X, i, x);
+        vld<W>(T1, i, t);
+#pragma unroll
+        for (int q = 0; q < W; ++q) x[q] = x[q] + al * t[q];
+        vst<W>(X, i, x);
+      });
       residual = sqrt(ss);
       info = EGPU_HUTI_BICGSTAB_SNORM;
       iters = k;
@@ -521,19 +637,31 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) bicgstab_kernel(KArgs<VT> a) {
     {
       const VT al = (VT)alpha, om = (VT)omega;
       double acc[2] = {0.0, 0.0};
-      for (int i = tid; i < n; i += nth) {
-        X[i] = X[i] + al * T1[i] + om * T2[i];
-        const VT r = S[i] - om * T[i];
-        R[i] = r;
-        acc[0] += (double)RT[i] * (double)r;
-        acc[1] += (double)r * (double)r;
-        if (ilu) {
-          T1[i] = SENT;
-          T2[i] = SENT;
-          Y1[i] = SENT;
-          Y2[i] = SENT;
+      vec_loop<VT>(n, [&](int i, auto w) {
+        constexpr int W = decltype(w)::value;
+        VT x[W], t1[W], t2[W], sv[W], t[W], rt[W], r[W];
+        vld<W>(X, i, x);
+        vld<W>(T1, i, t1);
+        vld<W>(T2, i, t2);
+        vld<W>(S, i, sv);
+        vld<W>(T, i, t);
+        vld<W>(RT, i, rt);
+#pragma unroll
+        for (int q = 0; q < W; ++q) {
+          x[q] = x[q] + al * t1[q] + om * t2[q];
+          r[q] = sv[q] - om * t[q];
+          acc[0] += (double)rt[q] * (double)r[q];
+          acc[1] += (double)r[q] * (double)r[q];
         }
-      }
+        vst<W>(X, i, x);
+        vst<W>(R, i, r);
+        if (ilu) {
+          vfill<W>(T1, i, SENT);
+          vfill<W>(T2, i, SENT);
+          vfill<W>(Y1, i, SENT);
+          vfill<W>(Y2, i, SENT);
+        }
+      });
       block_sum<2>(acc, sm);
       store_partials(a, SLOT_RHO, acc[0]);
       store_partials(a, SLOT_RR2, acc[1]);
