@@ -81,6 +81,8 @@ PROTOTYPES = {
     "egpu_ilu0_build": (C.c_int, [_vp, C.c_int]),
     "egpu_ilu0_download": (C.c_int, [_vp, _vp, _vp]),
     "egpu_lu_precondition": (C.c_int, [_vp, _f64p, _f64p]),
+    "egpu_cg_noalloc": (C.c_int, [C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, C.POINTER(Params),
+                                  C.POINTER(Result)]),
     "egpu_batch_create": (C.c_int, [_vp, C.POINTER(_vp)]),
     "egpu_batch_add": (C.c_int, [_vp, C.c_int, _i32p, _i32p, _i32p, _f64p, _f64p]),
     "egpu_batch_solve": (C.c_int, [_vp, C.POINTER(Params), _vp]),

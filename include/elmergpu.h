@@ -150,6 +150,24 @@ int egpu_assemble_elastic(egpu_mat *A, double young, double poisson, const doubl
 int egpu_dirichlet(egpu_mat *A, int ncon, const int *con_rows, const double *con_vals,
                    int symmetric);
 
+/* ---- allocation-free CG ------------------------------------------------------------
+ * No counterpart in the reference.  For callers that cannot let the library allocate
+ * device memory: code whose device memory belongs to another runtime (CUDA Fortran or
+ * OpenACC data regions around Elmer's arrays) and code that cannot afford the implicit
+ * synchronisation of cudaMalloc inside its loop.  Solves like egpu_iter_solve_dev with
+ * method CG, preconditioner Diagonal or None and system scaling on, taking the caller's
+ * Matrix_t arrays (1-based Rows/Cols/Diag, Values) and b, x in device memory; x is the
+ * initial guess on entry.  All scratch is one fixed device array inside the library
+ * (about 2.4 MB, held by every GPU that loads the library until the process exits), so:
+ * n is limited to EGPU_NOALLOC_MAX_ROWS (larger n returns EGPU_ERR_ARG); calls that
+ * overlap on the GPU race on that array; the first call on a device looks up the array's
+ * device address and should come before any stream capture.  Runs on the legacy default
+ * stream and returns when the solve has finished. */
+#define EGPU_NOALLOC_MAX_ROWS 32768
+int egpu_cg_noalloc(int device, int n, const int *rows_dev, const int *cols_dev, const int *diag_dev,
+                    const double *values_dev, const double *b_dev, double *x_dev, const egpu_params *prm,
+                    egpu_result *res);
+
 /* ---- batched solve: many independent systems in one persistent launch ------------
  * Systems are appended with their own CRS/RHS; egpu_batch_solve runs them all with
  * one cooperative kernel and per-system convergence masks. */
