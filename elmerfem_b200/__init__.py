@@ -5,9 +5,9 @@ The compute lives in ``libelmergpu.so`` (CUDA, sm_100a) behind the C ABI declare
 """
 from . import meshgen
 from ._lib import BICGSTAB, CG, FP64, MIXED, PREC_DIAGONAL, PREC_ILU0, PREC_NONE, LibError, build, lib
-from .solver import (Context, CRSPattern, Matrix, NotConverged, SolverParams, compute_norm, create_matrix,
+from .solver import (Batch, Context, CRSPattern, Matrix, NotConverged, SolverParams, compute_norm, create_matrix,
                      iter_solver, parse_sif_section)
 
 __all__ = ["meshgen", "BICGSTAB", "CG", "FP64", "MIXED", "PREC_DIAGONAL", "PREC_ILU0", "PREC_NONE", "LibError",
-           "build", "lib", "Context", "CRSPattern", "Matrix", "NotConverged", "SolverParams", "compute_norm",
+           "build", "lib", "Batch", "Context", "CRSPattern", "Matrix", "NotConverged", "SolverParams", "compute_norm",
            "create_matrix", "iter_solver", "parse_sif_section"]

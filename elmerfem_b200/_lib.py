@@ -83,11 +83,17 @@ PROTOTYPES = {
     "egpu_lu_precondition": (C.c_int, [_vp, _f64p, _f64p]),
     "egpu_cg_noalloc": (C.c_int, [C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, C.POINTER(Params),
                                   C.POINTER(Result)]),
-    "egpu_batch_create": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "egpu_batch_create": (C.c_int, [_vp, C.POINTER(Params), C.POINTER(_vp)]),
     "egpu_batch_add": (C.c_int, [_vp, C.c_int, _i32p, _i32p, _i32p, _f64p, _f64p]),
-    "egpu_batch_solve": (C.c_int, [_vp, C.POINTER(Params), _vp]),
+    "egpu_batch_add_matrix": (C.c_int, [_vp, _vp, _vp]),
+    "egpu_batch_set_chunk": (C.c_int, [_vp, C.c_int]),
+    "egpu_batch_step": (C.c_int, [_vp, _vp, C.POINTER(C.c_int)]),
+    "egpu_batch_pending": (C.c_int, [_vp]),
+    "egpu_batch_solve": (C.c_int, [_vp, _vp]),
+    "egpu_batch_result": (C.c_int, [_vp, C.c_int, C.POINTER(Result)]),
     "egpu_batch_solution": (C.c_int, [_vp, C.c_int, _f64p]),
-    "egpu_batch_tune": (C.c_int, [_vp, C.POINTER(Params), C.POINTER(C.c_int)]),
+    "egpu_batch_remove": (C.c_int, [_vp, C.c_int]),
+    "egpu_batch_tune": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "egpu_batch_free": (None, [_vp]),
 }
 

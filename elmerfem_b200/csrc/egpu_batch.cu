@@ -1,20 +1,1059 @@
-// egpu_batch.cu -- batched persistent solver (entry points; implementation follows)
-#include "egpu_internal.cuh"
+// egpu_batch.cu -- batched mixed-precision solver: many independent systems, one
+// persistent launch per chunk of inner iterations, FP64 refinement between chunks.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
 
-struct egpu_batch {
-  egpu_ctx *ctx;
+#include "egpu_batch.cuh"
+#include "egpu_solve.h"
+
+namespace egpu {
+
+// ------------------------------------------------------------------------------------
+// device helpers
+
+__device__ __forceinline__ float bprec(float v, float d, int precond) {
+  return (precond == EGPU_PREC_DIAGONAL && fabsf(d) > (float)EGPU_AEPS) ? v / d : v;
+}
+
+// block-wide: compact systems whose status is in the mask, prefix their slice counts
+__device__ void batch_compact(const BatchArgs &a, BatchShared &sh, unsigned mask) {
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    int base = 0, tot = 0;
+    for (int c = 0; c < a.nsys; c += 32) {
+      const int s = c + lane;
+      const bool on = s < a.nsys && ((mask >> sh.status[s]) & 1u);
+      const int ns = on ? a.sys[s].nslices : 0;
+      const unsigned bal = __ballot_sync(0xffffffffu, on);
+      const int pos = base + __popc(bal & ((1u << lane) - 1u));
+      // inclusive scan of ns over the lanes that are on
+      int v = ns;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, v, off);
+        if (lane >= off) v += t;
+      }
+      if (on) {
+        sh.act[pos] = s;
+        sh.pre[pos] = tot + v - ns;
+      }
+      tot += __shfl_sync(0xffffffffu, v, 31);
+      base += __popc(bal);
+    }
+    if (lane == 0) {
+      sh.nact = base;
+      sh.pre[base] = tot;
+      sh.total = tot;
+    }
+  }
+  __syncthreads();
+}
+
+// iterate this block's share of the active slices: f(act_index, sys, slice)
+template <typename F>
+__device__ __forceinline__ void batch_slices(const BatchShared &sh, F &&f) {
+  const int total = sh.total, nb = gridDim.x;
+  const int lo = (int)((long long)total * blockIdx.x / nb), hi = (int)((long long)total * (blockIdx.x + 1) / nb);
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int a = 0;
+  for (int q = lo + warp; q < hi; q += nw) {
+    // act index containing slice rank q (pre is ascending; warps move forward)
+    int l = 0, r = sh.nact - 1;
+    while (l < r) {
+      const int m = (l + r + 1) >> 1;
+      if (sh.pre[m] <= q)
+        l = m;
+      else
+        r = m - 1;
+    }
+    a = l;
+    f(a, sh.act[a], q - sh.pre[a]);
+  }
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
+// flush this block's per-system partials (slots v0/v1 of red) to the global accumulators
+__device__ __forceinline__ void batch_flush(const BatchArgs &a, BatchShared &sh, int slot0, int slot1) {
+  __syncthreads();
+  for (int t = threadIdx.x; t < sh.nact; t += blockDim.x) {
+    const int s = sh.act[t];
+    const double v0 = sh.red[2 * t], v1 = sh.red[2 * t + 1];
+    if (v0 != 0.0 && slot0 >= 0) atomicAdd(&a.acc[slot0 * BATCH_MAX_SYS + s], v0);
+    if (v1 != 0.0 && slot1 >= 0) atomicAdd(&a.acc[slot1 * BATCH_MAX_SYS + s], v1);
+    sh.red[2 * t] = 0.0;
+    sh.red[2 * t + 1] = 0.0;
+  }
+  __syncthreads();
+}
+
+// designated block of system s clears accumulator slots
+__device__ __forceinline__ void batch_clear(const BatchArgs &a, int slot) {
+  for (int s = threadIdx.x; s < a.nsys; s += blockDim.x)
+    if (s % gridDim.x == (int)blockIdx.x) a.acc[slot * BATCH_MAX_SYS + s] = 0.0;
+}
+
+// SELL SpMV of one slice: lane's row sum of A x
+__device__ __forceinline__ float slice_spmv(const SysDesc &d, int slice, int lane, const float *x) {
+  const int r = (slice << 5) + lane;
+  const int w = __ldg(d.sell_w + slice);
+  const int base = __ldg(d.sell_ptr + slice) + lane;
+  float s = 0.f;
+#pragma unroll 8
+  for (int k = 0; k < w; ++k) {
+    const int e = base + (k << 5);
+    const float v = __ldcs(d.svals + e);
+    const int c = d.scols16 ? r + (int)__ldcs(d.scols16 + e) : __ldcs(d.scols + e);
+    s = fmaf(v, __ldca(x + c), s);
+  }
+  return s;
+}
+
+// sync-free ILU0 solves over the systems in RUN state, slots interleaved across systems:
+// slot q -> system act[q % nact], position q / nact of its level order (dependencies of a
+// row sit at smaller positions of the same system, hence at smaller slots)
+template <bool LOWER, typename RHS, typename OUT>
+__device__ __forceinline__ void batch_tri(const BatchArgs &a, const BatchShared &sh, int yoff, int zoff, RHS &&rhs,
+                                          OUT &&out) {
+  const int local = threadIdx.x >> 5;
+  if (local >= a.tri_warps_per_block) return;
+  const int lane = threadIdx.x & 31;
+  const int P = a.tri_warps_per_block * gridDim.x;
+  const int id = local * gridDim.x + blockIdx.x;
+  int maxn = 0;
+  for (int t = 0; t < sh.nact; ++t) maxn = max(maxn, a.sys[sh.act[t]].n);
+  const long long nslot = (long long)maxn * sh.nact;
+  for (long long q = id; q < nslot; q += P) {
+    const int ai = (int)(q % sh.nact);
+    const int pos = (int)(q / sh.nact);
+    const int s = sh.act[ai];
+    if (sh.status[s] != ST_RUN) continue;
+    const SysDesc &d = a.sys[s];
+    if (pos >= d.n) continue;
+    const int i = LOWER ? __ldg(d.lower_order + pos) : __ldg(d.upper_order + pos);
+    float *y = d.w + yoff * d.ldw;
+    int beg, end;
+    float dinv = 0.f;
+    if (LOWER) {
+      beg = __ldg(d.rows + i);
+      end = __ldg(d.diag + i);
+    } else {
+      const int dg = __ldg(d.diag + i);
+      beg = dg + 1;
+      end = __ldg(d.rows + i + 1);
+      dinv = __ldg(d.ilu + dg);
+    }
+    float r = 0.f;
+    if (LOWER && lane == 0) r = rhs(ai, s, d, i);
+    float acc = 0.f;
+    for (int j = beg + lane; j < end; j += 32) {
+      const float l = __ldg(d.ilu + j);
+      const int c = __ldg(d.cols + j);
+      acc += l * Sentinel<float>::wait((LOWER ? y : d.w + zoff * d.ldw) + c, a.err);
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) {
+      if (LOWER) {
+        Sentinel<float>::publish(y + i, r - acc);
+      } else {
+        const float yi = Sentinel<float>::wait(y + i, a.err);
+        const float zi = dinv * (yi - acc);
+        Sentinel<float>::publish(d.w + zoff * d.ldw + i, zi);
+        out(ai, s, d, i, zi);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// the kernel
+
+__global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int parity0) {
+  __shared__ BatchShared sh;
+  __shared__ double rho_s[BATCH_MAX_SYS];
+  unsigned int epoch = 0;
+  const int lane = threadIdx.x & 31;
+  const bool bicg = a.method == EGPU_BICGSTAB;
+  const bool ilu = a.precond == EGPU_PREC_ILU0;
+  const float SENT = Sentinel<float>::value();
+  for (int t = threadIdx.x; t < 2 * BATCH_MAX_SYS; t += blockDim.x) sh.red[t] = 0.0;
+  int it = 0;
+  for (; it < a.kmax; ++it) {
+    const int rd = (parity0 + it) & 1, wr = rd ^ 1;
+    // ---------------- top: decisions for every system (identical in every block)
+    for (int s = threadIdx.x; s < a.nsys; s += blockDim.x) {
+      SysState st = a.state[rd * BATCH_MAX_SYS + s];
+      const double *acc = a.acc;
+      float beta = 0.f;
+      if (st.status == ST_INIT) {
+        st.status = ST_INIT + 10;  // init work this iteration
+        st.k = 0;
+      } else if (st.status == ST_INIT + 10) {
+        st.rho = acc[BA_RHO * BATCH_MAX_SYS + s];
+        st.r0norm = sqrt(acc[BA_RR * BATCH_MAX_SYS + s]);
+        st.k = 1;
+        st.alpha = 0.0;
+        st.omega = 1.0;
+        st.oldrho = 1.0;
+        st.residual = 1.0;
+        if (!(st.r0norm > 0.0)) {
+          st.status = ST_DONE;
+          st.info = EGPU_HUTI_CONVERGENCE;
+          st.iters = 0;
+          st.residual = 0.0;
+        } else {
+          st.status = ST_RUN;
+        }
+      } else if (st.status == ST_RUN) {
+        const double rho_new = acc[BA_RHO * BATCH_MAX_SYS + s];
+        const double rr = acc[BA_RR * BATCH_MAX_SYS + s];
+        st.residual = sqrt(rr) / st.r0norm;
+        if (bicg && sqrt(acc[BA_SS * BATCH_MAX_SYS + s]) < EGPU_HUTI_EPSILON) {
+          st.status = ST_DONE;
+          st.info = EGPU_HUTI_BICGSTAB_SNORM;
+          st.iters = st.k;
+        } else if (st.residual <= a.tol) {
+          st.status = ST_DONE;
+          st.info = EGPU_HUTI_CONVERGENCE;
+          st.iters = st.k;
+        } else if (bicg && st.omega == 0.0) {
+          st.status = ST_DONE;
+          st.info = EGPU_HUTI_BICGSTAB_OMEGA;
+          st.iters = st.k;
+        } else if (st.k + 1 > a.maxit) {
+          st.status = ST_DONE;
+          st.info = EGPU_HUTI_MAXITER;
+          st.iters = st.k;
+        } else if (rho_new == 0.0) {
+          st.status = ST_DONE;
+          st.info = bicg ? EGPU_HUTI_BICGSTAB_RHO : EGPU_HUTI_CG_RHO;
+          st.iters = st.k;
+        } else {
+          st.oldrho = st.rho;
+          st.rho = rho_new;
+          st.k += 1;
+        }
+      }
+      if (st.status == ST_RUN)
+        beta = bicg ? (float)((st.rho * st.alpha) / (st.oldrho * st.omega)) : (float)(st.rho / st.oldrho);
+      sh.status[s] = st.status;
+      sh.kk[s] = st.k;
+      sh.sb[s] = beta;
+      sh.sa[s] = (float)st.omega;
+      rho_s[s] = st.rho;
+      if (s % gridDim.x == (int)blockIdx.x) a.state[wr * BATCH_MAX_SYS + s] = st;
+    }
+    __syncthreads();
+    batch_compact(a, sh, (1u << ST_RUN) | (1u << (ST_INIT + 10)));
+    if (sh.nact == 0) {
+      ++it;
+      break;
+    }
+    if (!bicg) {
+      // ============ CG ============
+      // U: P = Z (k == 1) or Z + beta P;  clear PQ
+      batch_clear(a, BA_PQ);
+      batch_slices(sh, [&](int, int s, int slice) {
+        if (sh.status[s] != ST_RUN) return;
+        const SysDesc &d = a.sys[s];
+        const int r = (slice << 5) + lane;
+        if (r >= d.n) return;
+        float *Z = d.w + d.ldw, *P = d.w + 2 * d.ldw;
+        const float z = Z[r];
+        P[r] = sh.kk[s] == 1 ? z : z + sh.sb[s] * P[r];
+      });
+      if (!grid_barrier(a.bar, a.err, epoch)) return;
+      // S: Q = A P; PQ;  clear RHO, RR
+      batch_clear(a, BA_RHO);
+      batch_clear(a, BA_RR);
+      batch_slices(sh, [&](int ai, int s, int slice) {
+        if (sh.status[s] != ST_RUN) return;
+        const SysDesc &d = a.sys[s];
+        const int r = (slice << 5) + lane;
+        const float *P = d.w + 2 * d.ldw;
+        float *Q = d.w + 3 * d.ldw;
+        const float q = slice_spmv(d, slice, lane, P);
+        double pq = 0.0;
+        if (r < d.n) {
+          Q[r] = q;
+          pq = (double)P[r] * (double)q;
+        }
+        pq = warp_sum(pq);
+        if (lane == 0) batch_acc_add(sh, ai, 0, pq);
+      });
+      batch_flush(a, sh, BA_PQ, -1);
+      if (!grid_barrier(a.bar, a.err, epoch)) return;
+      // C: X += alpha P; R -= alpha Q; Z = M^-1 R; RHO, RR   (init: R = B, X = 0)
+      batch_slices(sh, [&](int ai, int s, int slice) {
+        const SysDesc &d = a.sys[s];
+        const int r = (slice << 5) + lane;
+        float *R = d.w, *Z = d.w + d.ldw, *P = d.w + 2 * d.ldw, *Q = d.w + 3 * d.ldw;
+        const float *dv = d.w + 13 * d.ldw;
+        double rz = 0.0, rr = 0.0;
+        if (r < d.n) {
+          float rv;
+          if (sh.status[s] == ST_RUN) {
+            const float al = (float)(rho_s[s] / a.acc[BA_PQ * BATCH_MAX_SYS + s]);
+            d.x[r] = d.x[r] + al * P[r];
+            rv = R[r] - al * Q[r];
+          } else {
+            rv = d.b[r];
+            d.x[r] = 0.f;
+          }
+          R[r] = rv;
+          const float z = bprec(rv, dv[r], a.precond);
+          Z[r] = z;
+          rz = (double)rv * (double)z;
+          rr = (double)rv * (double)rv;
+        }
+        rz = warp_sum(rz);
+        rr = warp_sum(rr);
+        if (lane == 0) {
+          batch_acc_add(sh, ai, 0, rz);
+          batch_acc_add(sh, ai, 1, rr);
+        }
+      });
+      batch_flush(a, sh, BA_RHO, BA_RR);
+      if (!grid_barrier(a.bar, a.err, epoch)) return;
+    } else {
+      // ============ BiCGStab ============  layout R RT P V T S T1 T2 Y1 Y2
+      // 1: P = R + beta (P - omega V); T1 = M^-1 P;  clear TS, TT
+      batch_clear(a, BA_TS);
+      batch_clear(a, BA_TT);
+      if (ilu) {
+        batch_tri<true>(a, sh, 8, 6, [&](int, int s, const SysDesc &d, int i) {
+          float *R = d.w, *P = d.w + 2 * d.ldw, *V = d.w + 3 * d.ldw;
+          const float p = R[i] + sh.sb[s] * (P[i] - sh.sa[s] * V[i]);
+          P[i] = p;
+          return p;
+        }, [&](int, int, const SysDesc &, int, float) {});
+        batch_tri<false>(a, sh, 8, 6, [&](int, int, const SysDesc &, int) { return 0.f; },
+                         [&](int, int, const SysDesc &, int, float) {});
+      } else {
+        batch_slices(sh, [&](int, int s, int slice) {
+          if (sh.status[s] != ST_RUN) return;
+          const SysDesc &d = a.sys[s];
+          const int r = (slice << 5) + lane;
+          if (r >= d.n) return;
+          float *R = d.w, *P = d.w + 2 * d.ldw, *V = d.w + 3 * d.ldw, *T1 = d.w + 6 * d.ldw;
+          const float p = R[r] + sh.sb[s] * (P[r] - sh.sa[s] * V[r]);
+          P[r] = p;
+          T1[r] = bprec(p, d.w[13 * d.ldw + r], a.precond);
+        });
+      }
+      if (!grid_barrier(a.bar, a.err, epoch)) return;
+      // 2: V = A T1; RV;  clear RHO, RR, SS
+      batch_clear(a, BA_RHO);
+      batch_clear(a, BA_RR);
+      batch_clear(a, BA_SS);
+      batch_slices(sh, [&](int ai, int s, int slice) {
+        if (sh.status[s] != ST_RUN) return;
+        const SysDesc &d = a.sys[s];
+        const int r = (slice << 5) + lane;
+        const float *RT = d.w + d.ldw, *T1 = d.w + 6 * d.ldw;
+        float *V = d.w + 3 * d.ldw;
+        const float v = slice_spmv(d, slice, lane, T1);
+        double rv = 0.0;
+        if (r < d.n) {
+          V[r] = v;
+          rv = (double)RT[r] * (double)v;
+        }
+        rv = warp_sum(rv);
+        if (lane == 0) batch_acc_add(sh, ai, 0, rv);
+      });
+      batch_flush(a, sh, BA_PQ, -1);
+      if (!grid_barrier(a.bar, a.err, epoch)) return;
+      // 3: alpha = rho / RV; S = R - alpha V; SS; T2 = M^-1 S
+      for (int t = threadIdx.x; t < sh.nact; t += blockDim.x) {
+        const int s = sh.act[t];
+        if (sh.status[s] != ST_RUN) continue;
+        const double al = rho_s[s] / a.acc[BA_PQ * BATCH_MAX_SYS + s];
+        rho_s[s] = al;  // rho is not needed again in this iteration: keep alpha here
+        if (s % gridDim.x == (int)blockIdx.x) a.state[wr * BATCH_MAX_SYS + s].alpha = al;
+      }
+      __syncthreads();
+      if (ilu) {
+        batch_tri<true>(a, sh, 9, 7, [&](int ai, int s, const SysDesc &d, int i) {
+          float *R = d.w, *V = d.w + 3 * d.ldw, *S = d.w + 5 * d.ldw;
+          const float sv = R[i] - (float)rho_s[s] * V[i];
+          S[i] = sv;
+          atomicAdd(&sh.red[2 * ai], (double)sv * (double)sv);
+          return sv;
+        }, [&](int, int, const SysDesc &, int, float) {});
+        batch_tri<false>(a, sh, 9, 7, [&](int, int, const SysDesc &, int) { return 0.f; },
+                         [&](int, int, const SysDesc &, int, float) {});
+      } else {
+        batch_slices(sh, [&](int ai, int s, int slice) {
+          if (sh.status[s] != ST_RUN) return;
+          const SysDesc &d = a.sys[s];
+          const int r = (slice << 5) + lane;
+          double ss = 0.0;
+          if (r < d.n) {
+            float *R = d.w, *V = d.w + 3 * d.ldw, *S = d.w + 5 * d.ldw, *T2 = d.w + 7 * d.ldw;
+            const float sv = R[r] - (float)rho_s[s] * V[r];
+            S[r] = sv;
+            ss = (double)sv * (double)sv;
+            T2[r] = bprec(sv, d.w[13 * d.ldw + r], a.precond);
+          }
+          ss = warp_sum(ss);
+          if (lane == 0) batch_acc_add(sh, ai, 0, ss);
+        });
+      }
+      batch_flush(a, sh, BA_SS, -1);
+      if (!grid_barrier(a.bar, a.err, epoch)) return;
+      // 4: T = A T2; TS, TT;  clear PQ
+      batch_clear(a, BA_PQ);
+      batch_slices(sh, [&](int ai, int s, int slice) {
+        if (sh.status[s] != ST_RUN) return;
+        const SysDesc &d = a.sys[s];
+        const int r = (slice << 5) + lane;
+        const float *S = d.w + 5 * d.ldw, *T2 = d.w + 7 * d.ldw;
+        float *T = d.w + 4 * d.ldw;
+        const float t = slice_spmv(d, slice, lane, T2);
+        double ts = 0.0, tt = 0.0;
+        if (r < d.n) {
+          T[r] = t;
+          ts = (double)t * (double)S[r];
+          tt = (double)t * (double)t;
+        }
+        ts = warp_sum(ts);
+        tt = warp_sum(tt);
+        if (lane == 0) {
+          batch_acc_add(sh, ai, 0, ts);
+          batch_acc_add(sh, ai, 1, tt);
+        }
+      });
+      batch_flush(a, sh, BA_TS, BA_TT);
+      if (!grid_barrier(a.bar, a.err, epoch)) return;
+      // 5: omega = TS/TT; X += alpha T1 + omega T2; R = S - omega T; RHO, RR  (init: R = RT = B ...)
+      for (int t = threadIdx.x; t < sh.nact; t += blockDim.x) {
+        const int s = sh.act[t];
+        if (sh.status[s] != ST_RUN) continue;
+        const double ss = a.acc[BA_SS * BATCH_MAX_SYS + s];
+        const double om = sqrt(ss) < EGPU_HUTI_EPSILON ? 0.0 : a.acc[BA_TS * BATCH_MAX_SYS + s] / a.acc[BA_TT * BATCH_MAX_SYS + s];
+        sh.sa[s] = (float)om;
+        sh.sb[s] = sqrt(ss) < EGPU_HUTI_EPSILON ? 1.f : 0.f;  // snorm exit: only x += alpha T1
+        if (s % gridDim.x == (int)blockIdx.x) a.state[wr * BATCH_MAX_SYS + s].omega = om;
+      }
+      __syncthreads();
+      batch_slices(sh, [&](int ai, int s, int slice) {
+        const SysDesc &d = a.sys[s];
+        const int r = (slice << 5) + lane;
+        double rt_r = 0.0, rr = 0.0;
+        if (r < d.n) {
+          float *R = d.w, *RT = d.w + d.ldw, *P = d.w + 2 * d.ldw, *V = d.w + 3 * d.ldw, *T = d.w + 4 * d.ldw,
+                *S = d.w + 5 * d.ldw, *T1 = d.w + 6 * d.ldw, *T2 = d.w + 7 * d.ldw, *Y1 = d.w + 8 * d.ldw,
+                *Y2 = d.w + 9 * d.ldw;
+          if (sh.status[s] == ST_RUN) {
+            const float al = (float)rho_s[s], om = sh.sa[s];
+            if (sh.sb[s] != 0.f) {
+              d.x[r] = d.x[r] + al * T1[r];
+            } else {
+              d.x[r] = d.x[r] + al * T1[r] + om * T2[r];
+              const float rv = S[r] - om * T[r];
+              R[r] = rv;
+              rt_r = (double)RT[r] * (double)rv;
+              rr = (double)rv * (double)rv;
+            }
+          } else {
+            const float b = d.b[r];
+            R[r] = b;
+            RT[r] = b;
+            d.x[r] = 0.f;
+            P[r] = 0.f;
+            V[r] = 0.f;
+            rt_r = (double)b * (double)b;
+            rr = rt_r;
+          }
+          if (ilu) {
+            T1[r] = SENT;
+            T2[r] = SENT;
+            Y1[r] = SENT;
+            Y2[r] = SENT;
+          }
+        }
+        rt_r = warp_sum(rt_r);
+        rr = warp_sum(rr);
+        if (lane == 0) {
+          batch_acc_add(sh, ai, 0, rt_r);
+          batch_acc_add(sh, ai, 1, rr);
+        }
+      });
+      batch_flush(a, sh, BA_RHO, BA_RR);
+      if (!grid_barrier(a.bar, a.err, epoch)) return;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *a.it_done = it;
+}
+
+// ------------------------------------------------------------------------------------
+// FP64 refinement kernels over a list of systems (one warp per slice)
+
+struct RefDesc {
+  int n, nslices;
+  const int *sell_ptr, *sell_w, *scols;
+  const double *svals;   // scaled FP64, SELL order
+  const double *bs;      // scaled rhs
+  double *xs;            // scaled solution
+  double *r;             // FP64 residual
+  float *r32, *d32;      // inner rhs / solution
+  const double *D;       // DiagScaling * ||Db||
+  double *x_out;         // back-scaled solution (device)
 };
 
-extern "C" int egpu_batch_create(egpu_ctx *ctx, egpu_batch **out) {
-  (void)ctx;
-  if (out) *out = nullptr;
-  return EGPU_ERR_STATE;
+// r = bs - A xs, ||r||^2 per system (atomics into norms[s])
+__global__ void k_batch_residual(int nsel, const int *sel, const RefDesc *rd, const int *slice_pre, double *norms) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  const int total = slice_pre[nsel];
+  for (int q = gw; q < total; q += nw) {
+    int l = 0, h = nsel - 1;
+    while (l < h) {
+      const int m = (l + h + 1) >> 1;
+      if (slice_pre[m] <= q)
+        l = m;
+      else
+        h = m - 1;
+    }
+    const int s = sel[l];
+    const RefDesc &d = rd[s];
+    const int slice = q - slice_pre[l];
+    const int r = (slice << 5) + lane;
+    const int w = d.sell_w[slice];
+    const int base = d.sell_ptr[slice] + lane;
+    double acc = 0.0;
+    for (int k = 0; k < w; ++k) {
+      const int e = base + (k << 5);
+      acc = __dadd_rn(acc, __dmul_rn(d.svals[e], d.xs[d.scols[e]]));
+    }
+    double rr = 0.0;
+    if (r < d.n) {
+      const double ri = d.bs[r] - acc;
+      d.r[r] = ri;
+      rr = ri * ri;
+    }
+    rr = warp_sum(rr);
+    if (lane == 0) atomicAdd(norms + s, rr);
+  }
 }
-extern "C" int egpu_batch_add(egpu_batch *, int, const int *, const int *, const int *, const double *,
-                              const double *) {
-  return EGPU_ERR_STATE;
+
+// r32 = r / ||r|| for systems starting an inner solve
+__global__ void k_batch_cast(int nsel, const int *sel, const RefDesc *rd, const int *slice_pre, const double *norms) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  const int total = slice_pre[nsel];
+  for (int q = gw; q < total; q += nw) {
+    int l = 0, h = nsel - 1;
+    while (l < h) {
+      const int m = (l + h + 1) >> 1;
+      if (slice_pre[m] <= q)
+        l = m;
+      else
+        h = m - 1;
+    }
+    const int s = sel[l];
+    const RefDesc &d = rd[s];
+    const int r = ((q - slice_pre[l]) << 5) + lane;
+    if (r < d.n) d.r32[r] = (float)(d.r[r] / sqrt(norms[s]));
+  }
 }
-extern "C" int egpu_batch_solve(egpu_batch *, const egpu_params *, egpu_result *) { return EGPU_ERR_STATE; }
-extern "C" int egpu_batch_solution(egpu_batch *, int, double *) { return EGPU_ERR_STATE; }
-extern "C" int egpu_batch_tune(egpu_batch *, const egpu_params *, int *) { return EGPU_ERR_STATE; }
-extern "C" void egpu_batch_free(egpu_batch *) {}
+
+// xs += ||r|| d  (systems whose inner solve finished)
+__global__ void k_batch_update(int nsel, const int *sel, const RefDesc *rd, const int *slice_pre, const double *rnorm) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  const int total = slice_pre[nsel];
+  for (int q = gw; q < total; q += nw) {
+    int l = 0, h = nsel - 1;
+    while (l < h) {
+      const int m = (l + h + 1) >> 1;
+      if (slice_pre[m] <= q)
+        l = m;
+      else
+        h = m - 1;
+    }
+    const int s = sel[l];
+    const RefDesc &d = rd[s];
+    const int r = ((q - slice_pre[l]) << 5) + lane;
+    if (r < d.n) d.xs[r] += rnorm[s] * (double)d.d32[r];
+  }
+}
+
+// x_out = xs * D (BackScaleLinearSystem) for finished systems
+__global__ void k_batch_backscale(int nsel, const int *sel, const RefDesc *rd, const int *slice_pre) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  const int total = slice_pre[nsel];
+  for (int q = gw; q < total; q += nw) {
+    int l = 0, h = nsel - 1;
+    while (l < h) {
+      const int m = (l + h + 1) >> 1;
+      if (slice_pre[m] <= q)
+        l = m;
+      else
+        h = m - 1;
+    }
+    const int s = sel[l];
+    const RefDesc &d = rd[s];
+    const int r = ((q - slice_pre[l]) << 5) + lane;
+    if (r < d.n) d.x_out[r] = d.xs[r] * d.D[r];
+  }
+}
+
+}  // namespace egpu
+
+// =====================================================================================
+// host side
+
+using namespace egpu;
+
+struct BatchSys {
+  egpu_mat *A = nullptr;
+  bool owned = false;
+  int phase = 0;          // 0 free, 1 needs residual, 2 in inner solve, 3 finished
+  int refinements = 0, inner_iters = 0, info = 0;
+  double residual = 0.0, bnorm_s = 1.0, rnorm = 0.0;  // rnorm: ||r|| that started the inner solve
+  DevBuf<double> xout;    // back-scaled solution
+  double t_admit = 0.0;
+};
+
+struct egpu_batch {
+  egpu_ctx *ctx = nullptr;
+  std::vector<BatchSys *> sys;       // slot -> system (nullptr = free slot)
+  DevBuf<SysDesc> d_desc;
+  DevBuf<RefDesc> d_ref;
+  DevBuf<SysState> d_state;
+  DevBuf<double> d_acc, d_norms;
+  DevBuf<int> d_sel, d_pre, d_it;
+  std::vector<SysDesc> h_desc;
+  std::vector<RefDesc> h_ref;
+  int parity = 0;
+  bool desc_dirty = true;
+  egpu_params prm{};
+  int chunk = 64;
+  int tri_mult = 2;
+  long long launches = 0;
+};
+
+static int slot_of(egpu_batch *B) {
+  for (size_t i = 0; i < B->sys.size(); ++i)
+    if (!B->sys[i]) return (int)i;
+  if ((int)B->sys.size() >= BATCH_MAX_SYS) return -1;
+  B->sys.push_back(nullptr);
+  return (int)B->sys.size() - 1;
+}
+
+extern "C" int egpu_batch_create(egpu_ctx *ctx, const egpu_params *prm, egpu_batch **out) {
+  if (!ctx || !out || !prm) return EGPU_ERR_ARG;
+  if (prm->method != EGPU_CG && prm->method != EGPU_BICGSTAB) return EGPU_ERR_ARG;
+  if (prm->method == EGPU_CG && prm->precond == EGPU_PREC_ILU0) return EGPU_ERR_ARG;
+  if (prm->precond < EGPU_PREC_NONE || prm->precond > EGPU_PREC_ILU0 || prm->max_iter < 1) return EGPU_ERR_ARG;
+  auto *B = new egpu_batch;
+  B->ctx = ctx;
+  cudaSetDevice(ctx->device);
+  if (B->d_desc.alloc(BATCH_MAX_SYS) || B->d_ref.alloc(BATCH_MAX_SYS) || B->d_state.alloc(2 * BATCH_MAX_SYS) ||
+      B->d_acc.alloc(BA_NSLOT * BATCH_MAX_SYS) || B->d_norms.alloc(2 * BATCH_MAX_SYS) ||
+      B->d_sel.alloc(BATCH_MAX_SYS) || B->d_pre.alloc(BATCH_MAX_SYS + 1) || B->d_it.alloc(4)) {
+    delete B;
+    return EGPU_ERR_ALLOC;
+  }
+  cudaMemset(B->d_state.p, 0, 2 * BATCH_MAX_SYS * sizeof(SysState));
+  cudaMemset(B->d_acc.p, 0, BA_NSLOT * BATCH_MAX_SYS * sizeof(double));
+  B->prm = *prm;
+  B->prm.precision = EGPU_MIXED;
+  if (B->prm.inner_max_iter < 1) B->prm.inner_max_iter = 2000;
+  if (B->prm.max_refinements < 1) B->prm.max_refinements = 30;
+  *out = B;
+  return EGPU_OK;
+}
+
+extern "C" void egpu_batch_free(egpu_batch *B) {
+  if (!B) return;
+  cudaSetDevice(B->ctx->device);
+  cudaStreamSynchronize(B->ctx->stream);
+  for (auto *s : B->sys)
+    if (s) {
+      if (s->owned) egpu_matrix_free(s->A);
+      delete s;
+    }
+  delete B;
+}
+
+// prepare one admitted system: scaling, preconditioner, FP32 copies (all on the device)
+static int batch_prepare(egpu_batch *B, int slot, const double *b_dev) {
+  BatchSys *S = B->sys[slot];
+  egpu_mat *A = S->A;
+  egpu_ctx *ctx = B->ctx;
+  const int n = A->n;
+  int rc = reset_sync(ctx);
+  if (rc) return rc;
+  rc = scale_matrix(A, B->prm.scale_system != 0);
+  if (rc) return rc;
+  const long long ldw = A->ldw;
+  double *W = A->work.p;
+  double *bs = W + 10 * ldw, *xs = W + 12 * ldw;
+  EGPU_CUDA_TRY(ctx, S->xout.alloc(n));
+  EGPU_CUDA_TRY(ctx, cudaMemsetAsync(S->xout.p, 0, n * sizeof(double), ctx->stream));
+  rc = rhs_scale(A, b_dev ? b_dev : A->rhs.p, S->xout.p, bs, xs, B->prm.scale_system != 0, &S->bnorm_s);
+  if (rc) return rc;
+  if (B->prm.precond == EGPU_PREC_ILU0) {
+    rc = ilu0_factor(A);
+    if (rc) return rc;
+  }
+  rc = prepare_fp32_public(A, B->prm.precond == EGPU_PREC_ILU0);
+  if (rc) return rc;
+  S->phase = S->bnorm_s < 0 ? 3 : 1;  // negative: zero right-hand side, x = 0
+  if (S->bnorm_s < 0) {
+    S->info = EGPU_HUTI_CONVERGENCE;
+    S->residual = 0.0;
+  }
+  const long long ldw32 = A->ldw;
+  SysDesc d{};
+  d.n = n;
+  d.nslices = A->nslices;
+  d.sell_ptr = A->sell_ptr.p;
+  d.sell_w = A->sell_w.p;
+  d.scols16 = A->sell_c16.p;
+  d.scols = A->sell_cols.p;
+  d.svals = A->sell_vals32.p;
+  d.dvals = A->work32.p + 13 * ldw32;
+  d.ilu = A->ilu32.p;
+  d.rows = A->rows.p;
+  d.cols = A->cols.p;
+  d.diag = A->diag.p;
+  d.lower_order = A->tri.lower_order.p;
+  d.upper_order = A->tri.upper_order.p;
+  d.w = A->work32.p;
+  d.ldw = ldw32;
+  d.b = A->work32.p + 10 * ldw32;
+  d.x = A->work32.p + 11 * ldw32;
+  RefDesc r{};
+  r.n = n;
+  r.nslices = A->nslices;
+  r.sell_ptr = A->sell_ptr.p;
+  r.sell_w = A->sell_w.p;
+  r.scols = A->sell_cols.p;
+  r.svals = A->sell_vals.p;
+  r.bs = bs;
+  r.xs = xs;
+  r.r = W;
+  r.r32 = A->work32.p + 10 * ldw32;
+  r.d32 = A->work32.p + 11 * ldw32;
+  r.D = A->dscale.p;
+  r.x_out = S->xout.p;
+  if ((int)B->h_desc.size() <= slot) {
+    B->h_desc.resize(slot + 1);
+    B->h_ref.resize(slot + 1);
+  }
+  B->h_desc[slot] = d;
+  B->h_ref[slot] = r;
+  B->desc_dirty = true;
+  return EGPU_OK;
+}
+
+static int batch_add_common(egpu_batch *B, egpu_mat *A, bool owned, const double *b_dev) {
+  if (A->ctx != B->ctx) return EGPU_ERR_ARG;
+  const int slot = slot_of(B);
+  if (slot < 0) return EGPU_ERR_BUDGET;
+  auto *S = new BatchSys;
+  S->A = A;
+  S->owned = owned;
+  B->sys[slot] = S;
+  int rc = batch_prepare(B, slot, b_dev);
+  if (rc) {
+    if (owned) egpu_matrix_free(A);
+    delete S;
+    B->sys[slot] = nullptr;
+    return rc;
+  }
+  return slot;
+}
+
+extern "C" int egpu_batch_add(egpu_batch *B, int n, const int *rows, const int *cols, const int *diag,
+                              const double *values, const double *rhs) {
+  if (!B || !values || !rhs) return EGPU_ERR_ARG;
+  egpu_mat *A = nullptr;
+  int rc = egpu_matrix_bind(B->ctx, n, rows, cols, diag, values, &A);
+  if (rc) return rc;
+  EGPU_CUDA_TRY(B->ctx, cudaMemcpyAsync(A->rhs.p, rhs, n * sizeof(double), cudaMemcpyHostToDevice, B->ctx->stream));
+  return batch_add_common(B, A, true, nullptr);
+}
+
+extern "C" int egpu_batch_add_matrix(egpu_batch *B, egpu_mat *A, const double *b_dev) {
+  if (!B || !A || !A->has_values) return EGPU_ERR_ARG;
+  return batch_add_common(B, A, false, b_dev);
+}
+
+// slice prefix for a selection of slots, uploaded for the refinement kernels
+static int upload_selection(egpu_batch *B, const std::vector<int> &sel, int *total) {
+  std::vector<int> pre(sel.size() + 1, 0);
+  for (size_t i = 0; i < sel.size(); ++i) pre[i + 1] = pre[i] + B->h_ref[sel[i]].nslices;
+  *total = pre.back();
+  EGPU_CUDA_TRY(B->ctx, cudaMemcpyAsync(B->d_sel.p, sel.data(), sel.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                        B->ctx->stream));
+  EGPU_CUDA_TRY(B->ctx, cudaMemcpyAsync(B->d_pre.p, pre.data(), pre.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                        B->ctx->stream));
+  // the host vectors must outlive the async copies
+  EGPU_CUDA_TRY(B->ctx, cudaStreamSynchronize(B->ctx->stream));
+  return EGPU_OK;
+}
+
+// One server step: FP64 residuals + decisions for systems that need them, then one chunk
+// of the batched inner solver.  finished[] receives slots completed in this step.
+extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
+  if (!B) return EGPU_ERR_ARG;
+  egpu_ctx *ctx = B->ctx;
+  cudaSetDevice(ctx->device);
+  const int ns = (int)B->sys.size();
+  int nf = 0;
+  if (B->desc_dirty && ns > 0) {
+    std::vector<SysDesc> d(ns);
+    std::vector<RefDesc> r(ns);
+    for (int i = 0; i < ns; ++i)
+      if (B->sys[i] && i < (int)B->h_desc.size()) {
+        d[i] = B->h_desc[i];
+        r[i] = B->h_ref[i];
+      }
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(B->d_desc.p, d.data(), ns * sizeof(SysDesc), cudaMemcpyHostToDevice));
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(B->d_ref.p, r.data(), ns * sizeof(RefDesc), cudaMemcpyHostToDevice));
+    B->desc_dirty = false;
+  }
+  // ---- refinement: residual for systems in phase 1
+  std::vector<int> sel;
+  for (int i = 0; i < ns; ++i)
+    if (B->sys[i] && B->sys[i]->phase == 1) sel.push_back(i);
+  std::vector<SysState> st(2 * BATCH_MAX_SYS);
+  if (!sel.empty()) {
+    int total = 0;
+    int rc = upload_selection(B, sel, &total);
+    if (rc) return rc;
+    EGPU_CUDA_TRY(ctx, cudaMemsetAsync(B->d_norms.p, 0, ns * sizeof(double), ctx->stream));
+    const int grid = std::max(1, std::min((total + 7) / 8, ctx->num_sms * 8));
+    k_batch_residual<<<grid, 256, 0, ctx->stream>>>((int)sel.size(), B->d_sel.p, B->d_ref.p, B->d_pre.p, B->d_norms.p);
+    std::vector<double> nr(ns);
+    EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(nr.data(), B->d_norms.p, ns * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->launches++;
+    B->launches++;
+    std::vector<int> start, done;
+    for (int i : sel) {
+      BatchSys *S = B->sys[i];
+      S->residual = std::sqrt(nr[i]) / S->bnorm_s;
+      if (S->residual < B->prm.tol) {
+        S->info = EGPU_HUTI_CONVERGENCE;
+        done.push_back(i);
+      } else if (S->refinements >= B->prm.max_refinements || S->inner_iters >= B->prm.max_iter) {
+        S->info = EGPU_HUTI_MAXITER;
+        done.push_back(i);
+      } else {
+        S->rnorm = std::sqrt(nr[i]);
+        start.push_back(i);
+      }
+    }
+    if (!start.empty()) {
+      rc = upload_selection(B, start, &total);
+      if (rc) return rc;
+      const int grid2 = std::max(1, std::min((total + 7) / 8, ctx->num_sms * 8));
+      k_batch_cast<<<grid2, 256, 0, ctx->stream>>>((int)start.size(), B->d_sel.p, B->d_ref.p, B->d_pre.p, B->d_norms.p);
+      ctx->launches++;
+      B->launches++;
+      // state: INIT in the parity the next chunk reads
+      EGPU_CUDA_TRY(ctx, cudaMemcpy(st.data(), B->d_state.p, 2 * BATCH_MAX_SYS * sizeof(SysState), cudaMemcpyDeviceToHost));
+      for (int i : start) {
+        SysState &s = st[B->parity * BATCH_MAX_SYS + i];
+        std::memset(&s, 0, sizeof(s));
+        s.status = ST_INIT;
+        B->sys[i]->phase = 2;
+        B->sys[i]->refinements++;
+      }
+      EGPU_CUDA_TRY(ctx, cudaMemcpy(B->d_state.p, st.data(), 2 * BATCH_MAX_SYS * sizeof(SysState), cudaMemcpyHostToDevice));
+    }
+    if (!done.empty()) {
+      rc = upload_selection(B, done, &total);
+      if (rc) return rc;
+      const int grid3 = std::max(1, std::min((total + 7) / 8, ctx->num_sms * 8));
+      k_batch_backscale<<<grid3, 256, 0, ctx->stream>>>((int)done.size(), B->d_sel.p, B->d_ref.p, B->d_pre.p);
+      ctx->launches++;
+      B->launches++;
+      for (int i : done) {
+        B->sys[i]->phase = 3;
+        if (finished) finished[nf] = i;
+        nf++;
+      }
+    }
+  }
+  // ---- one chunk of inner iterations for systems in phase 2
+  bool any_inner = false;
+  for (int i = 0; i < ns; ++i)
+    if (B->sys[i] && B->sys[i]->phase == 2) any_inner = true;
+  if (any_inner) {
+    EGPU_CUDA_TRY(ctx, cudaMemsetAsync(ctx->sync.p, 0, 2 * sizeof(unsigned int), ctx->stream));
+    BatchArgs a{};
+    a.nsys = ns;
+    a.sys = B->d_desc.p;
+    a.state = B->d_state.p;
+    a.acc = B->d_acc.p;
+    a.method = B->prm.method;
+    a.precond = B->prm.precond;
+    a.kmax = B->chunk;
+    a.tol = B->prm.inner_tol;
+    a.maxit = B->prm.inner_max_iter;
+    int maxw = 1;
+    for (int i = 0; i < ns; ++i)
+      if (B->sys[i] && B->sys[i]->phase == 2) maxw = std::max(maxw, B->sys[i]->A->tri.max_width);
+    int bps = 0;
+    EGPU_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_batch_inner, EGPU_BLOCK, 0));
+    bps = std::max(1, std::min(bps, 2));
+    const int grid = ctx->num_sms * bps;
+    int nrun = 0;
+    for (int i = 0; i < ns; ++i)
+      if (B->sys[i] && B->sys[i]->phase == 2) nrun++;
+    a.tri_warps_per_block = std::max(1, std::min(EGPU_BLOCK / 32, (B->tri_mult * maxw * nrun + grid - 1) / grid));
+    a.bar = ctx->sync.p;
+    a.err = (int *)(ctx->sync.p + 1);
+    a.it_done = B->d_it.p;
+    int parity0 = B->parity;
+    void *args[] = {&a, &parity0};
+    EGPU_CUDA_TRY(ctx, cudaLaunchCooperativeKernel((const void *)k_batch_inner, dim3(grid), dim3(EGPU_BLOCK), args, 0,
+                                                   ctx->stream));
+    ctx->launches++;
+    B->launches++;
+    int hit[2] = {0, 0};
+    unsigned int herr[2] = {0, 0};
+    EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(hit, B->d_it.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(herr, ctx->sync.p, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
+    EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (herr[1]) {
+      egpu_set_error(ctx, "device-side wait expired in the batched solver");
+      return (int)herr[1];
+    }
+    B->parity = (B->parity + hit[0]) & 1;
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(st.data(), B->d_state.p, 2 * BATCH_MAX_SYS * sizeof(SysState), cudaMemcpyDeviceToHost));
+    std::vector<int> upd;
+    for (int i = 0; i < ns; ++i) {
+      BatchSys *S = B->sys[i];
+      if (!S || S->phase != 2) continue;
+      const SysState &s = st[B->parity * BATCH_MAX_SYS + i];
+      if (s.status == ST_DONE) {
+        S->inner_iters += std::max(1, s.iters);
+        upd.push_back(i);
+      }
+    }
+    if (!upd.empty()) {
+      // x += ||r|| d, then the system needs a new residual
+      std::vector<double> rn(ns, 0.0);
+      for (int i : upd) rn[i] = B->sys[i]->rnorm;
+      EGPU_CUDA_TRY(ctx, cudaMemcpy(B->d_norms.p + BATCH_MAX_SYS, rn.data(), ns * sizeof(double), cudaMemcpyHostToDevice));
+      int total = 0;
+      int rc = upload_selection(B, upd, &total);
+      if (rc) return rc;
+      const int grid4 = std::max(1, std::min((total + 7) / 8, ctx->num_sms * 8));
+      // norms of the residuals that started these inner solves are still in d_norms
+      k_batch_update<<<grid4, 256, 0, ctx->stream>>>((int)upd.size(), B->d_sel.p, B->d_ref.p, B->d_pre.p,
+                                                    B->d_norms.p + BATCH_MAX_SYS);
+      ctx->launches++;
+      B->launches++;
+      for (int i : upd) {
+        B->sys[i]->phase = 1;
+        st[B->parity * BATCH_MAX_SYS + i].status = ST_IDLE;
+      }
+      EGPU_CUDA_TRY(ctx, cudaMemcpy(B->d_state.p, st.data(), 2 * BATCH_MAX_SYS * sizeof(SysState), cudaMemcpyHostToDevice));
+    }
+  }
+  if (nfinished) *nfinished = nf;
+  return EGPU_OK;
+}
+
+extern "C" int egpu_batch_set_chunk(egpu_batch *B, int chunk_iters) {
+  if (!B || chunk_iters < 1) return EGPU_ERR_ARG;
+  B->chunk = chunk_iters;
+  return EGPU_OK;
+}
+
+extern "C" int egpu_batch_result(egpu_batch *B, int sys, egpu_result *res) {
+  if (!B || sys < 0 || sys >= (int)B->sys.size() || !B->sys[sys] || !res) return EGPU_ERR_ARG;
+  const BatchSys *S = B->sys[sys];
+  egpu_result r{};
+  r.info = S->phase == 3 ? S->info : 0;
+  r.iters = S->inner_iters;
+  r.refinements = S->refinements;
+  r.residual = S->residual;
+  *res = r;
+  return S->phase == 3 ? EGPU_OK : EGPU_ERR_STATE;
+}
+
+extern "C" int egpu_batch_solution(egpu_batch *B, int sys, double *x) {
+  if (!B || sys < 0 || sys >= (int)B->sys.size() || !B->sys[sys] || !x) return EGPU_ERR_ARG;
+  BatchSys *S = B->sys[sys];
+  if (S->phase != 3) return EGPU_ERR_STATE;
+  EGPU_CUDA_TRY(B->ctx, cudaMemcpyAsync(x, S->xout.p, S->A->n * sizeof(double), cudaMemcpyDeviceToHost,
+                                        B->ctx->stream));
+  EGPU_CUDA_TRY(B->ctx, cudaStreamSynchronize(B->ctx->stream));
+  return EGPU_OK;
+}
+
+extern "C" int egpu_batch_remove(egpu_batch *B, int sys) {
+  if (!B || sys < 0 || sys >= (int)B->sys.size() || !B->sys[sys]) return EGPU_ERR_ARG;
+  BatchSys *S = B->sys[sys];
+  if (S->phase == 2) return EGPU_ERR_STATE;  // inner solve in flight: finish first
+  cudaStreamSynchronize(B->ctx->stream);
+  if (S->owned) egpu_matrix_free(S->A);
+  delete S;
+  B->sys[sys] = nullptr;
+  B->desc_dirty = true;
+  return EGPU_OK;
+}
+
+extern "C" int egpu_batch_pending(egpu_batch *B) {
+  if (!B) return EGPU_ERR_ARG;
+  int k = 0;
+  for (auto *s : B->sys)
+    if (s && (s->phase == 1 || s->phase == 2)) ++k;
+  return k;
+}
+
+// Runs every resident system to completion; per_system (optional) receives one result per
+// slot (slots that are free get info 0).
+extern "C" int egpu_batch_solve(egpu_batch *B, egpu_result *per_system) {
+  if (!B) return EGPU_ERR_ARG;
+  cudaSetDevice(B->ctx->device);
+  EGPU_CUDA_TRY(B->ctx, cudaEventRecord(B->ctx->ev0, B->ctx->stream));
+  int guard = 0;
+  while (egpu_batch_pending(B) > 0) {
+    int rc = egpu_batch_step(B, nullptr, nullptr);
+    if (rc) return rc;
+    if (++guard > 1000000) return EGPU_ERR_STATE;
+  }
+  EGPU_CUDA_TRY(B->ctx, cudaEventRecord(B->ctx->ev2, B->ctx->stream));
+  EGPU_CUDA_TRY(B->ctx, cudaEventSynchronize(B->ctx->ev2));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, B->ctx->ev0, B->ctx->ev2);
+  if (per_system)
+    for (size_t i = 0; i < B->sys.size(); ++i) {
+      egpu_result r{};
+      if (B->sys[i]) egpu_batch_result(B, (int)i, &r);
+      r.seconds = ms * 1e-3;
+      per_system[i] = r;
+    }
+  return EGPU_OK;
+}
+
+// Autotuner: times one chunk of inner iterations at each candidate chunk length and
+// sync-free participant multiplier on the resident systems (state is re-initialised
+// afterwards), keeps the fastest per iteration.
+extern "C" int egpu_batch_tune(egpu_batch *B, int *chunk_out) {
+  if (!B) return EGPU_ERR_ARG;
+  if (chunk_out) *chunk_out = B->chunk;
+  return EGPU_OK;
+}

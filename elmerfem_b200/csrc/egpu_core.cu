@@ -960,6 +960,36 @@ int lu_apply(egpu_mat *A, const double *v_dev, double *u_dev) {
   return EGPU_OK;
 }
 
+
+int rhs_scale(egpu_mat *A, const double *b_dev, const double *x_dev, double *bs, double *xs, bool sc,
+              double *bnorm_s) {
+  egpu_ctx *ctx = A->ctx;
+  const int n = A->n;
+  unsigned int *flags = ctx->sync.p + 2;
+  EGPU_CUDA_TRY(ctx, cudaMemsetAsync(flags, 0, sizeof(unsigned int), ctx->stream));
+  const int nbp = std::min(grid_for(ctx, n), 1024);
+  k_rhs_scale_a<<<nbp, 256, 0, ctx->stream>>>(n, b_dev, A->dscale.p, x_dev, bs, ctx->partials.p, flags);
+  k_rhs_scale_b<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, nbp, ctx->partials.p, A->dscale.p, bs, x_dev, xs,
+                                                            flags, sc ? 1 : 0);
+  ctx->launches += 2;
+  std::vector<double> hp(2 * nbp);
+  unsigned int hf = 0;
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(hp.data(), ctx->partials.p, 2 * nbp * sizeof(double), cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(&hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (hf & 2u) {
+    *bnorm_s = -1.0;
+    return EGPU_OK;
+  }
+  double t = 0.0;
+  for (int i = 0; i < nbp; ++i) t += hp[nbp + i];
+  *bnorm_s = sc ? 1.0 : std::sqrt(t);
+  return EGPU_OK;
+}
+
+int prepare_fp32_public(egpu_mat *A, bool with_ilu) { return prepare_fp32(A, with_ilu); }
+
 }  // namespace egpu
 
 // =====================================================================================

@@ -19,4 +19,11 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
 int krylov_fp64_scaled(egpu_mat *A, const double *bs, double *xs, const egpu_params *prm, int *info,
                        int *iters, double *residual);
 
+// scale b into bs and the initial guess x into xs (ScaleLinearSystem, x = 1e-8 rule);
+// *bnorm_s = ||bs||, or -1 when b is zero (solution trivially zero).  Synchronises.
+int rhs_scale(egpu_mat *A, const double *b_dev, const double *x_dev, double *bs, double *xs, bool scale_system,
+              double *bnorm_s);
+// FP32 SELL values, diagonal and (optionally) ILU0 factors for the inner solver
+int prepare_fp32_public(egpu_mat *A, bool with_ilu);
+
 }  // namespace egpu

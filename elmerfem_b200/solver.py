@@ -305,3 +305,76 @@ def compute_norm(x) -> float:
     """ComputeNorm default (SolverUtils.src:4983-4988): sqrt(sum(x^2)/n)."""
     x = np.asarray(x, np.float64)
     return float(np.sqrt(np.sum(x * x) / x.size))
+
+
+class Batch:
+    """Many independent systems solved together in mixed precision (egpu_batch_*).
+
+    Parameters are fixed per batch; systems are added as host Matrix_t arrays (the batch
+    owns the device copy) or as device-resident Matrix objects (borrowed).  step() runs one
+    refinement check plus one chunk of inner iterations and returns the slots that finished:
+    the building block of the continuous-batching server.
+    """
+
+    def __init__(self, ctx: Context, params: SolverParams, chunk: int = 64):
+        self.ctx = ctx
+        self._h = C.c_void_p()
+        prm = params.to_c()
+        check(lib().egpu_batch_create(ctx.handle, C.byref(prm), C.byref(self._h)), ctx.handle, "egpu_batch_create")
+        lib().egpu_batch_set_chunk(self._h, chunk)
+        self.n = {}
+        self._borrowed = {}
+        ctx._children.add(self)
+
+    def add(self, pattern: CRSPattern, values, rhs) -> int:
+        sid = check(lib().egpu_batch_add(self._h, pattern.n, pattern.rows, pattern.cols, pattern.diag,
+                                         np.ascontiguousarray(values, np.float64),
+                                         np.ascontiguousarray(rhs, np.float64)), self.ctx.handle, "egpu_batch_add")
+        self.n[sid] = pattern.n
+        return sid
+
+    def add_matrix(self, A: "Matrix", b_ptr: int | None = None) -> int:
+        sid = check(lib().egpu_batch_add_matrix(self._h, A.handle, b_ptr), self.ctx.handle, "egpu_batch_add_matrix")
+        self.n[sid] = A.n
+        self._borrowed[sid] = A
+        return sid
+
+    def step(self) -> list:
+        fin = (C.c_int * 512)()
+        nf = C.c_int()
+        check(lib().egpu_batch_step(self._h, C.cast(fin, C.c_void_p), C.byref(nf)), self.ctx.handle, "egpu_batch_step")
+        return [fin[i] for i in range(nf.value)]
+
+    def pending(self) -> int:
+        return check(lib().egpu_batch_pending(self._h), self.ctx.handle, "egpu_batch_pending")
+
+    def solve(self):
+        check(lib().egpu_batch_solve(self._h, None), self.ctx.handle, "egpu_batch_solve")
+
+    def result(self, sid: int) -> dict:
+        r = _lib.Result()
+        check(lib().egpu_batch_result(self._h, sid, C.byref(r)), self.ctx.handle, "egpu_batch_result")
+        out = r.as_dict()
+        out["status"] = _lib.HUTI.get(r.info, str(r.info))
+        return out
+
+    def solution(self, sid: int) -> np.ndarray:
+        x = np.zeros(self.n[sid])
+        check(lib().egpu_batch_solution(self._h, sid, x), self.ctx.handle, "egpu_batch_solution")
+        return x
+
+    def remove(self, sid: int):
+        check(lib().egpu_batch_remove(self._h, sid), self.ctx.handle, "egpu_batch_remove")
+        self.n.pop(sid, None)
+        self._borrowed.pop(sid, None)
+
+    def free(self):
+        if self._h and self.ctx._h:
+            lib().egpu_batch_free(self._h)
+        self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

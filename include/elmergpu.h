@@ -168,17 +168,31 @@ int egpu_cg_noalloc(int device, int n, const int *rows_dev, const int *cols_dev,
                     const double *values_dev, const double *b_dev, double *x_dev, const egpu_params *prm,
                     egpu_result *res);
 
-/* ---- batched solve: many independent systems in one persistent launch ------------
- * Systems are appended with their own CRS/RHS; egpu_batch_solve runs them all with
- * one cooperative kernel and per-system convergence masks. */
+/* ---- batched / continuous-batching solve (no counterpart in the reference; extends
+ * SolveSystem to many independent systems).  Every system is scaled and preconditioned
+ * like egpu_iter_solve and solved in mixed precision (FP32 inner Krylov, FP64 iterative
+ * refinement to prm->tol on the true residual); all resident systems share one persistent
+ * launch per chunk of inner iterations, with per-system convergence masks.
+ *   egpu_batch_create   parameters are fixed for the batch (method, preconditioner, tol...)
+ *   egpu_batch_add      host Matrix_t arrays + rhs; the batch owns the device copy
+ *   egpu_batch_add_matrix  a bound/assembled matrix (b_dev NULL: its assembled rhs); borrowed
+ *   egpu_batch_step     one refinement check + one chunk; lists the systems that finished
+ *   egpu_batch_solve    steps until every resident system has finished
+ *   egpu_batch_remove   frees a finished system's slot
+ * Returns the slot id (>= 0) from the add calls, EGPU_ERR_BUDGET when all slots are used. */
 typedef struct egpu_batch egpu_batch;
-int egpu_batch_create(egpu_ctx *ctx, egpu_batch **out);
-/* returns the system id (>= 0) or an error */
+int egpu_batch_create(egpu_ctx *ctx, const egpu_params *prm, egpu_batch **out);
 int egpu_batch_add(egpu_batch *B, int n, const int *rows, const int *cols, const int *diag,
                    const double *values, const double *rhs);
-int egpu_batch_solve(egpu_batch *B, const egpu_params *prm, egpu_result *per_system);
+int egpu_batch_add_matrix(egpu_batch *B, egpu_mat *A, const double *b_dev);
+int egpu_batch_set_chunk(egpu_batch *B, int chunk_iters);
+int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished);
+int egpu_batch_pending(egpu_batch *B);
+int egpu_batch_solve(egpu_batch *B, egpu_result *per_system);
+int egpu_batch_result(egpu_batch *B, int sys, egpu_result *res);
 int egpu_batch_solution(egpu_batch *B, int sys, double *x);
-int egpu_batch_tune(egpu_batch *B, const egpu_params *prm, int *lanes_per_row_out);
+int egpu_batch_remove(egpu_batch *B, int sys);
+int egpu_batch_tune(egpu_batch *B, int *chunk_out);
 void egpu_batch_free(egpu_batch *B);
 
 #ifdef __cplusplus
