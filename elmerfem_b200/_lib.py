@@ -68,6 +68,8 @@ PROTOTYPES = {
     "egpu_matrix_values_download": (C.c_int, [_vp, _f64p]),
     "egpu_matrix_rhs_download": (C.c_int, [_vp, _f64p]),
     "egpu_matrix_free": (None, [_vp]),
+    "egpu_matrix_clone": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "egpu_matrix_footprint": (C.c_longlong, [_vp, C.c_int]),
     "egpu_iter_solve": (C.c_int, [_vp, _f64p, _f64p, C.POINTER(Params), C.POINTER(Result)]),
     "egpu_iter_solve_dev": (C.c_int, [_vp, _vp, _vp, C.POINTER(Params), C.POINTER(Result)]),
     "egpu_mv": (C.c_int, [_vp, _f64p, _f64p]),

@@ -1197,7 +1197,94 @@ extern "C" void egpu_matrix_free(egpu_mat *A) {
   if (!A) return;
   cudaSetDevice(A->ctx->device);
   cudaStreamSynchronize(A->ctx->stream);
+  if (A->clones > 0) {  // clones still view this pattern
+    A->free_pending = true;
+    return;
+  }
+  egpu_mat *parent = A->parent;
   delete A;
+  if (parent && --parent->clones == 0 && parent->free_pending) delete parent;
+}
+
+// A matrix with the prototype's pattern, SELL layout, level orders and assembly data
+// (shared, read-only) and its own values, right-hand side and solve buffers: the matrix
+// structure of one mesh reused across solves, as Elmer keeps Solver % Matrix across steps.
+extern "C" int egpu_matrix_clone(egpu_mat *proto, egpu_mat **out) {
+  if (!proto || !out) return EGPU_ERR_ARG;
+  egpu_ctx *ctx = proto->ctx;
+  cudaSetDevice(ctx->device);
+  if (proto->parent) proto = proto->parent;
+  auto *A = new egpu_mat;
+  A->ctx = ctx;
+  A->n = proto->n;
+  A->nnz = proto->nnz;
+  A->max_row = proto->max_row;
+  A->max_bandwidth = proto->max_bandwidth;
+  A->rows.view(proto->rows);
+  A->cols.view(proto->cols);
+  A->diag.view(proto->diag);
+  A->nslices = proto->nslices;
+  A->sell_nnz = proto->sell_nnz;
+  A->ldw = proto->ldw;
+  A->sell_ptr.view(proto->sell_ptr);
+  A->sell_w.view(proto->sell_w);
+  A->sell_cols.view(proto->sell_cols);
+  A->sell_c16.view(proto->sell_c16);
+  if (proto->cols16.p) A->cols16.view(proto->cols16);
+  if (!proto->tri_built) {
+    int rc = ensure_tri_schedule(proto);
+    if (rc) {
+      delete A;
+      return rc;
+    }
+  }
+  A->tri.lower_order.view(proto->tri.lower_order);
+  A->tri.upper_order.view(proto->tri.upper_order);
+  A->tri.lower_levels = proto->tri.lower_levels;
+  A->tri.upper_levels = proto->tri.upper_levels;
+  A->tri.max_lower = proto->tri.max_lower;
+  A->tri.max_upper = proto->tri.max_upper;
+  A->tri.max_width = proto->tri.max_width;
+  A->tri_built = true;
+  const AssemblyData &P = proto->asmb;
+  AssemblyData &S = A->asmb;
+  S.nnodes = P.nnodes;
+  S.nelem = P.nelem;
+  S.nen = P.nen;
+  S.code = P.code;
+  S.dofs = P.dofs;
+  S.cdim = P.cdim;
+  S.color_ptr = P.color_ptr;
+  if (P.bound) {
+    S.xyz.view(P.xyz);
+    S.elem_nodes.view(P.elem_nodes);
+    S.perm.view(P.perm);
+    S.color_elems.view(P.color_elems);
+    S.slots.view(P.slots);
+    S.bound = true;
+  }
+  cudaError_t e;
+  if ((e = A->values.alloc(A->nnz)) || (e = A->rhs.alloc(A->n))) {
+    egpu_set_error(ctx, std::string("egpu_matrix_clone: ") + cudaGetErrorString(e));
+    delete A;
+    return EGPU_ERR_ALLOC;
+  }
+  A->parent = proto;
+  proto->clones++;
+  *out = A;
+  return EGPU_OK;
+}
+
+// device bytes a solve of this matrix holds (values, scaled and FP32 copies, factors,
+// work vectors), excluding the shared pattern: the admission footprint
+extern "C" long long egpu_matrix_footprint(const egpu_mat *A, int precond) {
+  if (!A) return EGPU_ERR_ARG;
+  const long long z = A->nnz, zs = A->sell_nnz, n = A->n, l = A->ldw;
+  long long b = 8 * z + 8 * n;              // values, rhs
+  b += 8 * z + 8 * zs + 4 * zs;             // scaled CRS, SELL FP64, SELL FP32
+  b += 8 * n + 13 * 8 * l + 14 * 4 * l;     // DiagScaling, work vectors
+  if (precond == EGPU_PREC_ILU0) b += 8 * z + 4 * z + 4 * n;  // ILU0 FP64/FP32, flags
+  return b + 8 * n;                         // back-scaled solution
 }
 
 static int check_params(const egpu_params *p) {

@@ -52,14 +52,22 @@ template <typename T>
 struct DevBuf {
   T *p = nullptr;
   size_t n = 0;
+  bool owned = true;  // false: a view of another object's buffer (matrix clones)
   DevBuf() = default;
   DevBuf(const DevBuf &) = delete;
   DevBuf &operator=(const DevBuf &) = delete;
   ~DevBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p && owned) cudaFree(p);
     p = nullptr;
     n = 0;
+    owned = true;
+  }
+  void view(const DevBuf &o) {
+    release();
+    p = o.p;
+    n = o.n;
+    owned = false;
   }
   cudaError_t alloc(size_t count) {
     if (count == n && p) return cudaSuccess;
@@ -141,6 +149,10 @@ struct egpu_mat {
   DevBuf<float> work32;
   DevBuf<double> bx;             // scratch b/x for host-pointer entry points
   AssemblyData asmb;
+  // clones share this matrix's pattern: it is deleted when its last clone goes
+  egpu_mat *parent = nullptr;
+  int clones = 0;
+  bool free_pending = false;
 };
 
 // ------------------------------------------------------------------------------------

@@ -188,6 +188,19 @@ class Matrix:
               ctx.handle, "egpu_matrix_bind")
         ctx._children.add(self)
 
+    @classmethod
+    def clone(cls, proto: "Matrix") -> "Matrix":
+        """A matrix sharing proto's pattern and bound mesh, with its own values (egpu_matrix_clone)."""
+        obj = cls.__new__(cls)
+        obj.ctx, obj.pattern, obj.n, obj.nnz = proto.ctx, proto.pattern, proto.n, proto.nnz
+        obj._h = C.c_void_p()
+        check(lib().egpu_matrix_clone(proto.handle, C.byref(obj._h)), proto.ctx.handle, "egpu_matrix_clone")
+        proto.ctx._children.add(obj)
+        return obj
+
+    def footprint(self, precond: int) -> int:
+        return int(lib().egpu_matrix_footprint(self._h, precond))
+
     @property
     def handle(self):
         return self._h

@@ -105,6 +105,13 @@ int egpu_matrix_update_values(egpu_mat *A, const double *values);
 int egpu_matrix_values_download(egpu_mat *A, double *values);
 int egpu_matrix_rhs_download(egpu_mat *A, double *rhs);
 void egpu_matrix_free(egpu_mat *A);
+/* No counterpart in the reference's C interface (Elmer reuses Solver % Matrix across steps):
+ * a matrix sharing proto's pattern, SELL layout, level orders and bound mesh (read-only)
+ * with its own Values, right-hand side and solve buffers.  proto may be freed before its
+ * clones; the shared data goes with the last of them. */
+int egpu_matrix_clone(egpu_mat *proto, egpu_mat **out);
+/* device bytes a solve of A holds beyond the shared pattern, for the given preconditioner */
+long long egpu_matrix_footprint(const egpu_mat *A, int precond);
 
 /* ---- IterSolver replacement (SolveLinearSystem semantics, SolverUtils.src:7151-7525):
  * zero-rhs short cut, symmetric scaling, x = 1e-8 when x is all zero, ILU0 factored on
