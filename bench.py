@@ -54,6 +54,14 @@ def workload_spec(name):
         return build, dict(method=1, precond=1, tol=1e-10, max_iter=20000), \
             {"workload": "poisson_hex96_lognormal_cg_jacobi", "mesh": "96^3 hex 808", "dofs": 912673,
              "method": "CG", "preconditioner": "Diagonal", "tol": 1e-10}
+    if name == "elastic64_bicgstab_ilu0":
+        def build():
+            m = meshgen.hex_cube(64)
+            return dict(mesh=m, elastic=True, bc=[1], symmetric=False)
+        return build, dict(method=2, precond=2, tol=1e-8, max_iter=20000), \
+            {"workload": "elasticity_hex64_bicgstab_ilu0", "mesh": "64^3 hex 808, 3 DOFs/node", "dofs": 823875,
+             "method": "BiCGStab", "preconditioner": "ILU0", "tol": 1e-8, "E": 200e9, "nu": 0.3,
+             "body_force": [0, 0, -1e4]}
     if name == "poisson32_bicgstab_ilu0":
         def build():
             m = meshgen.hex_cube(32)
@@ -169,7 +177,7 @@ def barrier(pg, device):
     if pg is not None:
         import torch
 
-        pg.all_reduce(torch.zeros(1, device=device))
+        pg.all_reduce(torch.zeros(1, device=device if device is not None else "cuda"))
 
 
 def read_peaks():
@@ -253,12 +261,18 @@ def run_gpu(args, rank, world, local, pg):
     build, solve_kw, cfg = workload_spec(args.workload)
     w = build()
     m = w["mesh"]
-    pat = eg.create_matrix(m)
+    dofs = 3 if w.get("elastic") else 1
+    pat = eg.create_matrix(m, dofs=dofs)
     A = eg.Matrix(ctx, pat)
     A.bind_assembly(m)
-    nodal_k = None if w["elem_k"] is not None else np.ones(m.nnodes)
-    A.assemble_poisson(elem_k=w["elem_k"], nodal_k=nodal_k, load=w["load"])
-    con = np.sort(pat.perm[m.boundary_nodes(w["bc"]) - 1]).astype(np.int32)
+    if w.get("elastic"):
+        A.assemble_elastic(200e9, 0.3, (0.0, 0.0, -1e4))
+        nodes = pat.perm[m.boundary_nodes(w["bc"]) - 1]
+        con = np.sort(np.concatenate([3 * (nodes - 1) + d for d in (1, 2, 3)])).astype(np.int32)
+    else:
+        nodal_k = None if w["elem_k"] is not None else np.ones(m.nnodes)
+        A.assemble_poisson(elem_k=w["elem_k"], nodal_k=nodal_k, load=w["load"])
+        con = np.sort(pat.perm[m.boundary_nodes(w["bc"]) - 1]).astype(np.int32)
     A.dirichlet(con, symmetric=w["symmetric"])
     n, nnz = pat.n, pat.nnz
     cols16 = True  # every structured workload here has |col-row| < 32768
@@ -357,7 +371,7 @@ def run_gpu(args, rank, world, local, pg):
 
         vals = A.values()
         rhs = A.rhs()
-        op = oracle.Pattern(n, nnz, 1, pat.perm, pat.rows, pat.cols, pat.diag, 0, 0, 0, 0)
+        op = oracle.Pattern(n, nnz, dofs, pat.perm, pat.rows, pat.cols, pat.diag, 0, 0, 0, 0)
         threads = os.cpu_count() or 1
         rate, info = cpu_solve_rate(op, vals, rhs, solve_kw, rr["iters"], threads)
         cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
@@ -391,6 +405,158 @@ def run_gpu(args, rank, world, local, pg):
     ctx.close()
 
 
+# ------------------------------------------------------------------------------------- batch (C4)
+def run_batch(args, rank, world, local, pg):
+    """512 independent tet Poisson systems (m log-uniform in [8, 60]) in one batched mixed solve."""
+    import torch
+
+    import elmerfem_b200 as eg
+    from elmerfem_b200 import meshgen
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ctx = eg.Context(local)
+    ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    nsys = args.systems
+    rng = np.random.Generator(np.random.PCG64(1))
+    ms = np.clip(np.floor(np.exp(rng.uniform(np.log(8), np.log(61), size=nsys))).astype(int), 8, 60)
+    protos, mats, bs = {}, [], []
+    for i, m in enumerate(ms):
+        if m not in protos:
+            mesh = meshgen.tet_cube(int(m))
+            pat = eg.create_matrix(mesh)
+            P = eg.Matrix(ctx, pat)
+            P.bind_assembly(mesh)
+            con = np.sort(pat.perm[mesh.boundary_nodes(range(1, 7)) - 1]).astype(np.int32)
+            protos[m] = (mesh, P, con)
+        mesh, P, con = protos[m]
+        A = eg.Matrix.clone(P)
+        k = meshgen.lognormal_conductivity(mesh.nelem, 0.5, 1000 + i)
+        A.assemble_poisson(elem_k=k, load=None)
+        A.dirichlet(con, symmetric=True)
+        b = np.random.Generator(np.random.PCG64(5000 + i)).random(A.n)
+        b[con - 1] = 0.0
+        mats.append(A)
+        bs.append(torch.from_numpy(b).to(dev))
+    torch.cuda.synchronize()
+    ndofs = int(sum(A.n for A in mats))
+    nnz = int(sum(A.nnz for A in mats))
+    prm = eg.SolverParams(method=eg.CG, precond=eg.PREC_DIAGONAL, tol=args.tol, max_iter=20000,
+                          inner_tol=args.inner_tol)
+
+    def batch_step():
+        B = eg.Batch(ctx, prm, chunk=args.chunk)
+        ids = [B.add_matrix(A, b.data_ptr()) for A, b in zip(mats, bs)]
+        B.solve()
+        res = [B.result(i) for i in ids]
+        return B, ids, res
+
+    for _ in range(args.warmup):
+        B, _, _ = batch_step()
+        B.free()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = ctx.kernel_launches
+    barrier(pg, dev)
+    torch.cuda.synchronize()
+    times, allres = [], None
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            e0.record(ext)
+            B, ids, res = batch_step()
+            e1.record(ext)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1) / 1000.0)
+            if allres is None:
+                allres = res
+                xs_b = [B.solution(i) for i in ids]
+            B.free()
+    launches = ctx.kernel_launches - launches0
+    t = reduce_max(pg, sum(times), dev)
+    value = world * nsys * args.steps / t
+    # FP64 drop-in one system at a time on the same systems
+    fp = eg.SolverParams(method=eg.CG, precond=eg.PREC_DIAGONAL, tol=args.tol, max_iter=20000)
+    x = torch.zeros(max(A.n for A in mats), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    e0.record(ext)
+    errs, it64 = [], 0
+    for j, (A, b) in enumerate(zip(mats, bs)):
+        xv = x[:A.n]
+        with torch.cuda.stream(ext):
+            xv.zero_()
+        r = A.solve_dev(b.data_ptr(), xv.data_ptr(), fp)
+        it64 += r["iters"]
+        errs.append(float(np.linalg.norm(xs_b[j] - xv.cpu().numpy()) / np.linalg.norm(xv.cpu().numpy())))
+    e1.record(ext)
+    torch.cuda.synchronize()
+    t64 = e0.elapsed_time(e1) / 1000.0
+    peak, peak_kind = read_peaks()
+    inner_iters = sum(r["iters"] for r in allres)
+    bpi = sum(algorithmic_bytes_per_iter(1, 1, "mixed", A.n, A.nnz, True) * r["iters"] for A, r in zip(mats, allres))
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1000 * t / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 refinement", "data": "synthetic",
+                "config": {"workload": "batched_tet_poisson_512_cg_jacobi", "systems": nsys, "dofs_total": ndofs,
+                           "nnz_total": nnz, "m_range": [8, 60], "method": "CG", "preconditioner": "Diagonal",
+                           "tol": args.tol, "precision": "mixed", "parallelism": f"replicas{world}",
+                           "l2": "working set larger than L2"},
+                "fp64_one_at_a_time": {"solves_per_s": nsys / t64, "seconds": t64, "iters_total": it64},
+                "speedup_batched_mixed_vs_fp64": value / world / (nsys / t64),
+                "rel_err_vs_fp64_max": max(errs), "iterations": {"inner_total": inner_iters},
+                "roofline": {"bound": "hbm", "achieved": bpi / (t / args.steps) / 1e9, "peak": peak,
+                             "unit": "GB/s", "frac": bpi / (t / args.steps) / 1e9 / peak, "traffic": None,
+                             "peak_kind": peak_kind, "kernel": "k_batch_inner (whole step incl. refinement)"},
+                "e2e": None, "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": None}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+# ------------------------------------------------------------------------------------- serving (C5)
+def run_serve(args, rank, world, local, pg):
+    """Poisson-process request stream (200 req/s) of hex Poisson solves, m log-uniform in [16, 128]."""
+    import torch
+
+    import elmerfem_b200 as eg
+    from elmerfem_b200 import server
+
+    torch.cuda.set_device(local)
+    ctx = eg.Context(local)
+    prm = eg.SolverParams(method=eg.BICGSTAB, precond=eg.PREC_ILU0, tol=args.tol, max_iter=20000,
+                          inner_tol=args.inner_tol, abort_not_converged=False)
+    reqs = server.poisson_stream(args.requests, rate=args.rate, m_lo=16, m_hi=128, seed=1 + rank, sigma=1.0)
+    srv = server.SolveServer(ctx, prm, hbm_budget=150e9, chunk=args.chunk)
+    for r in reqs:
+        srv.prototype(r.m)
+    warm = server.poisson_stream(4, rate=1e6, m_lo=16, m_hi=24, seed=99, sigma=1.0)
+    for r in warm:
+        srv.prototype(r.m)
+    srv.run(warm)
+    barrier(pg, None)
+    with ClockSampler(local) as clk:
+        stats = srv.run(reqs, keep_solutions=True)
+    alone = [server.Request(r.rid, r.m, r.seed, r.arrival) for r in reqs]
+    fp = eg.SolverParams(method=eg.BICGSTAB, precond=eg.PREC_ILU0, tol=args.tol, max_iter=20000)
+    stats64 = server.run_one_at_a_time(ctx, fp, alone, srv.protos, keep_solutions=True)
+    errs = [float(np.linalg.norm(r.x - a.x) / np.linalg.norm(a.x)) for r, a in zip(reqs, alone)]
+    if rank == 0:
+        line = {"metric": METRIC, "value": stats["solves_per_s"] * world, "unit": UNIT, "n_gpus": world,
+                "steps": len(reqs), "warmup": len(warm), "ms_per_step": 1000.0 / stats["solves_per_s"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 inner / f64 refinement", "data": "synthetic",
+                "config": {"workload": "serving_hex_poisson_bicgstab_ilu0", "requests": len(reqs),
+                           "rate_per_s": args.rate, "m_range": [16, 128], "hbm_budget_gb": 150,
+                           "method": "BiCGStab", "preconditioner": "ILU0", "tol": args.tol, "precision": "mixed",
+                           "parallelism": f"replicas{world}"},
+                "latency_ms": {"p50": stats["p50_ms"], "p99": stats["p99_ms"]},
+                "serving": stats, "fp64_one_at_a_time": stats64,
+                "speedup_vs_fp64_one_at_a_time": stats["solves_per_s"] / stats64["solves_per_s"],
+                "rel_err_vs_fp64_max": max(errs), "e2e": {"value": stats["solves_per_s"] * world, "unit": UNIT,
+                                                         "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+                "gpu_launches": None, "clocks": clk.summary(), "cpu_baseline": None}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -402,6 +568,11 @@ def main():
     ap.add_argument("--inner-tol", type=float, default=3e-4)
     ap.add_argument("--ref-iters", type=int, default=0, help="FP64 iteration count for the reference arm")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--systems", type=int, default=512, help="batched workload: number of systems")
+    ap.add_argument("--requests", type=int, default=48, help="serving workload: number of requests")
+    ap.add_argument("--rate", type=float, default=200.0, help="serving workload: mean arrivals per second")
+    ap.add_argument("--chunk", type=int, default=32, help="batched/serving: inner iterations per launch")
+    ap.add_argument("--tol", type=float, default=1e-10)
     args = ap.parse_args()
     rank, world, local, pg = dist_setup(args.gpus)
     try:
@@ -409,6 +580,10 @@ def main():
             if args.ref_iters <= 0:
                 args.ref_iters = {"poisson128_cg_jacobi": 2000, "poisson32_bicgstab_ilu0": 19}.get(args.workload, 100)
             run_reference(args, rank, world, pg)
+        elif args.workload == "batch512_tet_cg_jacobi":
+            run_batch(args, rank, world, local, pg)
+        elif args.workload == "serve_hex_bicgstab_ilu0":
+            run_serve(args, rank, world, local, pg)
         else:
             run_gpu(args, rank, world, local, pg)
     finally:
