@@ -120,9 +120,34 @@ __device__ __forceinline__ float slice_spmv(const SysDesc &d, int slice, int lan
   return s;
 }
 
-// sync-free ILU0 solves over the systems in RUN state, slots interleaved across systems:
-// slot q -> system act[q % nact], position q / nact of its level order (dependencies of a
-// row sit at smaller positions of the same system, hence at smaller slots)
+// Sync-free ILU0 solves of all systems in RUN state.  Every such system gets its own group
+// of participant warps, sized by its row count (at least one); inside a group the
+// system's slots are taken in level order, slot s by member s mod G, with the next slot's
+// packed entries fetched while the current one waits.  A row's dependencies are earlier
+// slots of its own group's members, all resident: deadlock free.
+__device__ void batch_tri_groups(const BatchArgs &a, BatchShared &sh) {
+  // weights n_s + ceil(W/P): every RUN system gets at least one participant
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    long long tot = 0;
+    for (int c = 0; c < sh.nact; c += 32) {
+      const int t = c + lane;
+      long long w = 0;
+      if (t < sh.nact && sh.status[sh.act[t]] == ST_RUN) w = a.sys[sh.act[t]].n;
+      long long v = w;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const long long u = __shfl_up_sync(0xffffffffu, v, off);
+        if (lane >= off) v += u;
+      }
+      if (t < sh.nact) sh.tcum[t + 1] = tot + v;
+      tot += __shfl_sync(0xffffffffu, v, 31);
+    }
+    if (lane == 0) sh.tcum[0] = 0;
+  }
+  __syncthreads();
+}
+
 template <bool LOWER, typename RHS, typename OUT>
 __device__ __forceinline__ void batch_tri(const BatchArgs &a, const BatchShared &sh, int yoff, int zoff, RHS &&rhs,
                                           OUT &&out) {
@@ -130,47 +155,64 @@ __device__ __forceinline__ void batch_tri(const BatchArgs &a, const BatchShared 
   if (local >= a.tri_warps_per_block) return;
   const int lane = threadIdx.x & 31;
   const int P = a.tri_warps_per_block * gridDim.x;
-  const int id = local * gridDim.x + blockIdx.x;
-  int maxn = 0;
-  for (int t = 0; t < sh.nact; ++t) maxn = max(maxn, a.sys[sh.act[t]].n);
-  const long long nslot = (long long)maxn * sh.nact;
-  for (long long q = id; q < nslot; q += P) {
-    const int ai = (int)(q % sh.nact);
-    const int pos = (int)(q / sh.nact);
-    const int s = sh.act[ai];
-    if (sh.status[s] != ST_RUN) continue;
-    const SysDesc &d = a.sys[s];
-    if (pos >= d.n) continue;
-    const int i = LOWER ? __ldg(d.lower_order + pos) : __ldg(d.upper_order + pos);
-    float *y = d.w + yoff * d.ldw;
-    int beg, end;
-    float dinv = 0.f;
-    if (LOWER) {
-      beg = __ldg(d.rows + i);
-      end = __ldg(d.diag + i);
-    } else {
-      const int dg = __ldg(d.diag + i);
-      beg = dg + 1;
-      end = __ldg(d.rows + i + 1);
-      dinv = __ldg(d.ilu + dg);
+  const int p = local * gridDim.x + blockIdx.x;
+  const long long W = sh.tcum[sh.nact];
+  if (W == 0) return;
+  // group boundaries b(t) = floor(t_weight * P / W') with W' = W + nrun*ceil(W/P) folded in by
+  // giving each RUN system an extra share: boundary(t) = floor((tcum[t] + t_run*e) * P / (W + nrun*e))
+  int nrun = 0;
+  for (int t = 0; t < sh.nact; ++t) nrun += sh.status[sh.act[t]] == ST_RUN;
+  const long long e = (W + P - 1) / P;
+  const long long Wp = W + (long long)nrun * e;
+  // run-count prefix is needed per boundary: recompute on the fly in the search
+  auto boundary = [&](int t) -> long long {
+    int r = 0;
+    for (int u = 0; u < t; ++u) r += sh.status[sh.act[u]] == ST_RUN;
+    return (sh.tcum[t] + (long long)r * e) * P / Wp;
+  };
+  int lo = 0, hi = sh.nact - 1;
+  while (lo < hi) {  // last t with boundary(t) <= p
+    const int mid = (lo + hi + 1) >> 1;
+    if (boundary(mid) <= p)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const int ai = lo;
+  const int s = sh.act[ai];
+  if (sh.status[s] != ST_RUN) return;
+  const long long g0 = boundary(ai), g1 = boundary(ai + 1);
+  const int G = (int)(g1 - g0), j = (int)(p - g0);
+  if (G <= 0 || j < 0 || j >= G) return;
+  const SysDesc &d = a.sys[s];
+  const int *order = LOWER ? d.lower_order : d.upper_order;
+  const int *ptr = LOWER ? d.lo_ptr : d.up_ptr;
+  const int *cols = LOWER ? d.lo_cols : d.up_cols;
+  const float *vals = LOWER ? d.lo_vals : d.up_vals;
+  float *y = d.w + yoff * d.ldw, *z = d.w + zoff * d.ldw;
+  if (j >= d.n) return;
+  TriRow<float> nxt;
+  tri_fetch(nxt, j, order, ptr, cols, vals, lane, d.n, a.err);
+  float dnext = LOWER ? 0.f : __ldg(d.up_dinv + j);
+  for (int q = j; q < d.n; q += G) {
+    const TriRow<float> cur = nxt;
+    const float dinv = dnext;
+    if (q + G < d.n) {
+      tri_fetch(nxt, q + G, order, ptr, cols, vals, lane, d.n, a.err);
+      if (!LOWER) dnext = __ldg(d.up_dinv + q + G);
     }
+    if (cur.row < 0) continue;
     float r = 0.f;
-    if (LOWER && lane == 0) r = rhs(ai, s, d, i);
-    float acc = 0.f;
-    for (int j = beg + lane; j < end; j += 32) {
-      const float l = __ldg(d.ilu + j);
-      const int c = __ldg(d.cols + j);
-      acc += l * Sentinel<float>::wait((LOWER ? y : d.w + zoff * d.ldw) + c, a.err);
-    }
-    acc = warp_sum(acc);
+    if (LOWER && lane == 0) r = rhs(ai, s, d, cur.row);
+    const float acc = tri_dot(cur, LOWER ? y : z, cols, vals, lane, a.err);
     if (lane == 0) {
       if (LOWER) {
-        Sentinel<float>::publish(y + i, r - acc);
+        Sentinel<float>::publish(y + cur.row, r - acc);
       } else {
-        const float yi = Sentinel<float>::wait(y + i, a.err);
+        const float yi = Sentinel<float>::wait(y + cur.row, a.err);
         const float zi = dinv * (yi - acc);
-        Sentinel<float>::publish(d.w + zoff * d.ldw + i, zi);
-        out(ai, s, d, i, zi);
+        Sentinel<float>::publish(z + cur.row, zi);
+        out(ai, s, d, cur.row, zi);
       }
     }
   }
@@ -260,6 +302,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       ++it;
       break;
     }
+    if (ilu) batch_tri_groups(a, sh);
     if (!bicg) {
       // ============ CG ============
       // U: P = Z (k == 1) or Z + beta P;  clear PQ
@@ -734,6 +777,13 @@ static int batch_prepare(egpu_batch *B, int slot, const double *b_dev) {
   d.diag = A->diag.p;
   d.lower_order = A->tri.lower_order.p;
   d.upper_order = A->tri.upper_order.p;
+  d.lo_ptr = A->tri.lo_ptr.p;
+  d.lo_cols = A->tri.lo_cols.p;
+  d.up_ptr = A->tri.up_ptr.p;
+  d.up_cols = A->tri.up_cols.p;
+  d.lo_vals = A->lo_vals32.p;
+  d.up_vals = A->up_vals32.p;
+  d.up_dinv = A->up_dinv32.p;
   d.w = A->work32.p;
   d.ldw = ldw32;
   d.b = A->work32.p + 10 * ldw32;
@@ -919,7 +969,9 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
     int nrun = 0;
     for (int i = 0; i < ns; ++i)
       if (B->sys[i] && B->sys[i]->phase == 2) nrun++;
-    a.tri_warps_per_block = std::max(1, std::min(EGPU_BLOCK / 32, (B->tri_mult * maxw * nrun + grid - 1) / grid));
+    a.tri_warps_per_block = std::max((nrun + grid - 1) / grid,
+                                     std::min(EGPU_BLOCK / 32, (B->tri_mult * maxw * nrun + grid - 1) / grid));
+    a.tri_warps_per_block = std::max(1, std::min(EGPU_BLOCK / 32, a.tri_warps_per_block));
     a.bar = ctx->sync.p;
     a.err = (int *)(ctx->sync.p + 1);
     a.it_done = B->d_it.p;

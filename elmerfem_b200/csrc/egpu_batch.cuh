@@ -37,6 +37,8 @@ struct SysDesc {
   const int *scols;        // absolute column (when scols16 is null)
   const float *svals, *dvals, *ilu;
   const int *rows, *cols, *diag, *lower_order, *upper_order;
+  const int *lo_ptr, *lo_cols, *up_ptr, *up_cols;   // ILU0 factors packed in solve order
+  const float *lo_vals, *up_vals, *up_dinv;
   float *w;                // work vectors, stride ldw
   long long ldw;
   const float *b;          // inner right-hand side (r / ||r||)
@@ -73,6 +75,7 @@ struct BatchShared {
   int kk[BATCH_MAX_SYS];
   float sa[BATCH_MAX_SYS], sb[BATCH_MAX_SYS];  // per-phase scalars (beta, alpha, omega)
   double red[BATCH_MAX_SYS * 2];               // per-block per-system accumulators
+  long long tcum[BATCH_MAX_SYS + 1];           // weights of the triangular-solve groups
   int nact, total;
 };
 

@@ -230,6 +230,31 @@ __global__ void __launch_bounds__(256) k_ilu0_factor(int n, const int *__restric
   }
 }
 
+// ILU0 factors gathered into solve (slot) order, FP64 and FP32
+__global__ void k_pack_tri(long long nl, long long nu, int n, const int *__restrict__ lo_src,
+                           const int *__restrict__ up_src, const int *__restrict__ up_dsrc,
+                           const double *__restrict__ ilu, double *lo, double *up, double *dinv, float *lo32,
+                           float *up32, float *dinv32) {
+  const long long tot = nl + nu + n;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+    if (t < nl) {
+      const double v = ilu[lo_src[t]];
+      lo[t] = v;
+      lo32[t] = (float)v;
+    } else if (t < nl + nu) {
+      const long long k = t - nl;
+      const double v = ilu[up_src[k]];
+      up[k] = v;
+      up32[k] = (float)v;
+    } else {
+      const long long k = t - nl - nu;
+      const double v = ilu[up_dsrc[k]];
+      dinv[k] = v;
+      dinv32[k] = (float)v;
+    }
+  }
+}
+
 // prescale the U diagonal (CRSMatrix.src:2359-2366)
 __global__ void k_ilu_invdiag(int n, const int *__restrict__ diag, double *ilu) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -418,6 +443,53 @@ int ensure_tri_schedule(egpu_mat *A) {
   EGPU_CUDA_TRY(ctx, A->tri.upper_order.alloc(n));
   EGPU_CUDA_TRY(ctx, cudaMemcpy(A->tri.lower_order.p, lo.data(), n * sizeof(int), cudaMemcpyHostToDevice));
   EGPU_CUDA_TRY(ctx, cudaMemcpy(A->tri.upper_order.p, up.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+  {
+    // packed strictly-lower / strictly-upper parts in slot order
+    std::vector<int> lp(n + 1, 0), upp(n + 1, 0), ud(n);
+    for (int q = 0; q < n; ++q) {
+      lp[q + 1] = lp[q] + (diag[lo[q]] - rows[lo[q]]);
+      upp[q + 1] = upp[q] + (rows[up[q] + 1] - diag[up[q]] - 1);
+      ud[q] = diag[up[q]];
+    }
+    std::vector<int> lc(std::max(1, lp[n])), ls(std::max(1, lp[n])), uc(std::max(1, upp[n])), us(std::max(1, upp[n]));
+    for (int q = 0; q < n; ++q) {
+      const int i = lo[q];
+      for (int j = rows[i], k = lp[q]; j < diag[i]; ++j, ++k) {
+        lc[k] = cols[j];
+        ls[k] = j;
+      }
+      const int u = up[q];
+      for (int j = diag[u] + 1, k = upp[q]; j < rows[u + 1]; ++j, ++k) {
+        uc[k] = cols[j];
+        us[k] = j;
+      }
+    }
+    for (size_t k = 0; k < (size_t)lp[n]; ++k)
+      if (lc[k] < 0 || lc[k] >= n || ls[k] < 0 || ls[k] >= A->nnz) {
+        egpu_set_error(ctx, "internal: packed lower factor out of range");
+        return EGPU_ERR_ARG;
+      }
+    for (size_t k = 0; k < (size_t)upp[n]; ++k)
+      if (uc[k] < 0 || uc[k] >= n || us[k] < 0 || us[k] >= A->nnz) {
+        egpu_set_error(ctx, "internal: packed upper factor out of range");
+        return EGPU_ERR_ARG;
+      }
+    TriSchedule &T = A->tri;
+    EGPU_CUDA_TRY(ctx, T.lo_ptr.alloc(n + 1));
+    EGPU_CUDA_TRY(ctx, T.up_ptr.alloc(n + 1));
+    EGPU_CUDA_TRY(ctx, T.up_dsrc.alloc(n));
+    EGPU_CUDA_TRY(ctx, T.lo_cols.alloc(lc.size()));
+    EGPU_CUDA_TRY(ctx, T.lo_src.alloc(ls.size()));
+    EGPU_CUDA_TRY(ctx, T.up_cols.alloc(uc.size()));
+    EGPU_CUDA_TRY(ctx, T.up_src.alloc(us.size()));
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(T.lo_ptr.p, lp.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(T.up_ptr.p, upp.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(T.up_dsrc.p, ud.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(T.lo_cols.p, lc.data(), lc.size() * sizeof(int), cudaMemcpyHostToDevice));
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(T.lo_src.p, ls.data(), ls.size() * sizeof(int), cudaMemcpyHostToDevice));
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(T.up_cols.p, uc.data(), uc.size() * sizeof(int), cudaMemcpyHostToDevice));
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(T.up_src.p, us.data(), us.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
   A->tri_built = true;
   return EGPU_OK;
 }
@@ -456,10 +528,42 @@ int ilu0_factor(egpu_mat *A) {
                                           : (const void *)k_ilu0_factor<256>;
   EGPU_CUDA_TRY(ctx, cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(256), args, 0, ctx->stream));
   k_ilu_invdiag<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, A->diag.p, A->ilu.p);
-  ctx->launches += 2;
+  const long long nl = A->tri.lo_cols.n, nu = A->tri.up_cols.n;
+  EGPU_CUDA_TRY(ctx, A->lo_vals.alloc(nl));
+  EGPU_CUDA_TRY(ctx, A->up_vals.alloc(nu));
+  EGPU_CUDA_TRY(ctx, A->up_dinv.alloc(n));
+  EGPU_CUDA_TRY(ctx, A->lo_vals32.alloc(nl));
+  EGPU_CUDA_TRY(ctx, A->up_vals32.alloc(nu));
+  EGPU_CUDA_TRY(ctx, A->up_dinv32.alloc(n));
+  k_pack_tri<<<grid_for(ctx, nl + nu + n), 256, 0, ctx->stream>>>(
+      nl, nu, n, A->tri.lo_src.p, A->tri.up_src.p, A->tri.up_dsrc.p, A->ilu.p, A->lo_vals.p, A->up_vals.p,
+      A->up_dinv.p, A->lo_vals32.p, A->up_vals32.p, A->up_dinv32.p);
+  ctx->launches += 3;
   EGPU_CUDA_TRY(ctx, cudaGetLastError());
   A->ilu_valid = true;
   return EGPU_OK;
+}
+
+static void set_tri_vals(KArgs<double> &a, const egpu_mat *A) {
+  a.lo_vals = A->lo_vals.p;
+  a.up_vals = A->up_vals.p;
+  a.up_dinv = A->up_dinv.p;
+}
+static void set_tri_vals(KArgs<float> &a, const egpu_mat *A) {
+  a.lo_vals = A->lo_vals32.p;
+  a.up_vals = A->up_vals32.p;
+  a.up_dinv = A->up_dinv32.p;
+}
+
+template <typename VT>
+static void set_tri(KArgs<VT> &a, const egpu_mat *A) {
+  a.lower_order = A->tri.lower_order.p;
+  a.upper_order = A->tri.upper_order.p;
+  a.lo_ptr = A->tri.lo_ptr.p;
+  a.lo_cols = A->tri.lo_cols.p;
+  a.up_ptr = A->tri.up_ptr.p;
+  a.up_cols = A->tri.up_cols.p;
+  set_tri_vals(a, A);
 }
 
 template <typename VT>
@@ -548,8 +652,7 @@ int solve_fp64(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_param
   set_sell(a, A, A->sell_vals.p, false);
   a.ilu = A->ilu.p;
   a.dvals = dvals;
-  a.lower_order = A->tri.lower_order.p;
-  a.upper_order = A->tri.upper_order.p;
+  set_tri(a, A);
   a.precond = prm->precond;
   a.maxit = prm->max_iter;
   a.true_residual = 1;
@@ -699,8 +802,7 @@ int krylov_fp64_scaled(egpu_mat *A, const double *bs, double *xs, const egpu_par
   set_sell(a, A, A->sell_vals.p, false);
   a.ilu = A->ilu.p;
   a.dvals = A->work.p + (size_t)11 * A->ldw;
-  a.lower_order = A->tri.lower_order.p;
-  a.upper_order = A->tri.upper_order.p;
+  set_tri(a, A);
   a.precond = prm->precond;
   a.maxit = prm->max_iter;
   a.true_residual = 1;
@@ -854,8 +956,7 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
       set_sell(a, A, A->sell_vals32.p, A->sell_c16.p != nullptr);
       a.ilu = A->ilu32.p;
       a.dvals = dv32;
-      a.lower_order = A->tri.lower_order.p;
-      a.upper_order = A->tri.upper_order.p;
+      set_tri(a, A);
       a.precond = prm->precond;
       a.maxit = std::max(1, std::min(prm->inner_max_iter, prm->max_iter - r.iters));
       a.true_residual = 0;
@@ -934,8 +1035,7 @@ int lu_apply(egpu_mat *A, const double *v_dev, double *u_dev) {
   a.cols = A->cols.p;
   a.diag = A->diag.p;
   a.ilu = A->ilu.p;
-  a.lower_order = A->tri.lower_order.p;
-  a.upper_order = A->tri.upper_order.p;
+  set_tri(a, A);
   a.w = A->work.p;
   a.err = (int *)(ctx->sync.p + 1);
   a.tri_per_block = tri_per_block(A, TRI_TS, ctx->num_sms * 2);
@@ -1240,6 +1340,13 @@ extern "C" int egpu_matrix_clone(egpu_mat *proto, egpu_mat **out) {
   }
   A->tri.lower_order.view(proto->tri.lower_order);
   A->tri.upper_order.view(proto->tri.upper_order);
+  A->tri.lo_ptr.view(proto->tri.lo_ptr);
+  A->tri.lo_cols.view(proto->tri.lo_cols);
+  A->tri.lo_src.view(proto->tri.lo_src);
+  A->tri.up_ptr.view(proto->tri.up_ptr);
+  A->tri.up_cols.view(proto->tri.up_cols);
+  A->tri.up_src.view(proto->tri.up_src);
+  A->tri.up_dsrc.view(proto->tri.up_dsrc);
   A->tri.lower_levels = proto->tri.lower_levels;
   A->tri.upper_levels = proto->tri.upper_levels;
   A->tri.max_lower = proto->tri.max_lower;

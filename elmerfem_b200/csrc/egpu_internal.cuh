@@ -99,6 +99,9 @@ struct egpu_ctx {
 struct TriSchedule {
   // rows in the order the sync-free solve processes them (ascending dependency level)
   DevBuf<int> lower_order, upper_order;
+  // the strictly lower / upper entries of those rows packed in slot order: slot s owns
+  // [lo_ptr[s], lo_ptr[s+1]); *_src is the CRS position each packed entry comes from
+  DevBuf<int> lo_ptr, lo_cols, lo_src, up_ptr, up_cols, up_src, up_dsrc;
   int lower_levels = 0, upper_levels = 0;
   int max_lower = 0, max_upper = 0;  // longest strictly-lower / strictly-upper row part
   int max_width = 0;                 // most rows in one level (lower or upper)
@@ -130,6 +133,8 @@ struct egpu_mat {
   DevBuf<double> dscale;         // DiagScaling (times the rhs norm during a solve)
   DevBuf<double> ilu;            // ILU0 values on the scaled matrix, inverted U diagonal
   DevBuf<float> scaled32, ilu32; // FP32 copies for the mixed-precision inner solver
+  DevBuf<double> lo_vals, up_vals, up_dinv;        // ILU0 factors packed in solve order
+  DevBuf<float> lo_vals32, up_vals32, up_dinv32;
   DevBuf<int16_t> cols16;        // column offsets (col - row) when |col-row| < 32768
   DevBuf<int> ilu_done;          // factorisation completion flags
   // SELL-32 copy of the pattern (slice s = rows 32s..32s+31, entry (k, lane) at

@@ -42,6 +42,9 @@ struct KArgs {
   double *out_d;                  // [0] residual [1] rhsnorm
   const unsigned int *skip;       // bit 1 set: zero right-hand side, return at once
   int tri_per_block;              // sub-warps per block taking part in the triangular solves
+  // ILU0 factors packed in solve order (see TriSchedule)
+  const int *lo_ptr, *lo_cols, *up_ptr, *up_cols;
+  const VT *lo_vals, *up_vals, *up_dinv;
   // SELL-32 copy of the scaled matrix used by every SpMV of the Krylov loop
   int nslices;
   const int *sell_ptr, *sell_w, *scols;
@@ -163,55 +166,110 @@ __device__ __forceinline__ void spmv_phase(const KArgs<VT> &a, const VT *x0, con
 //
 // lower: y_i = rhs_i - sum_{j<i} L_ij y_j            (CRS_LUSolve forward, CRSMatrix.src:3346-3352)
 // upper: z_i = u_ii^-1 (y_i - sum_{j>i} U_ij z_j)     (backward, :3355-3362)
-template <typename VT, int TS, typename RHS>
-__device__ __forceinline__ void lower_solve(const KArgs<VT> &a, VT *y, RHS &&rhs) {
-  const int lane = threadIdx.x & 31;
-  const int sl = lane & (TS - 1);
-  const unsigned submask = (TS == 32) ? 0xffffffffu : (((1u << TS) - 1u) << (lane & ~(TS - 1)));
-  int gsub, nsub;
-  if (!tri_participant<TS>(a.tri_per_block, gsub, nsub)) return;
-  for (int s = gsub; s < a.n; s += nsub) {
-    const int i = __ldg(a.lower_order + s);
-    const int beg = __ldg(a.rows + i), end = __ldg(a.diag + i);
-    // the right-hand side does not depend on the solve: form it before waiting
-    VT r = 0;
-    if (sl == 0) r = rhs(i);
-    VT acc = 0;
-    for (int j = beg + sl; j < end; j += TS) {
-      const VT l = __ldg(a.ilu + j);
-      const int c = __ldg(a.cols + j);
-      acc += l * Sentinel<VT>::wait(y + c, a.err);
-    }
-#pragma unroll
-    for (int off = TS / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(submask, acc, off, TS);
-    if (sl == 0) Sentinel<VT>::publish(y + i, r - acc);
+// One slot's packed entries held by a warp: lane t has entries t and t+32 (rows with more
+// than 64 strictly-lower / upper entries finish the rest with a plain loop).
+template <typename VT>
+struct TriRow {
+  int row, beg, end;
+  VT v0, v1;
+  int c0, c1;
+};
+
+// Self-check of the packed layout: a row or column outside [0, n) is recorded in err (as
+// EGPU_ERR_ARG) and the access is skipped.
+template <typename VT>
+__device__ __forceinline__ void tri_fetch(TriRow<VT> &t, int s, const int *order, const int *ptr, const int *cols,
+                                          const VT *vals, int lane, int n, int *err) {
+  t.row = __ldg(order + s);
+  t.beg = __ldg(ptr + s);
+  t.end = __ldg(ptr + s + 1);
+  t.c0 = t.c1 = -1;
+  t.v0 = t.v1 = 0;
+  if (t.row < 0 || t.row >= n || t.end < t.beg) {
+    if (lane == 0) atomicExch(err, (int)EGPU_ERR_ARG);
+    t.row = -1;
+    t.end = t.beg;
+    return;
+  }
+  if (t.beg + lane < t.end) {
+    t.v0 = __ldg(vals + t.beg + lane);
+    t.c0 = __ldg(cols + t.beg + lane);
+  }
+  if (t.beg + 32 + lane < t.end) {
+    t.v1 = __ldg(vals + t.beg + 32 + lane);
+    t.c1 = __ldg(cols + t.beg + 32 + lane);
+  }
+  if (t.c0 >= n || t.c1 >= n) {
+    atomicExch(err, (int)EGPU_ERR_ARG);
+    if (t.c0 >= n) t.c0 = -1;
+    if (t.c1 >= n) t.c1 = -1;
   }
 }
 
-template <typename VT, int TS, typename OUT>
-__device__ __forceinline__ void upper_solve(const KArgs<VT> &a, const VT *y, VT *z, OUT &&out) {
+// sum over the slot's entries of v * x[col], waiting (bounded) for every x[col] to be produced
+template <typename VT>
+__device__ __forceinline__ VT tri_dot(const TriRow<VT> &t, const VT *x, const int *cols, const VT *vals, int lane,
+                                      int *err) {
+  VT acc = 0;
+  if (t.c0 >= 0) acc += t.v0 * Sentinel<VT>::wait(x + t.c0, err);
+  if (t.c1 >= 0) acc += t.v1 * Sentinel<VT>::wait(x + t.c1, err);
+  for (int j = t.beg + 64 + lane; j < t.end; j += 32) {
+    const int c = __ldg(cols + j);
+    if (c >= 0) acc += __ldg(vals + j) * Sentinel<VT>::wait(x + c, err);
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  return acc;
+}
+
+// lower: y_i = rhs_i - sum_{j<i} L_ij y_j (CRS_LUSolve forward, CRSMatrix.src:3346-3352).
+// One warp per slot; the next slot's row and entries are fetched while this slot waits.
+template <typename VT, int TS, typename RHS>
+__device__ __forceinline__ void lower_solve(const KArgs<VT> &a, VT *y, RHS &&rhs) {
+  static_assert(TS == 32, "one warp per row");
   const int lane = threadIdx.x & 31;
-  const int sl = lane & (TS - 1);
-  const unsigned submask = (TS == 32) ? 0xffffffffu : (((1u << TS) - 1u) << (lane & ~(TS - 1)));
   int gsub, nsub;
   if (!tri_participant<TS>(a.tri_per_block, gsub, nsub)) return;
+  if (gsub >= a.n) return;
+  TriRow<VT> nxt;
+  tri_fetch(nxt, gsub, a.lower_order, a.lo_ptr, a.lo_cols, a.lo_vals, lane, a.n, a.err);
   for (int s = gsub; s < a.n; s += nsub) {
-    const int i = __ldg(a.upper_order + s);
-    const int dg = __ldg(a.diag + i), end = __ldg(a.rows + i + 1);
-    const VT dinv = __ldg(a.ilu + dg);
-    VT acc = 0;
-    for (int j = dg + 1 + sl; j < end; j += TS) {
-      const VT u = __ldg(a.ilu + j);
-      const int c = __ldg(a.cols + j);
-      acc += u * Sentinel<VT>::wait(z + c, a.err);
+    const TriRow<VT> cur = nxt;
+    if (s + nsub < a.n) tri_fetch(nxt, s + nsub, a.lower_order, a.lo_ptr, a.lo_cols, a.lo_vals, lane, a.n, a.err);
+    // the right-hand side does not depend on the solve: form it before waiting
+    VT r = 0;
+    if (cur.row < 0) continue;
+    if (lane == 0) r = rhs(cur.row);
+    const VT acc = tri_dot(cur, y, a.lo_cols, a.lo_vals, lane, a.err);
+    if (lane == 0) Sentinel<VT>::publish(y + cur.row, r - acc);
+  }
+}
+
+// upper: z_i = u_ii^-1 (y_i - sum_{j>i} U_ij z_j) (backward, CRSMatrix.src:3355-3362)
+template <typename VT, int TS, typename OUT>
+__device__ __forceinline__ void upper_solve(const KArgs<VT> &a, const VT *y, VT *z, OUT &&out) {
+  static_assert(TS == 32, "one warp per row");
+  const int lane = threadIdx.x & 31;
+  int gsub, nsub;
+  if (!tri_participant<TS>(a.tri_per_block, gsub, nsub)) return;
+  if (gsub >= a.n) return;
+  TriRow<VT> nxt;
+  tri_fetch(nxt, gsub, a.upper_order, a.up_ptr, a.up_cols, a.up_vals, lane, a.n, a.err);
+  VT dnext = __ldg(a.up_dinv + gsub);
+  for (int s = gsub; s < a.n; s += nsub) {
+    const TriRow<VT> cur = nxt;
+    const VT dinv = dnext;
+    if (s + nsub < a.n) {
+      tri_fetch(nxt, s + nsub, a.upper_order, a.up_ptr, a.up_cols, a.up_vals, lane, a.n, a.err);
+      dnext = __ldg(a.up_dinv + s + nsub);
     }
-#pragma unroll
-    for (int off = TS / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(submask, acc, off, TS);
-    if (sl == 0) {
-      const VT yi = Sentinel<VT>::wait(y + i, a.err);
+    if (cur.row < 0) continue;
+    const VT acc = tri_dot(cur, z, a.up_cols, a.up_vals, lane, a.err);
+    if (lane == 0) {
+      const VT yi = Sentinel<VT>::wait(y + cur.row, a.err);
       const VT zi = dinv * (yi - acc);
-      Sentinel<VT>::publish(z + i, zi);
-      out(i, zi);
+      Sentinel<VT>::publish(z + cur.row, zi);
+      out(cur.row, zi);
     }
   }
 }
