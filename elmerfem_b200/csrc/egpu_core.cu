@@ -347,19 +347,22 @@ static void build_levels(int n, const std::vector<int> &rows, const std::vector<
 
 // occupancy-sized cooperative launch
 template <typename K, typename Args>
-static int launch_coop(egpu_ctx *ctx, K kernel, Args &args, int *grid_out = nullptr) {
+static int launch_coop(egpu_ctx *ctx, K kernel, Args &args, int *grid_out = nullptr, size_t smem = 0) {
   int bps = 0;
-  EGPU_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, EGPU_BLOCK, 0));
+  if (smem > 48 * 1024)
+    EGPU_CUDA_TRY(ctx, cudaFuncSetAttribute((const void *)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem));
+  EGPU_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, EGPU_KBLOCK, smem));
   if (bps < 1) {
     egpu_set_error(ctx, "persistent kernel does not fit on an SM");
     return EGPU_ERR_CUDA;
   }
-  bps = std::min(bps, 2);
+  bps = std::min(bps, 2048 / EGPU_KBLOCK);
   int grid = ctx->num_sms * bps;
   if (grid_out) *grid_out = grid;
   void *kargs[] = {&args};
-  EGPU_CUDA_TRY(ctx, cudaLaunchCooperativeKernel((const void *)kernel, dim3(grid), dim3(EGPU_BLOCK),
-                                                 kargs, 0, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaLaunchCooperativeKernel((const void *)kernel, dim3(grid), dim3(EGPU_KBLOCK),
+                                                 kargs, smem, ctx->stream));
   ctx->launches++;
   return EGPU_OK;
 }
@@ -489,6 +492,8 @@ int ensure_tri_schedule(egpu_mat *A) {
     EGPU_CUDA_TRY(ctx, cudaMemcpy(T.lo_src.p, ls.data(), ls.size() * sizeof(int), cudaMemcpyHostToDevice));
     EGPU_CUDA_TRY(ctx, cudaMemcpy(T.up_cols.p, uc.data(), uc.size() * sizeof(int), cudaMemcpyHostToDevice));
     EGPU_CUDA_TRY(ctx, cudaMemcpy(T.up_src.p, us.data(), us.size() * sizeof(int), cudaMemcpyHostToDevice));
+    const int rc = build_cta_schedule(A, rows, cols, diag, lo, up, lp, lc, upp, uc);
+    if (rc) return rc;
   }
   A->tri_built = true;
   return EGPU_OK;
@@ -540,6 +545,8 @@ int ilu0_factor(egpu_mat *A) {
       A->up_dinv.p, A->lo_vals32.p, A->up_vals32.p, A->up_dinv32.p);
   ctx->launches += 3;
   EGPU_CUDA_TRY(ctx, cudaGetLastError());
+  rc = cta_fill_values(A);
+  if (rc) return rc;
   A->ilu_valid = true;
   return EGPU_OK;
 }
@@ -548,11 +555,15 @@ static void set_tri_vals(KArgs<double> &a, const egpu_mat *A) {
   a.lo_vals = A->lo_vals.p;
   a.up_vals = A->up_vals.p;
   a.up_dinv = A->up_dinv.p;
+  a.clo.vals = A->cta_lo_vals.p;
+  a.cup.vals = A->cta_up_vals.p;
 }
 static void set_tri_vals(KArgs<float> &a, const egpu_mat *A) {
   a.lo_vals = A->lo_vals32.p;
   a.up_vals = A->up_vals32.p;
   a.up_dinv = A->up_dinv32.p;
+  a.clo.vals = A->cta_lo_vals32.p;
+  a.cup.vals = A->cta_up_vals32.p;
 }
 
 template <typename VT>
@@ -563,6 +574,26 @@ static void set_tri(KArgs<VT> &a, const egpu_mat *A) {
   a.lo_cols = A->tri.lo_cols.p;
   a.up_ptr = A->tri.up_ptr.p;
   a.up_cols = A->tri.up_cols.p;
+  // level-synchronous single-block solves when the cost estimate prefers them
+  const TriSchedule &T = A->tri;
+  const int v = sizeof(VT) == 8 ? 0 : 1;
+  a.tri_cta = cta_use(A, v) ? 1 : 0;
+  a.cta_pd = T.cta_pd[v];
+  a.cta_rs = T.cta_rs;
+  a.cta_sb = T.cta_sb[v];
+  a.cta_sr = T.cta_sr[v];
+  a.cta_nl = std::max(T.cta_lo.nlev, T.cta_up.nlev);
+  a.cta_nt = cta_threads(A);
+  a.pos_lo = T.pos_lo.p;
+  a.pos_up = T.pos_up.p;
+  a.clo.nlev = T.cta_lo.nlev;
+  a.clo.lev = T.cta_lo.lev.p;
+  a.clo.ridx = T.cta_lo.ridx.p;
+  a.clo.map = T.cta_lo.map.p;
+  a.cup.nlev = T.cta_up.nlev;
+  a.cup.lev = T.cta_up.lev.p;
+  a.cup.ridx = T.cta_up.ridx.p;
+  a.cup.map = T.cta_up.map.p;
   set_tri_vals(a, A);
 }
 
@@ -578,8 +609,8 @@ static void set_sell(KArgs<VT> &a, const egpu_mat *A, const VT *vals, bool offs)
 
 // sub-warps per block for the sync-free solves: about twice the widest level in total,
 // at least one per block
-static int tri_per_block(const egpu_mat *A, int lpr, int grid) {
-  const int per_block_max = EGPU_BLOCK / lpr;
+static int tri_per_block(const egpu_mat *A, int lpr, int grid, int block = EGPU_KBLOCK) {
+  const int per_block_max = block / lpr;
   const int want = std::max(1, 2 * A->tri.max_width);
   return std::max(1, std::min(per_block_max, (want + grid - 1) / grid));
 }
@@ -593,13 +624,15 @@ template <typename VT>
 static int run_krylov(egpu_mat *A, const KArgs<VT> &a0, int method, bool offs) {
   egpu_ctx *ctx = A->ctx;
   KArgs<VT> a = a0;
-  a.tri_per_block = tri_per_block(A, TRI_TS, ctx->num_sms * 2);
+  a.tri_per_block = tri_per_block(A, TRI_TS, ctx->num_sms);
+  if (a.precond != EGPU_PREC_ILU0) a.tri_cta = 0;
+  const size_t smem = a.tri_cta ? A->tri.cta_smem[sizeof(VT) == 8 ? 0 : 1] : 0;
   if (method == EGPU_CG) {
-    if (offs) return launch_coop(ctx, cg_kernel<VT, TRI_TS, true>, a);
-    return launch_coop(ctx, cg_kernel<VT, TRI_TS, false>, a);
+    if (offs) return launch_coop(ctx, cg_kernel<VT, TRI_TS, true>, a, nullptr, smem);
+    return launch_coop(ctx, cg_kernel<VT, TRI_TS, false>, a, nullptr, smem);
   }
-  if (offs) return launch_coop(ctx, bicgstab_kernel<VT, TRI_TS, true>, a);
-  return launch_coop(ctx, bicgstab_kernel<VT, TRI_TS, false>, a);
+  if (offs) return launch_coop(ctx, bicgstab_kernel<VT, TRI_TS, true>, a, nullptr, smem);
+  return launch_coop(ctx, bicgstab_kernel<VT, TRI_TS, false>, a, nullptr, smem);
 }
 
 // FP64 drop-in solve on device buffers.  x_dev: in = initial guess, out = solution.
@@ -1016,6 +1049,15 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_lu_apply(KArgs<double> a, con
   (void)n;
 }
 
+// the same with the level-synchronous solves in one block (rhs gathered into slot order)
+__global__ void k_gather_slots(int n, const int *__restrict__ order, const double *__restrict__ v, double *slo) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) slo[s] = v[order[s]];
+}
+__global__ void __launch_bounds__(EGPU_KBLOCK, 1) k_lu_apply_block(KArgs<double> a, const double *slo, double *yup,
+                                                                   double *u) {
+  cta_ilu(a, slo, yup, (const double *)nullptr, u, [](int, double, double) {});
+}
+
 __global__ void k_fill_sentinel(double *p, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     p[i] = __longlong_as_double((long long)EGPU_SENTINEL64);
@@ -1038,9 +1080,19 @@ int lu_apply(egpu_mat *A, const double *v_dev, double *u_dev) {
   set_tri(a, A);
   a.w = A->work.p;
   a.err = (int *)(ctx->sync.p + 1);
-  a.tri_per_block = tri_per_block(A, TRI_TS, ctx->num_sms * 2);
+  a.tri_per_block = tri_per_block(A, TRI_TS, ctx->num_sms * 2, EGPU_BLOCK);
   int rc;
-  {
+  if (a.tri_cta) {
+    const size_t smem = A->tri.cta_smem[0];
+    if (smem > 48 * 1024)
+      EGPU_CUDA_TRY(ctx, cudaFuncSetAttribute((const void *)k_lu_apply_block,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    double *slo = A->work.p + A->ldw, *yup = A->work.p + 2 * A->ldw;
+    k_gather_slots<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, A->tri.lower_order.p, v_dev, slo);
+    k_lu_apply_block<<<1, EGPU_KBLOCK, smem, ctx->stream>>>(a, slo, yup, u_dev);
+    ctx->launches += 2;
+    rc = (int)cudaGetLastError();
+  } else {
     auto k = k_lu_apply<TRI_TS>;
     int bps = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, EGPU_BLOCK, 0);
@@ -1352,6 +1404,30 @@ extern "C" int egpu_matrix_clone(egpu_mat *proto, egpu_mat **out) {
   A->tri.max_lower = proto->tri.max_lower;
   A->tri.max_upper = proto->tri.max_upper;
   A->tri.max_width = proto->tri.max_width;
+  {
+    const TriSchedule &P = proto->tri;
+    TriSchedule &T = A->tri;
+    for (int v = 0; v < 2; ++v) {
+      T.cta_ok[v] = P.cta_ok[v];
+      T.cta_pd[v] = P.cta_pd[v];
+      T.cta_sb[v] = P.cta_sb[v];
+      T.cta_sr[v] = P.cta_sr[v];
+      T.cta_smem[v] = P.cta_smem[v];
+    }
+    T.cta_rs = P.cta_rs;
+    T.pos_lo.view(P.pos_lo);
+    T.pos_up.view(P.pos_up);
+    CtaTriHost *dst[2] = {&T.cta_lo, &T.cta_up};
+    const CtaTriHost *src[2] = {&P.cta_lo, &P.cta_up};
+    for (int k = 0; k < 2; ++k) {
+      dst[k]->nlev = src[k]->nlev;
+      dst[k]->nent = src[k]->nent;
+      dst[k]->lev.view(src[k]->lev);
+      dst[k]->ridx.view(src[k]->ridx);
+      dst[k]->src.view(src[k]->src);
+      dst[k]->map.view(src[k]->map);
+    }
+  }
   A->tri_built = true;
   const AssemblyData &P = proto->asmb;
   AssemblyData &S = A->asmb;
@@ -1391,6 +1467,7 @@ extern "C" long long egpu_matrix_footprint(const egpu_mat *A, int precond) {
   b += 8 * z + 8 * zs + 4 * zs;             // scaled CRS, SELL FP64, SELL FP32
   b += 8 * n + 13 * 8 * l + 14 * 4 * l;     // DiagScaling, work vectors
   if (precond == EGPU_PREC_ILU0) b += 8 * z + 4 * z + 4 * n;  // ILU0 FP64/FP32, flags
+  if (precond == EGPU_PREC_ILU0) b += 12 * (A->tri.cta_lo.nent + A->tri.cta_up.nent);  // single-block layout
   return b + 8 * n;                         // back-scaled solution
 }
 

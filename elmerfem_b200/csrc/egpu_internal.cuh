@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/elmergpu.h"
+#include "egpu_tri_plan.h"
 
 // ------------------------------------------------------------------------------------
 // constants
@@ -29,6 +30,10 @@
 #define EGPU_SENTINEL32 0x7FA5EED1u
 
 #define EGPU_BLOCK 512
+// the persistent Krylov kernels: one 1024-thread block per SM (32 warps, the register file
+// at 64 registers a thread), so block 0 has up to 227 KB of shared memory for the
+// level-synchronous triangular solves and the grid barrier has one arrival per SM
+#define EGPU_KBLOCK 1024
 
 // ------------------------------------------------------------------------------------
 // error plumbing
@@ -96,6 +101,22 @@ struct egpu_ctx {
   unsigned int *sync_host_err = nullptr;
 };
 
+// One triangle of the level-synchronous solve that a single block runs (CtaTri in
+// egpu_krylov.cuh).  Level L owns slots [lev.x, lev.x + lev.y) and an ELL block of
+// lev.z entries per row stored column-major at [lev.w, lev.w + round8(lev.y * lev.z)):
+// entry k of the level's row t sits at lev.w + k * lev.y + t.  ridx is the ring-buffer
+// slot of the entry's column (the column's solve slot modulo the ring size; padding
+// entries point at the ring's zero slot), src the packed factor entry it is filled
+// from (-1 for padding).  map: lower, the upper-order slot of the row; upper, the row.
+struct CtaTriHost {
+  int nlev = 0;
+  long long nent = 0;
+  DevBuf<int4> lev;
+  DevBuf<uint16_t> ridx;
+  DevBuf<int> src;
+  DevBuf<int> map;
+};
+
 struct TriSchedule {
   // rows in the order the sync-free solve processes them (ascending dependency level)
   DevBuf<int> lower_order, upper_order;
@@ -105,6 +126,13 @@ struct TriSchedule {
   int lower_levels = 0, upper_levels = 0;
   int max_lower = 0, max_upper = 0;  // longest strictly-lower / strictly-upper row part
   int max_width = 0;                 // most rows in one level (lower or upper)
+  // level-synchronous single-block schedule; cta_ok[v] for FP64 (v = 0) / FP32 (v = 1)
+  CtaTriHost cta_lo, cta_up;
+  DevBuf<int> pos_lo, pos_up;        // solve slot of every row in the lower / upper order
+  int cta_rs = 0;                    // ring slots
+  bool cta_ok[2] = {false, false};
+  int cta_pd[2] = {0, 0}, cta_sb[2] = {0, 0}, cta_sr[2] = {0, 0};
+  size_t cta_smem[2] = {0, 0};
 };
 
 struct AssemblyData {
@@ -135,6 +163,8 @@ struct egpu_mat {
   DevBuf<float> scaled32, ilu32; // FP32 copies for the mixed-precision inner solver
   DevBuf<double> lo_vals, up_vals, up_dinv;        // ILU0 factors packed in solve order
   DevBuf<float> lo_vals32, up_vals32, up_dinv32;
+  DevBuf<double> cta_lo_vals, cta_up_vals;        // the factors in the level-synchronous ELL layout
+  DevBuf<float> cta_lo_vals32, cta_up_vals32;
   DevBuf<int16_t> cols16;        // column offsets (col - row) when |col-row| < 32768
   DevBuf<int> ilu_done;          // factorisation completion flags
   // SELL-32 copy of the pattern (slice s = rows 32s..32s+31, entry (k, lane) at
@@ -288,6 +318,34 @@ __device__ __forceinline__ bool grid_barrier(unsigned int *count, int *err, unsi
   }
   __syncthreads();
   return *(volatile int *)err == 0;
+}
+
+// Asynchronous global -> shared copies (cp.async, completion tracked per thread in
+// commit groups).  16-byte copies bypass L1 (.cg); 4/8-byte copies go through it (.ca).
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+template <int B>
+__device__ __forceinline__ void cp_async_small(void *smem, const void *gmem) {
+  static_assert(B == 4 || B == 8, "4- or 8-byte copy");
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(s), "l"(gmem), "n"(B) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// wait until at most n (0..7) of this thread's most recent groups are still pending
+__device__ __forceinline__ void cp_async_wait(int n) {
+  switch (n) {
+    case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
+    case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
+    case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
+    case 3: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
+    case 4: asm volatile("cp.async.wait_group 4;" ::: "memory"); break;
+    case 5: asm volatile("cp.async.wait_group 5;" ::: "memory"); break;
+    case 6: asm volatile("cp.async.wait_group 6;" ::: "memory"); break;
+    case 7: asm volatile("cp.async.wait_group 7;" ::: "memory"); break;
+    default: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;  // conservative
+  }
 }
 
 // Deterministic block sum of NV values per thread (fixed shuffle tree, fixed warp order).

@@ -20,6 +20,16 @@ namespace egpu {
 
 enum { SLOT_BB = 0, SLOT_RHO, SLOT_PQ, SLOT_RR, SLOT_SS, SLOT_TS, SLOT_TT, SLOT_RR2, NUM_SLOTS };
 
+// One triangle of the level-synchronous solve (layout described at CtaTriHost)
+template <typename VT>
+struct CtaTri {
+  int nlev;
+  const int4 *lev;          // {first slot, rows, entries per row, ELL offset}
+  const uint16_t *ridx;     // ring slot of each ELL entry's column
+  const VT *vals;           // ELL values
+  const int *map;           // lower: upper-order slot of the row; upper: the row
+};
+
 template <typename VT>
 struct KArgs {
   int n;
@@ -50,6 +60,12 @@ struct KArgs {
   const int *sell_ptr, *sell_w, *scols;
   const int16_t *scols16;
   const VT *svals;
+  // level-synchronous triangular solves run by block 0 out of shared memory (tri_cta != 0):
+  // levels staged cta_pd ahead, ring of cta_rs slots, staging windows of cta_sb entries and
+  // cta_sr rows
+  int tri_cta, cta_pd, cta_rs, cta_sb, cta_sr, cta_nl, cta_nt;
+  const int *pos_lo, *pos_up;     // solve slot of each row, lower / upper order
+  CtaTri<VT> clo, cup;
 };
 
 // row sum step: FP64 keeps CRS_MatrixVectorProd's rounding (s = s + a*x, two roundings, row
@@ -274,6 +290,190 @@ __device__ __forceinline__ void upper_solve(const KArgs<VT> &a, const VT *y, VT 
   }
 }
 
+// -------------------------------------------------------------------------------------
+// Level-synchronous triangular solves in one block.
+//
+// Every dependency of a row lies in an earlier level, and (for the meshes this is used on)
+// only a few levels back, so block 0 runs the levels in order with one __syncthreads per
+// level and keeps the values of the recent slots in a shared-memory ring (slot s at
+// s mod cta_rs; the host sizes the ring so no slot is overwritten while a later row still
+// reads it).  A level's ELL block of factor entries, and its rows' right-hand sides,
+// inverted diagonals and output positions, are contiguous in global memory; they are
+// staged into shared-memory windows with cp.async cta_pd levels ahead, so the copies of
+// later levels are in flight while the current one computes.  One thread per row sums its
+// entries in CRS order with the reference's operation order:
+//   lower  s = b_i;  s = s - L_ij y_j ...;  y_i = s                (CRS_LUSolve :3348-3353)
+//   upper  s = y_i;  s = s - U_ij z_j ...;  z_i = u_ii^-1 * s      (:3357-3363)
+// so the FP64 solve rounds exactly as CRS_LUSolve does.
+__device__ __forceinline__ double row_msub(double s, double a, double x) { return __dsub_rn(s, __dmul_rn(a, x)); }
+__device__ __forceinline__ float row_msub(float s, float a, float x) { return fmaf(-a, x, s); }
+__device__ __forceinline__ double cta_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float cta_mul(float a, float b) { return a * b; }
+
+template <typename VT>
+struct CtaSmem {
+  int4 *lv;
+  VT *sv;
+  uint16_t *si;
+  VT *ring, *rr, *rd, *ra;
+  int *rm;
+};
+
+template <typename VT>
+__device__ __forceinline__ CtaSmem<VT> cta_smem(const KArgs<VT> &a, unsigned char *base) {
+  CtaSmem<VT> m;
+  size_t o = 0;
+  const int V = (int)sizeof(VT);
+  m.lv = reinterpret_cast<int4 *>(base + o);
+  o += (size_t)a.cta_nl * 16;
+  m.sv = reinterpret_cast<VT *>(base + o);
+  o += cta_align16((size_t)a.cta_sb * V);
+  m.si = reinterpret_cast<uint16_t *>(base + o);
+  o += cta_align16((size_t)a.cta_sb * 2);
+  m.ring = reinterpret_cast<VT *>(base + o);
+  o += cta_align16((size_t)(a.cta_rs + 1) * V);
+  m.rr = reinterpret_cast<VT *>(base + o);
+  o += cta_align16((size_t)a.cta_sr * V);
+  m.rd = reinterpret_cast<VT *>(base + o);
+  o += cta_align16((size_t)a.cta_sr * V);
+  m.ra = reinterpret_cast<VT *>(base + o);
+  o += cta_align16((size_t)a.cta_sr * V);
+  m.rm = reinterpret_cast<int *>(base + o);
+  return m;
+}
+
+// Positions of a level in the staging windows and the ring, advanced level by level (the
+// same for every thread): sb = ELL offset mod cta_sb, rb = first slot mod cta_sr,
+// qb = first slot mod cta_rs.  A level never exceeds a window, so one subtraction wraps.
+struct CtaPos {
+  int sb, rb, qb;
+  __device__ __forceinline__ void advance(int4 lv, int SB, int SR, int RS) {
+    sb += (lv.y * lv.z + 7) & ~7;
+    if (sb >= SB) sb -= SB;
+    rb += lv.y;
+    if (rb >= SR) rb -= SR;
+    qb += lv.y;
+    if (qb >= RS) qb -= RS;
+  }
+};
+
+__device__ __forceinline__ int cta_wrap(int i, int n) { return i >= n ? i - n : i; }
+
+// barrier among the first nt threads of the block (named barrier 1; nt a multiple of 32)
+__device__ __forceinline__ void cta_bar(int nt) { asm volatile("bar.sync 1, %0;" ::"r"(nt) : "memory"); }
+
+// issue the copies of level lv (window positions p) into the staging windows (threads
+// 0..nt-1)
+template <typename VT, bool UPPER>
+__device__ __forceinline__ void cta_issue(const KArgs<VT> &a, const CtaTri<VT> &T, const CtaSmem<VT> &m, int4 lv,
+                                          CtaPos p, int nt, const VT *rowv, const VT *dinv, const VT *aux) {
+  constexpr int PV = 16 / sizeof(VT);
+  const int SB = a.cta_sb, SR = a.cta_sr;
+  const int ne = (lv.y * lv.z + 7) & ~7;
+  for (int c = threadIdx.x; c < ne / PV; c += nt)
+    cp_async16(m.sv + cta_wrap(p.sb + c * PV, SB), T.vals + lv.w + c * PV);
+  for (int c = threadIdx.x; c < ne / 8; c += nt)
+    cp_async16(m.si + cta_wrap(p.sb + c * 8, SB), T.ridx + lv.w + c * 8);
+  for (int t = threadIdx.x; t < lv.y; t += nt) {
+    const int d = cta_wrap(p.rb + t, SR);
+    cp_async_small<sizeof(VT)>(m.rr + d, rowv + lv.x + t);
+    cp_async_small<4>(m.rm + d, T.map + lv.x + t);
+    if (UPPER) {
+      cp_async_small<sizeof(VT)>(m.rd + d, dinv + lv.x + t);
+      if (aux) cp_async_small<sizeof(VT)>(m.ra + d, aux + lv.x + t);
+    }
+  }
+}
+
+// One level: the solve's thread t takes the level's rows t, t + nt, ...; a row's entries
+// are read four at a time (ring indices, then ring values) and subtracted in CRS order,
+// s = s - L_ij y_j as CRS_LUSolve does, so the FP64 result is the reference's to the bit.
+template <typename VT, bool UPPER, typename OUT>
+__device__ __forceinline__ void cta_level(const KArgs<VT> &a, const CtaSmem<VT> &m, int4 lv, CtaPos p, int nt,
+                                          VT *outv, OUT &&out) {
+  const int SB = a.cta_sb, SR = a.cta_sr, RS = a.cta_rs;
+  const int w = lv.y, nk = lv.z;
+  for (int t = threadIdx.x; t < w; t += nt) {
+    const int r = cta_wrap(p.rb + t, SR);
+    VT s = m.rr[r];
+    int e = cta_wrap(p.sb + t, SB);
+    int k = 0;
+    for (; k + 4 <= nk; k += 4) {
+      const int e1 = cta_wrap(e + w, SB), e2 = cta_wrap(e1 + w, SB), e3 = cta_wrap(e2 + w, SB);
+      const int i0 = m.si[e], i1 = m.si[e1], i2 = m.si[e2], i3 = m.si[e3];
+      const VT v0 = m.sv[e], v1 = m.sv[e1], v2 = m.sv[e2], v3 = m.sv[e3];
+      const VT x0 = m.ring[i0], x1 = m.ring[i1], x2 = m.ring[i2], x3 = m.ring[i3];
+      s = row_msub(s, v0, x0);
+      s = row_msub(s, v1, x1);
+      s = row_msub(s, v2, x2);
+      s = row_msub(s, v3, x3);
+      e = cta_wrap(e3 + w, SB);
+    }
+    for (; k < nk; ++k) {
+      s = row_msub(s, m.sv[e], m.ring[m.si[e]]);
+      e = cta_wrap(e + w, SB);
+    }
+    if (UPPER) s = cta_mul(m.rd[r], s);
+    m.ring[cta_wrap(p.qb + t, RS)] = s;
+    const int dst = m.rm[r];
+    outv[dst] = s;
+    if (UPPER) out(dst, s, m.ra[r]);
+  }
+}
+
+// A whole triangle, run by the block's first a.cta_nt threads (the others go straight to
+// the closing __syncthreads).  rowv: right-hand side in this triangle's slot order; lower
+// results go to outv[map] (the upper slot order), upper results to outv[row] and
+// out(row, z, aux).
+template <typename VT, bool UPPER, typename OUT>
+__device__ __forceinline__ void cta_tri_solve(const KArgs<VT> &a, const CtaTri<VT> &T, const CtaSmem<VT> &m,
+                                              const VT *rowv, const VT *dinv, const VT *aux, VT *outv, OUT &&out) {
+  const int PD = a.cta_pd, nlev = T.nlev, nt = a.cta_nt;
+  const int SB = a.cta_sb, SR = a.cta_sr, RS = a.cta_rs;
+  if (threadIdx.x < nt) {
+    // the level table, once per solve
+    for (int L = threadIdx.x; L < nlev; L += nt) cp_async16(m.lv + L, T.lev + L);
+    cp_async_commit();
+    cp_async_wait(0);
+    if (threadIdx.x == 0) m.ring[RS] = VT(0);
+    cta_bar(nt);
+    CtaPos pi{0, 0, 0}, pp{0, 0, 0};  // issue / process positions
+    for (int L = 0; L < PD; ++L) {
+      if (L < nlev) {
+        const int4 lv = m.lv[L];
+        cta_issue<VT, UPPER>(a, T, m, lv, pi, nt, rowv, dinv, aux);
+        pi.advance(lv, SB, SR, RS);
+      }
+      cp_async_commit();
+    }
+    for (int L = 0; L < nlev; ++L) {
+      cp_async_wait(PD - 1);
+      cta_bar(nt);
+      if (L + PD < nlev) {
+        const int4 lv = m.lv[L + PD];
+        cta_issue<VT, UPPER>(a, T, m, lv, pi, nt, rowv, dinv, aux);
+        pi.advance(lv, SB, SR, RS);
+      }
+      cp_async_commit();
+      const int4 lv = m.lv[L];
+      cta_level<VT, UPPER>(a, m, lv, pp, nt, outv, out);
+      pp.advance(lv, SB, SR, RS);
+    }
+    cp_async_wait(0);
+  }
+  __syncthreads();
+}
+
+// M^-1 applied by block 0: rhs in lower slot order (slo) -> y in upper slot order (yup)
+// -> z (row order) with out(row, z, aux[upper slot]) per row
+template <typename VT, typename OUT>
+__device__ __forceinline__ void cta_ilu(const KArgs<VT> &a, const VT *slo, VT *yup, const VT *aux, VT *z, OUT &&out) {
+  extern __shared__ __align__(16) unsigned char egpu_dsm[];
+  const CtaSmem<VT> m = cta_smem(a, egpu_dsm);
+  cta_tri_solve<VT, false>(a, a.clo, m, slo, (const VT *)nullptr, (const VT *)nullptr, yup, [](int, VT, VT) {});
+  cta_tri_solve<VT, true>(a, a.cup, m, yup, a.up_dinv, aux, z, out);
+}
+
 // Jacobi: CRS_DiagPrecondition, CRSMatrix.src:1505-1509
 template <typename VT>
 __device__ __forceinline__ VT diag_prec(VT v, VT d) {
@@ -290,7 +490,7 @@ __device__ __forceinline__ void store_partials(const KArgs<VT> &a, int slot, dou
 //
 // w layout: R Z P Q Y(ILU lower result)
 template <typename VT, int LPR, bool OFFS>
-__global__ void __launch_bounds__(EGPU_BLOCK, 2) cg_kernel(KArgs<VT> a) {
+__global__ void __launch_bounds__(EGPU_KBLOCK, 1) cg_kernel(KArgs<VT> a) {
   if (a.skip && (*a.skip & 2u)) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       a.out_i[0] = EGPU_HUTI_CONVERGENCE;
@@ -308,13 +508,23 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) cg_kernel(KArgs<VT> a) {
      *Y = a.w + 4 * a.ldw;
   const VT *B = a.b;
   const bool ilu = a.precond == EGPU_PREC_ILU0;
+  const bool cta = ilu && a.tri_cta;  // block 0 runs the ILU0 solves level-synchronously
   const VT SENT = Sentinel<VT>::value();
+  // level-synchronous mode: R in lower / upper slot order, y in upper slot order
+  VT *SLO = a.w + 4 * a.ldw, *YUP = a.w + 5 * a.ldw, *AUX = a.w + 6 * a.ldw;
 
   // ---- init: R = B - A X  (x0 = 0 in inner mode: R = B)
   {
     double acc[1] = {0.0};
     if (a.true_residual) {
-      spmv_phase<VT, LPR, OFFS, false>(a, X, X, [&](int i, VT s, VT) { R[i] = B[i] - s; });
+      spmv_phase<VT, LPR, OFFS, false>(a, X, X, [&](int i, VT s, VT) {
+        const VT r = B[i] - s;
+        R[i] = r;
+        if (cta) {
+          SLO[a.pos_lo[i]] = r;
+          AUX[a.pos_up[i]] = r;
+        }
+      });
     } else {
       vec_loop<VT>(n, [&](int i, auto w) {
         constexpr int W = decltype(w)::value;
@@ -322,6 +532,13 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) cg_kernel(KArgs<VT> a) {
         vld<W>(B, i, b);
         vst<W>(R, i, b);
         vfill<W>(X, i, VT(0));
+        if (cta) {
+#pragma unroll
+          for (int k = 0; k < W; ++k) {
+            SLO[a.pos_lo[i + k]] = b[k];
+            AUX[a.pos_up[i + k]] = b[k];
+          }
+        }
       });
     }
     vec_loop<VT>(n, [&](int i, auto w) {
@@ -330,7 +547,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) cg_kernel(KArgs<VT> a) {
       vld<W>(B, i, b);
 #pragma unroll
       for (int k = 0; k < W; ++k) acc[0] += (double)b[k] * (double)b[k];
-      if (ilu) {
+      if (ilu && !cta) {
         vfill<W>(Y, i, SENT);
         vfill<W>(Z, i, SENT);
       }
@@ -344,7 +561,10 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) cg_kernel(KArgs<VT> a) {
   // ---- first preconditioning: Z = M^-1 R, partial rho = R.Z
   {
     double acc[1] = {0.0};
-    if (ilu) {
+    if (cta) {
+      if (blockIdx.x == 0)
+        cta_ilu(a, SLO, YUP, AUX, Z, [&](int, VT zi, VT ri) { acc[0] += (double)ri * (double)zi; });
+    } else if (ilu) {
       lower_solve<VT, LPR>(a, Y, [&](int i) { return R[i]; });
       upper_solve<VT, LPR>(a, Y, Z, [&](int i, VT zi) { acc[0] += (double)R[i] * (double)zi; });
     } else {
@@ -389,7 +609,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) cg_kernel(KArgs<VT> a) {
 #pragma unroll
         for (int q = 0; q < W; ++q) p[q] = first ? z[q] : z[q] + beta * p[q];
         vst<W>(P, i, p);
-        if (ilu) {
+        if (ilu && !cta) {
           vfill<W>(Z, i, SENT);
           vfill<W>(Y, i, SENT);
         }
@@ -430,41 +650,72 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) cg_kernel(KArgs<VT> a) {
       const double alpha_d = rho / pq;
       const VT alpha = (VT)alpha_d;
       double acc[2] = {0.0, 0.0};
-      if (ilu) {
-        lower_solve<VT, LPR>(a, Y, [&](int i) { return R[i] - alpha * Q[i]; });
-        upper_solve<VT, LPR>(a, Y, Z, [&](int i, VT zi) {
-          const VT r = R[i] - alpha * Q[i];
-          R[i] = r;
-          X[i] = X[i] + alpha * P[i];
-          acc[0] += (double)r * (double)zi;
-          acc[1] += (double)r * (double)r;
-        });
-      } else {
-        const bool jac = a.precond == EGPU_PREC_DIAGONAL;
+      if (cta) {
+        // X, R update and the scatter of R into slot order, then block 0's solve
         vec_loop<VT>(n, [&](int i, auto w) {
           constexpr int W = decltype(w)::value;
-          VT x[W], p[W], r[W], q[W], d[W], z[W];
+          VT x[W], p[W], r[W], q[W];
           vld<W>(X, i, x);
           vld<W>(P, i, p);
           vld<W>(R, i, r);
           vld<W>(Q, i, q);
-          if (jac) vld<W>(a.dvals, i, d);
 #pragma unroll
           for (int t = 0; t < W; ++t) {
             x[t] = x[t] + alpha * p[t];
             r[t] = r[t] - alpha * q[t];
-            z[t] = jac ? diag_prec(r[t], d[t]) : r[t];
-            acc[0] += (double)r[t] * (double)z[t];
             acc[1] += (double)r[t] * (double)r[t];
+            SLO[a.pos_lo[i + t]] = r[t];
+            AUX[a.pos_up[i + t]] = r[t];
           }
           vst<W>(X, i, x);
           vst<W>(R, i, r);
-          vst<W>(Z, i, z);
         });
+        double rr[1] = {acc[1]};
+        block_sum<1>(rr, sm);
+        store_partials(a, SLOT_RR2, rr[0]);
+        if (!grid_barrier(a.bar, a.err, epoch)) return;
+        double rh[1] = {0.0};
+        if (blockIdx.x == 0)
+          cta_ilu(a, SLO, YUP, AUX, Z, [&](int, VT zi, VT ri) { rh[0] += (double)ri * (double)zi; });
+        block_sum<1>(rh, sm);
+        store_partials(a, SLOT_RHO, rh[0]);
+      } else {
+        if (ilu) {
+          lower_solve<VT, LPR>(a, Y, [&](int i) { return R[i] - alpha * Q[i]; });
+          upper_solve<VT, LPR>(a, Y, Z, [&](int i, VT zi) {
+            const VT r = R[i] - alpha * Q[i];
+            R[i] = r;
+            X[i] = X[i] + alpha * P[i];
+            acc[0] += (double)r * (double)zi;
+            acc[1] += (double)r * (double)r;
+          });
+        } else {
+          const bool jac = a.precond == EGPU_PREC_DIAGONAL;
+          vec_loop<VT>(n, [&](int i, auto w) {
+            constexpr int W = decltype(w)::value;
+            VT x[W], p[W], r[W], q[W], d[W], z[W];
+            vld<W>(X, i, x);
+            vld<W>(P, i, p);
+            vld<W>(R, i, r);
+            vld<W>(Q, i, q);
+            if (jac) vld<W>(a.dvals, i, d);
+#pragma unroll
+            for (int t = 0; t < W; ++t) {
+              x[t] = x[t] + alpha * p[t];
+              r[t] = r[t] - alpha * q[t];
+              z[t] = jac ? diag_prec(r[t], d[t]) : r[t];
+              acc[0] += (double)r[t] * (double)z[t];
+              acc[1] += (double)r[t] * (double)r[t];
+            }
+            vst<W>(X, i, x);
+            vst<W>(R, i, r);
+            vst<W>(Z, i, z);
+          });
+        }
+        block_sum<2>(acc, sm);
+        store_partials(a, SLOT_RHO, acc[0]);
+        store_partials(a, SLOT_RR2, acc[1]);
       }
-      block_sum<2>(acc, sm);
-      store_partials(a, SLOT_RHO, acc[0]);
-      store_partials(a, SLOT_RR2, acc[1]);
     }
     if (!grid_barrier(a.bar, a.err, epoch)) return;
     if (!a.true_residual) rr_prev = reduce_partials(a.partials + SLOT_RR2 * nb, nb, sm);
@@ -484,7 +735,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) cg_kernel(KArgs<VT> a) {
 //
 // w layout: R RTLD P V T S T1V T2V Y1 Y2
 template <typename VT, int LPR, bool OFFS>
-__global__ void __launch_bounds__(EGPU_BLOCK, 2) bicgstab_kernel(KArgs<VT> a) {
+__global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstab_kernel(KArgs<VT> a) {
   if (a.skip && (*a.skip & 2u)) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       a.out_i[0] = EGPU_HUTI_CONVERGENCE;
@@ -505,7 +756,9 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) bicgstab_kernel(KArgs<VT> a) {
   const VT *B = a.b;
   const bool ilu = a.precond == EGPU_PREC_ILU0;
   const bool jac = a.precond == EGPU_PREC_DIAGONAL;
+  const bool cta = ilu && a.tri_cta;  // block 0 runs the ILU0 solves level-synchronously
   const VT SENT = Sentinel<VT>::value();
+  VT *SLO = Y1, *YUP = Y2;           // level-synchronous mode: rhs / y in slot order
 
   // ---- init: R = B - A X; RTLD = R; P = V = 0
   {
@@ -537,7 +790,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) bicgstab_kernel(KArgs<VT> a) {
       for (int k = 0; k < W; ++k) acc[0] += (double)b[k] * (double)b[k];
       vfill<W>(P, i, VT(0));
       vfill<W>(V, i, VT(0));
-      if (ilu) {
+      if (ilu && !cta) {
         vfill<W>(Y1, i, SENT);
         vfill<W>(Y2, i, SENT);
         vfill<W>(T1, i, SENT);
@@ -568,7 +821,23 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) bicgstab_kernel(KArgs<VT> a) {
     {
       const VT beta = (VT)((rho * alpha) / (oldrho * omega));
       const VT om = (VT)omega;
-      if (ilu) {
+      if (cta) {
+        vec_loop<VT>(n, [&](int i, auto w) {
+          constexpr int W = decltype(w)::value;
+          VT r[W], p[W], v[W];
+          vld<W>(R, i, r);
+          vld<W>(P, i, p);
+          vld<W>(V, i, v);
+#pragma unroll
+          for (int q = 0; q < W; ++q) {
+            p[q] = r[q] + beta * (p[q] - om * v[q]);
+            SLO[a.pos_lo[i + q]] = p[q];
+          }
+          vst<W>(P, i, p);
+        });
+        if (!grid_barrier(a.bar, a.err, epoch)) return;
+        if (blockIdx.x == 0) cta_ilu(a, SLO, YUP, (const VT *)nullptr, T1, [](int, VT, VT) {});
+      } else if (ilu) {
         lower_solve<VT, LPR>(a, Y1, [&](int i) {
           const VT p = R[i] + beta * (P[i] - om * V[i]);
           P[i] = p;
@@ -629,33 +898,53 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) bicgstab_kernel(KArgs<VT> a) {
     {
       const VT al = (VT)alpha;
       double acc[1] = {0.0};
-      if (ilu) {
-        lower_solve<VT, LPR>(a, Y2, [&](int i) {
-          const VT s = R[i] - al * V[i];
-          S[i] = s;
-          acc[0] += (double)s * (double)s;
-          return s;
-        });
-        upper_solve<VT, LPR>(a, Y2, T2, [&](int, VT) {});
-      } else {
+      if (cta) {
         vec_loop<VT>(n, [&](int i, auto w) {
           constexpr int W = decltype(w)::value;
-          VT r[W], v[W], d[W], sv[W], t[W];
+          VT r[W], v[W], sv[W];
           vld<W>(R, i, r);
           vld<W>(V, i, v);
-          if (jac) vld<W>(a.dvals, i, d);
 #pragma unroll
           for (int q = 0; q < W; ++q) {
             sv[q] = r[q] - al * v[q];
             acc[0] += (double)sv[q] * (double)sv[q];
-            t[q] = jac ? diag_prec(sv[q], d[q]) : sv[q];
+            SLO[a.pos_lo[i + q]] = sv[q];
           }
           vst<W>(S, i, sv);
-          vst<W>(T2, i, t);
         });
+        block_sum<1>(acc, sm);
+        store_partials(a, SLOT_SS, acc[0]);
+        if (!grid_barrier(a.bar, a.err, epoch)) return;
+        if (blockIdx.x == 0) cta_ilu(a, SLO, YUP, (const VT *)nullptr, T2, [](int, VT, VT) {});
+      } else {
+        if (ilu) {
+          lower_solve<VT, LPR>(a, Y2, [&](int i) {
+            const VT s = R[i] - al * V[i];
+            S[i] = s;
+            acc[0] += (double)s * (double)s;
+            return s;
+          });
+          upper_solve<VT, LPR>(a, Y2, T2, [&](int, VT) {});
+        } else {
+          vec_loop<VT>(n, [&](int i, auto w) {
+            constexpr int W = decltype(w)::value;
+            VT r[W], v[W], d[W], sv[W], t[W];
+            vld<W>(R, i, r);
+            vld<W>(V, i, v);
+            if (jac) vld<W>(a.dvals, i, d);
+#pragma unroll
+            for (int q = 0; q < W; ++q) {
+              sv[q] = r[q] - al * v[q];
+              acc[0] += (double)sv[q] * (double)sv[q];
+              t[q] = jac ? diag_prec(sv[q], d[q]) : sv[q];
+            }
+            vst<W>(S, i, sv);
+            vst<W>(T2, i, t);
+          });
+        }
+        block_sum<1>(acc, sm);
+        store_partials(a, SLOT_SS, acc[0]);
       }
-      block_sum<1>(acc, sm);
-      store_partials(a, SLOT_SS, acc[0]);
     }
     if (!grid_barrier(a.bar, a.err, epoch)) return;
     // ---- T = A T2V; partials T.S, T.T
@@ -713,7 +1002,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) bicgstab_kernel(KArgs<VT> a) {
         }
         vst<W>(X, i, x);
         vst<W>(R, i, r);
-        if (ilu) {
+        if (ilu && !cta) {
           vfill<W>(T1, i, SENT);
           vfill<W>(T2, i, SENT);
           vfill<W>(Y1, i, SENT);

@@ -26,4 +26,13 @@ int rhs_scale(egpu_mat *A, const double *b_dev, const double *x_dev, double *bs,
 // FP32 SELL values, diagonal and (optionally) ILU0 factors for the inner solver
 int prepare_fp32_public(egpu_mat *A, bool with_ilu);
 
+// level-synchronous single-block ILU0 solves (egpu_tri_cta.cu)
+int build_cta_schedule(egpu_mat *A, const std::vector<int> &rows, const std::vector<int> &cols,
+                       const std::vector<int> &diag, const std::vector<int> &lo, const std::vector<int> &up,
+                       const std::vector<int> &lp, const std::vector<int> &lc, const std::vector<int> &upp,
+                       const std::vector<int> &uc);
+int cta_fill_values(egpu_mat *A);
+bool cta_use(const egpu_mat *A, int v);
+int cta_threads(const egpu_mat *A);
+
 }  // namespace egpu
