@@ -538,19 +538,25 @@ def run_serve(args, rank, world, local, pg):
     prm = eg.SolverParams(method=eg.BICGSTAB, precond=eg.PREC_ILU0, tol=args.tol, max_iter=20000,
                           inner_tol=args.inner_tol, abort_not_converged=False)
     reqs = server.poisson_stream(args.requests, rate=args.rate, m_lo=16, m_hi=128, seed=1 + rank, sigma=1.0)
-    srv = server.SolveServer(ctx, prm, hbm_budget=150e9, chunk=args.chunk)
-    for r in reqs:
-        srv.prototype(r.m)
     warm = server.poisson_stream(4, rate=1e6, m_lo=16, m_hi=24, seed=99, sigma=1.0)
-    for r in warm:
-        srv.prototype(r.m)
+    if args.py_server:
+        srv = server.SolveServer(ctx, prm, hbm_budget=150e9, chunk=args.chunk)
+        for r in reqs + warm:
+            srv.prototype(r.m)
+    else:  # the library's native server (worker thread in C++)
+        srv = server.NativeSolveServer(local, prm, hbm_budget=150e9, chunk=args.chunk)
+        for r in reqs + warm:
+            srv.mesh_prototype(r.m)
     srv.run(warm)
     barrier(pg, None)
     with ClockSampler(local) as clk:
         stats = srv.run(reqs, keep_solutions=True)
+    if not args.py_server:
+        srv.close()
+    protos = {m: server.MeshPrototype(ctx, m, eg.PREC_ILU0) for m in sorted({r.m for r in reqs})}
     alone = [server.Request(r.rid, r.m, r.seed, r.arrival) for r in reqs]
     fp = eg.SolverParams(method=eg.BICGSTAB, precond=eg.PREC_ILU0, tol=args.tol, max_iter=20000)
-    stats64 = server.run_one_at_a_time(ctx, fp, alone, srv.protos, keep_solutions=True)
+    stats64 = server.run_one_at_a_time(ctx, fp, alone, protos, keep_solutions=True)
     errs = [float(np.linalg.norm(r.x - a.x) / np.linalg.norm(a.x)) for r, a in zip(reqs, alone)]
     if rank == 0:
         line = {"metric": METRIC, "value": stats["solves_per_s"] * world, "unit": UNIT, "n_gpus": world,
@@ -558,6 +564,7 @@ def run_serve(args, rank, world, local, pg):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32 inner / f64 refinement", "data": "synthetic",
                 "config": {"workload": "serving_hex_poisson_bicgstab_ilu0", "requests": len(reqs),
+                           "server": "python" if args.py_server else "native (egpu_server_*)",
                            "rate_per_s": args.rate, "m_range": [16, 128], "hbm_budget_gb": 150,
                            "method": "BiCGStab", "preconditioner": "ILU0", "tol": args.tol, "precision": "mixed",
                            "parallelism": f"replicas{world}"},
@@ -587,6 +594,7 @@ def main():
     ap.add_argument("--rate", type=float, default=200.0, help="serving workload: mean arrivals per second")
     ap.add_argument("--chunk", type=int, default=32, help="batched/serving: inner iterations per launch")
     ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--py-server", action="store_true", help="serving workload: the Python server loop")
     args = ap.parse_args()
     rank, world, local, pg = dist_setup(args.gpus)
     try:

@@ -47,6 +47,14 @@ class Result(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ServerStats(C.Structure):
+    _fields_ = [("queued", C.c_longlong), ("resident", C.c_longlong), ("done", C.c_longlong),
+                ("steps", C.c_longlong), ("used_bytes", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class LibError(RuntimeError):
     pass
 
@@ -70,6 +78,7 @@ PROTOTYPES = {
     "egpu_matrix_free": (None, [_vp]),
     "egpu_matrix_clone": (C.c_int, [_vp, C.POINTER(_vp)]),
     "egpu_matrix_footprint": (C.c_longlong, [_vp, C.c_int]),
+    "egpu_matrix_prepare": (C.c_int, [_vp, C.c_int]),
     "egpu_iter_solve": (C.c_int, [_vp, _f64p, _f64p, C.POINTER(Params), C.POINTER(Result)]),
     "egpu_iter_solve_dev": (C.c_int, [_vp, _vp, _vp, C.POINTER(Params), C.POINTER(Result)]),
     "egpu_mv": (C.c_int, [_vp, _f64p, _f64p]),
@@ -97,6 +106,17 @@ PROTOTYPES = {
     "egpu_batch_remove": (C.c_int, [_vp, C.c_int]),
     "egpu_batch_tune": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "egpu_batch_free": (None, [_vp]),
+    "egpu_server_create": (C.c_int, [C.c_int, C.POINTER(Params), C.c_double, C.c_int, C.c_int, C.POINTER(_vp)]),
+    "egpu_server_pattern": (C.c_int, [_vp, C.c_int, _i32p, _i32p, _i32p, C.POINTER(C.c_int)]),
+    "egpu_server_pattern_mesh": (C.c_int, [_vp, C.c_int, C.c_int, _f64p, C.c_int, C.c_int, C.c_int, _i32p, _i32p,
+                                           C.c_int]),
+    "egpu_server_submit": (C.c_int, [_vp, C.c_int, _f64p, _f64p, C.POINTER(C.c_longlong)]),
+    "egpu_server_submit_poisson": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_int, _vp, C.c_int,
+                                             C.POINTER(C.c_longlong)]),
+    "egpu_server_poll": (C.c_int, [_vp, C.c_longlong, _vp, C.POINTER(Result)]),
+    "egpu_server_wait": (C.c_int, [_vp, C.c_longlong, C.c_double, _vp, C.POINTER(Result)]),
+    "egpu_server_info": (C.c_int, [_vp, C.POINTER(ServerStats)]),
+    "egpu_server_free": (None, [_vp]),
 }
 
 

@@ -120,101 +120,75 @@ __device__ __forceinline__ float slice_spmv(const SysDesc &d, int slice, int lan
   return s;
 }
 
-// Sync-free ILU0 solves of all systems in RUN state.  Every such system gets its own group
-// of participant warps, sized by its row count (at least one); inside a group the
-// system's slots are taken in level order, slot s by member s mod G, with the next slot's
-// packed entries fetched while the current one waits.  A row's dependencies are earlier
-// slots of its own group's members, all resident: deadlock free.
-__device__ void batch_tri_groups(const BatchArgs &a, BatchShared &sh) {
-  // weights n_s + ceil(W/P): every RUN system gets at least one participant
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    long long tot = 0;
-    for (int c = 0; c < sh.nact; c += 32) {
-      const int t = c + lane;
-      long long w = 0;
-      if (t < sh.nact && sh.status[sh.act[t]] == ST_RUN) w = a.sys[sh.act[t]].n;
-      long long v = w;
-#pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const long long u = __shfl_up_sync(0xffffffffu, v, off);
-        if (lane >= off) v += u;
-      }
-      if (t < sh.nact) sh.tcum[t + 1] = tot + v;
-      tot += __shfl_sync(0xffffffffu, v, 31);
-    }
-    if (lane == 0) sh.tcum[0] = 0;
-  }
-  __syncthreads();
+// Sync-free ILU0 solves over the systems in RUN state, slots interleaved across systems:
+// slot q -> system act[q % nact], position q / nact of its level order.  A row's
+// dependencies sit at smaller positions of the same system, hence at smaller slots, and
+// every participant takes its slots in increasing order: deadlock free.  The next slot's
+// packed entries are fetched while the current one waits.
+__device__ __forceinline__ bool batch_slot(const BatchArgs &a, const BatchShared &sh, long long q, int &ai, int &pos) {
+  ai = (int)(q % sh.nact);
+  pos = (int)(q / sh.nact);
+  const int s = sh.act[ai];
+  return sh.status[s] == ST_RUN && pos < a.sys[s].n;
 }
 
 template <bool LOWER, typename RHS, typename OUT>
 __device__ __forceinline__ void batch_tri(const BatchArgs &a, const BatchShared &sh, int yoff, int zoff, RHS &&rhs,
                                           OUT &&out) {
   const int local = threadIdx.x >> 5;
-  if (local >= a.tri_warps_per_block) return;
+  if (local >= a.tri_warps_per_block || sh.nact == 0) return;
   const int lane = threadIdx.x & 31;
   const int P = a.tri_warps_per_block * gridDim.x;
-  const int p = local * gridDim.x + blockIdx.x;
-  const long long W = sh.tcum[sh.nact];
-  if (W == 0) return;
-  // group boundaries b(t) = floor(t_weight * P / W') with W' = W + nrun*ceil(W/P) folded in by
-  // giving each RUN system an extra share: boundary(t) = floor((tcum[t] + t_run*e) * P / (W + nrun*e))
-  int nrun = 0;
-  for (int t = 0; t < sh.nact; ++t) nrun += sh.status[sh.act[t]] == ST_RUN;
-  const long long e = (W + P - 1) / P;
-  const long long Wp = W + (long long)nrun * e;
-  // run-count prefix is needed per boundary: recompute on the fly in the search
-  auto boundary = [&](int t) -> long long {
-    int r = 0;
-    for (int u = 0; u < t; ++u) r += sh.status[sh.act[u]] == ST_RUN;
-    return (sh.tcum[t] + (long long)r * e) * P / Wp;
+  int maxn = 0;
+  for (int t = 0; t < sh.nact; ++t)
+    if (sh.status[sh.act[t]] == ST_RUN) maxn = max(maxn, a.sys[sh.act[t]].n);
+  const long long nslot = (long long)maxn * sh.nact;
+  auto fetch = [&](long long q, int ai, int pos, TriRow<float> &t, float &dinv) {
+    const SysDesc &d = a.sys[sh.act[ai]];
+    const int *order = LOWER ? d.lower_order : d.upper_order;
+    const int *ptr = LOWER ? d.lo_ptr : d.up_ptr;
+    const int *cols = LOWER ? d.lo_cols : d.up_cols;
+    const float *vals = LOWER ? d.lo_vals : d.up_vals;
+    tri_fetch(t, pos, order, ptr, cols, vals, lane, d.n, a.err);
+    dinv = LOWER ? 0.f : __ldg(d.up_dinv + pos);
+    (void)q;
   };
-  int lo = 0, hi = sh.nact - 1;
-  while (lo < hi) {  // last t with boundary(t) <= p
-    const int mid = (lo + hi + 1) >> 1;
-    if (boundary(mid) <= p)
-      lo = mid;
-    else
-      hi = mid - 1;
-  }
-  const int ai = lo;
-  const int s = sh.act[ai];
-  if (sh.status[s] != ST_RUN) return;
-  const long long g0 = boundary(ai), g1 = boundary(ai + 1);
-  const int G = (int)(g1 - g0), j = (int)(p - g0);
-  if (G <= 0 || j < 0 || j >= G) return;
-  const SysDesc &d = a.sys[s];
-  const int *order = LOWER ? d.lower_order : d.upper_order;
-  const int *ptr = LOWER ? d.lo_ptr : d.up_ptr;
-  const int *cols = LOWER ? d.lo_cols : d.up_cols;
-  const float *vals = LOWER ? d.lo_vals : d.up_vals;
-  float *y = d.w + yoff * d.ldw, *z = d.w + zoff * d.ldw;
-  if (j >= d.n) return;
+  // first valid slot of this participant, and its successor
+  long long q = local * gridDim.x + blockIdx.x;
+  int ai = 0, pos = 0;
+  while (q < nslot && !batch_slot(a, sh, q, ai, pos)) q += P;
+  if (q >= nslot) return;
   TriRow<float> nxt;
-  tri_fetch(nxt, j, order, ptr, cols, vals, lane, d.n, a.err);
-  float dnext = LOWER ? 0.f : __ldg(d.up_dinv + j);
-  for (int q = j; q < d.n; q += G) {
+  float dnext;
+  fetch(q, ai, pos, nxt, dnext);
+  while (q < nslot) {
     const TriRow<float> cur = nxt;
     const float dinv = dnext;
-    if (q + G < d.n) {
-      tri_fetch(nxt, q + G, order, ptr, cols, vals, lane, d.n, a.err);
-      if (!LOWER) dnext = __ldg(d.up_dinv + q + G);
-    }
-    if (cur.row < 0) continue;
-    float r = 0.f;
-    if (LOWER && lane == 0) r = rhs(ai, s, d, cur.row);
-    const float acc = tri_dot(cur, LOWER ? y : z, cols, vals, lane, a.err);
-    if (lane == 0) {
-      if (LOWER) {
-        Sentinel<float>::publish(y + cur.row, r - acc);
-      } else {
-        const float yi = Sentinel<float>::wait(y + cur.row, a.err);
-        const float zi = dinv * (yi - acc);
-        Sentinel<float>::publish(z + cur.row, zi);
-        out(ai, s, d, cur.row, zi);
+    const int cai = ai;
+    long long qn = q + P;
+    while (qn < nslot && !batch_slot(a, sh, qn, ai, pos)) qn += P;
+    if (qn < nslot) fetch(qn, ai, pos, nxt, dnext);
+    const int s = sh.act[cai];
+    const SysDesc &d = a.sys[s];
+    const int *cols = LOWER ? d.lo_cols : d.up_cols;
+    const float *vals = LOWER ? d.lo_vals : d.up_vals;
+    float *y = d.w + yoff * d.ldw, *z = d.w + zoff * d.ldw;
+    if (cur.row >= 0) {
+      float r = 0.f;
+      if (LOWER && lane == 0) r = rhs(cai, s, d, cur.row);
+      const float acc = tri_dot(cur, LOWER ? y : z, cols, vals, lane, a.err);
+      if (lane == 0) {
+        if (LOWER) {
+          Sentinel<float>::publish(y + cur.row, r - acc);
+        } else {
+          const float yi = Sentinel<float>::wait(y + cur.row, a.err);
+          const float zi = dinv * (yi - acc);
+          Sentinel<float>::publish(z + cur.row, zi);
+          out(cai, s, d, cur.row, zi);
+        }
       }
     }
+    q = qn;
   }
 }
 
@@ -302,7 +276,6 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       ++it;
       break;
     }
-    if (ilu) batch_tri_groups(a, sh);
     if (!bicg) {
       // ============ CG ============
       // U: P = Z (k == 1) or Z + beta P;  clear PQ

@@ -75,7 +75,6 @@ struct BatchShared {
   int kk[BATCH_MAX_SYS];
   float sa[BATCH_MAX_SYS], sb[BATCH_MAX_SYS];  // per-phase scalars (beta, alpha, omega)
   double red[BATCH_MAX_SYS * 2];               // per-block per-system accumulators
-  long long tcum[BATCH_MAX_SYS + 1];           // weights of the triangular-solve groups
   int nact, total;
 };
 

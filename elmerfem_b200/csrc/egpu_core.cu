@@ -426,8 +426,57 @@ int scale_matrix(egpu_mat *A, bool scale_system) {
   return EGPU_OK;
 }
 
+// a clone's view of its prototype's level schedules (sync-free and single-block)
+static void view_tri(egpu_mat *A, const egpu_mat *proto) {
+  A->tri.lower_order.view(proto->tri.lower_order);
+  A->tri.upper_order.view(proto->tri.upper_order);
+  A->tri.lo_ptr.view(proto->tri.lo_ptr);
+  A->tri.lo_cols.view(proto->tri.lo_cols);
+  A->tri.lo_src.view(proto->tri.lo_src);
+  A->tri.up_ptr.view(proto->tri.up_ptr);
+  A->tri.up_cols.view(proto->tri.up_cols);
+  A->tri.up_src.view(proto->tri.up_src);
+  A->tri.up_dsrc.view(proto->tri.up_dsrc);
+  A->tri.lower_levels = proto->tri.lower_levels;
+  A->tri.upper_levels = proto->tri.upper_levels;
+  A->tri.max_lower = proto->tri.max_lower;
+  A->tri.max_upper = proto->tri.max_upper;
+  A->tri.max_width = proto->tri.max_width;
+  {
+    const TriSchedule &P = proto->tri;
+    TriSchedule &T = A->tri;
+    for (int v = 0; v < 2; ++v) {
+      T.cta_ok[v] = P.cta_ok[v];
+      T.cta_pd[v] = P.cta_pd[v];
+      T.cta_sb[v] = P.cta_sb[v];
+      T.cta_sr[v] = P.cta_sr[v];
+      T.cta_smem[v] = P.cta_smem[v];
+    }
+    T.cta_rs = P.cta_rs;
+    T.pos_lo.view(P.pos_lo);
+    T.pos_up.view(P.pos_up);
+    CtaTriHost *dst[2] = {&T.cta_lo, &T.cta_up};
+    const CtaTriHost *src[2] = {&P.cta_lo, &P.cta_up};
+    for (int k = 0; k < 2; ++k) {
+      dst[k]->nlev = src[k]->nlev;
+      dst[k]->nent = src[k]->nent;
+      dst[k]->lev.view(src[k]->lev);
+      dst[k]->ridx.view(src[k]->ridx);
+      dst[k]->src.view(src[k]->src);
+      dst[k]->map.view(src[k]->map);
+    }
+  }
+  A->tri_built = true;
+}
+
 int ensure_tri_schedule(egpu_mat *A) {
   if (A->tri_built) return EGPU_OK;
+  if (A->parent) {  // a clone shares its prototype's schedules, built once
+    const int rc = ensure_tri_schedule(A->parent);
+    if (rc) return rc;
+    view_tri(A, A->parent);
+    return EGPU_OK;
+  }
   egpu_ctx *ctx = A->ctx;
   const int n = A->n;
   std::vector<int> rows(n + 1), cols(A->nnz), diag(n);
@@ -1383,52 +1432,7 @@ extern "C" int egpu_matrix_clone(egpu_mat *proto, egpu_mat **out) {
   A->sell_cols.view(proto->sell_cols);
   A->sell_c16.view(proto->sell_c16);
   if (proto->cols16.p) A->cols16.view(proto->cols16);
-  if (!proto->tri_built) {
-    int rc = ensure_tri_schedule(proto);
-    if (rc) {
-      delete A;
-      return rc;
-    }
-  }
-  A->tri.lower_order.view(proto->tri.lower_order);
-  A->tri.upper_order.view(proto->tri.upper_order);
-  A->tri.lo_ptr.view(proto->tri.lo_ptr);
-  A->tri.lo_cols.view(proto->tri.lo_cols);
-  A->tri.lo_src.view(proto->tri.lo_src);
-  A->tri.up_ptr.view(proto->tri.up_ptr);
-  A->tri.up_cols.view(proto->tri.up_cols);
-  A->tri.up_src.view(proto->tri.up_src);
-  A->tri.up_dsrc.view(proto->tri.up_dsrc);
-  A->tri.lower_levels = proto->tri.lower_levels;
-  A->tri.upper_levels = proto->tri.upper_levels;
-  A->tri.max_lower = proto->tri.max_lower;
-  A->tri.max_upper = proto->tri.max_upper;
-  A->tri.max_width = proto->tri.max_width;
-  {
-    const TriSchedule &P = proto->tri;
-    TriSchedule &T = A->tri;
-    for (int v = 0; v < 2; ++v) {
-      T.cta_ok[v] = P.cta_ok[v];
-      T.cta_pd[v] = P.cta_pd[v];
-      T.cta_sb[v] = P.cta_sb[v];
-      T.cta_sr[v] = P.cta_sr[v];
-      T.cta_smem[v] = P.cta_smem[v];
-    }
-    T.cta_rs = P.cta_rs;
-    T.pos_lo.view(P.pos_lo);
-    T.pos_up.view(P.pos_up);
-    CtaTriHost *dst[2] = {&T.cta_lo, &T.cta_up};
-    const CtaTriHost *src[2] = {&P.cta_lo, &P.cta_up};
-    for (int k = 0; k < 2; ++k) {
-      dst[k]->nlev = src[k]->nlev;
-      dst[k]->nent = src[k]->nent;
-      dst[k]->lev.view(src[k]->lev);
-      dst[k]->ridx.view(src[k]->ridx);
-      dst[k]->src.view(src[k]->src);
-      dst[k]->map.view(src[k]->map);
-    }
-  }
-  A->tri_built = true;
+  if (proto->tri_built) view_tri(A, proto);
   const AssemblyData &P = proto->asmb;
   AssemblyData &S = A->asmb;
   S.nnodes = P.nnodes;
@@ -1456,6 +1460,15 @@ extern "C" int egpu_matrix_clone(egpu_mat *proto, egpu_mat **out) {
   proto->clones++;
   *out = A;
   return EGPU_OK;
+}
+
+// the preconditioner's one-time structures ahead of the first solve (ILU0 level schedules,
+// shared with every clone of the prototype)
+extern "C" int egpu_matrix_prepare(egpu_mat *A, int precond) {
+  if (!A || precond < EGPU_PREC_NONE || precond > EGPU_PREC_ILU0) return EGPU_ERR_ARG;
+  cudaSetDevice(A->ctx->device);
+  if (precond != EGPU_PREC_ILU0) return EGPU_OK;
+  return egpu::ensure_tri_schedule(A);
 }
 
 // device bytes a solve of this matrix holds (values, scaled and FP32 copies, factors,

@@ -33,14 +33,12 @@ int tri_mode_env() {
   return 0;
 }
 
-// Estimated seconds of one M^-1 application: sync-free, about 2 us per dependency level
-// (a cross-SM publish/observe round trip); single block, about 0.3 us per level plus the
-// factor stream at one SM's share of L2 bandwidth plus the extra grid barrier.
+// Estimated seconds of one M^-1 application, from B200 measurements of both solves on hex
+// meshes: sync-free, about 2 us per dependency level (a cross-SM publish/observe round
+// trip); single block, about 0.6 us per level plus 4 ns per row (its entries streamed and
+// summed by one SM), plus the extra grid barrier.
 double est_syncfree(int nlev_lo, int nlev_up) { return 2.0e-6 * (nlev_lo + nlev_up); }
-double est_block(int nlev_lo, int nlev_up, long long nent, int vsize, int n) {
-  const double bytes = (double)nent * (vsize + 2) + (double)n * (3 * vsize + 8);
-  return 0.3e-6 * (nlev_lo + nlev_up) + bytes / 120e9 + 4e-6;
-}
+double est_block(int nlev_lo, int nlev_up, int n) { return 0.6e-6 * (nlev_lo + nlev_up) + 4e-9 * 2.0 * n + 3e-6; }
 
 }  // namespace
 
@@ -78,11 +76,9 @@ int build_cta_schedule(egpu_mat *A, const std::vector<int> &rows, const std::vec
   plan::Plan P;
   plan::make_plan(n, rows, cols, diag, lo, up, lp, lc, upp, uc, CTA_SMEM_MAX, P);
   if (!P.ok) return EGPU_OK;
-  const long long nent = P.lo.nent + P.up.nent;
   bool any = false;
   for (int v = 0; v < 2; ++v)
-    if (P.fits[v] && (mode == 2 || est_block(P.lo.nlev, P.up.nlev, nent, v ? 4 : 8, n) <
-                                       est_syncfree(P.lo.nlev, P.up.nlev)))
+    if (P.fits[v] && (mode == 2 || est_block(P.lo.nlev, P.up.nlev, n) < est_syncfree(P.lo.nlev, P.up.nlev)))
       any = true;
   if (!any) return EGPU_OK;
   if (!plan::plan_arrays(P, n, lo, up, lp, lc, upp, uc)) {
@@ -158,8 +154,7 @@ bool cta_use(const egpu_mat *A, int v) {
   const int mode = tri_mode_env();
   if (mode == 1) return false;
   if (mode == 2) return true;
-  return est_block(S.cta_lo.nlev, S.cta_up.nlev, S.cta_lo.nent + S.cta_up.nent, v == 0 ? 8 : 4, A->n) <
-         est_syncfree(S.cta_lo.nlev, S.cta_up.nlev);
+  return est_block(S.cta_lo.nlev, S.cta_up.nlev, A->n) < est_syncfree(S.cta_lo.nlev, S.cta_up.nlev);
 }
 
 }  // namespace egpu

@@ -52,14 +52,17 @@ def poisson_stream(n: int, rate: float, m_lo: int, m_hi: int, seed: int, sigma: 
 
 
 class MeshPrototype:
-    """Resident pattern + bound mesh of one mesh size (built once, cloned per request)."""
+    """Resident pattern + bound mesh of one mesh size (built once, cloned per request); with a
+    preconditioner given, its one-time structures are built here too."""
 
-    def __init__(self, ctx: Context, m: int):
+    def __init__(self, ctx: Context, m: int, precond: int | None = None):
         self.m = m
         self.mesh = meshgen.hex_cube(m)
         self.pattern = create_matrix(self.mesh)
         self.A = Matrix(ctx, self.pattern)
         self.A.bind_assembly(self.mesh)
+        if precond is not None:
+            self.A.prepare(precond)
         self.con = np.sort(self.pattern.perm[self.mesh.boundary_nodes(range(1, 7)) - 1]).astype(np.int32)
 
 
@@ -77,7 +80,7 @@ class SolveServer:
 
     def prototype(self, m: int) -> MeshPrototype:
         if m not in self.protos:
-            self.protos[m] = MeshPrototype(self.ctx, m)
+            self.protos[m] = MeshPrototype(self.ctx, m, self.params.precond)
         return self.protos[m]
 
     def footprint(self, req: Request) -> float:
@@ -138,6 +141,137 @@ class SolveServer:
         return {"solves": len(done), "makespan_s": makespan, "solves_per_s": len(done) / makespan,
                 "p50_ms": 1000 * float(np.percentile(lat, 50)), "p99_ms": 1000 * float(np.percentile(lat, 99)),
                 "steps": steps, "converged": sum(1 for r in done if r.result.get("info") == 1)}
+
+
+class NativeSolveServer:
+    """The library's own continuous-batching server (egpu_server_*): admission, batch stepping
+    and retirement run on a native worker thread; this class registers mesh patterns, submits
+    requests and collects results."""
+
+    def __init__(self, device: int, params: SolverParams, hbm_budget: float = 150e9, chunk: int = 32,
+                 max_resident: int = 512):
+        import ctypes as C
+
+        from . import _lib
+        self._C, self._lib = C, _lib
+        self.params = params
+        self._prm = params.to_c()
+        h = C.c_void_p()
+        rc = _lib.lib().egpu_server_create(device, C.byref(self._prm), float(hbm_budget), chunk, max_resident,
+                                           C.byref(h))
+        if rc:
+            raise _lib.LibError(f"egpu_server_create: {_lib.ERRORS.get(rc, rc)}")
+        self._h = h
+        self.patterns: dict[int, tuple] = {}  # m -> (pattern id, (mesh, CRS pattern, Dirichlet rows))
+
+    def _check(self, rc, what):
+        if rc < 0:
+            raise self._lib.LibError(f"{what}: {self._lib.ERRORS.get(rc, rc)}")
+        return rc
+
+    def pattern(self, pat) -> int:
+        C = self._C
+        pid = C.c_int()
+        self._check(self._lib.lib().egpu_server_pattern(self._h, pat.n, pat.rows, pat.cols, pat.diag, C.byref(pid)),
+                    "egpu_server_pattern")
+        return pid.value
+
+    def mesh_prototype(self, m: int) -> int:
+        """Pattern of the m^3 hex mesh with the mesh bound for device assembly (once per m)."""
+        if m in self.patterns:
+            return self.patterns[m][0]
+        mesh = meshgen.hex_cube(m)
+        pat = create_matrix(mesh)
+        pid = self.pattern(pat)
+        self._check(self._lib.lib().egpu_server_pattern_mesh(
+            self._h, pid, mesh.nnodes, np.ascontiguousarray(mesh.coords, np.float64), 3, mesh.nelem,
+            mesh.elem_code, np.ascontiguousarray(mesh.elements, np.int32), pat.perm, pat.dofs),
+            "egpu_server_pattern_mesh")
+        con = np.sort(pat.perm[mesh.boundary_nodes(range(1, 7)) - 1]).astype(np.int32)
+        self.patterns[m] = (pid, (mesh, pat, con))
+        return pid
+
+    def submit(self, pid: int, values, rhs) -> int:
+        C = self._C
+        rid = C.c_longlong()
+        self._check(self._lib.lib().egpu_server_submit(self._h, pid, np.ascontiguousarray(values, np.float64),
+                                                       np.ascontiguousarray(rhs, np.float64), C.byref(rid)),
+                    "egpu_server_submit")
+        return rid.value
+
+    def submit_poisson(self, pid: int, elem_k=None, nodal_k=None, load=None, con=None, symmetric=False) -> int:
+        C = self._C
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float64) for a in (elem_k, nodal_k, load)]
+        c = np.ascontiguousarray(con if con is not None else [], np.int32)
+        rid = C.c_longlong()
+        self._check(self._lib.lib().egpu_server_submit_poisson(
+            self._h, pid, *[None if a is None else a.ctypes.data for a in arrs], c.size,
+            c.ctypes.data if c.size else None, int(symmetric), C.byref(rid)), "egpu_server_submit_poisson")
+        return rid.value
+
+    def poll(self, rid: int, n: int | None = None):
+        """(x, result) when the request has finished (x None when n is None), else None."""
+        C = self._C
+        res = self._lib.Result()
+        x = None if n is None else np.zeros(n)
+        rc = self._check(self._lib.lib().egpu_server_poll(self._h, rid, None if x is None else x.ctypes.data,
+                                                          C.byref(res)), "egpu_server_poll")
+        return (x, res.as_dict()) if rc == 1 else None
+
+    def wait(self, rid: int, n: int | None = None, timeout: float = 600.0):
+        C = self._C
+        res = self._lib.Result()
+        x = None if n is None else np.zeros(n)
+        self._check(self._lib.lib().egpu_server_wait(self._h, rid, float(timeout),
+                                                     None if x is None else x.ctypes.data, C.byref(res)),
+                    "egpu_server_wait")
+        return x, res.as_dict()
+
+    def info(self) -> dict:
+        st = self._lib.ServerStats()
+        self._check(self._lib.lib().egpu_server_info(self._h, self._C.byref(st)), "egpu_server_info")
+        return st.as_dict()
+
+    def close(self):
+        if self._h:
+            self._lib.lib().egpu_server_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, requests: list[Request], keep_solutions: bool = False, clock=time.perf_counter) -> dict:
+        """Submit the stream at its arrival times (device assembly per request), wait for every
+        result; latency = the server's own submission-to-completion time."""
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        for r in reqs:
+            self.mesh_prototype(r.m)
+        ids = []
+        t0 = clock()
+        for r in reqs:
+            now = clock() - t0
+            if r.arrival > now:
+                time.sleep(r.arrival - now)
+            pid, (mesh, pat, con) = self.patterns[r.m]
+            rng = np.random.Generator(np.random.PCG64(r.seed))
+            k = np.exp(rng.normal(0.0, r.sigma, size=mesh.nelem))
+            load = rng.random(mesh.nnodes)
+            r.admitted = clock() - t0
+            ids.append(self.submit_poisson(pid, elem_k=k, load=load, con=con))
+        for r, rid in zip(reqs, ids):
+            n = self.patterns[r.m][1][1].n
+            x, res = self.wait(rid, n if keep_solutions else None)
+            r.result = res
+            r.x = x
+            r.finished = r.admitted + res["seconds"]
+        lat = np.array([r.result["seconds"] for r in reqs])
+        makespan = max(r.finished for r in reqs) - min(r.arrival for r in reqs)
+        return {"solves": len(reqs), "makespan_s": makespan, "solves_per_s": len(reqs) / makespan,
+                "p50_ms": 1000 * float(np.percentile(lat, 50)), "p99_ms": 1000 * float(np.percentile(lat, 99)),
+                "steps": self.info()["steps"], "converged": sum(1 for r in reqs if r.result.get("info") == 1)}
 
 
 def run_one_at_a_time(ctx: Context, params: SolverParams, requests: list[Request], protos: dict,

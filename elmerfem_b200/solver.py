@@ -238,6 +238,10 @@ class Matrix:
         return v
 
     # ---- preconditioner state (A%ILUValues, A%DiagScaling)
+    def prepare(self, precond: int):
+        """One-time preconditioner structures (ILU0 level schedules) before the first solve."""
+        check(lib().egpu_matrix_prepare(self._h, int(precond)), self.ctx.handle, "egpu_matrix_prepare")
+
     def ilu0(self, scale_system: bool = True):
         """Factor ILU0 on the device; returns (ILUValues with inverted U diagonal, DiagScaling)."""
         check(lib().egpu_ilu0_build(self._h, int(scale_system)), self.ctx.handle, "egpu_ilu0_build")

@@ -110,6 +110,10 @@ void egpu_matrix_free(egpu_mat *A);
  * with its own Values, right-hand side and solve buffers.  proto may be freed before its
  * clones; the shared data goes with the last of them. */
 int egpu_matrix_clone(egpu_mat *proto, egpu_mat **out);
+/* Builds the preconditioner's one-time structures before the first solve (for ILU0 the
+ * level schedules of the triangular solves; nothing for Diagonal / None), so that the first
+ * IterSolver call on a pattern costs what later ones do.  Clones share their prototype's. */
+int egpu_matrix_prepare(egpu_mat *A, int precond);
 /* device bytes a solve of A holds beyond the shared pattern, for the given preconditioner */
 long long egpu_matrix_footprint(const egpu_mat *A, int precond);
 
@@ -201,6 +205,46 @@ int egpu_batch_solution(egpu_batch *B, int sys, double *x);
 int egpu_batch_remove(egpu_batch *B, int sys);
 int egpu_batch_tune(egpu_batch *B, int *chunk_out);
 void egpu_batch_free(egpu_batch *B);
+
+/* ---- solve server (no counterpart in the reference; the serving extension of SolveSystem,
+ * SolverUtils.src:7531, for a stream of independent systems).  The server owns its own
+ * context and a batch, and runs a host worker thread: it admits submitted requests in
+ * arrival order while their device footprint fits hbm_budget_bytes and a batch slot is free
+ * (at most max_resident at once; one request larger than the budget runs alone), prepares
+ * them (clone of the registered pattern's resident prototype; Values and RHS from the
+ * request, or GPU assembly + Dirichlet rows), steps the batch (egpu_batch_step: mixed
+ * precision, prm's method / preconditioner / tolerance) and retires converged systems.
+ * Every entry point may be called from any thread.
+ *   egpu_server_pattern       registers a Matrix_t pattern (1-based Rows/Cols/Diag); once per mesh
+ *   egpu_server_pattern_mesh  binds the mesh to a pattern (as egpu_assembly_bind) for
+ *                             egpu_server_submit_poisson
+ *   egpu_server_submit        Values (nnz) and RHS (n) from the host, copied at the call
+ *   egpu_server_submit_poisson  per-element / per-node conductivity, nodal load (NULL: as in
+ *                             egpu_assemble_poisson), 1-based Dirichlet rows set to zero
+ *   egpu_server_poll          1 and the solution (x, n values; NULL to skip) and result when
+ *                             the request has finished, releasing it; 0 while it has not
+ *   egpu_server_wait          egpu_server_poll blocking up to timeout_s (EGPU_ERR_TIMEOUT)
+ * A finished request's res.seconds is its latency from submission to completion and
+ * res.seconds_setup its time in the queue; res.info is its HUTI status, or a negative
+ * library error when its preparation or the batch failed. */
+typedef struct egpu_server egpu_server;
+typedef struct {
+  long long queued, resident, done, steps;
+  double used_bytes;
+} egpu_server_stats;
+int egpu_server_create(int device, const egpu_params *prm, double hbm_budget_bytes, int chunk_iters,
+                       int max_resident, egpu_server **out);
+int egpu_server_pattern(egpu_server *S, int n, const int *rows, const int *cols, const int *diag, int *pattern);
+int egpu_server_pattern_mesh(egpu_server *S, int pattern, int nnodes, const double *xyz, int cdim, int nelem,
+                             int code, const int *elem_nodes, const int *perm, int dofs);
+int egpu_server_submit(egpu_server *S, int pattern, const double *values, const double *rhs, long long *request);
+int egpu_server_submit_poisson(egpu_server *S, int pattern, const double *elem_k, const double *nodal_k,
+                               const double *load, int ncon, const int *con_rows, int symmetric,
+                               long long *request);
+int egpu_server_poll(egpu_server *S, long long request, double *x, egpu_result *res);
+int egpu_server_wait(egpu_server *S, long long request, double timeout_s, double *x, egpu_result *res);
+int egpu_server_info(egpu_server *S, egpu_server_stats *st);
+void egpu_server_free(egpu_server *S);
 
 #ifdef __cplusplus
 }
