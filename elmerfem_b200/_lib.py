@@ -47,6 +47,14 @@ class Result(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BatchConfig(C.Structure):
+    _fields_ = [("chunk_iters", C.c_int), ("blocks_per_sm", C.c_int), ("tri_mult", C.c_int),
+                ("candidates", C.c_int), ("rate", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class ServerStats(C.Structure):
     _fields_ = [("queued", C.c_longlong), ("resident", C.c_longlong), ("done", C.c_longlong),
                 ("steps", C.c_longlong), ("used_bytes", C.c_double)]
@@ -104,7 +112,8 @@ PROTOTYPES = {
     "egpu_batch_result": (C.c_int, [_vp, C.c_int, C.POINTER(Result)]),
     "egpu_batch_solution": (C.c_int, [_vp, C.c_int, _f64p]),
     "egpu_batch_remove": (C.c_int, [_vp, C.c_int]),
-    "egpu_batch_tune": (C.c_int, [_vp, C.POINTER(C.c_int)]),
+    "egpu_batch_tune": (C.c_int, [_vp, C.POINTER(BatchConfig)]),
+    "egpu_batch_set_config": (C.c_int, [_vp, C.POINTER(BatchConfig)]),
     "egpu_batch_free": (None, [_vp]),
     "egpu_server_create": (C.c_int, [C.c_int, C.POINTER(Params), C.c_double, C.c_int, C.c_int, C.POINTER(_vp)]),
     "egpu_server_pattern": (C.c_int, [_vp, C.c_int, _i32p, _i32p, _i32p, C.POINTER(C.c_int)]),

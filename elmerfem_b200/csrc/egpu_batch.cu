@@ -642,6 +642,7 @@ struct BatchSys {
   double residual = 0.0, bnorm_s = 1.0, rnorm = 0.0;  // rnorm: ||r|| that started the inner solve
   DevBuf<double> xout;    // back-scaled solution
   double t_admit = 0.0;
+  bool reported = false;  // listed as finished by egpu_batch_step
 };
 
 struct egpu_batch {
@@ -658,8 +659,13 @@ struct egpu_batch {
   bool desc_dirty = true;
   egpu_params prm{};
   int chunk = 64;
-  int tri_mult = 2;
+  int tri_mult = 2;       // sync-free participants: tri_mult x widest level x running systems
+  int bps = 2;            // blocks of the persistent inner kernel per SM (1 or 2)
   long long launches = 0;
+  // the last inner launch: device milliseconds, inner iterations run, nonzeros of its systems
+  float last_ms = 0.f;
+  int last_iters = 0;
+  long long last_nnz = 0;
 };
 
 static int slot_of(egpu_batch *B) {
@@ -852,6 +858,13 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
     EGPU_CUDA_TRY(ctx, cudaMemcpy(B->d_ref.p, r.data(), ns * sizeof(RefDesc), cudaMemcpyHostToDevice));
     B->desc_dirty = false;
   }
+  // systems that finished while nobody collected the list (egpu_batch_tune) are listed now
+  if (finished)
+    for (int i = 0; i < ns; ++i)
+      if (B->sys[i] && B->sys[i]->phase == 3 && !B->sys[i]->reported) {
+        finished[nf++] = i;
+        B->sys[i]->reported = true;
+      }
   // ---- refinement: residual for systems in phase 1
   std::vector<int> sel;
   for (int i = 0; i < ns; ++i)
@@ -911,7 +924,10 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
       B->launches++;
       for (int i : done) {
         B->sys[i]->phase = 3;
-        if (finished) finished[nf] = i;
+        if (finished) {
+          finished[nf] = i;
+          B->sys[i]->reported = true;
+        }
         nf++;
       }
     }
@@ -937,11 +953,15 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
       if (B->sys[i] && B->sys[i]->phase == 2) maxw = std::max(maxw, B->sys[i]->A->tri.max_width);
     int bps = 0;
     EGPU_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_batch_inner, EGPU_BLOCK, 0));
-    bps = std::max(1, std::min(bps, 2));
+    bps = std::max(1, std::min(bps, B->bps));
     const int grid = ctx->num_sms * bps;
     int nrun = 0;
+    long long nnz_run = 0;
     for (int i = 0; i < ns; ++i)
-      if (B->sys[i] && B->sys[i]->phase == 2) nrun++;
+      if (B->sys[i] && B->sys[i]->phase == 2) {
+        nrun++;
+        nnz_run += B->sys[i]->A->nnz;
+      }
     a.tri_warps_per_block = std::max((nrun + grid - 1) / grid,
                                      std::min(EGPU_BLOCK / 32, (B->tri_mult * maxw * nrun + grid - 1) / grid));
     a.tri_warps_per_block = std::max(1, std::min(EGPU_BLOCK / 32, a.tri_warps_per_block));
@@ -950,8 +970,10 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
     a.it_done = B->d_it.p;
     int parity0 = B->parity;
     void *args[] = {&a, &parity0};
+    EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ek0, ctx->stream));
     EGPU_CUDA_TRY(ctx, cudaLaunchCooperativeKernel((const void *)k_batch_inner, dim3(grid), dim3(EGPU_BLOCK), args, 0,
                                                    ctx->stream));
+    EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ek1, ctx->stream));
     ctx->launches++;
     B->launches++;
     int hit[2] = {0, 0};
@@ -964,6 +986,9 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
       return (int)herr[1];
     }
     B->parity = (B->parity + hit[0]) & 1;
+    cudaEventElapsedTime(&B->last_ms, ctx->ek0, ctx->ek1);
+    B->last_iters = hit[0];
+    B->last_nnz = nnz_run;
     EGPU_CUDA_TRY(ctx, cudaMemcpy(st.data(), B->d_state.p, 2 * BATCH_MAX_SYS * sizeof(SysState), cudaMemcpyDeviceToHost));
     std::vector<int> upd;
     for (int i = 0; i < ns; ++i) {
@@ -997,6 +1022,15 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
     }
   }
   if (nfinished) *nfinished = nf;
+  return EGPU_OK;
+}
+
+extern "C" int egpu_batch_set_config(egpu_batch *B, const egpu_batch_config *cfg) {
+  if (!B || !cfg || cfg->chunk_iters < 1 || cfg->blocks_per_sm < 1 || cfg->blocks_per_sm > 2 || cfg->tri_mult < 1)
+    return EGPU_ERR_ARG;
+  B->chunk = cfg->chunk_iters;
+  B->bps = cfg->blocks_per_sm;
+  B->tri_mult = cfg->tri_mult;
   return EGPU_OK;
 }
 
@@ -1074,11 +1108,58 @@ extern "C" int egpu_batch_solve(egpu_batch *B, egpu_result *per_system) {
   return EGPU_OK;
 }
 
-// Autotuner: times one chunk of inner iterations at each candidate chunk length and
-// sync-free participant multiplier on the resident systems (state is re-initialised
-// afterwards), keeps the fastest per iteration.
-extern "C" int egpu_batch_tune(egpu_batch *B, int *chunk_out) {
+// Autotuner.  Runs real steps of the resident systems (their progress is kept) with each
+// candidate configuration in turn: chunk length (inner iterations per launch), blocks of
+// the persistent kernel per SM, and, with ILU0, the sync-free participant multiplier.  The
+// rate of a step is inner iterations x nonzeros of the systems in the launch per device
+// second of the launch; the fastest configuration is kept.  Candidates are tried once each,
+// in a fixed order, while systems remain in inner solves; systems that finish meanwhile are
+// listed by the next egpu_batch_step.
+extern "C" int egpu_batch_tune(egpu_batch *B, egpu_batch_config *cfg) {
   if (!B) return EGPU_ERR_ARG;
-  if (chunk_out) *chunk_out = B->chunk;
+  struct Cand {
+    int chunk, bps, tri_mult;
+  };
+  std::vector<Cand> cands;
+  const bool ilu = B->prm.precond == EGPU_PREC_ILU0;
+  for (int bps : {2, 1})
+    for (int chunk : {16, 32, 64})
+      for (int tm : {1, 2, 4}) {
+        if (!ilu && tm != 2) continue;
+        cands.push_back({chunk, bps, tm});
+      }
+  Cand best{B->chunk, B->bps, B->tri_mult};
+  double best_rate = 0.0;
+  int tried = 0;
+  // a first step brings every system into its inner solve
+  int rc = egpu_batch_step(B, nullptr, nullptr);
+  if (rc) return rc;
+  for (const Cand &c : cands) {
+    if (egpu_batch_pending(B) == 0) break;
+    B->chunk = c.chunk;
+    B->bps = c.bps;
+    B->tri_mult = c.tri_mult;
+    B->last_iters = 0;
+    B->last_ms = 0.f;
+    rc = egpu_batch_step(B, nullptr, nullptr);
+    if (rc) return rc;
+    if (B->last_iters <= 0 || B->last_ms <= 0.f) continue;
+    const double rate = (double)B->last_iters * (double)B->last_nnz / (B->last_ms * 1e-3);
+    ++tried;
+    if (rate > best_rate) {
+      best_rate = rate;
+      best = c;
+    }
+  }
+  B->chunk = best.chunk;
+  B->bps = best.bps;
+  B->tri_mult = best.tri_mult;
+  if (cfg) {
+    cfg->chunk_iters = best.chunk;
+    cfg->blocks_per_sm = best.bps;
+    cfg->tri_mult = best.tri_mult;
+    cfg->candidates = tried;
+    cfg->rate = best_rate;
+  }
   return EGPU_OK;
 }

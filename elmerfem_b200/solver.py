@@ -365,6 +365,17 @@ class Batch:
     def pending(self) -> int:
         return check(lib().egpu_batch_pending(self._h), self.ctx.handle, "egpu_batch_pending")
 
+    def tune(self) -> dict:
+        """egpu_batch_tune: picks chunk length, blocks per SM and triangular-solve participants
+        by timing real steps of the resident systems; returns the kept configuration."""
+        cfg = _lib.BatchConfig()
+        check(lib().egpu_batch_tune(self._h, C.byref(cfg)), self.ctx.handle, "egpu_batch_tune")
+        return cfg.as_dict()
+
+    def set_config(self, cfg: dict):
+        c = _lib.BatchConfig(**{k: cfg[k] for k, _ in _lib.BatchConfig._fields_})
+        check(lib().egpu_batch_set_config(self._h, C.byref(c)), self.ctx.handle, "egpu_batch_set_config")
+
     def solve(self):
         check(lib().egpu_batch_solve(self._h, None), self.ctx.handle, "egpu_batch_solve")
 

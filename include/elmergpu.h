@@ -203,7 +203,17 @@ int egpu_batch_solve(egpu_batch *B, egpu_result *per_system);
 int egpu_batch_result(egpu_batch *B, int sys, egpu_result *res);
 int egpu_batch_solution(egpu_batch *B, int sys, double *x);
 int egpu_batch_remove(egpu_batch *B, int sys);
-int egpu_batch_tune(egpu_batch *B, int *chunk_out);
+/* Autotuner: runs real steps of the resident systems with each candidate configuration
+ * (inner iterations per launch, persistent-kernel blocks per SM, sync-free triangular-solve
+ * participants) and keeps the fastest by nonzeros x iterations per device second.  Systems
+ * that finish while tuning are listed by the next egpu_batch_step. */
+typedef struct {
+  int chunk_iters, blocks_per_sm, tri_mult, candidates;
+  double rate;  /* nonzeros x inner iterations per second of the kept configuration */
+} egpu_batch_config;
+int egpu_batch_tune(egpu_batch *B, egpu_batch_config *cfg);
+/* applies a configuration (e.g. one egpu_batch_tune chose for an earlier batch of the same kind) */
+int egpu_batch_set_config(egpu_batch *B, const egpu_batch_config *cfg);
 void egpu_batch_free(egpu_batch *B);
 
 /* ---- solve server (no counterpart in the reference; the serving extension of SolveSystem,

@@ -107,3 +107,33 @@ def test_admission_while_running(ctx):
     p, v, b = later[0]
     assert B.add(_pat(p), v, b) == victim
     B.free()
+
+
+@pytest.mark.parametrize("method,prec,make", [(eg.CG, eg.PREC_DIAGONAL, _tet_system),
+                                              (eg.BICGSTAB, eg.PREC_ILU0, _hex_system)])
+def test_autotuner_keeps_results_and_reports_every_system(ctx, method, prec, make):
+    """egpu_batch_tune runs real steps: afterwards every system is still solved to the oracle's
+    answer, and each one is listed as finished exactly once by the step loop."""
+    sizes = [3, 4, 5, 6, 7, 8, 9, 10, 4, 6, 8, 5]
+    systems = [make(m, 40 + i) for i, m in enumerate(sizes)]
+    prm = eg.SolverParams(method=method, precond=prec, tol=TOL, max_iter=5000, inner_tol=3e-4)
+    B = eg.Batch(ctx, prm, chunk=16)
+    ids = [B.add(_pat(p), v, b) for p, v, b in systems]
+    cfg = B.tune()
+    assert cfg["candidates"] >= 1 and cfg["rate"] > 0
+    assert cfg["chunk_iters"] in (16, 32, 64) and cfg["blocks_per_sm"] in (1, 2) and cfg["tri_mult"] in (1, 2, 4)
+    seen = []
+    for _ in range(100000):
+        seen += B.step()
+        if B.pending() == 0:
+            seen += B.step()  # lists any system that finished in the last step's refinement check
+            break
+    assert sorted(seen) == sorted(ids)
+    for sid, (p, v, b) in zip(ids, systems):
+        assert B.result(sid)["info"] == 1
+        x_ref, _ = oracle.solve(p, v, b, method=method, precond=prec, max_iter=5000, tol=TOL)
+        assert rel(B.solution(sid), x_ref) < 1e-8
+    B2 = eg.Batch(ctx, prm)
+    B2.set_config(cfg)
+    B2.free()
+    B.free()
