@@ -592,7 +592,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="poisson128_cg_jacobi")
     ap.add_argument("--fp64-steps", type=int, default=2)
-    ap.add_argument("--inner-tol", type=float, default=3e-4)
+    ap.add_argument("--inner-tol", type=float, default=0.0, help="0: the library's choice by preconditioner")
     ap.add_argument("--ref-iters", type=int, default=0, help="FP64 iteration count for the reference arm")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--systems", type=int, default=512, help="batched workload: number of systems")

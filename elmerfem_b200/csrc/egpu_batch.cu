@@ -946,7 +946,7 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
     a.method = B->prm.method;
     a.precond = B->prm.precond;
     a.kmax = B->chunk;
-    a.tol = B->prm.inner_tol;
+    a.tol = inner_tol_of(&B->prm);
     a.maxit = B->prm.inner_max_iter;
     int maxw = 1;
     for (int i = 0; i < ns; ++i)

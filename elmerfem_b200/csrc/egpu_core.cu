@@ -1042,7 +1042,7 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
       a.precond = prm->precond;
       a.maxit = std::max(1, std::min(prm->inner_max_iter, prm->max_iter - r.iters));
       a.true_residual = 0;
-      a.tol = prm->inner_tol;
+      a.tol = inner_tol_of(prm);
       a.b = r32;
       a.x = d32;
       a.w = W32;
@@ -1206,7 +1206,7 @@ extern "C" void egpu_params_default(egpu_params *p, int method, int precond) {
   p->precision = EGPU_FP64;
   p->refactorize = 1;
   p->precond_recompute = 1;
-  p->inner_tol = 1e-4;
+  p->inner_tol = 0.0;  // by preconditioner (inner_tol_of)
   p->inner_max_iter = 2000;
   p->max_refinements = 30;
 }

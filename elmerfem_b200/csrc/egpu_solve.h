@@ -5,6 +5,14 @@
 
 namespace egpu {
 
+// inner tolerance of the mixed-precision refinement; 0 picks it by preconditioner (tuned on
+// B200: 3e-4 for CG/BiCGStab with Diagonal or none, 3e-3 with ILU0, whose latency-bound
+// iterations make more, shorter refinements pay)
+inline double inner_tol_of(const egpu_params *p) {
+  if (p->inner_tol > 0) return p->inner_tol;
+  return p->precond == EGPU_PREC_ILU0 ? 3e-3 : 3e-4;
+}
+
 int ensure_ctx_scratch(egpu_ctx *ctx);
 int reset_sync(egpu_ctx *ctx);
 int scale_matrix(egpu_mat *A, bool scale_system);
