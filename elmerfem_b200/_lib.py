@@ -106,6 +106,7 @@ PROTOTYPES = {
     "egpu_batch_add": (C.c_int, [_vp, C.c_int, _i32p, _i32p, _i32p, _f64p, _f64p]),
     "egpu_batch_add_matrix": (C.c_int, [_vp, _vp, _vp]),
     "egpu_batch_set_chunk": (C.c_int, [_vp, C.c_int]),
+    "egpu_batch_set_latency_mode": (C.c_int, [_vp, C.c_int]),
     "egpu_batch_step": (C.c_int, [_vp, _vp, C.POINTER(C.c_int)]),
     "egpu_batch_pending": (C.c_int, [_vp]),
     "egpu_batch_solve": (C.c_int, [_vp, _vp]),

@@ -207,9 +207,12 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
   int it = 0;
   for (; it < a.kmax; ++it) {
     const int rd = (parity0 + it) & 1, wr = rd ^ 1;
+    if (threadIdx.x == 0) sh.any_done = 0;
+    __syncthreads();
     // ---------------- top: decisions for every system (identical in every block)
     for (int s = threadIdx.x; s < a.nsys; s += blockDim.x) {
       SysState st = a.state[rd * BATCH_MAX_SYS + s];
+      const int status0 = st.status;
       const double *acc = a.acc;
       float beta = 0.f;
       if (st.status == ST_INIT) {
@@ -219,9 +222,13 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
         st.rho = acc[BA_RHO * BATCH_MAX_SYS + s];
         st.r0norm = sqrt(acc[BA_RR * BATCH_MAX_SYS + s]);
         st.k = 1;
-        st.alpha = 0.0;
-        st.omega = 1.0;
-        st.oldrho = 1.0;
+        if (st.resume) {  // alpha, omega carried; rho_{k-1} given in the new scale
+          st.oldrho = st.carry_rho;
+        } else {
+          st.alpha = 0.0;
+          st.omega = 1.0;
+          st.oldrho = 1.0;
+        }
         st.residual = 1.0;
         if (!(st.r0norm > 0.0)) {
           st.status = ST_DONE;
@@ -261,9 +268,11 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
           st.k += 1;
         }
       }
+      if (st.status == ST_DONE && status0 != ST_DONE) sh.any_done = 1;
       if (st.status == ST_RUN)
         beta = bicg ? (float)((st.rho * st.alpha) / (st.oldrho * st.omega)) : (float)(st.rho / st.oldrho);
       sh.status[s] = st.status;
+      sh.fresh[s] = st.resume ? 0 : 1;
       sh.kk[s] = st.k;
       sh.sb[s] = beta;
       sh.sa[s] = (float)st.omega;
@@ -287,7 +296,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
         if (r >= d.n) return;
         float *Z = d.w + d.ldw, *P = d.w + 2 * d.ldw;
         const float z = Z[r];
-        P[r] = sh.kk[s] == 1 ? z : z + sh.sb[s] * P[r];
+        P[r] = (sh.kk[s] == 1 && sh.fresh[s]) ? z : z + sh.sb[s] * P[r];
       });
       if (!grid_barrier(a.bar, a.err, epoch)) return;
       // S: Q = A P; PQ;  clear RHO, RR
@@ -482,15 +491,17 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
               rt_r = (double)RT[r] * (double)rv;
               rr = (double)rv * (double)rv;
             }
-          } else {
+          } else {  // init: R = B, X = 0; fresh: RT = B, P = V = 0 (resumed: kept)
             const float b = d.b[r];
             R[r] = b;
-            RT[r] = b;
             d.x[r] = 0.f;
-            P[r] = 0.f;
-            V[r] = 0.f;
-            rt_r = (double)b * (double)b;
-            rr = rt_r;
+            if (sh.fresh[s]) {
+              RT[r] = b;
+              P[r] = 0.f;
+              V[r] = 0.f;
+            }
+            rt_r = (double)RT[r] * (double)b;
+            rr = (double)b * (double)b;
           }
           if (ilu) {
             T1[r] = SENT;
@@ -508,6 +519,12 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       });
       batch_flush(a, sh, BA_RHO, BA_RR);
       if (!grid_barrier(a.bar, a.err, epoch)) return;
+    }
+    // latency mode: hand a finished system back to the host at once (its refinement and
+    // retirement happen between launches); the iteration just run completes for the others
+    if (a.exit_on_done && sh.any_done) {
+      ++it;
+      break;
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) *a.it_done = it;
@@ -643,6 +660,8 @@ struct BatchSys {
   DevBuf<double> xout;    // back-scaled solution
   double t_admit = 0.0;
   bool reported = false;  // listed as finished by egpu_batch_step
+  double rnorm_prev = 1.0;  // ||r|| that started the previous inner segment
+  int last_info = 0;        // how the previous inner segment ended
 };
 
 struct egpu_batch {
@@ -661,6 +680,8 @@ struct egpu_batch {
   int chunk = 64;
   int tri_mult = 2;       // sync-free participants: tri_mult x widest level x running systems
   int bps = 2;            // blocks of the persistent inner kernel per SM (1 or 2)
+  bool resume_ok = true;  // reliable updating between segments (EGPU_MIXED_RESTART=1: off)
+  bool exit_on_done = false;  // latency mode (egpu_batch_set_latency_mode)
   long long launches = 0;
   // the last inner launch: device milliseconds, inner iterations run, nonzeros of its systems
   float last_ms = 0.f;
@@ -694,8 +715,9 @@ extern "C" int egpu_batch_create(egpu_ctx *ctx, const egpu_params *prm, egpu_bat
   cudaMemset(B->d_acc.p, 0, BA_NSLOT * BATCH_MAX_SYS * sizeof(double));
   B->prm = *prm;
   B->prm.precision = EGPU_MIXED;
+  if (const char *e = std::getenv("EGPU_MIXED_RESTART")) B->resume_ok = e[0] != '1';
   if (B->prm.inner_max_iter < 1) B->prm.inner_max_iter = 2000;
-  if (B->prm.max_refinements < 1) B->prm.max_refinements = 30;
+  if (B->prm.max_refinements < 1) B->prm.max_refinements = 100;
   *out = B;
   return EGPU_OK;
 }
@@ -893,6 +915,7 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
         S->info = EGPU_HUTI_MAXITER;
         done.push_back(i);
       } else {
+        S->rnorm_prev = S->rnorm;
         S->rnorm = std::sqrt(nr[i]);
         start.push_back(i);
       }
@@ -908,10 +931,19 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
       EGPU_CUDA_TRY(ctx, cudaMemcpy(st.data(), B->d_state.p, 2 * BATCH_MAX_SYS * sizeof(SysState), cudaMemcpyDeviceToHost));
       for (int i : start) {
         SysState &s = st[B->parity * BATCH_MAX_SYS + i];
-        std::memset(&s, 0, sizeof(s));
+        BatchSys *S = B->sys[i];
+        // reliable updating: continue the last segment if it converged normally
+        const bool resume = B->resume_ok && S->refinements > 0 && s.status == ST_IDLE && S->last_info == EGPU_HUTI_CONVERGENCE;
+        if (resume) {
+          const double c = S->rnorm_prev / S->rnorm;  // old scale / new scale
+          s.carry_rho = B->prm.method == EGPU_CG ? s.rho * c : s.rho;
+          s.resume = 1;
+        } else {
+          std::memset(&s, 0, sizeof(s));
+        }
         s.status = ST_INIT;
-        B->sys[i]->phase = 2;
-        B->sys[i]->refinements++;
+        S->phase = 2;
+        S->refinements++;
       }
       EGPU_CUDA_TRY(ctx, cudaMemcpy(B->d_state.p, st.data(), 2 * BATCH_MAX_SYS * sizeof(SysState), cudaMemcpyHostToDevice));
     }
@@ -946,6 +978,7 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
     a.method = B->prm.method;
     a.precond = B->prm.precond;
     a.kmax = B->chunk;
+    a.exit_on_done = B->exit_on_done ? 1 : 0;
     a.tol = inner_tol_of(&B->prm);
     a.maxit = B->prm.inner_max_iter;
     int maxw = 1;
@@ -997,6 +1030,7 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
       const SysState &s = st[B->parity * BATCH_MAX_SYS + i];
       if (s.status == ST_DONE) {
         S->inner_iters += std::max(1, s.iters);
+        S->last_info = s.info;
         upd.push_back(i);
       }
     }
@@ -1031,6 +1065,15 @@ extern "C" int egpu_batch_set_config(egpu_batch *B, const egpu_batch_config *cfg
   B->chunk = cfg->chunk_iters;
   B->bps = cfg->blocks_per_sm;
   B->tri_mult = cfg->tri_mult;
+  return EGPU_OK;
+}
+
+// Latency mode: a launch returns after the iteration in which any system finished its inner
+// segment, so its FP64 refinement (or retirement) follows at once instead of at the end of
+// the chunk: lower latency for short requests, more launches.
+extern "C" int egpu_batch_set_latency_mode(egpu_batch *B, int on) {
+  if (!B) return EGPU_ERR_ARG;
+  B->exit_on_done = on != 0;
   return EGPU_OK;
 }
 

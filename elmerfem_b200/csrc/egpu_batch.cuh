@@ -50,6 +50,10 @@ struct SysDesc {
 struct SysState {
   int status, k, info, iters;
   double rho, oldrho, alpha, omega, r0norm, residual;
+  // reliable updating: resume != 0 continues the previous segment's recurrences (keeps
+  // P, V, RTLD, alpha, omega) with rho_{k-1} = carry_rho (already in the new residual scale)
+  int resume, pad;
+  double carry_rho;
 };
 
 enum { BA_BB = 0, BA_RHO, BA_RR, BA_PQ, BA_SS, BA_TS, BA_TT, BA_NSLOT };
@@ -60,6 +64,7 @@ struct BatchArgs {
   SysState *state;          // 2 * nsys
   double *acc;              // BA_NSLOT * nsys
   int method, precond, kmax;
+  int exit_on_done;         // end the launch after an iteration in which a system finished
   double tol;
   int maxit;
   int tri_warps_per_block;
@@ -70,12 +75,14 @@ struct BatchArgs {
 
 struct BatchShared {
   int act[BATCH_MAX_SYS];        // systems with work this iteration
+  unsigned char fresh[BATCH_MAX_SYS];  // 1: this inner solve started from zero, 0: resumed
   int pre[BATCH_MAX_SYS + 1];    // prefix of their slice counts
   int status[BATCH_MAX_SYS];     // status decided for this iteration
   int kk[BATCH_MAX_SYS];
   float sa[BATCH_MAX_SYS], sb[BATCH_MAX_SYS];  // per-phase scalars (beta, alpha, omega)
   double red[BATCH_MAX_SYS * 2];               // per-block per-system accumulators
   int nact, total;
+  int any_done;                  // a system finished at this iteration's top
 };
 
 __device__ __forceinline__ void batch_acc_add(BatchShared &sh, int s_local, int v, double x) {

@@ -991,6 +991,13 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
   }
   double prev = 0.0;
   int stagnant = 0;
+  // reliable updating: each inner segment continues the previous one's recurrences from the
+  // replaced (FP64 true) residual; EGPU_MIXED_RESTART=1 restarts every segment instead
+  double *carry = (double *)(ctx->sync.p + 16) + 4;
+  const char *restart_env = std::getenv("EGPU_MIXED_RESTART");
+  const bool allow_resume = !(restart_env && restart_env[0] == '1');
+  bool resume = false;
+  double sigma_prev = 1.0;
   if (hflags & 2u) {
     r.info = EGPU_HUTI_CONVERGENCE;
   } else {
@@ -1053,19 +1060,24 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
       a.out_i = (int *)(ctx->sync.p + 8);
       a.out_d = (double *)(ctx->sync.p + 16);
       a.skip = nullptr;
+      a.resume = resume ? 1 : 0;
+      a.ru_c = resume ? sigma_prev / hn[0] : 1.0;
+      a.carry = carry;
+      sigma_prev = hn[0];
       EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ek0, ctx->stream));
       rc = run_krylov<float>(A, a, prm->method, A->sell_c16.p != nullptr);
       if (rc) return rc;
       EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ek1, ctx->stream));
       k_refine_update<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, d32, norms, xs);
       ctx->launches++;
-      unsigned int h[24];
+      unsigned int h[32];
       EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(h, ctx->sync.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
       EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
       if (h[1]) {
         egpu_set_error(ctx, "device-side wait expired in the FP32 inner solver");
         return (int)h[1];
       }
+      resume = allow_resume && ((const double *)(h + 16))[7] == 1.0;
       r.iters += std::max(1, ((int *)(h + 8))[1]);
       r.refinements++;
       float ms_k = 0;
@@ -1208,7 +1220,7 @@ extern "C" void egpu_params_default(egpu_params *p, int method, int precond) {
   p->precond_recompute = 1;
   p->inner_tol = 0.0;  // by preconditioner (inner_tol_of)
   p->inner_max_iter = 2000;
-  p->max_refinements = 30;
+  p->max_refinements = 100;
 }
 
 extern "C" int egpu_create(int device, egpu_ctx **out) {

@@ -11,7 +11,10 @@
 // untouched until then, which returns the same iterate and HUTI_ITERS as HUTI.
 //
 // FP32 inner mode (true_residual = 0) is the inner solver of the mixed-precision
-// refinement: x0 = 0, stopping on the recursive residual ||r_k|| <= tol * ||r_0||.
+// refinement: x0 = 0, stopping on the recursive residual ||r_k|| <= tol * ||r_0||.  With
+// resume set, a segment continues the previous one's search directions after its residual
+// was replaced by the FP64 true residual (reliable updating, Sleijpen & van der Vorst 1996):
+// no Krylov information is thrown away at a refinement.
 #pragma once
 
 #include "egpu_internal.cuh"
@@ -64,6 +67,13 @@ struct KArgs {
   // levels staged cta_pd ahead, ring of cta_rs slots, staging windows of cta_sb entries and
   // cta_sr rows
   int tri_cta, cta_pd, cta_rs, cta_sb, cta_sr, cta_nl, cta_nt;
+  // inner mode, reliable update: continue the previous segment's recurrences from a replaced
+  // residual (B = the new true residual / its norm) instead of restarting.  carry holds
+  // the previous segment's scalars (rho_{k-1}, alpha, omega; [3] = 1 when valid) and is
+  // written back at a converged exit; ru_c = old residual norm / new residual norm.
+  int resume;
+  double ru_c;
+  double *carry;
   const int *pos_lo, *pos_up;     // solve slot of each row, lower / upper order
   CtaTri<VT> clo, cup;
 };
@@ -589,6 +599,10 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) cg_kernel(KArgs<VT> a) {
 
   int k = 1, info = 0, iters = 0;
   double rho, oldrho = 1.0, residual = 0.0, rr_prev = 0.0;
+  // resumed segment: p_k = z_k + (rho_k / rho_{k-1}) (sigma_new / sigma_old) p_{k-1} in the new
+  // scale (rho is quadratic in the residual's scale, P linear)
+  const bool resumed = a.resume && !a.true_residual;
+  if (resumed) oldrho = a.carry[0] * a.ru_c;
   while (true) {
     rho = reduce_partials(a.partials + SLOT_RHO * nb, nb, sm);
     if (!a.true_residual && k > 1) {
@@ -600,7 +614,7 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) cg_kernel(KArgs<VT> a) {
     // ---- P = Z (first iteration) or Z + beta P
     {
       const VT beta = (VT)(rho / oldrho);
-      const bool first = k == 1;
+      const bool first = k == 1 && !resumed;
       vec_loop<VT>(n, [&](int i, auto w) {
         constexpr int W = decltype(w)::value;
         VT z[W], p[W];
@@ -727,6 +741,10 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) cg_kernel(KArgs<VT> a) {
     a.out_i[1] = iters;
     a.out_d[0] = residual;
     a.out_d[1] = rhsnorm;
+    if (a.carry) {  // state for the next segment: P was built with oldrho
+      a.carry[0] = oldrho;
+      a.carry[3] = (!a.true_residual && info == EGPU_HUTI_CONVERGENCE && k > 1) ? 1.0 : 0.0;
+    }
   }
 }
 
@@ -759,6 +777,9 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstab_kernel(KArgs<VT> a) {
   const bool cta = ilu && a.tri_cta;  // block 0 runs the ILU0 solves level-synchronously
   const VT SENT = Sentinel<VT>::value();
   VT *SLO = Y1, *YUP = Y2;           // level-synchronous mode: rhs / y in slot order
+  // resumed segment: RTLD, P, V and rho_{k-1}, alpha, omega carry over unchanged (BiCGStab's
+  // recurrences are invariant to the residual's scale)
+  const bool resumed = a.resume && !a.true_residual;
 
   // ---- init: R = B - A X; RTLD = R; P = V = 0
   {
@@ -777,7 +798,7 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstab_kernel(KArgs<VT> a) {
         vld<W>(B, i, b);
         vfill<W>(X, i, VT(0));
         vst<W>(R, i, b);
-        vst<W>(RT, i, b);
+        if (!resumed) vst<W>(RT, i, b);
 #pragma unroll
         for (int k = 0; k < W; ++k) acc[1] += (double)b[k] * (double)b[k];
       });
@@ -788,8 +809,10 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstab_kernel(KArgs<VT> a) {
       vld<W>(B, i, b);
 #pragma unroll
       for (int k = 0; k < W; ++k) acc[0] += (double)b[k] * (double)b[k];
-      vfill<W>(P, i, VT(0));
-      vfill<W>(V, i, VT(0));
+      if (!resumed) {
+        vfill<W>(P, i, VT(0));
+        vfill<W>(V, i, VT(0));
+      }
       if (ilu && !cta) {
         vfill<W>(Y1, i, SENT);
         vfill<W>(Y2, i, SENT);
@@ -797,9 +820,20 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstab_kernel(KArgs<VT> a) {
         vfill<W>(T2, i, SENT);
       }
     });
+    double rt[1] = {0.0};
+    if (resumed)  // rho_k = RTLD . R with the kept shadow residual
+      vec_loop<VT>(n, [&](int i, auto w) {
+        constexpr int W = decltype(w)::value;
+        VT b[W], t[W];
+        vld<W>(B, i, b);
+        vld<W>(RT, i, t);
+#pragma unroll
+        for (int k = 0; k < W; ++k) rt[0] += (double)t[k] * (double)b[k];
+      });
     block_sum<2>(acc, sm);
+    block_sum<1>(rt, sm);
     store_partials(a, SLOT_BB, acc[0]);
-    store_partials(a, SLOT_RHO, acc[1]);
+    store_partials(a, SLOT_RHO, resumed ? rt[0] : acc[1]);
     store_partials(a, SLOT_RR2, acc[1]);
   }
   if (!grid_barrier(a.bar, a.err, epoch)) return;
@@ -807,6 +841,11 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstab_kernel(KArgs<VT> a) {
 
   int k = 1, info = 0, iters = 0;
   double rho, oldrho = 1.0, omega = 1.0, alpha = 0.0, residual = 0.0, r0norm = 0.0;
+  if (resumed) {
+    oldrho = a.carry[0];
+    alpha = a.carry[1];
+    omega = a.carry[2];
+  }
   if (!a.true_residual) r0norm = sqrt(reduce_partials(a.partials + SLOT_RR2 * nb, nb, sm));
   while (true) {
     rho = reduce_partials(a.partials + SLOT_RHO * nb, nb, sm);
@@ -1022,6 +1061,12 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstab_kernel(KArgs<VT> a) {
     a.out_i[1] = iters;
     a.out_d[0] = residual;
     a.out_d[1] = rhsnorm;
+    if (a.carry) {  // state for the next segment: P, V were built with oldrho, alpha, omega
+      a.carry[0] = oldrho;
+      a.carry[1] = alpha;
+      a.carry[2] = omega;
+      a.carry[3] = (!a.true_residual && info == EGPU_HUTI_CONVERGENCE && k > 1) ? 1.0 : 0.0;
+    }
   }
 }
 

@@ -13,7 +13,8 @@
 // and device memory returned, so requests arriving meanwhile join the next step.
 //
 // Every GPU call on the server's context happens under one mutex (the worker and pattern
-// registration), so callers may submit and poll from any thread.
+// registration).  Submissions and polls take only the pattern-table and queue locks, so
+// they never wait for a GPU step, and callers may use any thread.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -46,6 +47,7 @@ enum class St { QUEUED, RESIDENT, DONE };
 struct Request {
   long long id = 0;
   int pattern = 0;
+  egpu_mat *proto = nullptr;  // the pattern's resident prototype
   int n = 0;                 // rows of the pattern
   double footprint = 0;      // device bytes while resident
   St state = St::QUEUED;
@@ -73,7 +75,8 @@ struct egpu_server {
   int max_resident = 0;
   egpu_ctx *ctx = nullptr;
   egpu_batch *batch = nullptr;
-  std::mutex gpu_mu;  // every call on ctx / batch, and the pattern table
+  std::mutex gpu_mu;  // every call on ctx / batch
+  std::mutex pat_mu;  // the pattern table (never held across a GPU call)
   std::vector<Pattern> patterns;
   std::unordered_map<int, int> mesh_nodes, mesh_elems;
   std::mutex mu;      // queue, request table and states, counters (taken before gpu_mu when both)
@@ -91,8 +94,7 @@ namespace {
 
 // device setup of one admitted request (under gpu_mu); its batch slot or a negative error
 int prepare(egpu_server *S, Request *r) {
-  const Pattern &P = S->patterns[r->pattern];
-  int rc = egpu_matrix_clone(P.proto, &r->A);
+  int rc = egpu_matrix_clone(r->proto, &r->A);
   if (rc) return rc;
   if (r->assemble) {
     rc = egpu_assemble_poisson(r->A, r->elem_k.empty() ? nullptr : r->elem_k.data(),
@@ -218,9 +220,9 @@ void work(egpu_server *S) {
   }
 }
 
-// pattern size and footprint, checked under gpu_mu
+// pattern size and footprint (submission never waits for a GPU step)
 bool pattern_info(egpu_server *S, int pattern, Pattern &out, int *nnodes = nullptr, int *nelem = nullptr) {
-  std::lock_guard<std::mutex> g(S->gpu_mu);
+  std::lock_guard<std::mutex> g(S->pat_mu);
   if (pattern < 0 || pattern >= (int)S->patterns.size()) return false;
   out = S->patterns[pattern];
   if (nnodes) *nnodes = S->mesh_nodes.count(pattern) ? S->mesh_nodes[pattern] : 0;
@@ -231,6 +233,7 @@ bool pattern_info(egpu_server *S, int pattern, Pattern &out, int *nnodes = nullp
 Request *new_request(egpu_server *S, const Pattern &P, int pattern, long long *id) {
   auto r = std::make_unique<Request>();
   r->pattern = pattern;
+  r->proto = P.proto;
   r->n = P.n;
   r->footprint = (double)P.footprint;
   r->t_submit = Clock::now();
@@ -263,6 +266,7 @@ extern "C" int egpu_server_create(int device, const egpu_params *prm, double hbm
   int rc = egpu_create(device, &S->ctx);
   if (!rc) rc = egpu_batch_create(S->ctx, prm, &S->batch);
   if (!rc && chunk_iters > 0) rc = egpu_batch_set_chunk(S->batch, chunk_iters);
+  if (!rc) rc = egpu_batch_set_latency_mode(S->batch, 1);  // retire each request as it finishes
   if (rc) {
     if (S->batch) egpu_batch_free(S->batch);
     if (S->ctx) egpu_destroy(S->ctx);
@@ -280,17 +284,20 @@ extern "C" int egpu_server_pattern(egpu_server *S, int n, const int *rows, const
   const long long nnz = (long long)rows[n] - rows[0];
   if (nnz < 1) return EGPU_ERR_ARG;
   std::vector<double> zero(nnz, 0.0);
-  std::lock_guard<std::mutex> g(S->gpu_mu);
   Pattern P;
   P.n = n;
   P.nnz = nnz;
-  int rc = egpu_matrix_bind(S->ctx, n, rows, cols, diag, zero.data(), &P.proto);
-  if (!rc) rc = egpu_matrix_prepare(P.proto, S->prm.precond);
-  if (rc) {
-    if (P.proto) egpu_matrix_free(P.proto);
-    return rc;
+  {
+    std::lock_guard<std::mutex> g(S->gpu_mu);
+    int rc = egpu_matrix_bind(S->ctx, n, rows, cols, diag, zero.data(), &P.proto);
+    if (!rc) rc = egpu_matrix_prepare(P.proto, S->prm.precond);
+    if (rc) {
+      if (P.proto) egpu_matrix_free(P.proto);
+      return rc;
+    }
+    P.footprint = egpu_matrix_footprint(P.proto, S->prm.precond);
   }
-  P.footprint = egpu_matrix_footprint(P.proto, S->prm.precond);
+  std::lock_guard<std::mutex> g(S->pat_mu);
   S->patterns.push_back(P);
   *pattern = (int)S->patterns.size() - 1;
   return EGPU_OK;
@@ -298,13 +305,16 @@ extern "C" int egpu_server_pattern(egpu_server *S, int n, const int *rows, const
 
 extern "C" int egpu_server_pattern_mesh(egpu_server *S, int pattern, int nnodes, const double *xyz, int cdim,
                                         int nelem, int code, const int *elem_nodes, const int *perm, int dofs) {
-  if (!S) return EGPU_ERR_ARG;
-  std::lock_guard<std::mutex> g(S->gpu_mu);
-  if (pattern < 0 || pattern >= (int)S->patterns.size()) return EGPU_ERR_ARG;
-  Pattern &P = S->patterns[pattern];
-  const int rc = egpu_assembly_bind(P.proto, nnodes, xyz, cdim, nelem, code, elem_nodes, perm, dofs);
+  Pattern P;
+  if (!S || !pattern_info(S, pattern, P)) return EGPU_ERR_ARG;
+  int rc;
+  {
+    std::lock_guard<std::mutex> g(S->gpu_mu);
+    rc = egpu_assembly_bind(P.proto, nnodes, xyz, cdim, nelem, code, elem_nodes, perm, dofs);
+  }
   if (!rc) {
-    P.mesh = true;
+    std::lock_guard<std::mutex> g(S->pat_mu);
+    S->patterns[pattern].mesh = true;
     S->mesh_nodes[pattern] = nnodes;
     S->mesh_elems[pattern] = nelem;
   }
@@ -396,7 +406,7 @@ extern "C" void egpu_server_free(egpu_server *S) {
   }
   S->requests.clear();
   egpu_batch_free(S->batch);
-  for (Pattern &P : S->patterns) egpu_matrix_free(P.proto);
+  for (Pattern &P : S->patterns) egpu_matrix_free(P.proto);  // no other thread runs now
   egpu_destroy(S->ctx);
   delete S;
 }

@@ -99,9 +99,9 @@ class SolverParams:
     precision: int = FP64
     refactorize: bool = True
     precond_recompute: int = 1
-    inner_tol: float = 0.0        # 0: chosen by preconditioner (3e-4 Diagonal/none, 3e-3 ILU0)
+    inner_tol: float = 0.0        # 0: chosen by preconditioner (1e-2 Diagonal/none, 3e-2 ILU0)
     inner_max_iter: int = 2000
-    max_refinements: int = 30
+    max_refinements: int = 100
     abort_not_converged: bool = True
     symmetric: bool = False
 

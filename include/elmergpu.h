@@ -57,8 +57,10 @@ typedef struct {
   int refactorize;        /* Linear System Refactorize (Elmer default 1) */
   int precond_recompute;  /* Linear System Precondition Recompute (Elmer default 1) */
   /* mixed precision only */
-  double inner_tol;       /* relative reduction of the FP32 inner residual per refinement;
-                             0 (the default): 3e-4 with Diagonal / none, 3e-3 with ILU0 */
+  double inner_tol;       /* relative reduction of the FP32 inner residual per segment
+                             (each segment continues the previous one's recurrences from the
+                             FP64 true residual); 0 (the default): 1e-2 with Diagonal / none,
+                             3e-2 with ILU0 */
   int inner_max_iter;     /* cap on inner iterations per refinement */
   int max_refinements;    /* cap on FP64 refinement steps */
 } egpu_params;
@@ -198,6 +200,9 @@ int egpu_batch_add(egpu_batch *B, int n, const int *rows, const int *cols, const
                    const double *values, const double *rhs);
 int egpu_batch_add_matrix(egpu_batch *B, egpu_mat *A, const double *b_dev);
 int egpu_batch_set_chunk(egpu_batch *B, int chunk_iters);
+/* on != 0: a launch returns as soon as some system finishes its inner segment, so that system
+ * is refined or retired at once (lower latency for short requests, more launches) */
+int egpu_batch_set_latency_mode(egpu_batch *B, int on);
 int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished);
 int egpu_batch_pending(egpu_batch *B);
 int egpu_batch_solve(egpu_batch *B, egpu_result *per_system);
