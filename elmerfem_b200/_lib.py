@@ -35,7 +35,7 @@ class Params(C.Structure):
     _fields_ = [("method", C.c_int), ("precond", C.c_int), ("max_iter", C.c_int), ("tol", C.c_double),
                 ("scale_system", C.c_int), ("precision", C.c_int), ("refactorize", C.c_int),
                 ("precond_recompute", C.c_int), ("inner_tol", C.c_double), ("inner_max_iter", C.c_int),
-                ("max_refinements", C.c_int)]
+                ("max_refinements", C.c_int), ("ilu_order", C.c_int)]
 
 
 class Result(C.Structure):
@@ -86,7 +86,9 @@ PROTOTYPES = {
     "egpu_matrix_free": (None, [_vp]),
     "egpu_matrix_clone": (C.c_int, [_vp, C.POINTER(_vp)]),
     "egpu_matrix_footprint": (C.c_longlong, [_vp, C.c_int]),
-    "egpu_matrix_prepare": (C.c_int, [_vp, C.c_int]),
+    "egpu_matrix_prepare": (C.c_int, [_vp, C.POINTER(Params)]),
+    "egpu_ilu_pattern": (C.c_longlong, [C.c_int, _i32p, _i32p, _i32p, C.c_int, C.c_longlong, _vp, _vp, _vp]),
+    "egpu_ilu_download": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "egpu_iter_solve": (C.c_int, [_vp, _f64p, _f64p, C.POINTER(Params), C.POINTER(Result)]),
     "egpu_iter_solve_dev": (C.c_int, [_vp, _vp, _vp, C.POINTER(Params), C.POINTER(Result)]),
     "egpu_mv": (C.c_int, [_vp, _f64p, _f64p]),
@@ -98,6 +100,7 @@ PROTOTYPES = {
     "egpu_assemble_elastic": (C.c_int, [_vp, C.c_double, C.c_double, _f64p]),
     "egpu_dirichlet": (C.c_int, [_vp, C.c_int, _vp, _vp, C.c_int]),
     "egpu_ilu0_build": (C.c_int, [_vp, C.c_int]),
+    "egpu_ilu_build": (C.c_int, [_vp, C.c_int, C.c_int]),
     "egpu_ilu0_download": (C.c_int, [_vp, _vp, _vp]),
     "egpu_lu_precondition": (C.c_int, [_vp, _f64p, _f64p]),
     "egpu_cg_noalloc": (C.c_int, [C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, C.POINTER(Params),

@@ -752,7 +752,7 @@ static int batch_prepare(egpu_batch *B, int slot, const double *b_dev) {
   rc = rhs_scale(A, b_dev ? b_dev : A->rhs.p, S->xout.p, bs, xs, B->prm.scale_system != 0, &S->bnorm_s);
   if (rc) return rc;
   if (B->prm.precond == EGPU_PREC_ILU0) {
-    rc = ilu0_factor(A);
+    rc = ilu_factor(A, B->prm.ilu_order);
     if (rc) return rc;
   }
   rc = prepare_fp32_public(A, B->prm.precond == EGPU_PREC_ILU0);

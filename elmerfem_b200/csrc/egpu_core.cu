@@ -426,6 +426,88 @@ int scale_matrix(egpu_mat *A, bool scale_system) {
   return EGPU_OK;
 }
 
+// a clone's view of its prototype's ILU structure
+static void view_ilu(egpu_mat *A, const egpu_mat *proto) {
+  A->ilu_order = proto->ilu_order;
+  A->ilu_nnz = proto->ilu_nnz;
+  A->ilu_max_row = proto->ilu_max_row;
+  A->ilu_rows.view(proto->ilu_rows);
+  A->ilu_cols.view(proto->ilu_cols);
+  A->ilu_diag.view(proto->ilu_diag);
+  A->ilu_scatter.view(proto->ilu_scatter);
+}
+
+// The structure ILU(order) factors live on: the matrix's pattern for order 0, else
+// InitializeILU1 applied order times (CRS_IncompleteLU, CRSMatrix.src:2196-2218).  A new
+// order invalidates the schedules and factors.  Clones share the prototype's structure, so
+// a prototype with clones keeps the order it was first built with.
+int ensure_ilu_structure(egpu_mat *A, int order) {
+  if (A->ilu_order == order) return EGPU_OK;
+  egpu_ctx *ctx = A->ctx;
+  if (order < 0 || order > 9) return EGPU_ERR_ARG;
+  if (A->parent) {
+    egpu_mat *P = A->parent;
+    if (P->ilu_order >= 0 && P->ilu_order != order && P->clones > 1) {
+      egpu_set_error(ctx, "clones of one pattern share its ILU structure: use one ILU order for all of them");
+      return EGPU_ERR_STATE;
+    }
+    int rc = ensure_ilu_structure(P, order);
+    if (rc) return rc;
+    view_ilu(A, P);
+    A->tri_built = false;
+    A->ilu_valid = false;
+    return EGPU_OK;
+  }
+  if (A->ilu_order >= 0 && A->clones > 0) {
+    egpu_set_error(ctx, "clones of one pattern share its ILU structure: use one ILU order for all of them");
+    return EGPU_ERR_STATE;
+  }
+  const int n = A->n;
+  if (order == 0) {
+    A->ilu_rows.view(A->rows);
+    A->ilu_cols.view(A->cols);
+    A->ilu_diag.view(A->diag);
+    A->ilu_scatter.release();
+    A->ilu_in.release();
+    A->ilu_nnz = A->nnz;
+    A->ilu_max_row = A->max_row;
+  } else {
+    std::vector<int> rows(n + 1), cols(A->nnz), diag(n), r, c, d;
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(rows.data(), A->rows.p, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(cols.data(), A->cols.p, A->nnz * sizeof(int), cudaMemcpyDeviceToHost));
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(diag.data(), A->diag.p, n * sizeof(int), cudaMemcpyDeviceToHost));
+    ::egpu_ilu_structure(n, rows, cols, diag, order, r, c, d);
+    std::vector<int> scatter(A->nnz);
+    int maxrow = 0;
+    for (int i = 0; i < n; ++i) {
+      maxrow = std::max(maxrow, r[i + 1] - r[i]);
+      int q = r[i];
+      for (int e = rows[i]; e < rows[i + 1]; ++e) {  // both rows sorted: merge
+        while (q < r[i + 1] && c[q] < cols[e]) ++q;
+        if (q >= r[i + 1] || c[q] != cols[e] || d[i] < r[i]) {
+          egpu_set_error(ctx, "internal: ILU structure does not contain the matrix pattern");
+          return EGPU_ERR_ARG;
+        }
+        scatter[e] = q;
+      }
+    }
+    A->ilu_nnz = r[n];
+    A->ilu_max_row = maxrow;
+    EGPU_CUDA_TRY(ctx, A->ilu_rows.alloc(n + 1));
+    EGPU_CUDA_TRY(ctx, A->ilu_cols.alloc(A->ilu_nnz));
+    EGPU_CUDA_TRY(ctx, A->ilu_diag.alloc(n));
+    EGPU_CUDA_TRY(ctx, A->ilu_scatter.alloc(A->nnz));
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(A->ilu_rows.p, r.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(A->ilu_cols.p, c.data(), A->ilu_nnz * sizeof(int), cudaMemcpyHostToDevice));
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(A->ilu_diag.p, d.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(A->ilu_scatter.p, scatter.data(), A->nnz * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  A->ilu_order = order;
+  A->tri_built = false;
+  A->ilu_valid = false;
+  return EGPU_OK;
+}
+
 // a clone's view of its prototype's level schedules (sync-free and single-block)
 static void view_tri(egpu_mat *A, const egpu_mat *proto) {
   A->tri.lower_order.view(proto->tri.lower_order);
@@ -471,6 +553,10 @@ static void view_tri(egpu_mat *A, const egpu_mat *proto) {
 
 int ensure_tri_schedule(egpu_mat *A) {
   if (A->tri_built) return EGPU_OK;
+  if (A->ilu_order < 0) {
+    const int rc = ensure_ilu_structure(A, 0);
+    if (rc) return rc;
+  }
   if (A->parent) {  // a clone shares its prototype's schedules, built once
     const int rc = ensure_tri_schedule(A->parent);
     if (rc) return rc;
@@ -479,10 +565,12 @@ int ensure_tri_schedule(egpu_mat *A) {
   }
   egpu_ctx *ctx = A->ctx;
   const int n = A->n;
-  std::vector<int> rows(n + 1), cols(A->nnz), diag(n);
-  EGPU_CUDA_TRY(ctx, cudaMemcpy(rows.data(), A->rows.p, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost));
-  EGPU_CUDA_TRY(ctx, cudaMemcpy(cols.data(), A->cols.p, A->nnz * sizeof(int), cudaMemcpyDeviceToHost));
-  EGPU_CUDA_TRY(ctx, cudaMemcpy(diag.data(), A->diag.p, n * sizeof(int), cudaMemcpyDeviceToHost));
+  // the schedules follow the ILU structure (the matrix's pattern for ILU0)
+  const long long inz = A->ilu_nnz;
+  std::vector<int> rows(n + 1), cols(inz), diag(n);
+  EGPU_CUDA_TRY(ctx, cudaMemcpy(rows.data(), A->ilu_rows.p, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+  EGPU_CUDA_TRY(ctx, cudaMemcpy(cols.data(), A->ilu_cols.p, inz * sizeof(int), cudaMemcpyDeviceToHost));
+  EGPU_CUDA_TRY(ctx, cudaMemcpy(diag.data(), A->ilu_diag.p, n * sizeof(int), cudaMemcpyDeviceToHost));
   for (int i = 0; i < n; ++i)
     if (diag[i] < 0) {
       egpu_set_error(ctx, "ILU0 needs a stored diagonal in every row");
@@ -517,12 +605,12 @@ int ensure_tri_schedule(egpu_mat *A) {
       }
     }
     for (size_t k = 0; k < (size_t)lp[n]; ++k)
-      if (lc[k] < 0 || lc[k] >= n || ls[k] < 0 || ls[k] >= A->nnz) {
+      if (lc[k] < 0 || lc[k] >= n || ls[k] < 0 || ls[k] >= inz) {
         egpu_set_error(ctx, "internal: packed lower factor out of range");
         return EGPU_ERR_ARG;
       }
     for (size_t k = 0; k < (size_t)upp[n]; ++k)
-      if (uc[k] < 0 || uc[k] >= n || us[k] < 0 || us[k] >= A->nnz) {
+      if (uc[k] < 0 || uc[k] >= n || us[k] < 0 || us[k] >= inz) {
         egpu_set_error(ctx, "internal: packed upper factor out of range");
         return EGPU_ERR_ARG;
       }
@@ -548,26 +636,45 @@ int ensure_tri_schedule(egpu_mat *A) {
   return EGPU_OK;
 }
 
-// ILU0 of the scaled matrix (IterSolve.src:420-575 -> CRS_IncompleteLU(A,0))
-int ilu0_factor(egpu_mat *A) {
+// the scaled matrix scattered into the ILU(n) structure (fill entries start at zero, as
+// the reference's dense row S does)
+__global__ void k_ilu_scatter(long long nnz, const int *__restrict__ pos, const double *__restrict__ v, double *out) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nnz; e += (long long)gridDim.x * blockDim.x)
+    out[pos[e]] = v[e];
+}
+
+// ILU(order) of the scaled matrix (IterSolve.src:420-575 -> CRS_IncompleteLU(A, order))
+int ilu_factor(egpu_mat *A, int order) {
   egpu_ctx *ctx = A->ctx;
-  int rc = ensure_tri_schedule(A);
+  int rc = ensure_ilu_structure(A, order);
+  if (rc) return rc;
+  rc = ensure_tri_schedule(A);
   if (rc) return rc;
   const int n = A->n;
-  EGPU_CUDA_TRY(ctx, A->ilu.alloc(A->nnz));
+  EGPU_CUDA_TRY(ctx, A->ilu.alloc(A->ilu_nnz));
   EGPU_CUDA_TRY(ctx, A->ilu_done.alloc(n));
   EGPU_CUDA_TRY(ctx, cudaMemsetAsync(A->ilu_done.p, 0, n * sizeof(int), ctx->stream));
   EGPU_CUDA_TRY(ctx, cudaMemsetAsync(ctx->sync.p + 1, 0, sizeof(int), ctx->stream));
   int *err = (int *)(ctx->sync.p + 1);
-  if (A->max_row > 256) {
-    egpu_set_error(ctx, "ILU0: rows longer than 256 entries are not supported");
+  if (A->ilu_max_row > 256) {
+    egpu_set_error(ctx, "ILU: rows of the ILU structure longer than 256 entries are not supported");
     return EGPU_ERR_ARG;
   }
+  const double *input = A->scaled.p;
+  if (order > 0) {
+    EGPU_CUDA_TRY(ctx, A->ilu_in.alloc(A->ilu_nnz));
+    EGPU_CUDA_TRY(ctx, cudaMemsetAsync(A->ilu_in.p, 0, A->ilu_nnz * sizeof(double), ctx->stream));
+    k_ilu_scatter<<<grid_for(ctx, A->nnz), 256, 0, ctx->stream>>>(A->nnz, A->ilu_scatter.p, A->scaled.p,
+                                                                    A->ilu_in.p);
+    ctx->launches++;
+    input = A->ilu_in.p;
+  }
+  const int mr = A->ilu_max_row;
   // every warp resident: one block of 8 warps per slot, grid sized by occupancy
   int bps = 0;
-  if (A->max_row <= 32) {
+  if (mr <= 32) {
     EGPU_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_ilu0_factor<32>, 256, 0));
-  } else if (A->max_row <= 128) {
+  } else if (mr <= 128) {
     EGPU_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_ilu0_factor<128>, 256, 0));
   } else {
     EGPU_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_ilu0_factor<256>, 256, 0));
@@ -575,13 +682,13 @@ int ilu0_factor(egpu_mat *A) {
   // enough warps for about twice the widest level, never more than fit at once
   const int want_blocks = (2 * std::max(1, A->tri.max_width) + 7) / 8;
   int grid = std::max(1, std::min(std::min(bps, 4) * ctx->num_sms, std::max(ctx->num_sms, want_blocks)));
-  void *args[] = {(void *)&n, &A->rows.p, &A->cols.p, &A->diag.p, &A->tri.lower_order.p, &A->scaled.p,
+  void *args[] = {(void *)&n, &A->ilu_rows.p, &A->ilu_cols.p, &A->ilu_diag.p, &A->tri.lower_order.p, &input,
                   &A->ilu.p, &A->ilu_done.p, &err};
-  const void *kern = A->max_row <= 32 ? (const void *)k_ilu0_factor<32>
-                     : A->max_row <= 128 ? (const void *)k_ilu0_factor<128>
-                                          : (const void *)k_ilu0_factor<256>;
+  const void *kern = mr <= 32 ? (const void *)k_ilu0_factor<32>
+                     : mr <= 128 ? (const void *)k_ilu0_factor<128>
+                                  : (const void *)k_ilu0_factor<256>;
   EGPU_CUDA_TRY(ctx, cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(256), args, 0, ctx->stream));
-  k_ilu_invdiag<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, A->diag.p, A->ilu.p);
+  k_ilu_invdiag<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, A->ilu_diag.p, A->ilu.p);
   const long long nl = A->tri.lo_cols.n, nu = A->tri.up_cols.n;
   EGPU_CUDA_TRY(ctx, A->lo_vals.alloc(nl));
   EGPU_CUDA_TRY(ctx, A->up_vals.alloc(nu));
@@ -712,8 +819,9 @@ int solve_fp64(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_param
   A->solve_count++;
   if (prm->precond == EGPU_PREC_ILU0) {
     const int every = prm->precond_recompute > 0 ? prm->precond_recompute : 1;
-    if (!A->ilu_valid || (prm->refactorize && (A->solve_count - 1) % every == 0)) {
-      rc = ilu0_factor(A);
+    if (!A->ilu_valid || A->ilu_order != prm->ilu_order ||
+        (prm->refactorize && (A->solve_count - 1) % every == 0)) {
+      rc = ilu_factor(A, prm->ilu_order);
       if (rc) return rc;
     } else {
       rc = ensure_tri_schedule(A);
@@ -925,8 +1033,8 @@ static int prepare_fp32(egpu_mat *A, bool with_ilu) {
   k_to_f32<<<grid_for(ctx, A->sell_nnz), 256, 0, ctx->stream>>>(A->sell_vals.p, A->sell_vals32.p, A->sell_nnz);
   ctx->launches += 3;
   if (with_ilu) {
-    EGPU_CUDA_TRY(ctx, A->ilu32.alloc(A->nnz));
-    k_to_f32<<<grid_for(ctx, A->nnz), 256, 0, ctx->stream>>>(A->ilu.p, A->ilu32.p, A->nnz);
+    EGPU_CUDA_TRY(ctx, A->ilu32.alloc(A->ilu_nnz));
+    k_to_f32<<<grid_for(ctx, A->ilu_nnz), 256, 0, ctx->stream>>>(A->ilu.p, A->ilu32.p, A->ilu_nnz);
     ctx->launches++;
   }
   if (A->max_bandwidth < 32768 && !A->cols16.p) {
@@ -964,7 +1072,7 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
   A->solve_count++;
   const bool ilu = prm->precond == EGPU_PREC_ILU0;
   if (ilu) {
-    rc = ilu0_factor(A);
+    rc = ilu_factor(A, prm->ilu_order);
     if (rc) return rc;
   }
   rc = prepare_fp32(A, ilu);
@@ -1444,6 +1552,7 @@ extern "C" int egpu_matrix_clone(egpu_mat *proto, egpu_mat **out) {
   A->sell_cols.view(proto->sell_cols);
   A->sell_c16.view(proto->sell_c16);
   if (proto->cols16.p) A->cols16.view(proto->cols16);
+  if (proto->ilu_order >= 0) view_ilu(A, proto);
   if (proto->tri_built) view_tri(A, proto);
   const AssemblyData &P = proto->asmb;
   AssemblyData &S = A->asmb;
@@ -1476,10 +1585,12 @@ extern "C" int egpu_matrix_clone(egpu_mat *proto, egpu_mat **out) {
 
 // the preconditioner's one-time structures ahead of the first solve (ILU0 level schedules,
 // shared with every clone of the prototype)
-extern "C" int egpu_matrix_prepare(egpu_mat *A, int precond) {
-  if (!A || precond < EGPU_PREC_NONE || precond > EGPU_PREC_ILU0) return EGPU_ERR_ARG;
+extern "C" int egpu_matrix_prepare(egpu_mat *A, const egpu_params *prm) {
+  if (!A || !prm || prm->precond < EGPU_PREC_NONE || prm->precond > EGPU_PREC_ILU0) return EGPU_ERR_ARG;
   cudaSetDevice(A->ctx->device);
-  if (precond != EGPU_PREC_ILU0) return EGPU_OK;
+  if (prm->precond != EGPU_PREC_ILU0) return EGPU_OK;
+  const int rc = egpu::ensure_ilu_structure(A, prm->ilu_order);
+  if (rc) return rc;
   return egpu::ensure_tri_schedule(A);
 }
 
@@ -1491,7 +1602,8 @@ extern "C" long long egpu_matrix_footprint(const egpu_mat *A, int precond) {
   long long b = 8 * z + 8 * n;              // values, rhs
   b += 8 * z + 8 * zs + 4 * zs;             // scaled CRS, SELL FP64, SELL FP32
   b += 8 * n + 13 * 8 * l + 14 * 4 * l;     // DiagScaling, work vectors
-  if (precond == EGPU_PREC_ILU0) b += 8 * z + 4 * z + 4 * n;  // ILU0 FP64/FP32, flags
+  const long long zi = std::max(z, A->ilu_nnz);   // ILU structure (ILU(n) fill included once built)
+  if (precond == EGPU_PREC_ILU0) b += 8 * zi + 4 * zi + 4 * n + (zi > z ? 8 * zi : 0);  // factors, flags, scatter
   if (precond == EGPU_PREC_ILU0) b += 12 * (A->tri.cta_lo.nent + A->tri.cta_up.nent);  // single-block layout
   return b + 8 * n;                         // back-scaled solution
 }
@@ -1502,6 +1614,7 @@ static int check_params(const egpu_params *p) {
   if (p->precond < EGPU_PREC_NONE || p->precond > EGPU_PREC_ILU0) return EGPU_ERR_ARG;
   if (p->max_iter < 1) return EGPU_ERR_ARG;
   if (p->precision != EGPU_FP64 && p->precision != EGPU_MIXED) return EGPU_ERR_ARG;
+  if (p->ilu_order < 0 || p->ilu_order > 9) return EGPU_ERR_ARG;
   return EGPU_OK;
 }
 
@@ -1599,15 +1712,16 @@ extern "C" void egpu_matvec_subr(void **spmv, int *n, int *rows, int *cols, doub
   egpu_mv(A, u, v);
 }
 
-extern "C" int egpu_ilu0_build(egpu_mat *A, int scale_system) {
+extern "C" int egpu_ilu_build(egpu_mat *A, int scale_system, int order) {
   if (!A || !A->has_values) return EGPU_ERR_STATE;
+  if (order < 0 || order > 9) return EGPU_ERR_ARG;
   egpu_ctx *ctx = A->ctx;
   cudaSetDevice(ctx->device);
   int rc = egpu::reset_sync(ctx);
   if (rc) return rc;
   rc = egpu::scale_matrix(A, scale_system != 0);
   if (rc) return rc;
-  rc = egpu::ilu0_factor(A);
+  rc = egpu::ilu_factor(A, order);
   if (rc) return rc;
   unsigned int h[2];
   EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(h, ctx->sync.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1619,8 +1733,35 @@ extern "C" int egpu_ilu0_build(egpu_mat *A, int scale_system) {
   return EGPU_OK;
 }
 
+extern "C" int egpu_ilu0_build(egpu_mat *A, int scale_system) { return egpu_ilu_build(A, scale_system, 0); }
+
+// the current factors on their structure, 1-based; returns the number of entries
+extern "C" int egpu_ilu_download(egpu_mat *A, int *ilu_rows, int *ilu_cols, int *ilu_diag, double *ilu_values) {
+  if (!A || !A->ilu_valid) return EGPU_ERR_STATE;
+  egpu_ctx *ctx = A->ctx;
+  cudaSetDevice(ctx->device);
+  const int n = A->n;
+  const long long nz = A->ilu_nnz;
+  std::vector<int> tmp;
+  auto down1 = [&](int *dst, const int *src, long long cnt) -> int {
+    tmp.resize(cnt);
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(tmp.data(), src, cnt * sizeof(int), cudaMemcpyDeviceToHost));
+    for (long long k = 0; k < cnt; ++k) dst[k] = tmp[k] + 1;
+    return EGPU_OK;
+  };
+  int rc = EGPU_OK;
+  if (ilu_rows) rc = down1(ilu_rows, A->ilu_rows.p, n + 1);
+  if (!rc && ilu_cols) rc = down1(ilu_cols, A->ilu_cols.p, nz);
+  if (!rc && ilu_diag) rc = down1(ilu_diag, A->ilu_diag.p, n);
+  if (rc) return rc;
+  if (ilu_values)
+    EGPU_CUDA_TRY(ctx, cudaMemcpy(ilu_values, A->ilu.p, nz * sizeof(double), cudaMemcpyDeviceToHost));
+  return (int)nz;
+}
+
 extern "C" int egpu_ilu0_download(egpu_mat *A, double *ilu_values, double *diag_scaling) {
   if (!A || !A->ilu_valid) return EGPU_ERR_STATE;
+  if (A->ilu_order != 0) return EGPU_ERR_STATE;  // ILU(n > 0): egpu_ilu_download
   egpu_ctx *ctx = A->ctx;
   if (ilu_values)
     EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(ilu_values, A->ilu.p, A->nnz * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));

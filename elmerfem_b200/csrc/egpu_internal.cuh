@@ -74,8 +74,10 @@ struct DevBuf {
     n = o.n;
     owned = false;
   }
+  // a buffer of count elements owned by this object: reused when it already is one, never
+  // written through a view (a view is detached first)
   cudaError_t alloc(size_t count) {
-    if (count == n && p) return cudaSuccess;
+    if (count == n && p && owned) return cudaSuccess;
     release();
     if (count == 0) return cudaSuccess;
     cudaError_t e = cudaMalloc(&p, count * sizeof(T));
@@ -176,6 +178,14 @@ struct egpu_mat {
   DevBuf<int16_t> sell_c16;      // col - row, when every |col - row| < 32768
   DevBuf<double> sell_vals;      // scaled values (FP64)
   DevBuf<float> sell_vals32;     // scaled values (FP32)
+  // ILU structure: the matrix's own pattern for ILU0, the ILU(n) fill structure otherwise
+  // (0-based); the triangular-solve schedules in tri are built on it
+  int ilu_order = -1;            // order the structure was built for (-1: not yet)
+  long long ilu_nnz = 0;
+  int ilu_max_row = 0;
+  DevBuf<int> ilu_rows, ilu_cols, ilu_diag;
+  DevBuf<int> ilu_scatter;       // ILU(n): position of every matrix entry in the structure
+  DevBuf<double> ilu_in;         // ILU(n): the scaled matrix scattered into the structure
   TriSchedule tri;
   bool tri_built = false;
   int solve_count = 0;

@@ -323,3 +323,103 @@ int egpu_color_elements(int nnodes, int nelem, int nen, const int *elem_nodes, s
   }
   return ncol;
 }
+
+// ---------------------------------------------------------------------------------------
+// ILU(n) structure.  CRS_IncompleteLU(A, n > 0) (CRSMatrix.src:2196-2218) applies
+// InitializeILU1 (:2391-2497) n times: row i of the next structure holds row i's entries
+// plus, for every entry k < i that row i had before this step, the entries of row k to the
+// right of its diagonal.  Each step here: a per-row union over those upper parts (rows in
+// parallel), counted first and then written, columns ascending.
+namespace {
+
+void ilu_fill_step(int n, const std::vector<int> &rows, const std::vector<int> &cols, const std::vector<int> &diag,
+                   std::vector<int> &orows, std::vector<int> &ocols, std::vector<int> &odiag) {
+  std::vector<int> cnt(n + 1, 0);
+  auto row_union = [&](int i, std::vector<int> &mark, std::vector<int> &out) {
+    out.clear();
+    for (int e = rows[i]; e < rows[i + 1]; ++e) {
+      mark[cols[e]] = i + 1;
+      out.push_back(cols[e]);
+    }
+    for (int e = rows[i]; e < diag[i]; ++e) {  // entries k < i of the input structure
+      const int k = cols[e];
+      for (int l = diag[k] + 1; l < rows[k + 1]; ++l) {
+        const int j = cols[l];
+        if (mark[j] != i + 1) {
+          mark[j] = i + 1;
+          out.push_back(j);
+        }
+      }
+    }
+    std::sort(out.begin(), out.end());
+  };
+#pragma omp parallel
+  {
+    std::vector<int> mark(n, 0), out;
+#pragma omp for schedule(dynamic, 256)
+    for (int i = 0; i < n; ++i) {
+      row_union(i, mark, out);
+      cnt[i + 1] = (int)out.size();
+    }
+  }
+  orows.assign(n + 1, 0);
+  for (int i = 0; i < n; ++i) orows[i + 1] = orows[i] + cnt[i + 1];
+  ocols.assign(orows[n], 0);
+  odiag.assign(n, -1);
+#pragma omp parallel
+  {
+    std::vector<int> mark(n, 0), out;
+#pragma omp for schedule(dynamic, 256)
+    for (int i = 0; i < n; ++i) {
+      row_union(i, mark, out);
+      for (size_t t = 0; t < out.size(); ++t) {
+        ocols[orows[i] + t] = out[t];
+        if (out[t] == i) odiag[i] = orows[i] + (int)t;
+      }
+    }
+  }
+}
+
+}  // namespace
+
+// 0-based input and output; order 0 returns the input structure
+void egpu_ilu_structure(int n, const std::vector<int> &rows, const std::vector<int> &cols,
+                        const std::vector<int> &diag, int order, std::vector<int> &orows, std::vector<int> &ocols,
+                        std::vector<int> &odiag) {
+  orows = rows;
+  ocols = cols;
+  odiag = diag;
+  for (int step = 0; step < order; ++step) {
+    std::vector<int> r, c, d;
+    ilu_fill_step(n, orows, ocols, odiag, r, c, d);
+    orows.swap(r);
+    ocols.swap(c);
+    odiag.swap(d);
+  }
+}
+
+extern "C" long long egpu_ilu_pattern(int n, const int *rows, const int *cols, const int *diag, int order,
+                                      long long cap, int *ilu_rows, int *ilu_cols, int *ilu_diag) {
+  if (n < 1 || !rows || !cols || !diag || order < 0 || order > 9) return EGPU_ERR_ARG;
+  const int base = rows[0];
+  const long long nnz = (long long)rows[n] - base;
+  std::vector<int> r(n + 1), c(nnz), d(n);
+  for (int i = 0; i <= n; ++i) r[i] = rows[i] - base;
+  for (long long e = 0; e < nnz; ++e) {
+    c[e] = cols[e] - base;
+    if (c[e] < 0 || c[e] >= n) return EGPU_ERR_ARG;
+  }
+  for (int i = 0; i < n; ++i) {
+    d[i] = diag[i] - base;
+    if (d[i] < r[i] || d[i] >= r[i + 1] || c[d[i]] != i) return EGPU_ERR_ARG;
+  }
+  std::vector<int> orows, ocols, odiag;
+  egpu_ilu_structure(n, r, c, d, order, orows, ocols, odiag);
+  const long long onnz = orows[n];
+  if (cap >= onnz && ilu_rows && ilu_cols && ilu_diag) {
+    for (int i = 0; i <= n; ++i) ilu_rows[i] = orows[i] + base;
+    for (long long e = 0; e < onnz; ++e) ilu_cols[e] = ocols[e] + base;
+    for (int i = 0; i < n; ++i) ilu_diag[i] = odiag[i] + base;
+  }
+  return onnz;
+}

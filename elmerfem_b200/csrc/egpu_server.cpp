@@ -290,7 +290,7 @@ extern "C" int egpu_server_pattern(egpu_server *S, int n, const int *rows, const
   {
     std::lock_guard<std::mutex> g(S->gpu_mu);
     int rc = egpu_matrix_bind(S->ctx, n, rows, cols, diag, zero.data(), &P.proto);
-    if (!rc) rc = egpu_matrix_prepare(P.proto, S->prm.precond);
+    if (!rc) rc = egpu_matrix_prepare(P.proto, &S->prm);
     if (rc) {
       if (P.proto) egpu_matrix_free(P.proto);
       return rc;

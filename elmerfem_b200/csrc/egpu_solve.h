@@ -3,6 +3,11 @@
 
 #include "egpu_internal.cuh"
 
+// ILU(n) fill structure (egpu_pattern.cpp), 0-based; order 0 returns the input
+void egpu_ilu_structure(int n, const std::vector<int> &rows, const std::vector<int> &cols,
+                        const std::vector<int> &diag, int order, std::vector<int> &orows, std::vector<int> &ocols,
+                        std::vector<int> &odiag);
+
 namespace egpu {
 
 // inner tolerance of one FP32 segment of the mixed-precision solve; 0 picks it by
@@ -18,8 +23,9 @@ inline double inner_tol_of(const egpu_params *p) {
 int ensure_ctx_scratch(egpu_ctx *ctx);
 int reset_sync(egpu_ctx *ctx);
 int scale_matrix(egpu_mat *A, bool scale_system);
+int ensure_ilu_structure(egpu_mat *A, int order);
 int ensure_tri_schedule(egpu_mat *A);
-int ilu0_factor(egpu_mat *A);
+int ilu_factor(egpu_mat *A, int order);
 int solve_fp64(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_params *prm,
                egpu_result *res);
 int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_params *prm,

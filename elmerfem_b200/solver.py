@@ -104,11 +104,12 @@ class SolverParams:
     max_refinements: int = 100
     abort_not_converged: bool = True
     symmetric: bool = False
+    ilu_order: int = 0            # ILU(n) with precond PREC_ILU0 (Linear System ILU Order)
 
     def to_c(self) -> _lib.Params:
         return _lib.Params(self.method, self.precond, self.max_iter, self.tol, int(self.scale_system),
                            self.precision, int(self.refactorize), self.precond_recompute, self.inner_tol,
-                           self.inner_max_iter, self.max_refinements)
+                           self.inner_max_iter, self.max_refinements, self.ilu_order)
 
     @classmethod
     def from_sif(cls, keywords) -> "SolverParams":
@@ -121,15 +122,17 @@ class SolverParams:
         if meth not in ("bicgstab", "cg"):
             raise NotImplementedError(f"Linear System Iterative Method = {meth}")
         prec = str(kw.get("linear system preconditioning", "none")).lower()
+        ilu_n = 0
         if prec.startswith("none"):
             pc = PREC_NONE
         elif prec.startswith("diagonal"):
             pc = PREC_DIAGONAL
         elif prec.startswith("ilu") and not prec.startswith("ilut"):
+            # IterSolve.src: "ILU<n>" or "ILU" with Linear System ILU Order
             order = kw.get("linear system ilu order")
-            n = int(round(float(order))) if order is not None else (int(prec[3]) if len(prec) > 3 and prec[3].isdigit() else 0)
-            if n != 0:
-                raise NotImplementedError(f"ILU{n}: only ILU0 is on this path")
+            ilu_n = int(round(float(order))) if order is not None else (int(prec[3]) if len(prec) > 3 and prec[3].isdigit() else 0)
+            if not 0 <= ilu_n <= 9:
+                raise ValueError(f"ILU order {ilu_n} outside 0..9")
             pc = PREC_ILU0
         else:
             raise NotImplementedError(f"Linear System Preconditioning = {prec}")
@@ -138,6 +141,7 @@ class SolverParams:
         if "linear system convergence tolerance" not in kw:
             raise KeyError("Linear System Convergence Tolerance is required")
         p = cls(method=CG if meth == "cg" else BICGSTAB, precond=pc,
+                ilu_order=ilu_n if pc == PREC_ILU0 else 0,
                 max_iter=int(kw["linear system max iterations"]),
                 tol=float(kw["linear system convergence tolerance"]),
                 scale_system=_bool(kw.get("linear system scaling", True)),
@@ -238,9 +242,26 @@ class Matrix:
         return v
 
     # ---- preconditioner state (A%ILUValues, A%DiagScaling)
-    def prepare(self, precond: int):
-        """One-time preconditioner structures (ILU0 level schedules) before the first solve."""
-        check(lib().egpu_matrix_prepare(self._h, int(precond)), self.ctx.handle, "egpu_matrix_prepare")
+    def prepare(self, params: "SolverParams | int"):
+        """One-time preconditioner structures (ILU(n) fill and level schedules) before the first
+        solve; params is a SolverParams or a preconditioner code (ILU order 0)."""
+        if not isinstance(params, SolverParams):
+            params = SolverParams(precond=int(params))
+        prm = params.to_c()
+        check(lib().egpu_matrix_prepare(self._h, C.byref(prm)), self.ctx.handle, "egpu_matrix_prepare")
+
+    def ilu(self, order: int, scale_system: bool = True):
+        """Factor ILU(order) on the device (egpu_ilu_build); returns ilu_factors()."""
+        check(lib().egpu_ilu_build(self._h, int(scale_system), int(order)), self.ctx.handle, "egpu_ilu_build")
+        return self.ilu_factors()
+
+    def ilu_factors(self):
+        """The current ILU factors on their structure: (rows, cols, diag 1-based, values)."""
+        nz = check(lib().egpu_ilu_download(self._h, None, None, None, None), self.ctx.handle, "egpu_ilu_download")
+        r, c, d, v = np.zeros(self.n + 1, np.int32), np.zeros(nz, np.int32), np.zeros(self.n, np.int32), np.zeros(nz)
+        check(lib().egpu_ilu_download(self._h, r.ctypes.data, c.ctypes.data, d.ctypes.data, v.ctypes.data),
+              self.ctx.handle, "egpu_ilu_download")
+        return r, c, d, v
 
     def ilu0(self, scale_system: bool = True):
         """Factor ILU0 on the device; returns (ILUValues with inverted U diagonal, DiagScaling)."""

@@ -63,6 +63,9 @@ typedef struct {
                              3e-2 with ILU0 */
   int inner_max_iter;     /* cap on inner iterations per refinement */
   int max_refinements;    /* cap on FP64 refinement steps */
+  /* with EGPU_PREC_ILU0: fill order n of ILU(n) (Linear System Preconditioning = ILUn /
+   * Linear System ILU Order, IterSolve.src:420-575); 0 = ILU0 (the default), at most 9 */
+  int ilu_order;
 } egpu_params;
 
 typedef struct {
@@ -113,10 +116,11 @@ void egpu_matrix_free(egpu_mat *A);
  * with its own Values, right-hand side and solve buffers.  proto may be freed before its
  * clones; the shared data goes with the last of them. */
 int egpu_matrix_clone(egpu_mat *proto, egpu_mat **out);
-/* Builds the preconditioner's one-time structures before the first solve (for ILU0 the
- * level schedules of the triangular solves; nothing for Diagonal / None), so that the first
- * IterSolver call on a pattern costs what later ones do.  Clones share their prototype's. */
-int egpu_matrix_prepare(egpu_mat *A, int precond);
+/* Builds the preconditioner's one-time structures before the first solve (for ILU(n) the
+ * fill structure and the level schedules of the triangular solves; nothing for Diagonal /
+ * None), so that the first IterSolver call on a pattern costs what later ones do.  Clones
+ * share their prototype's. */
+int egpu_matrix_prepare(egpu_mat *A, const egpu_params *prm);
 /* device bytes a solve of A holds beyond the shared pattern, for the given preconditioner */
 long long egpu_matrix_footprint(const egpu_mat *A, int precond);
 
@@ -135,6 +139,16 @@ int egpu_iter_solve_dev(egpu_mat *A, const double *b_dev, double *x_dev, const e
  * Values, inverted U diagonal) and the DiagScaling vector (NULL to skip);
  * egpu_lu_precondition applies u = (LU)^-1 v with the device factors (pcondProc). */
 int egpu_ilu0_build(egpu_mat *A, int scale_system);
+/* the same for ILU(order), order 0..9 (CRS_IncompleteLU(A, order)) */
+int egpu_ilu_build(egpu_mat *A, int scale_system, int order);
+/* ILU(n) structure of a Matrix_t pattern (CRS_IncompleteLU(A, n), CRSMatrix.src:2196-2218:
+ * InitializeILU1 applied n times), host only, index base as given.  Returns the number of
+ * entries; ilu_rows (n+1), ilu_cols and ilu_diag (n) are written when cap >= it. */
+long long egpu_ilu_pattern(int n, const int *rows, const int *cols, const int *diag, int order, long long cap,
+                           int *ilu_rows, int *ilu_cols, int *ilu_diag);
+/* the matrix's current ILU factors on their structure (1-based, as egpu_ilu_pattern
+ * returns it), inverted U diagonal; NULL arrays are skipped.  Returns the number of entries. */
+int egpu_ilu_download(egpu_mat *A, int *ilu_rows, int *ilu_cols, int *ilu_diag, double *ilu_values);
 int egpu_ilu0_download(egpu_mat *A, double *ilu_values, double *diag_scaling);
 int egpu_lu_precondition(egpu_mat *A, const double *v, double *u);
 

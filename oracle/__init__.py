@@ -26,7 +26,8 @@ _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 
 class _Params(C.Structure):
     _fields_ = [("method", C.c_int), ("precond", C.c_int), ("max_iter", C.c_int),
-                ("tol", C.c_double), ("scale_system", C.c_int), ("omp_threads", C.c_int)]
+                ("tol", C.c_double), ("scale_system", C.c_int), ("omp_threads", C.c_int),
+                ("ilu_order", C.c_int)]
 
 
 class _Result(C.Structure):
@@ -64,6 +65,10 @@ def lib():
         L.orc_spmv.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int]
         L.orc_ilu0.argtypes = [C.c_int, _i32p, _i32p, _i32p, _f64p, _f64p]
         L.orc_lusolve.argtypes = [C.c_int, _i32p, _i32p, _i32p, _f64p, _f64p]
+        L.orc_ilu_pattern.restype = C.c_longlong
+        L.orc_ilu_pattern.argtypes = [C.c_int, _i32p, _i32p, _i32p, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p,
+                                      C.c_void_p]
+        L.orc_iluk.argtypes = [C.c_int, _i32p, _i32p, _f64p, _i32p, _i32p, _i32p, _f64p]
         L.orc_scale.argtypes = [C.c_int, _i32p, _i32p, _i32p, _f64p, C.c_void_p, C.c_void_p,
                                 _f64p, C.POINTER(C.c_double), C.c_int]
         L.orc_compute_norm.restype = C.c_double
@@ -144,9 +149,9 @@ def dirichlet(pat: Pattern, values, rhs, con_rows, con_vals=None, symmetric=Fals
 
 
 def solve(pat: Pattern, values, b, method=BICGSTAB, precond=PREC_ILU0, max_iter=1000, tol=1e-10,
-          x0=None, scale=True, threads=0):
+          x0=None, scale=True, threads=0, ilu_order=0):
     x = np.zeros(pat.n) if x0 is None else np.array(x0, dtype=np.float64)
-    p = _Params(method, precond, max_iter, tol, int(scale), threads)
+    p = _Params(method, precond, max_iter, tol, int(scale), threads, ilu_order)
     r = _Result()
     lib().orc_solve(pat.n, pat.rows, pat.cols, pat.diag, np.ascontiguousarray(values, np.float64),
                     np.ascontiguousarray(b, np.float64), x, C.byref(p), C.byref(r))
@@ -165,6 +170,23 @@ def ilu0(pat: Pattern, values):
     out = np.zeros(pat.nnz)
     lib().orc_ilu0(pat.n, pat.rows, pat.cols, pat.diag, np.ascontiguousarray(values, np.float64), out)
     return out
+
+
+def ilu_pattern(pat: Pattern, order: int):
+    """ILU(order) structure (1-based rows, cols, diag): InitializeILU1 applied order times."""
+    nz = lib().orc_ilu_pattern(pat.n, pat.rows, pat.cols, pat.diag, order, 0, None, None, None)
+    r, c, d = np.zeros(pat.n + 1, np.int32), np.zeros(nz, np.int32), np.zeros(pat.n, np.int32)
+    lib().orc_ilu_pattern(pat.n, pat.rows, pat.cols, pat.diag, order, nz, r.ctypes.data, c.ctypes.data,
+                          d.ctypes.data)
+    return r, c, d
+
+
+def iluk(pat: Pattern, values, order: int):
+    """ILU(order) factors on its structure; returns (rows, cols, diag, values), 1-based."""
+    r, c, d = ilu_pattern(pat, order)
+    out = np.zeros(c.size)
+    lib().orc_iluk(pat.n, pat.rows, pat.cols, np.ascontiguousarray(values, np.float64), r, c, d, out)
+    return r, c, d, out
 
 
 def lusolve(pat: Pattern, ilu, b):

@@ -894,6 +894,95 @@ extern "C" void orc_lusolve(int n, const int *rows, const int *cols, const int *
   }
 }
 
+// InitializeILU1, CRSMatrix.src:2391-2497: row i keeps its own entries plus, for every
+// original entry k < i of row i, the upper part of row k (the structure one elimination
+// step fills); RowMin/RowMax bound the column scan as in the reference.
+static void ilu1_step(int n, const std::vector<int> &rows, const std::vector<int> &cols,
+                      const std::vector<int> &diag, std::vector<int> &irows, std::vector<int> &icols,
+                      std::vector<int> &idiag) {
+  std::vector<int> C(n + 1, 0);
+  irows.assign(n + 1, 0);
+  idiag.assign(n, 0);
+  icols.clear();
+  irows[0] = 1;
+  for (int i = 1; i <= n; ++i) {
+    for (int k = rows[i - 1]; k <= rows[i] - 1; ++k) C[cols[k - 1]] = 1;
+    const int rowmin = cols[rows[i - 1] - 1];
+    int rowmax = cols[rows[i] - 2];
+    for (int k = rowmin; k <= i - 1; ++k) {
+      if (C[k] == 1) {
+        for (int l = diag[k - 1] + 1; l <= rows[k] - 1; ++l) {
+          const int j = cols[l - 1];
+          if (C[j] == 0) {
+            C[j] = 2;
+            rowmax = std::max(rowmax, j);
+          }
+        }
+      }
+    }
+    int j = irows[i - 1] - 1;
+    for (int k = rowmin; k <= rowmax; ++k) {
+      if (C[k] > 0) {
+        j = j + 1;
+        C[k] = 0;
+        icols.push_back(k);
+        if (k == i) idiag[i - 1] = j;
+      }
+    }
+    irows[i] = j + 1;
+  }
+}
+
+extern "C" long long orc_ilu_pattern(int n, const int *rows, const int *cols, const int *diag, int order,
+                                     long long cap, int *ilu_rows, int *ilu_cols, int *ilu_diag) {
+  std::vector<int> r(rows, rows + n + 1), c(cols, cols + (rows[n] - 1)), d(diag, diag + n);
+  for (int round = 0; round < order; ++round) {  // CRS_IncompleteLU :2200-2218
+    std::vector<int> ir, ic, id;
+    ilu1_step(n, r, c, d, ir, ic, id);
+    r.swap(ir);
+    c.swap(ic);
+    d.swap(id);
+  }
+  const long long nnz = (long long)r[n] - 1;
+  if (cap >= nnz && ilu_rows && ilu_cols && ilu_diag) {
+    std::copy(r.begin(), r.end(), ilu_rows);
+    std::copy(c.begin(), c.end(), ilu_cols);
+    std::copy(d.begin(), d.end(), ilu_diag);
+  }
+  return nnz;
+}
+
+// CRS_IncompleteLU LU branch, CRSMatrix.src:2312-2366, on the ILU structure
+extern "C" void orc_iluk(int n, const int *rows, const int *cols, const double *values, const int *ilu_rows,
+                         const int *ilu_cols, const int *ilu_diag, double *ilu) {
+  std::vector<double> S(n + 1, 0.0);
+  std::vector<char> C(n + 1, 0);
+  for (int i = 1; i <= n; ++i) {
+    for (int k = rows[i - 1]; k <= rows[i] - 1; ++k) S[cols[k - 1]] = values[k - 1];
+    for (int k = ilu_rows[i - 1]; k <= ilu_rows[i] - 1; ++k) C[ilu_cols[k - 1]] = 1;
+    for (int m = ilu_rows[i - 1]; m <= ilu_diag[i - 1] - 1; ++m) {
+      const int k = ilu_cols[m - 1];
+      if (S[k] == 0.0) continue;
+      if (std::fabs(ilu[ilu_diag[k - 1] - 1]) > AEPS) S[k] = S[k] / ilu[ilu_diag[k - 1] - 1];
+      for (int l = ilu_diag[k - 1] + 1; l <= ilu_rows[k] - 1; ++l) {
+        const int j = ilu_cols[l - 1];
+        if (C[j]) S[j] = S[j] - S[k] * ilu[l - 1];
+      }
+    }
+    for (int k = ilu_rows[i - 1]; k <= ilu_rows[i] - 1; ++k) {
+      if (C[ilu_cols[k - 1]]) {
+        ilu[k - 1] = S[ilu_cols[k - 1]];
+        S[ilu_cols[k - 1]] = 0.0;
+        C[ilu_cols[k - 1]] = 0;
+      }
+    }
+  }
+  for (int i = 1; i <= n; ++i) {
+    double &dv = ilu[ilu_diag[i - 1] - 1];
+    dv = std::fabs(dv) < AEPS ? 1.0 : 1.0 / dv;
+  }
+}
+
 extern "C" int orc_lower_levels(int n, const int *rows, const int *cols, const int *diag, int *level) {
   int maxl = 0;
   for (int i = 1; i <= n; ++i) {
@@ -921,6 +1010,7 @@ struct Ctx {
   const double *ilu;
   int precond;
   int threads;
+  const int *irows, *icols, *idiag;  // ILU structure (the matrix's for ILU0)
 };
 
 double dot(int n, const double *x, const double *y) {  // ddot, restated as a plain sum
@@ -944,7 +1034,7 @@ void pcond(const Ctx &c, double *u, const double *v) {
   const int n = c.n;
   if (c.precond == ORC_PREC_ILU0) {
     for (int i = 0; i < n; ++i) u[i] = v[i];
-    orc_lusolve(n, c.rows, c.cols, c.diag, c.ilu, u);
+    orc_lusolve(n, c.irows, c.icols, c.idiag, c.ilu, u);
   } else if (c.precond == ORC_PREC_DIAGONAL) {
     for (int i = 1; i <= n; ++i) {
       double d = c.values[c.diag[i - 1] - 1];
@@ -1098,14 +1188,27 @@ extern "C" int orc_solve(int n, const int *rows, const int *cols, const int *dia
     for (int i = 0; i < n; ++i) x[i] = 1.0e-8;
 
   std::vector<double> ilu;
+  std::vector<int> ir, ic, id;
+  const int *irows = rows, *icols = cols, *idiag = diag;
   double tp = now();
-  if (prm->precond == ORC_PREC_ILU0) {
+  if (prm->precond == ORC_PREC_ILU0 && prm->ilu_order > 0) {  // ILU(n), CRS_IncompleteLU(A,n)
+    const long long nz = orc_ilu_pattern(n, rows, cols, diag, prm->ilu_order, 0, nullptr, nullptr, nullptr);
+    ir.resize(n + 1);
+    ic.resize(nz);
+    id.resize(n);
+    orc_ilu_pattern(n, rows, cols, diag, prm->ilu_order, nz, ir.data(), ic.data(), id.data());
+    irows = ir.data();
+    icols = ic.data();
+    idiag = id.data();
+    ilu.assign(nz, 0.0);
+    orc_iluk(n, rows, cols, values.data(), irows, icols, idiag, ilu.data());
+  } else if (prm->precond == ORC_PREC_ILU0) {
     ilu.assign(values.size(), 0.0);
     orc_ilu0(n, rows, cols, diag, values.data(), ilu.data());
   }
   r.seconds_precond_setup = now() - tp;
   Ctx c{n, rows, cols, diag, values.data(), ilu.empty() ? nullptr : ilu.data(), prm->precond,
-        prm->omp_threads};
+        prm->omp_threads, irows, icols, idiag};
   if (prm->method == ORC_CG)
     r.info = huti_cg(c, x, b.data(), prm->max_iter, prm->tol, &r.iters, &r.residual);
   else

@@ -54,6 +54,7 @@ typedef struct {
   double tol;          /* Linear System Convergence Tolerance */
   int scale_system;    /* Linear System Scaling (default 1) */
   int omp_threads;     /* threads for the SpMV loop (CRSMatrix.src:3565), <=0: all */
+  int ilu_order;       /* ORC_PREC_ILU0 with ilu_order n > 0: ILU(n) (Linear System ILU Order) */
 } orc_params;
 typedef struct {
   int info;            /* HUTI status code (huti_fdefs.h) */
@@ -75,6 +76,16 @@ void orc_ilu0(int n, const int *rows, const int *cols, const int *diag, const do
               double *ilu_values);
 void orc_lusolve(int n, const int *rows, const int *cols, const int *diag,
                  const double *ilu_values, double *b);
+/* ILU(n) structure: InitializeILU1 (CRSMatrix.src:2391-2497) applied n times to the matrix
+ * pattern (CRS_IncompleteLU :2196-2218).  1-based arrays.  Returns the number of entries;
+ * the arrays are written when cap >= that number. */
+long long orc_ilu_pattern(int n, const int *rows, const int *cols, const int *diag, int order, long long cap,
+                          int *ilu_rows, int *ilu_cols, int *ilu_diag);
+/* CRS_IncompleteLU LU branch (:2312-2366) on the ILU(n) structure: the matrix values
+ * (rows/cols/values) enter the dense row, the structure's flags decide which entries are
+ * kept; inverted U diagonal (:2359-2366). */
+void orc_iluk(int n, const int *rows, const int *cols, const double *values, const int *ilu_rows,
+              const int *ilu_cols, const int *ilu_diag, double *ilu_values);
 void orc_scale(int n, const int *rows, const int *cols, const int *diag, double *values,
                double *b, double *x, double *diag_scaling, double *rhs_scaling, int rhs_scale);
 double orc_compute_norm(int n, const double *x);

@@ -61,8 +61,17 @@ def test_sif_keywords():
     assert (q.method, q.precond, q.symmetric, q.precision) == (eg.CG, eg.PREC_DIAGONAL, True, eg.MIXED)
 
 
+def test_sif_ilu_order():
+    base = {"Linear System Max Iterations": 10, "Linear System Convergence Tolerance": 1e-6}
+    assert eg.SolverParams.from_sif(dict(base, **{"Linear System Preconditioning": "ILU2"})).ilu_order == 2
+    p = eg.SolverParams.from_sif(dict(base, **{"Linear System Preconditioning": "ILU",
+                                               "Linear System ILU Order": 1}))
+    assert (p.precond, p.ilu_order) == (eg.PREC_ILU0, 1)
+    assert eg.SolverParams.from_sif(dict(base, **{"Linear System Preconditioning": "ILU0"})).ilu_order == 0
+
+
 @pytest.mark.parametrize("bad", [{"Linear System Solver": "Direct"}, {"Linear System Iterative Method": "GMRES"},
-                                 {"Linear System Preconditioning": "ILU1"}])
+                                 {"Linear System Preconditioning": "ILUT"}])
 def test_sif_outside_the_path(bad):
     kw = {"Linear System Max Iterations": 10, "Linear System Convergence Tolerance": 1e-6}
     kw.update(bad)

@@ -6,7 +6,7 @@ import pytest
 
 import elmerfem_b200 as eg
 import oracle
-from elmerfem_b200 import meshgen
+from elmerfem_b200 import _lib, meshgen
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
@@ -44,3 +44,25 @@ def test_pattern_rejects_bad_connectivity():
     m2 = meshgen.Mesh(m.coords, 808, bad, 404, m.bnd_elements, m.bnd_ids)
     with pytest.raises(eg.LibError):
         eg.create_matrix(m2)
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+@pytest.mark.parametrize("mk", [lambda: meshgen.hex_cube(7), lambda: meshgen.tet_cube(6),
+                                lambda: meshgen.hex_cube(4), lambda: _heateq()],
+                         ids=["hex7", "tet6", "hex4", "heateq"])
+def test_ilu_structure_matches_oracle(mk, order):
+    """egpu_ilu_pattern (the library's host ILU(n) structure) equals the oracle's restatement
+    of InitializeILU1 applied n times, entry for entry."""
+    import ctypes as C
+    mesh = mk()
+    p = oracle.create_pattern(mesh)
+    ref = oracle.ilu_pattern(p, order)
+    L = _lib.lib()
+    nz = L.egpu_ilu_pattern(p.n, p.rows, p.cols, p.diag, order, 0, None, None, None)
+    assert nz == ref[1].size
+    r, c, d = np.zeros(p.n + 1, np.int32), np.zeros(nz, np.int32), np.zeros(p.n, np.int32)
+    assert L.egpu_ilu_pattern(p.n, p.rows, p.cols, p.diag, order, nz, r.ctypes.data, c.ctypes.data,
+                              d.ctypes.data) == nz
+    assert np.array_equal(r, ref[0]) and np.array_equal(c, ref[1]) and np.array_equal(d, ref[2])
+    # the structure contains the matrix pattern and grows with the order
+    assert nz >= p.nnz
