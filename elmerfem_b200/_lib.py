@@ -19,10 +19,10 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "elmergpu.h")
 EGPU_OK = 0
 ERRORS = {-1: "EGPU_ERR_ARG", -2: "EGPU_ERR_CUDA", -3: "EGPU_ERR_ALLOC", -4: "EGPU_ERR_TIMEOUT",
           -5: "EGPU_ERR_STATE", -6: "EGPU_ERR_BUDGET"}
-HUTI = {1: "HUTI_CONVERGENCE", 2: "HUTI_MAXITER", 20: "HUTI_CG_RHO", 35: "HUTI_BICGSTAB_RHO",
+HUTI = {1: "HUTI_CONVERGENCE", 2: "HUTI_MAXITER", 3: "HUTI_DIVERGENCE", 20: "HUTI_CG_RHO", 35: "HUTI_BICGSTAB_RHO",
         36: "HUTI_BICGSTAB_SNORM", 37: "HUTI_BICGSTAB_OMEGA"}
 
-CG, BICGSTAB = 1, 2
+CG, BICGSTAB, GCR, BICGSTABL = 1, 2, 3, 4
 PREC_NONE, PREC_DIAGONAL, PREC_ILU0 = 0, 1, 2
 FP64, MIXED = 0, 1
 
@@ -35,7 +35,7 @@ class Params(C.Structure):
     _fields_ = [("method", C.c_int), ("precond", C.c_int), ("max_iter", C.c_int), ("tol", C.c_double),
                 ("scale_system", C.c_int), ("precision", C.c_int), ("refactorize", C.c_int),
                 ("precond_recompute", C.c_int), ("inner_tol", C.c_double), ("inner_max_iter", C.c_int),
-                ("max_refinements", C.c_int), ("ilu_order", C.c_int)]
+                ("max_refinements", C.c_int), ("ilu_order", C.c_int), ("restart", C.c_int)]
 
 
 class Result(C.Structure):

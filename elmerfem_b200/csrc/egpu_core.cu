@@ -387,7 +387,9 @@ namespace egpu {
 int ensure_ctx_scratch(egpu_ctx *ctx) {
   if (!ctx->sync.p) {
     EGPU_CUDA_TRY(ctx, ctx->sync.alloc(64));
-    EGPU_CUDA_TRY(ctx, ctx->partials.alloc((size_t)NUM_SLOTS * ctx->num_sms * 8 + 4096));
+    // NUM_SLOTS partial slots and, from slot 16 on, BiCGStab(l)'s Gram matrix ((l+1)(l+2)/2 <= 45
+    // slots), for up to two blocks per SM; the rest is the mixed path's residual partials
+    EGPU_CUDA_TRY(ctx, ctx->partials.alloc((size_t)(16 + 45) * ctx->num_sms * 2 + 8192));
   }
   return EGPU_OK;
 }
@@ -787,8 +789,44 @@ static int run_krylov(egpu_mat *A, const KArgs<VT> &a0, int method, bool offs) {
     if (offs) return launch_coop(ctx, cg_kernel<VT, TRI_TS, true>, a, nullptr, smem);
     return launch_coop(ctx, cg_kernel<VT, TRI_TS, false>, a, nullptr, smem);
   }
+  if constexpr (sizeof(VT) == 8) {
+    if (method == EGPU_GCR) return launch_coop(ctx, gcr_kernel<TRI_TS>, a, nullptr, smem);
+    if (method == EGPU_BICGSTABL) return launch_coop(ctx, bicgstabl_kernel<TRI_TS>, a, nullptr, smem);
+  }
   if (offs) return launch_coop(ctx, bicgstab_kernel<VT, TRI_TS, true>, a, nullptr, smem);
   return launch_coop(ctx, bicgstab_kernel<VT, TRI_TS, false>, a, nullptr, smem);
+}
+
+// stored vectors of GCR (2 (m-1) directions) / BiCGStab(l) (r_0..r_l, u_0..u_l, shadow, x,
+// xp, bp, t): allocated per matrix, refused when they would take more than half the free
+// device memory
+static int ensure_ext_work(egpu_mat *A, const egpu_params *prm, int *m_out) {
+  egpu_ctx *ctx = A->ctx;
+  int m = 0;
+  long long nvec = 0;
+  if (prm->method == EGPU_GCR) {
+    m = prm->restart > 0 ? prm->restart : prm->max_iter;
+    m = std::max(1, std::min(m, prm->max_iter));
+    nvec = 2LL * (m - 1);
+  } else if (prm->method == EGPU_BICGSTABL) {
+    m = prm->restart >= 2 ? prm->restart : 2;
+    if (m > 8) {
+      egpu_set_error(ctx, "BiCGStab(l): polynomial degrees above 8 are not supported");
+      return EGPU_ERR_ARG;
+    }
+    nvec = 2LL * (m + 1) + 6;
+  }
+  *m_out = m;
+  if (nvec == 0) return EGPU_OK;
+  const size_t bytes = (size_t)nvec * A->ldw * sizeof(double);
+  size_t fr = 0, tot = 0;
+  EGPU_CUDA_TRY(ctx, cudaMemGetInfo(&fr, &tot));
+  if (A->ext_work.n < (size_t)nvec * A->ldw && bytes > fr / 2) {
+    egpu_set_error(ctx, "GCR restart too long for the free device memory: set Linear System GCR Restart");
+    return EGPU_ERR_ALLOC;
+  }
+  if (A->ext_work.n < (size_t)nvec * A->ldw) EGPU_CUDA_TRY(ctx, A->ext_work.alloc((size_t)nvec * A->ldw));
+  return EGPU_OK;
 }
 
 // FP64 drop-in solve on device buffers.  x_dev: in = initial guess, out = solution.
@@ -859,6 +897,13 @@ int solve_fp64(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_param
   // zero right-hand side short cut (SolverUtils.src:7309-7320): k_rhs_scale_b sets bit 1
   // of flags; the Krylov kernel then returns at once and the back-scaling writes x = 0.
   a.skip = flags;
+  if (prm->method == EGPU_GCR || prm->method == EGPU_BICGSTABL) {
+    rc = ensure_ext_work(A, prm, &a.ext_m);
+    if (rc) return rc;
+    a.ext = A->ext_work.p;
+    a.ext_lds = ldw;
+    a.true_residual = 0;  // the internal methods stop on the recursive residual
+  }
   EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ek0, ctx->stream));
   rc = run_krylov<double>(A, a, prm->method, false);
   if (rc) return rc;
@@ -1048,6 +1093,7 @@ static int prepare_fp32(egpu_mat *A, bool with_ilu) {
 
 int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_params *prm,
                 egpu_result *res) {
+  if (prm->method == EGPU_GCR || prm->method == EGPU_BICGSTABL) return solve_fp64(A, b_dev, x_dev, prm, res);
   egpu_ctx *ctx = A->ctx;
   const int n = A->n;
   int rc = ensure_ctx_scratch(ctx);
@@ -1610,7 +1656,8 @@ extern "C" long long egpu_matrix_footprint(const egpu_mat *A, int precond) {
 
 static int check_params(const egpu_params *p) {
   if (!p) return EGPU_ERR_ARG;
-  if (p->method != EGPU_CG && p->method != EGPU_BICGSTAB) return EGPU_ERR_ARG;
+  if (p->method < EGPU_CG || p->method > EGPU_BICGSTABL) return EGPU_ERR_ARG;
+  if (p->restart < 0) return EGPU_ERR_ARG;
   if (p->precond < EGPU_PREC_NONE || p->precond > EGPU_PREC_ILU0) return EGPU_ERR_ARG;
   if (p->max_iter < 1) return EGPU_ERR_ARG;
   if (p->precision != EGPU_FP64 && p->precision != EGPU_MIXED) return EGPU_ERR_ARG;

@@ -191,6 +191,7 @@ struct egpu_mat {
   int solve_count = 0;
   bool ilu_valid = false;
   DevBuf<double> work;           // Krylov work vectors
+  DevBuf<double> ext_work;       // GCR directions / BiCGStab(l) vectors
   DevBuf<float> work32;
   DevBuf<double> bx;             // scratch b/x for host-pointer entry points
   AssemblyData asmb;

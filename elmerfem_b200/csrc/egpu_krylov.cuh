@@ -74,6 +74,11 @@ struct KArgs {
   int resume;
   double ru_c;
   double *carry;
+  // GCR / BiCGStab(l): restart length or polynomial degree, and extra stored vectors
+  // (ext_nvec of them, stride ext_lds)
+  int ext_m;
+  VT *ext;
+  long long ext_lds;
   const int *pos_lo, *pos_up;     // solve slot of each row, lower / upper order
   CtaTri<VT> clo, cup;
 };
@@ -1067,6 +1072,614 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstab_kernel(KArgs<VT> a) {
       a.carry[2] = omega;
       a.carry[3] = (!a.true_residual && info == EGPU_HUTI_CONVERGENCE && k > 1) ? 1.0 : 0.0;
     }
+  }
+}
+
+// =====================================================================================
+// GCR with restart m (IterativeMethods.src:919-1055), FP64.
+//
+// Search directions T1 = M^-1 r, T2 = A T1; T2 is orthogonalised against the stored
+// V_1..V_{j-1} by modified Gram-Schmidt (one dot product and one update pass each, in the
+// reference's order), normalised by multiplying with 1/||T2||; x += beta T1, r -= beta T2 with
+// beta = T2 . r.  The stopping test is the recursive residual ||r|| / ||b|| < tol; at every
+// restart (j = 1, k > 1) r is recomputed as b - A x.
+//
+// w layout: R T1 T2 Y(ILU lower result) SLO YUP(level-synchronous slot order)
+// stored directions: S_i = ext + i * ext_lds, V_i = ext + (m - 1 + i) * ext_lds, i < m - 1
+template <int LPR>
+__global__ void __launch_bounds__(EGPU_KBLOCK, 1) gcr_kernel(KArgs<double> a) {
+  using VT = double;
+  struct {
+    int m;
+    double *S, *V;
+    long long lds;
+  } g{a.ext_m, a.ext, a.ext + (long long)(a.ext_m - 1) * a.ext_lds, a.ext_lds};
+  if (a.skip && (*a.skip & 2u)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      a.out_i[0] = EGPU_HUTI_CONVERGENCE;
+      a.out_i[1] = 0;
+      a.out_d[0] = 0.0;
+    }
+    return;
+  }
+  __shared__ double sm[32 * 4];
+  unsigned int epoch = 0;
+  const int n = a.n, nb = gridDim.x;
+  VT *X = a.x, *R = a.w, *T1 = a.w + a.ldw, *T2 = a.w + 2 * a.ldw, *Y = a.w + 3 * a.ldw,
+     *SLO = a.w + 4 * a.ldw, *YUP = a.w + 5 * a.ldw;
+  const VT *B = a.b;
+  const bool ilu = a.precond == EGPU_PREC_ILU0, jac = a.precond == EGPU_PREC_DIAGONAL;
+  const bool cta = ilu && a.tri_cta;
+  const VT SENT = Sentinel<VT>::value();
+  // per row after r changed: prepare the next M^-1 (sentinels, or r in slot order)
+  auto prep = [&](int i, VT r) {
+    if (cta) {
+      SLO[a.pos_lo[i]] = r;
+    } else if (ilu) {
+      Y[i] = SENT;
+      T1[i] = SENT;
+    }
+  };
+  // ---- init: R = B - A X; ||B||, ||R||
+  {
+    double acc[2] = {0.0, 0.0};
+    spmv_phase<VT, LPR, false, false>(a, X, X, [&](int i, VT s, VT) {
+      const VT r = B[i] - s;
+      R[i] = r;
+      prep(i, r);
+      acc[0] += (double)B[i] * (double)B[i];
+      acc[1] += (double)r * (double)r;
+    });
+    block_sum<2>(acc, sm);
+    store_partials(a, SLOT_BB, acc[0]);
+    store_partials(a, SLOT_RR, acc[1]);
+  }
+  if (!grid_barrier(a.bar, a.err, epoch)) return;
+  const double bnorm = sqrt(reduce_partials(a.partials + SLOT_BB * nb, nb, sm));
+  double residual = sqrt(reduce_partials(a.partials + SLOT_RR * nb, nb, sm)) / bnorm;
+  int info = 0, iters = 0;
+  if (residual < a.tol) info = EGPU_HUTI_CONVERGENCE;
+  if (residual != residual) info = 3;  // HUTI_DIVERGENCE
+  for (int k = 1; info == 0; ++k) {
+    if (k > a.maxit) {
+      info = EGPU_HUTI_MAXITER;
+      break;
+    }
+    const int j = (k % g.m == 0) ? g.m : k % g.m;
+    if (j == 1 && k > 1) {  // restart: the true residual
+      spmv_phase<VT, LPR, false, false>(a, X, X, [&](int i, VT s, VT) {
+        const VT r = B[i] - s;
+        R[i] = r;
+        prep(i, r);
+      });
+      if (!grid_barrier(a.bar, a.err, epoch)) return;
+    }
+    // ---- T1 = M^-1 R
+    if (cta) {
+      if (blockIdx.x == 0) cta_ilu(a, SLO, YUP, (const VT *)nullptr, T1, [](int, VT, VT) {});
+    } else if (ilu) {
+      lower_solve<VT, 32>(a, Y, [&](int i) { return R[i]; });
+      upper_solve<VT, 32>(a, Y, T1, [&](int, VT) {});
+    } else {
+      vec_loop<VT>(n, [&](int i, auto w) {
+        constexpr int W = decltype(w)::value;
+        VT r[W], d[W], t[W];
+        vld<W>(R, i, r);
+        if (jac) vld<W>(a.dvals, i, d);
+#pragma unroll
+        for (int q = 0; q < W; ++q) t[q] = jac ? diag_prec(r[q], d[q]) : r[q];
+        vst<W>(T1, i, t);
+      });
+    }
+    if (!grid_barrier(a.bar, a.err, epoch)) return;
+    // ---- T2 = A T1, and the first dot of the orthogonalisation (or ||T2||^2 when j == 1)
+    {
+      double acc[1] = {0.0};
+      const VT *V0 = g.V;
+      spmv_phase<VT, LPR, false, false>(a, T1, T1, [&](int i, VT s, VT) {
+        T2[i] = s;
+        acc[0] += j > 1 ? (double)V0[i] * (double)s : (double)s * (double)s;
+      });
+      block_sum<1>(acc, sm);
+      store_partials(a, j > 1 ? SLOT_PQ : SLOT_TT, acc[0]);
+    }
+    if (!grid_barrier(a.bar, a.err, epoch)) return;
+    // ---- modified Gram-Schmidt against V_1..V_{j-1}
+    for (int i = 0; i < j - 1; ++i) {
+      const int rd = (i & 1) ? SLOT_SS : SLOT_PQ, wr = (i & 1) ? SLOT_PQ : SLOT_SS;
+      const double beta = reduce_partials(a.partials + rd * nb, nb, sm);
+      const VT *Si = g.S + (long long)i * g.lds, *Vi = g.V + (long long)i * g.lds;
+      const VT *Vn = g.V + (long long)(i + 1) * g.lds;
+      const bool last = i + 1 == j - 1;
+      double acc[1] = {0.0};
+      vec_loop<VT>(n, [&](int q0, auto w) {
+        constexpr int W = decltype(w)::value;
+        VT t1[W], t2[W], s[W], v[W], vn[W];
+        vld<W>(T1, q0, t1);
+        vld<W>(T2, q0, t2);
+        vld<W>(Si, q0, s);
+        vld<W>(Vi, q0, v);
+        if (!last) vld<W>(Vn, q0, vn);
+#pragma unroll
+        for (int q = 0; q < W; ++q) {
+          t1[q] = t1[q] - beta * s[q];
+          t2[q] = t2[q] - beta * v[q];
+          acc[0] += last ? (double)t2[q] * (double)t2[q] : (double)vn[q] * (double)t2[q];
+        }
+        vst<W>(T1, q0, t1);
+        vst<W>(T2, q0, t2);
+      });
+      block_sum<1>(acc, sm);
+      store_partials(a, last ? SLOT_TT : wr, acc[0]);
+      if (!grid_barrier(a.bar, a.err, epoch)) return;
+    }
+    // ---- normalise: T1, T2 times 1/||T2||; beta = T2 . R
+    {
+      const double alpha = sqrt(reduce_partials(a.partials + SLOT_TT * nb, nb, sm));
+      const double inv = 1.0 / alpha;
+      double acc[1] = {0.0};
+      vec_loop<VT>(n, [&](int q0, auto w) {
+        constexpr int W = decltype(w)::value;
+        VT t1[W], t2[W], r[W];
+        vld<W>(T1, q0, t1);
+        vld<W>(T2, q0, t2);
+        vld<W>(R, q0, r);
+#pragma unroll
+        for (int q = 0; q < W; ++q) {
+          t1[q] = inv * t1[q];
+          t2[q] = inv * t2[q];
+          acc[0] += (double)t2[q] * (double)r[q];
+        }
+        vst<W>(T1, q0, t1);
+        vst<W>(T2, q0, t2);
+      });
+      block_sum<1>(acc, sm);
+      store_partials(a, SLOT_TS, acc[0]);
+    }
+    if (!grid_barrier(a.bar, a.err, epoch)) return;
+    // ---- x += beta T1; r -= beta T2; store the direction; ||r||
+    {
+      const double beta = reduce_partials(a.partials + SLOT_TS * nb, nb, sm);
+      VT *Sj = g.S + (long long)(j - 1) * g.lds, *Vj = g.V + (long long)(j - 1) * g.lds;
+      const bool keep = j != g.m;
+      double acc[1] = {0.0};
+      for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const VT t1 = T1[i], t2 = T2[i];
+        X[i] = X[i] + beta * t1;
+        const VT r = R[i] - beta * t2;
+        R[i] = r;
+        if (keep) {
+          Sj[i] = t1;
+          Vj[i] = t2;
+        }
+        acc[0] += (double)r * (double)r;
+        prep(i, r);
+      }
+      block_sum<1>(acc, sm);
+      store_partials(a, SLOT_RR, acc[0]);
+    }
+    if (!grid_barrier(a.bar, a.err, epoch)) return;
+    residual = sqrt(reduce_partials(a.partials + SLOT_RR * nb, nb, sm)) / bnorm;
+    iters = k;
+    if (residual < a.tol) info = EGPU_HUTI_CONVERGENCE;
+    else if (residual != residual) info = 3;  // HUTI_DIVERGENCE
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.out_i[0] = info;
+    a.out_i[1] = iters;
+    a.out_d[0] = residual;
+    a.out_d[1] = bnorm;
+  }
+}
+
+// =====================================================================================
+// BiCGStab(l) (IterativeMethods.src:559-834), FP64: right-preconditioned (the iteration
+// runs on A M^-1 and x = M^-1 x~ + xp at the end), l BiCG steps then the convex minimal-
+// residual polynomial of degree l, reliable residual / solution updates with delta = 1e-2,
+// stopping on the recursive residual.
+//
+// ext layout (stride ext_lds): r_0..r_l, u_0..u_l, RR(shadow) XT(x~) XP BP T
+// w layout: Y(ILU lower result, w[3]) SLO YUP(level-synchronous slot order, w[4], w[5])
+
+// small dense LU with partial pivoting (dgetrf) and solve (dgetrs 'n'), column major
+__device__ inline void bl_lu(int m, double *a, int lda, int *piv) {
+  for (int k = 0; k < m; ++k) {
+    int p = k;
+    for (int i = k + 1; i < m; ++i)
+      if (fabs(a[i + k * lda]) > fabs(a[p + k * lda])) p = i;
+    piv[k] = p;
+    if (p != k)
+      for (int j = 0; j < m; ++j) {
+        const double t = a[k + j * lda];
+        a[k + j * lda] = a[p + j * lda];
+        a[p + j * lda] = t;
+      }
+    if (a[k + k * lda] != 0.0)
+      for (int i = k + 1; i < m; ++i) a[i + k * lda] = a[i + k * lda] / a[k + k * lda];
+    for (int j = k + 1; j < m; ++j)
+      for (int i = k + 1; i < m; ++i) a[i + j * lda] = a[i + j * lda] - a[i + k * lda] * a[k + j * lda];
+  }
+}
+__device__ inline void bl_lu_solve(int m, const double *a, int lda, const int *piv, double *b) {
+  for (int k = 0; k < m; ++k)
+    if (piv[k] != k) {
+      const double t = b[k];
+      b[k] = b[piv[k]];
+      b[piv[k]] = t;
+    }
+  for (int k = 0; k < m; ++k)
+    for (int i = k + 1; i < m; ++i) b[i] = b[i] - a[i + k * lda] * b[k];
+  for (int k = m - 1; k >= 0; --k) {
+    b[k] = b[k] / a[k + k * lda];
+    for (int i = 0; i < k; ++i) b[i] = b[i] - a[i + k * lda] * b[k];
+  }
+}
+
+constexpr int BL_MAXL = 8;
+
+template <int LPR>
+__global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstabl_kernel(KArgs<double> a) {
+  using VT = double;
+  if (a.skip && (*a.skip & 2u)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      a.out_i[0] = EGPU_HUTI_CONVERGENCE;
+      a.out_i[1] = 0;
+      a.out_d[0] = 0.0;
+    }
+    return;
+  }
+  __shared__ double sm[32 * 4];
+  __shared__ double Zs[(BL_MAXL + 1) * (BL_MAXL + 1)], y0s[BL_MAXL + 1];
+  unsigned int epoch = 0;
+  const int n = a.n, nb = gridDim.x, l = a.ext_m, L1 = l + 1;
+  const long long ld = a.ext_lds;
+  auto rv = [&](int j) { return a.ext + (long long)j * ld; };
+  auto uv = [&](int j) { return a.ext + (long long)(L1 + j) * ld; };
+  VT *RR = a.ext + (long long)(2 * L1) * ld, *XT = RR + ld, *XP = RR + 2 * ld, *BP = RR + 3 * ld, *T = RR + 4 * ld;
+  VT *X = a.x, *Y = a.w + 3 * a.ldw, *SLO = a.w + 4 * a.ldw, *YUP = a.w + 5 * a.ldw;
+  const VT *B = a.b;
+  const bool ilu = a.precond == EGPU_PREC_ILU0, jac = a.precond == EGPU_PREC_DIAGONAL;
+  const bool cta = ilu && a.tri_cta;
+  const VT SENT = Sentinel<VT>::value();
+  double *gram = a.partials + 16 * nb;  // (l+1)(l+2)/2 slots of nb partials
+  // dst = M^-1 src (pcondlsubr); ends after a grid barrier
+  auto precond = [&](const VT *src, VT *dst) -> bool {
+    if (ilu) {
+      vec_loop<VT>(n, [&](int i, auto w) {
+        constexpr int W = decltype(w)::value;
+        if (cta) {
+          VT v[W];
+          vld<W>(src, i, v);
+#pragma unroll
+          for (int q = 0; q < W; ++q) SLO[a.pos_lo[i + q]] = v[q];
+        } else {
+          vfill<W>(Y, i, SENT);
+          vfill<W>(dst, i, SENT);
+        }
+      });
+      if (!grid_barrier(a.bar, a.err, epoch)) return false;
+      if (cta) {
+        if (blockIdx.x == 0) cta_ilu(a, SLO, YUP, (const VT *)nullptr, dst, [](int, VT, VT) {});
+      } else {
+        lower_solve<VT, 32>(a, Y, [&](int i) { return src[i]; });
+        upper_solve<VT, 32>(a, Y, dst, [&](int, VT) {});
+      }
+    } else {
+      vec_loop<VT>(n, [&](int i, auto w) {
+        constexpr int W = decltype(w)::value;
+        VT v[W], d[W], t[W];
+        vld<W>(src, i, v);
+        if (jac) vld<W>(a.dvals, i, d);
+#pragma unroll
+        for (int q = 0; q < W; ++q) t[q] = jac ? diag_prec(v[q], d[q]) : v[q];
+        vst<W>(dst, i, t);
+      });
+    }
+    return grid_barrier(a.bar, a.err, epoch);
+  };
+  // ---- init: r_0 = B - A X; ||B||, ||r_0||; shadow, bp, xp; x~ = 0
+  {
+    double acc[2] = {0.0, 0.0};
+    VT *R0 = rv(0);
+    spmv_phase<VT, LPR, false, false>(a, X, X, [&](int i, VT s, VT) {
+      const VT r = B[i] - s;
+      R0[i] = r;
+      RR[i] = r;
+      BP[i] = r;
+      XP[i] = X[i];
+      XT[i] = 0.0;
+      acc[0] += (double)B[i] * (double)B[i];
+      acc[1] += (double)r * (double)r;
+    });
+    for (int j = 0; j < L1; ++j)  // u_j start at zero (RealBiCGStabl zeroes its work array)
+      vec_loop<VT>(n, [&](int i, auto w) {
+        constexpr int W = decltype(w)::value;
+        vfill<W>(uv(j), i, VT(0));
+      });
+    block_sum<2>(acc, sm);
+    store_partials(a, SLOT_BB, acc[0]);
+    store_partials(a, SLOT_RR, acc[1]);
+    store_partials(a, SLOT_RHO, acc[1]);  // rr . r_0 = ||r_0||^2
+  }
+  if (!grid_barrier(a.bar, a.err, epoch)) return;
+  const double bnrm = sqrt(reduce_partials(a.partials + SLOT_BB * nb, nb, sm));
+  const double rnrm0 = sqrt(reduce_partials(a.partials + SLOT_RR * nb, nb, sm));
+  double errorind = rnrm0 / bnrm, rnrm = rnrm0, mxnrmx = rnrm0, mxnrmr = rnrm0;
+  double alpha = 0.0, omega = 1.0, sigma = 1.0, rho0 = 1.0, rho1 = 0.0;
+  int info = 0, round = 0, rounds = 0;
+  if (errorind < a.tol) info = EGPU_HUTI_CONVERGENCE;
+  bool done_x = info != 0;  // converged at the initial guess: x unchanged
+  for (round = 1; info == 0 && round <= a.maxit; ++round) {
+    // --------------------------------------------------------------- the BiCG part
+    rounds = round;
+    rho0 = -omega * rho0;
+    bool early = false;
+    for (int k = 1; k <= l; ++k) {
+      rho1 = reduce_partials(a.partials + SLOT_RHO * nb, nb, sm);
+      if (rho0 == 0.0 || rho1 != rho1) {
+        info = 3;  // HUTI_DIVERGENCE (the reference stops with Fatal)
+        early = true;
+        break;
+      }
+      const double beta = alpha * (rho1 / rho0);
+      rho0 = rho1;
+      for (int j = 0; j <= k - 1; ++j) {
+        VT *U = uv(j);
+        const VT *Rj = rv(j);
+        vec_loop<VT>(n, [&](int i, auto w) {
+          constexpr int W = decltype(w)::value;
+          VT u[W], r[W];
+          vld<W>(U, i, u);
+          vld<W>(Rj, i, r);
+#pragma unroll
+          for (int q = 0; q < W; ++q) u[q] = r[q] - beta * u[q];
+          vst<W>(U, i, u);
+        });
+      }
+      if (!grid_barrier(a.bar, a.err, epoch)) return;
+      if (!precond(uv(k - 1), T)) return;
+      {
+        double acc[1] = {0.0};
+        VT *Uk = uv(k);
+        spmv_phase<VT, LPR, false, false>(a, T, T, [&](int i, VT s, VT) {
+          Uk[i] = s;
+          acc[0] += (double)RR[i] * (double)s;
+        });
+        block_sum<1>(acc, sm);
+        store_partials(a, SLOT_PQ, acc[0]);
+      }
+      if (!grid_barrier(a.bar, a.err, epoch)) return;
+      sigma = reduce_partials(a.partials + SLOT_PQ * nb, nb, sm);
+      if (sigma == 0.0 || sigma != sigma) {
+        info = 3;
+        early = true;
+        break;
+      }
+      alpha = rho1 / sigma;
+      {
+        double acc[1] = {0.0};
+        const VT *U0 = uv(0);
+        vec_loop<VT>(n, [&](int i, auto w) {
+          constexpr int W = decltype(w)::value;
+          VT xt[W], u0[W];
+          vld<W>(XT, i, xt);
+          vld<W>(U0, i, u0);
+#pragma unroll
+          for (int q = 0; q < W; ++q) xt[q] = xt[q] + alpha * u0[q];
+          vst<W>(XT, i, xt);
+        });
+        for (int j = 0; j <= k - 1; ++j) {
+          VT *Rj = rv(j);
+          const VT *Un = uv(j + 1);
+          vec_loop<VT>(n, [&](int i, auto w) {
+            constexpr int W = decltype(w)::value;
+            VT r[W], u[W];
+            vld<W>(Rj, i, r);
+            vld<W>(Un, i, u);
+#pragma unroll
+            for (int q = 0; q < W; ++q) {
+              r[q] = r[q] - alpha * u[q];
+              if (j == 0) acc[0] += (double)r[q] * (double)r[q];
+            }
+            vst<W>(Rj, i, r);
+          });
+        }
+        block_sum<1>(acc, sm);
+        store_partials(a, SLOT_RR, acc[0]);
+      }
+      if (!grid_barrier(a.bar, a.err, epoch)) return;
+      rnrm = sqrt(reduce_partials(a.partials + SLOT_RR * nb, nb, sm));
+      mxnrmx = fmax(mxnrmx, rnrm);
+      mxnrmr = fmax(mxnrmr, rnrm);
+      errorind = rnrm / bnrm;
+      if (errorind < a.tol || errorind != errorind) {
+        info = errorind < a.tol ? EGPU_HUTI_CONVERGENCE : 3;
+        early = true;
+        break;
+      }
+      if (!precond(rv(k - 1), T)) return;
+      {
+        double acc[1] = {0.0};
+        VT *Rk = rv(k);
+        spmv_phase<VT, LPR, false, false>(a, T, T, [&](int i, VT s, VT) {
+          Rk[i] = s;
+          acc[0] += (double)RR[i] * (double)s;  // rho of the next step
+        });
+        block_sum<1>(acc, sm);
+        store_partials(a, SLOT_RHO, acc[0]);
+      }
+      if (!grid_barrier(a.bar, a.err, epoch)) return;
+    }
+    if (early) break;
+    // --------------------------------------------------------------- the polynomial part
+    {
+      // Gram matrix Z_ij = r_i . r_j, j <= i, one pass over the l+1 vectors per entry
+      int slot = 0;
+      for (int i2 = 0; i2 < L1; ++i2)
+        for (int j2 = 0; j2 <= i2; ++j2, ++slot) {
+          double acc[1] = {0.0};
+          const VT *Ri = rv(i2), *Rj = rv(j2);
+          vec_loop<VT>(n, [&](int i, auto w) {
+            constexpr int W = decltype(w)::value;
+            VT x1[W], x2[W];
+            vld<W>(Ri, i, x1);
+            vld<W>(Rj, i, x2);
+#pragma unroll
+            for (int q = 0; q < W; ++q) acc[0] += (double)x1[q] * (double)x2[q];
+          });
+          block_sum<1>(acc, sm);
+          if (threadIdx.x == 0) gram[slot * nb + blockIdx.x] = acc[0];
+        }
+    }
+    if (!grid_barrier(a.bar, a.err, epoch)) return;
+    {
+      int slot = 0;
+      for (int i2 = 0; i2 < L1; ++i2)
+        for (int j2 = 0; j2 <= i2; ++j2, ++slot) {
+          const double z = reduce_partials(gram + slot * nb, nb, sm);
+          if (threadIdx.x == 0) {
+            Zs[i2 + j2 * L1] = z;
+            Zs[j2 + i2 * L1] = z;
+          }
+        }
+      __syncthreads();
+      // every block solves the small system redundantly (identical inputs, identical result)
+      if (threadIdx.x == 0) {
+        double M[(BL_MAXL - 1) * (BL_MAXL - 1)], y0[BL_MAXL + 1], yl[BL_MAXL + 1], yv[BL_MAXL + 1];
+        int piv[BL_MAXL];
+        const int lm = l - 1;
+        for (int j = 0; j < lm; ++j)
+          for (int i = 0; i < lm; ++i) M[i + j * lm] = Zs[(i + 1) + (j + 1) * L1];
+        if (lm > 0) bl_lu(lm, M, lm, piv);
+        y0[0] = -1.0;
+        for (int i = 1; i < l; ++i) y0[i] = Zs[i];
+        if (lm > 0) bl_lu_solve(lm, M, lm, piv, y0 + 1);
+        y0[l] = 0.0;
+        yl[0] = 0.0;
+        for (int i = 1; i < l; ++i) yl[i] = Zs[i + l * L1];
+        if (lm > 0) bl_lu_solve(lm, M, lm, piv, yl + 1);
+        yl[l] = -1.0;
+        auto symv = [&](const double *v, double *o) {
+          for (int i = 0; i < L1; ++i) {
+            double t = 0.0;
+            for (int j = 0; j < L1; ++j) t = t + Zs[i + j * L1] * v[j];
+            o[i] = t;
+          }
+        };
+        auto sdot = [&](const double *p, const double *q) {
+          double t = 0.0;
+          for (int i = 0; i < L1; ++i) t = t + p[i] * q[i];
+          return t;
+        };
+        symv(y0, yv);
+        const double kappa0 = sqrt(sdot(y0, yv));
+        symv(yl, yv);
+        const double kappal = sqrt(sdot(yl, yv));
+        symv(y0, yv);
+        const double varrho = sdot(yl, yv) / (kappa0 * kappal);
+        const double hatgamma = varrho / fabs(varrho) * fmax(fabs(varrho), 7e-1) * kappa0 / kappal;
+        for (int i = 0; i < L1; ++i) y0s[i] = y0[i] - hatgamma * yl[i];
+      }
+      __syncthreads();
+    }
+    omega = y0s[l];
+    // update u_0, x~, r_0 (j = 1..l in order, per element)
+    vec_loop<VT>(n, [&](int i, auto w) {
+      constexpr int W = decltype(w)::value;
+      VT u0[W], xt[W], r0[W], t1[W], t2[W];
+      vld<W>(uv(0), i, u0);
+      vld<W>(XT, i, xt);
+      vld<W>(rv(0), i, r0);
+      for (int j = 1; j <= l; ++j) {
+        const double c = y0s[j];
+        vld<W>(uv(j), i, t1);
+#pragma unroll
+        for (int q = 0; q < W; ++q) u0[q] = u0[q] - c * t1[q];
+        vld<W>(rv(j - 1), i, t2);
+#pragma unroll
+        for (int q = 0; q < W; ++q) xt[q] = xt[q] + c * t2[q];
+        vld<W>(rv(j), i, t1);
+#pragma unroll
+        for (int q = 0; q < W; ++q) r0[q] = r0[q] - c * t1[q];
+      }
+      vst<W>(uv(0), i, u0);
+      vst<W>(XT, i, xt);
+      vst<W>(rv(0), i, r0);
+    });
+    {
+      double yv[BL_MAXL + 1];
+      for (int i = 0; i < L1; ++i) {
+        double t = 0.0;
+        for (int j = 0; j < L1; ++j) t = t + Zs[i + j * L1] * y0s[j];
+        yv[i] = t;
+      }
+      double t = 0.0;
+      for (int i = 0; i < L1; ++i) t = t + y0s[i] * yv[i];
+      rnrm = sqrt(t);
+    }
+    if (!grid_barrier(a.bar, a.err, epoch)) return;
+    // --------------------------------------------------------------- reliable updates
+    const double delta = 1.0e-2;
+    mxnrmx = fmax(mxnrmx, rnrm);
+    mxnrmr = fmax(mxnrmr, rnrm);
+    const bool xpdt = rnrm < delta * rnrm0 && rnrm0 < mxnrmx;
+    const bool rcmp = (rnrm < delta * mxnrmr && rnrm0 < mxnrmr) || xpdt;
+    if (rcmp) {
+      if (!precond(XT, T)) return;
+      VT *R0 = rv(0);
+      spmv_phase<VT, LPR, false, false>(a, T, T, [&](int i, VT s, VT) {
+        const VT r = BP[i] - s;
+        R0[i] = r;
+        if (xpdt) {
+          XP[i] = XP[i] + T[i];
+          XT[i] = 0.0;
+          BP[i] = r;
+        }
+      });
+      mxnrmr = rnrm;
+      if (xpdt) mxnrmx = rnrm;
+      if (!grid_barrier(a.bar, a.err, epoch)) return;
+    }
+    // rho for the next round's first step: rr . r_0
+    {
+      double acc[1] = {0.0};
+      const VT *R0 = rv(0);
+      vec_loop<VT>(n, [&](int i, auto w) {
+        constexpr int W = decltype(w)::value;
+        VT x1[W], x2[W];
+        vld<W>(RR, i, x1);
+        vld<W>(R0, i, x2);
+#pragma unroll
+        for (int q = 0; q < W; ++q) acc[0] += (double)x1[q] * (double)x2[q];
+      });
+      block_sum<1>(acc, sm);
+      store_partials(a, SLOT_RHO, acc[0]);
+    }
+    if (!grid_barrier(a.bar, a.err, epoch)) return;
+    errorind = rnrm / bnrm;
+    if (errorind < a.tol) info = EGPU_HUTI_CONVERGENCE;
+    else if (errorind != errorind) info = 3;
+  }
+  if (info == 0) info = EGPU_HUTI_MAXITER;
+  const int iters = rounds;
+  // x = M^-1 x~ + xp
+  if (!done_x) {
+    if (!precond(XT, T)) return;
+    vec_loop<VT>(n, [&](int i, auto w) {
+      constexpr int W = decltype(w)::value;
+      VT t[W], xp[W];
+      vld<W>(T, i, t);
+      vld<W>(XP, i, xp);
+#pragma unroll
+      for (int q = 0; q < W; ++q) t[q] = t[q] + xp[q];
+      vst<W>(X, i, t);
+    });
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.out_i[0] = info;
+    a.out_i[1] = iters;
+    a.out_d[0] = errorind;
+    a.out_d[1] = bnrm;
   }
 }
 

@@ -16,7 +16,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from ._lib import BICGSTAB, CG, FP64, MIXED, PREC_DIAGONAL, PREC_ILU0, PREC_NONE, LibError, check, lib
+from ._lib import BICGSTAB, BICGSTABL, CG, FP64, GCR, MIXED, PREC_DIAGONAL, PREC_ILU0, PREC_NONE, LibError, check, lib
 
 
 class NotConverged(RuntimeError):
@@ -105,11 +105,12 @@ class SolverParams:
     abort_not_converged: bool = True
     symmetric: bool = False
     ilu_order: int = 0            # ILU(n) with precond PREC_ILU0 (Linear System ILU Order)
+    restart: int = 0              # GCR restart (0: max_iter) / BiCGStab(l) degree (0: 2)
 
     def to_c(self) -> _lib.Params:
         return _lib.Params(self.method, self.precond, self.max_iter, self.tol, int(self.scale_system),
                            self.precision, int(self.refactorize), self.precond_recompute, self.inner_tol,
-                           self.inner_max_iter, self.max_refinements, self.ilu_order)
+                           self.inner_max_iter, self.max_refinements, self.ilu_order, self.restart)
 
     @classmethod
     def from_sif(cls, keywords) -> "SolverParams":
@@ -119,7 +120,8 @@ class SolverParams:
         if solver != "iterative":
             raise NotImplementedError(f"Linear System Solver = {solver}: only 'iterative' is on this path")
         meth = str(kw.get("linear system iterative method", "bicgstab")).lower()
-        if meth not in ("bicgstab", "cg"):
+        methods = {"bicgstab": BICGSTAB, "cg": CG, "gcr": GCR, "bicgstabl": BICGSTABL}
+        if meth not in methods:
             raise NotImplementedError(f"Linear System Iterative Method = {meth}")
         prec = str(kw.get("linear system preconditioning", "none")).lower()
         ilu_n = 0
@@ -140,7 +142,14 @@ class SolverParams:
             raise KeyError("Linear System Max Iterations is required (ListGetInteger without default)")
         if "linear system convergence tolerance" not in kw:
             raise KeyError("Linear System Convergence Tolerance is required")
-        p = cls(method=CG if meth == "cg" else BICGSTAB, precond=pc,
+        restart = 0
+        if meth == "gcr" and "linear system gcr restart" in kw:
+            restart = int(kw["linear system gcr restart"])
+        if meth == "bicgstabl" and "bicgstabl polynomial degree" in kw:
+            restart = int(kw["bicgstabl polynomial degree"])
+            if restart < 2:
+                raise ValueError("BiCGstabl polynomial degree < 2")
+        p = cls(method=methods[meth], precond=pc, restart=restart,
                 ilu_order=ilu_n if pc == PREC_ILU0 else 0,
                 max_iter=int(kw["linear system max iterations"]),
                 tol=float(kw["linear system convergence tolerance"]),

@@ -43,7 +43,7 @@ extern "C" {
 #define EGPU_HUTI_BICGSTAB_OMEGA 37
 
 /* ---- keyword surface (IterSolve.src:221-420) ------------------------------------ */
-enum { EGPU_CG = 1, EGPU_BICGSTAB = 2 };                           /* Linear System Iterative Method */
+enum { EGPU_CG = 1, EGPU_BICGSTAB = 2, EGPU_GCR = 3, EGPU_BICGSTABL = 4 }; /* Linear System Iterative Method */
 enum { EGPU_PREC_NONE = 0, EGPU_PREC_DIAGONAL = 1, EGPU_PREC_ILU0 = 2 }; /* Linear System Preconditioning */
 enum { EGPU_FP64 = 0, EGPU_MIXED = 1 };  /* FP64 drop-in | FP32 inner Krylov in FP64 refinement */
 
@@ -66,6 +66,10 @@ typedef struct {
   /* with EGPU_PREC_ILU0: fill order n of ILU(n) (Linear System Preconditioning = ILUn /
    * Linear System ILU Order, IterSolve.src:420-575); 0 = ILU0 (the default), at most 9 */
   int ilu_order;
+  /* EGPU_GCR: Linear System GCR Restart (0: Max Iterations, IterSolve.src:298-304);
+   * EGPU_BICGSTABL: BiCGstabl polynomial degree (0: 2, :306-310).  Both run in FP64 whatever
+   * the precision, stopping on the recursive residual as the reference's internal methods do. */
+  int restart;
 } egpu_params;
 
 typedef struct {

@@ -29,6 +29,7 @@ constexpr double HUTI_EPSILON = 1.17549435E-38;         // hutiter/src/huti_defs
 // HUTI status codes, hutiter/src/huti_fdefs.h:18-52
 constexpr int HUTI_CONVERGENCE = 1;
 constexpr int HUTI_MAXITER = 2;
+constexpr int HUTI_DIVERGENCE = 3;
 constexpr int HUTI_CG_RHO = 20;
 constexpr int HUTI_BICGSTAB_RHO = 35;
 constexpr int HUTI_BICGSTAB_SNORM = 36;
@@ -1155,6 +1156,225 @@ int huti_bicgstab(const Ctx &c, double *X, const double *B, int maxit, double to
   return info;
 }
 
+// GCR with restart m, IterativeMethods.src:919-1055 (preconditioned search directions
+// T1 = M^-1 r, modified Gram-Schmidt of A T1 against the stored ones, recursive residual
+// stopping test ||r|| / ||b|| < tol)
+int gcr(const Ctx &c, double *x, const double *b, int rounds, double tol, int m, int *iters, double *resid) {
+  const int n = c.n;
+  std::vector<double> r(n), T1(n), T2(n);
+  std::vector<std::vector<double>> S(std::max(0, m - 1), std::vector<double>(n, 0.0)),
+      V(std::max(0, m - 1), std::vector<double>(n, 0.0));
+  matvec(c, x, r.data());
+  for (int i = 0; i < n; ++i) r[i] = b[i] - r[i];
+  const double bnorm = nrm2(n, b);
+  double rnorm = nrm2(n, r.data());
+  double residual = rnorm / bnorm;
+  *iters = 0;
+  *resid = residual;
+  if (residual < tol) return HUTI_CONVERGENCE;
+  if (residual != residual) return HUTI_DIVERGENCE;
+  for (int k = 1; k <= rounds; ++k) {
+    int j;
+    if (k % m == 0) {
+      j = m;
+    } else {
+      j = k % m;
+      if (j == 1 && k > 1) {  // true residual at a restart
+        matvec(c, x, r.data());
+        for (int i = 0; i < n; ++i) r[i] = b[i] - r[i];
+      }
+    }
+    pcond(c, T1.data(), r.data());
+    matvec(c, T1.data(), T2.data());
+    for (int i = 1; i <= j - 1; ++i) {
+      const double beta = dot(n, V[i - 1].data(), T2.data());
+      for (int t = 0; t < n; ++t) T1[t] = T1[t] - beta * S[i - 1][t];
+      for (int t = 0; t < n; ++t) T2[t] = T2[t] - beta * V[i - 1][t];
+    }
+    const double alpha = nrm2(n, T2.data());
+    for (int t = 0; t < n; ++t) T1[t] = 1.0 / alpha * T1[t];
+    for (int t = 0; t < n; ++t) T2[t] = 1.0 / alpha * T2[t];
+    const double beta = dot(n, T2.data(), r.data());
+    for (int t = 0; t < n; ++t) x[t] = x[t] + beta * T1[t];
+    for (int t = 0; t < n; ++t) r[t] = r[t] - beta * T2[t];
+    if (j != m) {
+      S[j - 1] = T1;
+      V[j - 1] = T2;
+    }
+    rnorm = nrm2(n, r.data());
+    residual = rnorm / bnorm;
+    *iters = k;
+    *resid = residual;
+    if (residual < tol) return HUTI_CONVERGENCE;
+    if (residual != residual) return HUTI_DIVERGENCE;
+  }
+  return HUTI_MAXITER;
+}
+
+// LU with partial pivoting of a small dense column-major matrix (dgetrf) and the solve with
+// it (dgetrs 'n'), as RealBiCGStabl calls them on its (l-1) x (l-1) block
+void small_lu(int m, double *a, int lda, int *piv) {
+  for (int k = 0; k < m; ++k) {
+    int p = k;
+    for (int i = k + 1; i < m; ++i)
+      if (std::fabs(a[i + k * lda]) > std::fabs(a[p + k * lda])) p = i;
+    piv[k] = p;
+    if (p != k)
+      for (int j = 0; j < m; ++j) std::swap(a[k + j * lda], a[p + j * lda]);
+    if (a[k + k * lda] != 0.0)
+      for (int i = k + 1; i < m; ++i) a[i + k * lda] = a[i + k * lda] / a[k + k * lda];
+    for (int j = k + 1; j < m; ++j)
+      for (int i = k + 1; i < m; ++i) a[i + j * lda] = a[i + j * lda] - a[i + k * lda] * a[k + j * lda];
+  }
+}
+void small_lu_solve(int m, const double *a, int lda, const int *piv, double *bv) {
+  for (int k = 0; k < m; ++k)
+    if (piv[k] != k) std::swap(bv[k], bv[piv[k]]);
+  for (int k = 0; k < m; ++k)
+    for (int i = k + 1; i < m; ++i) bv[i] = bv[i] - a[i + k * lda] * bv[k];
+  for (int k = m - 1; k >= 0; --k) {
+    bv[k] = bv[k] / a[k + k * lda];
+    for (int i = 0; i < k; ++i) bv[i] = bv[i] - a[i + k * lda] * bv[k];
+  }
+}
+
+// BiCGStab(l), IterativeMethods.src:559-834 (right preconditioned, convex polynomial part,
+// reliable residual / solution updates with delta = 1e-2; stop on the recursive residual)
+int bicgstabl(const Ctx &c, double *x_out, const double *b, int max_rounds, double tol, int l, int *iters,
+              double *resid) {
+  const int n = c.n;
+  const double delta = 1.0e-2;
+  std::vector<double> x(x_out, x_out + n), t(n, 0.0), rr(n), xp(n), bp(n);
+  std::vector<std::vector<double>> r(l + 1, std::vector<double>(n, 0.0)), u(l + 1, std::vector<double>(n, 0.0));
+  bool all_zero = true;
+  for (int i = 0; i < n; ++i)
+    if (x[i] != 0.0) all_zero = false;
+  if (all_zero) x.assign(b, b + n);
+  matvec(c, x.data(), r[0].data());
+  for (int i = 0; i < n; ++i) r[0][i] = b[i] - r[0][i];
+  const double bnrm = nrm2(n, b);
+  const double rnrm0 = nrm2(n, r[0].data());
+  double errorind = rnrm0 / bnrm;
+  *iters = 0;
+  *resid = errorind;
+  if (errorind < tol) return HUTI_CONVERGENCE;
+  rr = r[0];
+  bp = r[0];
+  xp = x;
+  double rnrm = rnrm0, mxnrmx = rnrm0, mxnrmr = rnrm0;
+  std::fill(x.begin(), x.end(), 0.0);
+  double alpha = 0.0, omega = 1.0, sigma = 1.0, rho0 = 1.0, rho1 = 0.0, beta = 0.0;
+  const int L1 = l + 1;
+  std::vector<double> Z(L1 * L1), ZZ(L1 * L1), y0(L1), yl(L1), y(L1);
+  std::vector<int> piv(std::max(1, l - 1));
+  auto symv = [&](const std::vector<double> &v, std::vector<double> &out) {
+    for (int i = 0; i < L1; ++i) {
+      double s = 0.0;
+      for (int j = 0; j < L1; ++j) s = s + Z[i + j * L1] * v[j];
+      out[i] = s;
+    }
+  };
+  auto small_dot = [&](const std::vector<double> &a, const std::vector<double> &bb) {
+    double s = 0.0;
+    for (int i = 0; i < L1; ++i) s = s + a[i] * bb[i];
+    return s;
+  };
+  int round = 0, info = HUTI_MAXITER;
+  bool early = false;
+  for (round = 1; round <= max_rounds; ++round) {
+    // --- the BiCG part
+    rho0 = -omega * rho0;
+    for (int k = 1; k <= l; ++k) {
+      rho1 = dot(n, rr.data(), r[k - 1].data());
+      if (rho0 == 0.0 || rho1 != rho1) { info = HUTI_DIVERGENCE; early = true; break; }
+      beta = alpha * (rho1 / rho0);
+      rho0 = rho1;
+      for (int j = 0; j <= k - 1; ++j)
+        for (int i = 0; i < n; ++i) u[j][i] = r[j][i] - beta * u[j][i];
+      pcond(c, t.data(), u[k - 1].data());
+      matvec(c, t.data(), u[k].data());
+      sigma = dot(n, rr.data(), u[k].data());
+      if (sigma == 0.0 || sigma != sigma) { info = HUTI_DIVERGENCE; early = true; break; }
+      alpha = rho1 / sigma;
+      for (int i = 0; i < n; ++i) x[i] = x[i] + alpha * u[0][i];
+      for (int j = 0; j <= k - 1; ++j)
+        for (int i = 0; i < n; ++i) r[j][i] = r[j][i] - alpha * u[j + 1][i];
+      pcond(c, t.data(), r[k - 1].data());
+      matvec(c, t.data(), r[k].data());
+      rnrm = nrm2(n, r[0].data());
+      mxnrmx = std::max(mxnrmx, rnrm);
+      mxnrmr = std::max(mxnrmr, rnrm);
+      errorind = rnrm / bnrm;
+      if (errorind < tol) { info = HUTI_CONVERGENCE; early = true; break; }
+      if (errorind != errorind) { info = HUTI_DIVERGENCE; early = true; break; }
+    }
+    if (early) break;
+    // --- the convex polynomial part
+    for (int i = 0; i < L1; ++i)
+      for (int j = 0; j <= i; ++j) Z[i + j * L1] = dot(n, r[i].data(), r[j].data());
+    for (int j = 1; j < L1; ++j)
+      for (int i = 0; i < j; ++i) Z[i + j * L1] = Z[j + i * L1];
+    ZZ = Z;
+    // the (l-1) x (l-1) block rows/cols 2..l of ZZ
+    std::vector<double> M((l - 1) * (l - 1));
+    for (int j = 0; j < l - 1; ++j)
+      for (int i = 0; i < l - 1; ++i) M[i + j * (l - 1)] = ZZ[(i + 1) + (j + 1) * L1];
+    if (l > 1) small_lu(l - 1, M.data(), l - 1, piv.data());
+    y0[0] = -1.0;
+    for (int i = 1; i < l; ++i) y0[i] = Z[i + 0 * L1];
+    if (l > 1) small_lu_solve(l - 1, M.data(), l - 1, piv.data(), &y0[1]);
+    y0[l] = 0.0;
+    yl[0] = 0.0;
+    for (int i = 1; i < l; ++i) yl[i] = Z[i + l * L1];
+    if (l > 1) small_lu_solve(l - 1, M.data(), l - 1, piv.data(), &yl[1]);
+    yl[l] = -1.0;
+    symv(y0, y);
+    const double kappa0 = std::sqrt(small_dot(y0, y));
+    symv(yl, y);
+    const double kappal = std::sqrt(small_dot(yl, y));
+    symv(y0, y);
+    const double varrho = small_dot(yl, y) / (kappa0 * kappal);
+    const double hatgamma = varrho / std::fabs(varrho) * std::max(std::fabs(varrho), 7e-1) * kappa0 / kappal;
+    for (int i = 0; i < L1; ++i) y0[i] = y0[i] - hatgamma * yl[i];
+    // --- update
+    omega = y0[l];
+    for (int j = 1; j <= l; ++j) {
+      for (int i = 0; i < n; ++i) u[0][i] = u[0][i] - y0[j] * u[j][i];
+      for (int i = 0; i < n; ++i) x[i] = x[i] + y0[j] * r[j - 1][i];
+      for (int i = 0; i < n; ++i) r[0][i] = r[0][i] - y0[j] * r[j][i];
+    }
+    symv(y0, y);
+    rnrm = std::sqrt(small_dot(y0, y));
+    // --- the reliable update part
+    mxnrmx = std::max(mxnrmx, rnrm);
+    mxnrmr = std::max(mxnrmr, rnrm);
+    const bool xpdt = rnrm < delta * rnrm0 && rnrm0 < mxnrmx;
+    const bool rcmp = (rnrm < delta * mxnrmr && rnrm0 < mxnrmr) || xpdt;
+    if (rcmp) {
+      pcond(c, t.data(), x.data());
+      matvec(c, t.data(), r[0].data());
+      for (int i = 0; i < n; ++i) r[0][i] = bp[i] - r[0][i];
+      mxnrmr = rnrm;
+      if (xpdt) {
+        for (int i = 0; i < n; ++i) xp[i] = xp[i] + t[i];
+        std::fill(x.begin(), x.end(), 0.0);
+        bp = r[0];
+        mxnrmx = rnrm;
+      }
+    }
+    errorind = rnrm / bnrm;
+    if (errorind < tol) { info = HUTI_CONVERGENCE; break; }
+    if (errorind != errorind) { info = HUTI_DIVERGENCE; break; }
+  }
+  *iters = std::min(round, max_rounds);
+  *resid = errorind;
+  // x = M^-1 x + xp
+  t = x;
+  pcond(c, x.data(), t.data());
+  for (int i = 0; i < n; ++i) x_out[i] = x[i] + xp[i];
+  return info;
+}
+
 }  // namespace
 
 // SolveLinearSystem (SolverUtils.src:7151-7525) for Linear System Solver = Iterative:
@@ -1211,6 +1431,12 @@ extern "C" int orc_solve(int n, const int *rows, const int *cols, const int *dia
         prm->omp_threads, irows, icols, idiag};
   if (prm->method == ORC_CG)
     r.info = huti_cg(c, x, b.data(), prm->max_iter, prm->tol, &r.iters, &r.residual);
+  else if (prm->method == ORC_GCR)  // restart: Linear System GCR Restart, else Max Iterations
+    r.info = gcr(c, x, b.data(), prm->max_iter, prm->tol, prm->restart > 0 ? prm->restart : prm->max_iter,
+                 &r.iters, &r.residual);
+  else if (prm->method == ORC_BICGSTABL)  // BiCGstabl polynomial degree, default 2
+    r.info = bicgstabl(c, x, b.data(), prm->max_iter, prm->tol, prm->restart >= 2 ? prm->restart : 2, &r.iters,
+                       &r.residual);
   else
     r.info = huti_bicgstab(c, x, b.data(), prm->max_iter, prm->tol, &r.iters, &r.residual);
   if (prm->scale_system) backscale(n, rows, cols, values.data(), b.data(), x, D.data(), rs);

@@ -45,7 +45,7 @@ void orc_dirichlet(int n, const int *rows, const int *cols, const int *diag, dou
                    int symmetric, int scale);
 
 /* ---- linear solve (SolveLinearSystem -> IterSolver -> HUTI) */
-enum { ORC_CG = 1, ORC_BICGSTAB = 2 };
+enum { ORC_CG = 1, ORC_BICGSTAB = 2, ORC_GCR = 3, ORC_BICGSTABL = 4 };
 enum { ORC_PREC_NONE = 0, ORC_PREC_DIAGONAL = 1, ORC_PREC_ILU0 = 2 };
 typedef struct {
   int method;          /* ORC_CG | ORC_BICGSTAB */
@@ -55,6 +55,7 @@ typedef struct {
   int scale_system;    /* Linear System Scaling (default 1) */
   int omp_threads;     /* threads for the SpMV loop (CRSMatrix.src:3565), <=0: all */
   int ilu_order;       /* ORC_PREC_ILU0 with ilu_order n > 0: ILU(n) (Linear System ILU Order) */
+  int restart;         /* GCR: Linear System GCR Restart (0: Max Iterations); BiCGStab(l): degree l */
 } orc_params;
 typedef struct {
   int info;            /* HUTI status code (huti_fdefs.h) */

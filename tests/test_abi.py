@@ -61,6 +61,20 @@ def test_sif_keywords():
     assert (q.method, q.precond, q.symmetric, q.precision) == (eg.CG, eg.PREC_DIAGONAL, True, eg.MIXED)
 
 
+def test_sif_gcr_bicgstabl():
+    base = {"Linear System Max Iterations": 100, "Linear System Convergence Tolerance": 1e-8}
+    p = eg.SolverParams.from_sif(dict(base, **{"Linear System Iterative Method": "GCR",
+                                               "Linear System GCR Restart": 20}))
+    assert (p.method, p.restart) == (eg.GCR, 20)
+    q = eg.SolverParams.from_sif(dict(base, **{"Linear System Iterative Method": "BiCGStabl",
+                                               "BiCGstabl polynomial degree": 4}))
+    assert (q.method, q.restart) == (eg.BICGSTABL, 4)
+    assert eg.SolverParams.from_sif(dict(base, **{"Linear System Iterative Method": "BiCGStabl"})).restart == 0
+    with pytest.raises(ValueError):
+        eg.SolverParams.from_sif(dict(base, **{"Linear System Iterative Method": "BiCGStabl",
+                                               "BiCGstabl polynomial degree": 1}))
+
+
 def test_sif_ilu_order():
     base = {"Linear System Max Iterations": 10, "Linear System Convergence Tolerance": 1e-6}
     assert eg.SolverParams.from_sif(dict(base, **{"Linear System Preconditioning": "ILU2"})).ilu_order == 2
