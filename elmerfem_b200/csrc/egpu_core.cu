@@ -762,6 +762,8 @@ static void set_sell(KArgs<VT> &a, const egpu_mat *A, const VT *vals, bool offs)
   a.sell_w = A->sell_w.p;
   a.scols = A->sell_cols.p;
   a.scols16 = offs ? A->sell_c16.p : nullptr;
+  a.sell_cptr = offs ? A->sell_cptr.p : nullptr;
+  a.scolsc = offs ? A->sell_csc.p : nullptr;
   a.svals = vals;
 }
 
@@ -1518,12 +1520,46 @@ extern "C" int egpu_matrix_bind(egpu_ctx *ctx, int n, const int *rows, const int
           if (c16) s16[e] = (int16_t)(k < len ? c - r : 0);
         }
       }
+    // Compact column offsets for the FP32 inner solver: a slice whose 32 rows all exist and
+    // have the same offsets (col - row) in the same order (interior rows of structured
+    // meshes) stores them once (w entries, marked by a negative start); other slices keep
+    // one offset per entry.  The values layout is unchanged.
+    std::vector<int> cptr;
+    std::vector<int16_t> csc;
+    if (c16) {
+      cptr.resize(ns);
+      csc.reserve(total / 4 + 64);
+      for (int sl = 0; sl < ns; ++sl) {
+        const int w = sw[sl];
+        bool shared = sl * 32 + 31 < n && w > 0;
+        for (int t = 1; shared && t < 32; ++t) {
+          const int r = sl * 32 + t;
+          if (rows[r + 1] - rows[r] != w) shared = false;
+          for (int k = 0; shared && k < w; ++k)
+            if (s16[sp[sl] + 32LL * k + t] != s16[sp[sl] + 32LL * k]) shared = false;
+        }
+        if (rows[sl * 32 + 1 < n ? sl * 32 + 1 : sl * 32] - rows[sl * 32] != w) shared = false;
+        const int start = (int)csc.size();
+        if (shared) {
+          for (int k = 0; k < w; ++k) csc.push_back(s16[sp[sl] + 32LL * k]);
+          cptr[sl] = -start - 1;
+        } else {
+          for (long long q = 0; q < 32LL * w; ++q) csc.push_back(s16[sp[sl] + q]);
+          cptr[sl] = start;
+        }
+      }
+    }
     A->nslices = ns;
     A->sell_nnz = total;
     A->ldw = ((long long)n + 32 + 63) / 64 * 64;
     if ((e = A->sell_ptr.alloc(ns)) || (e = A->sell_w.alloc(ns)) || (e = A->sell_cols.alloc(total)) ||
-        (c16 && (e = A->sell_c16.alloc(total))))
+        (c16 && (e = A->sell_c16.alloc(total))) || (c16 && (e = A->sell_cptr.alloc(ns))) ||
+        (c16 && (e = A->sell_csc.alloc(std::max<size_t>(1, csc.size())))))
       return fail(e);
+    if (c16) {
+      cudaMemcpy(A->sell_cptr.p, cptr.data(), ns * sizeof(int), cudaMemcpyHostToDevice);
+      cudaMemcpy(A->sell_csc.p, csc.data(), csc.size() * sizeof(int16_t), cudaMemcpyHostToDevice);
+    }
     cudaMemcpy(A->sell_ptr.p, sp.data(), ns * sizeof(int), cudaMemcpyHostToDevice);
     cudaMemcpy(A->sell_w.p, sw.data(), ns * sizeof(int), cudaMemcpyHostToDevice);
     cudaMemcpy(A->sell_cols.p, sc.data(), total * sizeof(int), cudaMemcpyHostToDevice);
@@ -1597,6 +1633,8 @@ extern "C" int egpu_matrix_clone(egpu_mat *proto, egpu_mat **out) {
   A->sell_w.view(proto->sell_w);
   A->sell_cols.view(proto->sell_cols);
   A->sell_c16.view(proto->sell_c16);
+  A->sell_cptr.view(proto->sell_cptr);
+  A->sell_csc.view(proto->sell_csc);
   if (proto->cols16.p) A->cols16.view(proto->cols16);
   if (proto->ilu_order >= 0) view_ilu(A, proto);
   if (proto->tri_built) view_tri(A, proto);

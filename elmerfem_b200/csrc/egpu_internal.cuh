@@ -176,6 +176,10 @@ struct egpu_mat {
   long long ldw = 0;             // stride of the work vectors (>= n + 32, multiple of 64)
   DevBuf<int> sell_ptr, sell_w, sell_cols;
   DevBuf<int16_t> sell_c16;      // col - row, when every |col - row| < 32768
+  // the same offsets compacted: slice s starts at sell_cptr[s] (per entry) or, for a slice
+  // whose rows share one offset list, at -sell_cptr[s] - 1 (w entries)
+  DevBuf<int> sell_cptr;
+  DevBuf<int16_t> sell_csc;
   DevBuf<double> sell_vals;      // scaled values (FP64)
   DevBuf<float> sell_vals32;     // scaled values (FP32)
   // ILU structure: the matrix's own pattern for ILU0, the ILU(n) fill structure otherwise
@@ -344,6 +348,11 @@ __device__ __forceinline__ void cp_async_small(void *smem, const void *gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(s), "l"(gmem), "n"(B) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// bulk prefetch of a contiguous global range into L2 (no completion to wait for); the
+// address must be 16-byte aligned and the size a multiple of 16 bytes
+__device__ __forceinline__ void prefetch_l2_bulk(const void *gmem, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(gmem), "r"(bytes) : "memory");
+}
 // wait until at most n (0..7) of this thread's most recent groups are still pending
 __device__ __forceinline__ void cp_async_wait(int n) {
   switch (n) {

@@ -63,6 +63,8 @@ struct KArgs {
   const int *sell_ptr, *sell_w, *scols;
   const int16_t *scols16;
   const VT *svals;
+  const int *sell_cptr;           // compact offsets (OFFS path): see egpu_mat::sell_cptr
+  const int16_t *scolsc;
   // level-synchronous triangular solves run by block 0 out of shared memory (tri_cta != 0):
   // levels staged cta_pd ahead, ring of cta_rs slots, staging windows of cta_sb entries and
   // cta_sr rows
@@ -171,19 +173,57 @@ __device__ __forceinline__ void spmv_phase(const KArgs<VT> &a, const VT *x0, con
   const int lane = threadIdx.x & 31;
   const int gw = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int nw = (int)(((long long)gridDim.x * blockDim.x) >> 5);
+  // the values of the slice this warp takes next are prefetched into L2 (one bulk request)
+  // while the current one is summed; the next slice's position is loaded a slice ahead so
+  // the request never waits for it
+  int nw_w = 0, nw_p = 0;
+  if (gw < a.nslices) {
+    nw_w = __ldg(a.sell_w + gw);
+    nw_p = __ldg(a.sell_ptr + gw);
+  }
   for (int s = gw; s < a.nslices; s += nw) {
     const int r = (s << 5) + lane;
-    const int w = __ldg(a.sell_w + s);
-    const int base = __ldg(a.sell_ptr + s) + lane;
-    VT s0 = 0, s1 = 0;
-#pragma unroll 8
-    for (int k = 0; k < w; ++k) {
-      const int e = base + (k << 5);
-      const VT v = ld_stream(a.svals + e);
-      const int c = OFFS ? r + (int)ld_stream(a.scols16 + e) : ld_stream(a.scols + e);
-      s0 = row_madd(s0, v, ld_l2(x0 + c));
-      if (TWO) s1 = row_madd(s1, v, ld_l2(x1 + c));
+    const int w = nw_w;
+    const int base = nw_p + lane;
+    const int s2 = s + nw;
+    if (s2 < a.nslices) {
+      nw_w = __ldg(a.sell_w + s2);
+      nw_p = __ldg(a.sell_ptr + s2);
     }
+    VT s0 = 0, s1 = 0;
+    if (OFFS && a.scolsc) {
+      const int cp = __ldg(a.sell_cptr + s);
+      if (cp < 0) {  // one offset list for the whole slice: a broadcast load per entry
+        const int16_t *co = a.scolsc + (-cp - 1);
+#pragma unroll 8
+        for (int k = 0; k < w; ++k) {
+          const VT v = ld_stream(a.svals + base + (k << 5));
+          const int c = r + (int)__ldg(co + k);
+          s0 = row_madd(s0, v, ld_l2(x0 + c));
+          if (TWO) s1 = row_madd(s1, v, ld_l2(x1 + c));
+        }
+      } else {
+        const int16_t *co = a.scolsc + cp + lane;
+#pragma unroll 8
+        for (int k = 0; k < w; ++k) {
+          const VT v = ld_stream(a.svals + base + (k << 5));
+          const int c = r + (int)ld_stream(co + (k << 5));
+          s0 = row_madd(s0, v, ld_l2(x0 + c));
+          if (TWO) s1 = row_madd(s1, v, ld_l2(x1 + c));
+        }
+      }
+    } else {
+#pragma unroll 8
+      for (int k = 0; k < w; ++k) {
+        const int e = base + (k << 5);
+        const VT v = ld_stream(a.svals + e);
+        const int c = OFFS ? r + (int)ld_stream(a.scols16 + e) : ld_stream(a.scols + e);
+        s0 = row_madd(s0, v, ld_l2(x0 + c));
+        if (TWO) s1 = row_madd(s1, v, ld_l2(x1 + c));
+      }
+    }
+    if (lane == 0 && s2 < a.nslices && nw_w > 0)
+      prefetch_l2_bulk(a.svals + nw_p, (unsigned)(32 * nw_w * (int)sizeof(VT)));
     if (r < a.n) epi(r, s0, s1);
   }
 }
