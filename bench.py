@@ -103,20 +103,20 @@ def algorithmic_bytes_per_iter(method, precond, precision, n, nnz, cols16, off_f
     CG+Diagonal, FP32 inner (refinement): SpMV 4z values + 2z·off_frac offsets (int16 column
     offsets, stored once per slice where all rows share them) or 4z cols + 4n rowptr + P gather
     4n + Q write 4n + epilogue P 4n; P update 12n; x/r/z update 32n.
-    CG+Diagonal, FP64 drop-in (x_k residual fused in the next SpMV): SpMV 8z + 4z + 4n + 16n gathers
-    + 8n write + 16n epilogue; P update 24n; update 64n.
+    CG+Diagonal, FP64 drop-in (x_k residual fused in the next SpMV): SpMV 8z + the same offsets
+    + 4n + 16n gathers + 8n write + 16n epilogue; P update 24n; update 64n.
     """
     cbytes = (2 * off_frac if cols16 else 4) * nnz
     if method == 1 and precond in (0, 1):
         if precision == "mixed":
             return 4 * nnz + cbytes + 60 * n
-        return 12 * nnz + 132 * n
+        return 8 * nnz + cbytes + 132 * n
     # BiCGStab: two SpMV passes (+x fused in FP64) and two preconditioner applications
     if precision == "mixed":
         m = 4 * nnz + cbytes
         tri = (8 * nnz + 16 * n) if precond == 2 else 0
         return 2 * m + tri + 120 * n
-    m = 12 * nnz
+    m = 8 * nnz + cbytes
     tri = (12 * nnz + 32 * n) if precond == 2 else 0
     return 2 * m + tri + 260 * n
 
@@ -390,7 +390,7 @@ def run_gpu(args, rank, world, local, pg):
         torch.cuda.synchronize()
         t64.append(e0.elapsed_time(e1) / 1000.0)
     fp64_rate = 1.0 / statistics.median(t64)
-    bpi64 = algorithmic_bytes_per_iter(solve_kw["method"], solve_kw["precond"], "fp64", n, nnz, cols16)
+    bpi64 = algorithmic_bytes_per_iter(solve_kw["method"], solve_kw["precond"], "fp64", n, nnz, cols16, off_frac)
     ach64 = bpi64 * rr["iters"] / rr["seconds_krylov"] / 1e9
 
     # ---- end to end through the public C ABI with host buffers (pinned)

@@ -879,7 +879,7 @@ int solve_fp64(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_param
   a.diag = A->diag.p;
   a.cols16 = nullptr;
   a.vals = A->scaled.p;
-  set_sell(a, A, A->sell_vals.p, false);
+  set_sell(a, A, A->sell_vals.p, A->sell_c16.p != nullptr);
   a.ilu = A->ilu.p;
   a.dvals = dvals;
   set_tri(a, A);
@@ -907,7 +907,7 @@ int solve_fp64(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_param
     a.true_residual = 0;  // the internal methods stop on the recursive residual
   }
   EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ek0, ctx->stream));
-  rc = run_krylov<double>(A, a, prm->method, false);
+  rc = run_krylov<double>(A, a, prm->method, A->sell_c16.p != nullptr);
   if (rc) return rc;
   EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ek1, ctx->stream));
   k_backscale_x<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, xs, A->dscale.p, x_dev, flags, sc ? 1 : 0);
@@ -1036,7 +1036,7 @@ int krylov_fp64_scaled(egpu_mat *A, const double *bs, double *xs, const egpu_par
   a.cols = A->cols.p;
   a.diag = A->diag.p;
   a.vals = A->scaled.p;
-  set_sell(a, A, A->sell_vals.p, false);
+  set_sell(a, A, A->sell_vals.p, A->sell_c16.p != nullptr);
   a.ilu = A->ilu.p;
   a.dvals = A->work.p + (size_t)11 * A->ldw;
   set_tri(a, A);
@@ -1054,7 +1054,7 @@ int krylov_fp64_scaled(egpu_mat *A, const double *bs, double *xs, const egpu_par
   a.out_i = (int *)(ctx->sync.p + 8);
   a.out_d = (double *)(ctx->sync.p + 16);
   a.skip = nullptr;
-  int rc = run_krylov<double>(A, a, prm->method, false);
+  int rc = run_krylov<double>(A, a, prm->method, A->sell_c16.p != nullptr);
   if (rc) return rc;
   unsigned int h[64];
   EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(h, ctx->sync.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
