@@ -89,6 +89,7 @@ PROTOTYPES = {
     "egpu_matrix_prepare": (C.c_int, [_vp, C.POINTER(Params)]),
     "egpu_ilu_pattern": (C.c_longlong, [C.c_int, _i32p, _i32p, _i32p, C.c_int, C.c_longlong, _vp, _vp, _vp]),
     "egpu_ilu_download": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "egpu_tri_info": (C.c_int, [_vp, _vp]),
     "egpu_iter_solve": (C.c_int, [_vp, _f64p, _f64p, C.POINTER(Params), C.POINTER(Result)]),
     "egpu_iter_solve_dev": (C.c_int, [_vp, _vp, _vp, C.POINTER(Params), C.POINTER(Result)]),
     "egpu_mv": (C.c_int, [_vp, _f64p, _f64p]),

@@ -150,10 +150,48 @@ __global__ void k_backscale_x(int n, const double *__restrict__ xs, const double
     x[i] = zero ? 0.0 : (scale_system ? xs[i] * D[i] : xs[i]);
 }
 
-// CRS_IncompleteLU(A,0), CRSMatrix.src:2312-2356, one warp per row in ascending
-// dependency level.  Row i waits (bounded) for every row k of its strictly lower part;
-// the IKJ update keeps the reference's order of operations per entry, so the factor is
-// bit-identical to the sequential routine.  The U diagonal stays un-inverted here.
+// CRS_IncompleteLU(A,0), CRSMatrix.src:2312-2356, one warp per row in a dependency order
+// (every row after the rows of its strictly lower part).  The warp first waits (bounded,
+// all lanes polling together) until every row k of its strictly lower part is done, then
+// runs the IKJ loop over those k in ascending column order: S_m /= u_kk, then
+// S_j -= S_m * U_kj for the U entries of row k that fall in the row's pattern (found by
+// binary search in the row's columns).  Row k+1's U entries and u_kk are loaded while row
+// k's update runs.  Every entry of the row sees its updates in the reference's order, so
+// the factor is bit-identical to the sequential routine.  The U diagonal stays un-inverted.
+struct IluDep {
+  int dk, kend;
+  int c0, c1;
+  double v0, v1, ukk;
+};
+
+__device__ __forceinline__ void ilu_dep_fetch(IluDep &d, int k, const int *__restrict__ rows,
+                                              const int *__restrict__ cols, const int *__restrict__ diag,
+                                              const double *ilu, int lane) {
+  d.dk = __ldg(diag + k);
+  d.kend = __ldg(rows + k + 1);
+  const int l0 = d.dk + 1 + lane, l1 = l0 + 32;
+  d.c0 = l0 < d.kend ? __ldg(cols + l0) : -1;
+  d.c1 = l1 < d.kend ? __ldg(cols + l1) : -1;
+  d.v0 = l0 < d.kend ? __ldcg(ilu + l0) : 0.0;
+  d.v1 = l1 < d.kend ? __ldcg(ilu + l1) : 0.0;
+  d.ukk = __ldcg(ilu + d.dk);
+}
+
+// position of column j among the row's sorted columns Cc[0..len), -1 if absent
+__device__ __forceinline__ int ilu_find(const int *Cc, int len, int j) {
+  int lo = 0, hi = len - 1;
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1;
+    const int cm = Cc[mid];
+    if (cm == j) return mid;
+    if (cm < j)
+      lo = mid + 1;
+    else
+      hi = mid - 1;
+  }
+  return -1;
+}
+
 template <int MAXROW>
 __global__ void __launch_bounds__(256) k_ilu0_factor(int n, const int *__restrict__ rows,
                                                      const int *__restrict__ cols,
@@ -170,53 +208,63 @@ __global__ void __launch_bounds__(256) k_ilu0_factor(int n, const int *__restric
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int s = gw; s < n; s += nw) {
     const int i = order[s];
+    if (i < 0 || i >= n) {
+      if (lane == 0) atomicExch(err, (int)EGPU_ERR_ARG);
+      return;
+    }
     const int beg = rows[i], len = rows[i + 1] - beg, nl = diag[i] - beg;
+    if (len > MAXROW || nl < 0 || nl > len) {
+      if (lane == 0) atomicExch(err, (int)EGPU_ERR_ARG);
+      return;
+    }
     for (int t = lane; t < len; t += 32) {
       S[t] = A[beg + t];
       Cc[t] = cols[beg + t];
     }
     __syncwarp();
-    for (int m = 0; m < nl; ++m) {
-      const int k = Cc[m];
-      if (lane == 0) {
-        if (ld_acquire_s32(done + k) == 0) {
-          unsigned long long t0 = egpu_globaltimer();
-          while (ld_acquire_s32(done + k) == 0) {
-            if (egpu_globaltimer() - t0 > EGPU_WAIT_NS) {
-              atomicExch(err, (int)EGPU_ERR_TIMEOUT);
-              break;
+    // every row of the strictly lower part done (acquire), all lanes polling together
+    {
+      bool pend = false;
+      for (int m = lane; m < nl; m += 32) pend |= ld_acquire_s32(done + Cc[m]) == 0;
+      if (__any_sync(0xffffffffu, pend)) {
+        const unsigned long long t0 = egpu_globaltimer();
+        for (unsigned int spin = 1;; ++spin) {
+          pend = false;
+          for (int m = lane; m < nl; m += 32) pend |= ld_acquire_s32(done + Cc[m]) == 0;
+          if (!__any_sync(0xffffffffu, pend)) break;
+          if ((spin & 31u) == 0) {
+            int stop = 0;
+            if (lane == 0) stop = egpu_globaltimer() - t0 > EGPU_WAIT_NS ? 1 : (*(volatile int *)err ? 2 : 0);
+            stop = __shfl_sync(0xffffffffu, stop, 0);
+            if (stop) {
+              if (stop == 1 && lane == 0) atomicExch(err, (int)EGPU_ERR_TIMEOUT);
+              return;
             }
-            if (*(volatile int *)err) break;
           }
         }
       }
-      __syncwarp();
-      int e = 0;
-      if (lane == 0) e = *(volatile int *)err;
-      if (__shfl_sync(0xffffffffu, e, 0)) return;
+    }
+    __syncwarp();
+    IluDep nxt;
+    if (nl > 0) ilu_dep_fetch(nxt, Cc[0], rows, cols, diag, ilu, lane);
+    for (int m = 0; m < nl; ++m) {
+      const IluDep cur = nxt;
+      if (m + 1 < nl) ilu_dep_fetch(nxt, Cc[m + 1], rows, cols, diag, ilu, lane);
       double sk = S[m];
       if (sk == 0.0) continue;
-      const int dk = diag[k];
-      const double ukk = __ldcg(ilu + dk);
-      if (fabs(ukk) > EGPU_AEPS) sk = sk / ukk;
+      if (fabs(cur.ukk) > EGPU_AEPS) sk = sk / cur.ukk;
       __syncwarp();
       if (lane == 0) S[m] = sk;
-      const int kend = rows[k + 1];
-      for (int l = dk + 1 + lane; l < kend; l += 32) {
-        const int j = cols[l];
-        int lo = 0, hi = len - 1, pos = -1;
-        while (lo <= hi) {
-          const int mid = (lo + hi) >> 1;
-          const int cm = Cc[mid];
-          if (cm == j) {
-            pos = mid;
-            break;
-          }
-          if (cm < j)
-            lo = mid + 1;
-          else
-            hi = mid - 1;
-        }
+      if (cur.c0 >= 0) {
+        const int pos = ilu_find(Cc, len, cur.c0);
+        if (pos >= 0) S[pos] = __dsub_rn(S[pos], __dmul_rn(sk, cur.v0));
+      }
+      if (cur.c1 >= 0) {
+        const int pos = ilu_find(Cc, len, cur.c1);
+        if (pos >= 0) S[pos] = __dsub_rn(S[pos], __dmul_rn(sk, cur.v1));
+      }
+      for (int l = cur.dk + 65 + lane; l < cur.kend; l += 32) {
+        const int pos = ilu_find(Cc, len, cols[l]);
         if (pos >= 0) S[pos] = __dsub_rn(S[pos], __dmul_rn(sk, __ldcg(ilu + l)));
       }
       __syncwarp();
@@ -343,6 +391,80 @@ static void build_levels(int n, const std::vector<int> &rows, const std::vector<
   for (int l = 0; l < nup; ++l) maxw = std::max(maxw, cnt[l + 1] - cnt[l]);
   upper.assign(n, 0);
   for (int i = n - 1; i >= 0; --i) upper[cnt[lev[i]]++] = i;
+}
+
+// Node blocks: the largest bs <= TRI_BS_MAX dividing n such that every aligned group of bs
+// rows shares one sorted column set that holds the group's own bs columns (the DOF blocks
+// CRS_CreateMatrix lays out per node pair, CRSMatrix.src:816-875).  1 if there is none.
+static int node_block_size(int n, const std::vector<int> &rows, const std::vector<int> &cols,
+                           const std::vector<int> &diag) {
+  for (int bs = TRI_BS_MAX; bs >= 2; --bs) {
+    if (n % bs) continue;
+    bool ok = true;
+    for (int r0 = 0; r0 < n && ok; r0 += bs) {
+      const int len = rows[r0 + 1] - rows[r0];
+      const int d = diag[r0];
+      if (d < 0 || d + bs > rows[r0 + 1]) {
+        ok = false;
+        break;
+      }
+      for (int t = 0; t < bs && ok; ++t) ok = cols[d + t] == r0 + t;
+      for (int k = 1; k < bs && ok; ++k) {
+        const int i = r0 + k;
+        if (rows[i + 1] - rows[i] != len) {
+          ok = false;
+          break;
+        }
+        for (int j = 0; j < len && ok; ++j) ok = cols[rows[i] + j] == cols[rows[r0] + j];
+      }
+    }
+    if (ok) return bs;
+  }
+  return 1;
+}
+
+// Dependency levels of the node blocks and the block-expanded solve orders (lower: blocks
+// by level, rows ascending inside; upper: rows descending inside).  maxw counts rows.
+static void build_block_levels(int n, int bs, const std::vector<int> &rows, const std::vector<int> &cols,
+                               const std::vector<int> &diag, std::vector<int> &lower, std::vector<int> &upper,
+                               int &nlow, int &nup, int &maxw) {
+  const int nb = n / bs;
+  std::vector<int> lev(nb, 0);
+  nlow = nup = maxw = 0;
+  for (int m = 0; m < nb; ++m) {
+    int l = 0;
+    for (int i = m * bs; i < (m + 1) * bs; ++i)
+      for (int j = rows[i]; j < diag[i]; ++j)
+        if (cols[j] < m * bs) l = std::max(l, lev[cols[j] / bs] + 1);
+    lev[m] = l;
+    nlow = std::max(nlow, l + 1);
+  }
+  std::vector<int> cnt(nlow + 1, 0);
+  for (int m = 0; m < nb; ++m) cnt[lev[m] + 1]++;
+  for (int l = 0; l < nlow; ++l) cnt[l + 1] += cnt[l];
+  for (int l = 0; l < nlow; ++l) maxw = std::max(maxw, bs * (cnt[l + 1] - cnt[l]));
+  lower.assign(n, 0);
+  for (int m = 0; m < nb; ++m) {
+    const int q = cnt[lev[m]]++;
+    for (int k = 0; k < bs; ++k) lower[q * bs + k] = m * bs + k;
+  }
+  for (int m = nb - 1; m >= 0; --m) {
+    int l = 0;
+    for (int i = m * bs; i < (m + 1) * bs; ++i)
+      for (int j = diag[i] + 1; j < rows[i + 1]; ++j)
+        if (cols[j] >= (m + 1) * bs) l = std::max(l, lev[cols[j] / bs] + 1);
+    lev[m] = l;  // blocks after m already hold upper levels
+    nup = std::max(nup, l + 1);
+  }
+  cnt.assign(nup + 1, 0);
+  for (int m = 0; m < nb; ++m) cnt[lev[m] + 1]++;
+  for (int l = 0; l < nup; ++l) cnt[l + 1] += cnt[l];
+  for (int l = 0; l < nup; ++l) maxw = std::max(maxw, bs * (cnt[l + 1] - cnt[l]));
+  upper.assign(n, 0);
+  for (int m = nb - 1; m >= 0; --m) {
+    const int q = cnt[lev[m]]++;
+    for (int k = 0; k < bs; ++k) upper[q * bs + k] = m * bs + bs - 1 - k;
+  }
 }
 
 // occupancy-sized cooperative launch
@@ -526,6 +648,7 @@ static void view_tri(egpu_mat *A, const egpu_mat *proto) {
   A->tri.max_lower = proto->tri.max_lower;
   A->tri.max_upper = proto->tri.max_upper;
   A->tri.max_width = proto->tri.max_width;
+  A->tri.bs = proto->tri.bs;
   {
     const TriSchedule &P = proto->tri;
     TriSchedule &T = A->tri;
@@ -581,6 +704,23 @@ int ensure_tri_schedule(egpu_mat *A) {
   std::vector<int> lo, up;
   build_levels(n, rows, cols, diag, lo, up, A->tri.lower_levels, A->tri.upper_levels, A->tri.max_lower,
                A->tri.max_upper, A->tri.max_width);
+  A->tri.bs = 1;
+  {
+    const int bs = node_block_size(n, rows, cols, diag);
+    if (bs > 1) {
+      std::vector<int> blo, bup;
+      int bl = 0, bu = 0, bw = 0;
+      build_block_levels(n, bs, rows, cols, diag, blo, bup, bl, bu, bw);
+      if (tri_prefer_node_blocks(A->tri.lower_levels, A->tri.upper_levels, bl, bu, n)) {
+        lo.swap(blo);
+        up.swap(bup);
+        A->tri.bs = bs;
+        A->tri.lower_levels = bl;
+        A->tri.upper_levels = bu;
+        A->tri.max_width = bw;
+      }
+    }
+  }
   EGPU_CUDA_TRY(ctx, A->tri.lower_order.alloc(n));
   EGPU_CUDA_TRY(ctx, A->tri.upper_order.alloc(n));
   EGPU_CUDA_TRY(ctx, cudaMemcpy(A->tri.lower_order.p, lo.data(), n * sizeof(int), cudaMemcpyHostToDevice));
@@ -631,8 +771,13 @@ int ensure_tri_schedule(egpu_mat *A) {
     EGPU_CUDA_TRY(ctx, cudaMemcpy(T.lo_src.p, ls.data(), ls.size() * sizeof(int), cudaMemcpyHostToDevice));
     EGPU_CUDA_TRY(ctx, cudaMemcpy(T.up_cols.p, uc.data(), uc.size() * sizeof(int), cudaMemcpyHostToDevice));
     EGPU_CUDA_TRY(ctx, cudaMemcpy(T.up_src.p, us.data(), us.size() * sizeof(int), cudaMemcpyHostToDevice));
-    const int rc = build_cta_schedule(A, rows, cols, diag, lo, up, lp, lc, upp, uc);
-    if (rc) return rc;
+    // the single-block schedule needs rows sorted by row level: not with node blocks
+    if (A->tri.bs == 1) {
+      const int rc = build_cta_schedule(A, rows, cols, diag, lo, up, lp, lc, upp, uc);
+      if (rc) return rc;
+    } else {
+      T.cta_ok[0] = T.cta_ok[1] = false;
+    }
   }
   A->tri_built = true;
   return EGPU_OK;
@@ -732,6 +877,7 @@ static void set_tri(KArgs<VT> &a, const egpu_mat *A) {
   a.lo_cols = A->tri.lo_cols.p;
   a.up_ptr = A->tri.up_ptr.p;
   a.up_cols = A->tri.up_cols.p;
+  a.tri_bs = A->tri.bs;
   // level-synchronous single-block solves when the cost estimate prefers them
   const TriSchedule &T = A->tri;
   const int v = sizeof(VT) == 8 ? 0 : 1;
@@ -771,7 +917,8 @@ static void set_sell(KArgs<VT> &a, const egpu_mat *A, const VT *vals, bool offs)
 // at least one per block
 static int tri_per_block(const egpu_mat *A, int lpr, int grid, int block = EGPU_KBLOCK) {
   const int per_block_max = block / lpr;
-  const int want = std::max(1, 2 * A->tri.max_width);
+  // a warp per row slot, or per node block
+  const int want = std::max(1, 2 * A->tri.max_width / std::max(1, A->tri.bs));
   return std::max(1, std::min(per_block_max, (want + grid - 1) / grid));
 }
 
@@ -1842,6 +1989,19 @@ extern "C" int egpu_ilu_download(egpu_mat *A, int *ilu_rows, int *ilu_cols, int 
   if (ilu_values)
     EGPU_CUDA_TRY(ctx, cudaMemcpy(ilu_values, A->ilu.p, nz * sizeof(double), cudaMemcpyDeviceToHost));
   return (int)nz;
+}
+
+extern "C" int egpu_tri_info(egpu_mat *A, int info[6]) {
+  if (!A || !info) return EGPU_ERR_ARG;
+  if (!A->tri_built) return EGPU_ERR_STATE;
+  const TriSchedule &T = A->tri;
+  info[0] = T.bs;
+  info[1] = T.lower_levels;
+  info[2] = T.upper_levels;
+  info[3] = T.max_width;
+  info[4] = T.cta_ok[0] ? 1 : 0;
+  info[5] = T.cta_ok[1] ? 1 : 0;
+  return EGPU_OK;
 }
 
 extern "C" int egpu_ilu0_download(egpu_mat *A, double *ilu_values, double *diag_scaling) {

@@ -128,6 +128,11 @@ struct TriSchedule {
   int lower_levels = 0, upper_levels = 0;
   int max_lower = 0, max_upper = 0;  // longest strictly-lower / strictly-upper row part
   int max_width = 0;                 // most rows in one level (lower or upper)
+  // rows per sync-free slot group: bs > 1 when the matrix is made of dense diagonal blocks
+  // of bs consecutive rows (node DOFs) and the node-block solve was chosen; the orders then
+  // hold whole blocks (slots s*bs .. s*bs+bs-1: lower ascending, upper descending rows) and
+  // the levels count blocks
+  int bs = 1;
   // level-synchronous single-block schedule; cta_ok[v] for FP64 (v = 0) / FP32 (v = 1)
   CtaTriHost cta_lo, cta_up;
   DevBuf<int> pos_lo, pos_up;        // solve slot of every row in the lower / upper order
@@ -278,6 +283,10 @@ struct Sentinel<double> {
     }
     return __longlong_as_double((long long)v);
   }
+  // one relaxed load, no wait (the sentinel if not produced yet)
+  __device__ __forceinline__ static double peek(const double *p) {
+    return __longlong_as_double((long long)ld_relaxed_u64(p));
+  }
   __device__ __forceinline__ static void publish(double *p, double v) {
     st_relaxed_u64(p, (unsigned long long)__double_as_longlong(v));
   }
@@ -303,6 +312,7 @@ struct Sentinel<float> {
     }
     return __uint_as_float(v);
   }
+  __device__ __forceinline__ static float peek(const float *p) { return __uint_as_float(ld_relaxed_u32(p)); }
   __device__ __forceinline__ static void publish(float *p, float v) { st_relaxed_u32(p, __float_as_uint(v)); }
 };
 

@@ -55,6 +55,7 @@ struct KArgs {
   double *out_d;                  // [0] residual [1] rhsnorm
   const unsigned int *skip;       // bit 1 set: zero right-hand side, return at once
   int tri_per_block;              // sub-warps per block taking part in the triangular solves
+  int tri_bs;                     // rows per sync-free slot group (node blocks; 1 = row per slot)
   // ILU0 factors packed in solve order (see TriSchedule)
   const int *lo_ptr, *lo_cols, *up_ptr, *up_cols;
   const VT *lo_vals, *up_vals, *up_dinv;
@@ -239,6 +240,39 @@ __device__ __forceinline__ void spmv_phase(const KArgs<VT> &a, const VT *x0, con
 // upper: z_i = u_ii^-1 (y_i - sum_{j>i} U_ij z_j)     (backward, :3355-3362)
 // One slot's packed entries held by a warp: lane t has entries t and t+32 (rows with more
 // than 64 strictly-lower / upper entries finish the rest with a plain loop).
+// Warp-collective bounded wait: every lane re-polls all of its unproduced entries (c[u] >= 0
+// and x[u] still the sentinel) in one round, all loads in flight together, until no lane of
+// the warp has one left.  No lane spins alone, so a warp costs one L2 round trip per round
+// however its entries are spread over its lanes.  On expiry (or another block's error) the
+// entries keep the sentinel and the error flag is set.  Called by all 32 lanes.
+template <typename VT, int E>
+__device__ __forceinline__ void warp_wait_all(VT (&xv)[E], const int (&c)[E], const VT *x, int *err) {
+  bool pend = false;
+#pragma unroll
+  for (int u = 0; u < E; ++u) pend |= c[u] >= 0 && Sentinel<VT>::is(xv[u]);
+  if (!__any_sync(0xffffffffu, pend)) return;
+  const unsigned long long t0 = egpu_globaltimer();
+  for (unsigned int spin = 1;; ++spin) {
+    pend = false;
+#pragma unroll
+    for (int u = 0; u < E; ++u)
+      if (c[u] >= 0 && Sentinel<VT>::is(xv[u])) xv[u] = Sentinel<VT>::peek(x + c[u]);
+#pragma unroll
+    for (int u = 0; u < E; ++u) pend |= c[u] >= 0 && Sentinel<VT>::is(xv[u]);
+    if (!__any_sync(0xffffffffu, pend)) return;
+    if ((spin & 31u) == 0) {
+      int stop = 0;
+      if ((threadIdx.x & 31) == 0)
+        stop = egpu_globaltimer() - t0 > EGPU_WAIT_NS ? 1 : (*(volatile int *)err ? 2 : 0);
+      stop = __shfl_sync(0xffffffffu, stop, 0);
+      if (stop) {
+        if (stop == 1 && (threadIdx.x & 31) == 0) atomicExch(err, (int)EGPU_ERR_TIMEOUT);
+        return;
+      }
+    }
+  }
+}
+
 template <typename VT>
 struct TriRow {
   int row, beg, end;
@@ -281,9 +315,15 @@ __device__ __forceinline__ void tri_fetch(TriRow<VT> &t, int s, const int *order
 template <typename VT>
 __device__ __forceinline__ VT tri_dot(const TriRow<VT> &t, const VT *x, const int *cols, const VT *vals, int lane,
                                       int *err) {
+  // both loads in flight before either is waited on; the warp polls together
   VT acc = 0;
-  if (t.c0 >= 0) acc += t.v0 * Sentinel<VT>::wait(x + t.c0, err);
-  if (t.c1 >= 0) acc += t.v1 * Sentinel<VT>::wait(x + t.c1, err);
+  const int c[2] = {t.c0, t.c1};
+  VT xv[2];
+  xv[0] = t.c0 >= 0 ? Sentinel<VT>::peek(x + t.c0) : (VT)0;
+  xv[1] = t.c1 >= 0 ? Sentinel<VT>::peek(x + t.c1) : (VT)0;
+  warp_wait_all<VT, 2>(xv, c, x, err);
+  if (t.c0 >= 0) acc += t.v0 * xv[0];
+  if (t.c1 >= 0) acc += t.v1 * xv[1];
   for (int j = t.beg + 64 + lane; j < t.end; j += 32) {
     const int c = __ldg(cols + j);
     if (c >= 0) acc += __ldg(vals + j) * Sentinel<VT>::wait(x + c, err);
@@ -293,11 +333,195 @@ __device__ __forceinline__ VT tri_dot(const TriRow<VT> &t, const VT *x, const in
   return acc;
 }
 
+// Node-block variant (tri_bs = bs > 1).  When the matrix is made of dense diagonal blocks of
+// bs consecutive rows (the DOFs of one node, CRS_CreateMatrix with DOFs > 1), the rows of a
+// block form a dependency chain, so a row-per-slot schedule has bs times the levels of the
+// node graph.  Here one warp owns a whole block: slots s*bs .. s*bs+bs-1 of the orders are
+// its rows (lower: ascending, upper: descending), and each row's packed entries end (lower)
+// or start (upper) with its k in-block entries.  The warp sums the out-of-block entries of
+// all bs rows at once (all loads in flight, polled together), then resolves the in-block
+// chain in registers:
+//   lower  y_k = (rhs_k - sum_ext L y) - sum_{j<k} L_kj y_j
+//   upper  z_k = u_kk^-1 ((y_k - sum_ext U z) - sum_{j>k} U_kj z_j)
+// The blocks are waited on and published exactly like single rows.
+constexpr int TRI_BS_MAX = 4;
+constexpr int TRI_BS_E = 4;  // entries per lane loaded ahead (32 * 4 per block)
+
+template <typename VT>
+__device__ __forceinline__ void blk_add(VT (&acc)[TRI_BS_MAX], int k, VT v) {
+#pragma unroll
+  for (int q = 0; q < TRI_BS_MAX; ++q)
+    if (q == k) acc[q] += v;
+}
+
+// p[q] by a runtime q, without indexing the array (it stays in registers); p[q] = p[bs]
+// for q >= bs
+__device__ __forceinline__ int blk_at(const int (&p)[TRI_BS_MAX + 1], int q) {
+  int r = p[0];
+#pragma unroll
+  for (int t = 1; t <= TRI_BS_MAX; ++t)
+    if (q == t) r = p[t];
+  return r;
+}
+
+// slot k of entry e, and whether e is an out-of-block entry of the block (slot k's k
+// in-block entries are the last (lower) or first (upper) of its range)
+template <bool LOWER>
+__device__ __forceinline__ bool blk_ext(const int (&p)[TRI_BS_MAX + 1], int bs, int e, int &k) {
+  k = 0;
+#pragma unroll
+  for (int q = 1; q < TRI_BS_MAX; ++q) k += (q < bs && e >= p[q]) ? 1 : 0;
+  return e < p[TRI_BS_MAX] && (LOWER ? e < blk_at(p, k + 1) - k : e >= blk_at(p, k) + k);
+}
+
+// out-of-block sum of each of the block's rows; p[0..bs] are its packed row bounds
+template <typename VT, bool LOWER>
+__device__ __forceinline__ void blk_dot(VT (&acc)[TRI_BS_MAX], const int (&p)[TRI_BS_MAX + 1], int bs, const VT *x,
+                                        const int *cols, const VT *vals, int lane, int n, int *err) {
+#pragma unroll
+  for (int q = 0; q < TRI_BS_MAX; ++q) acc[q] = 0;
+  int c[TRI_BS_E];
+#pragma unroll
+  for (int u = 0; u < TRI_BS_E; ++u) {
+    const int e = p[0] + lane + 32 * u;
+    int k;
+    c[u] = blk_ext<LOWER>(p, bs, e, k) ? __ldg(cols + e) : -1;
+    if (c[u] >= n) {
+      atomicExch(err, (int)EGPU_ERR_ARG);
+      c[u] = -1;
+    }
+  }
+  VT xv[TRI_BS_E], v[TRI_BS_E];
+#pragma unroll
+  for (int u = 0; u < TRI_BS_E; ++u) {
+    xv[u] = c[u] >= 0 ? Sentinel<VT>::peek(x + c[u]) : (VT)0;
+    v[u] = c[u] >= 0 ? __ldg(vals + p[0] + lane + 32 * u) : (VT)0;
+  }
+  warp_wait_all<VT, TRI_BS_E>(xv, c, x, err);
+#pragma unroll
+  for (int u = 0; u < TRI_BS_E; ++u) {
+    if (c[u] < 0) continue;
+    int k;
+    blk_ext<LOWER>(p, bs, p[0] + lane + 32 * u, k);
+    blk_add(acc, k, v[u] * xv[u]);
+  }
+  for (int e = p[0] + lane + 32 * TRI_BS_E; e < p[TRI_BS_MAX]; e += 32) {
+    int k;
+    if (!blk_ext<LOWER>(p, bs, e, k)) continue;
+    const int cc = __ldg(cols + e);
+    if (cc < 0 || cc >= n) {
+      atomicExch(err, (int)EGPU_ERR_ARG);
+      continue;
+    }
+    blk_add(acc, k, __ldg(vals + e) * Sentinel<VT>::wait(x + cc, err));
+  }
+#pragma unroll
+  for (int q = 0; q < TRI_BS_MAX; ++q)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
+}
+
+// the block's first row and packed row bounds; false (error recorded) if out of range
+__device__ __forceinline__ bool blk_fetch(int q0, int bs, const int *order, const int *ptr, int n, int lower,
+                                          int &r0, int (&p)[TRI_BS_MAX + 1], int *err) {
+  const int r = __ldg(order + q0);
+  r0 = lower ? r : r - (bs - 1);
+#pragma unroll
+  for (int q = 0; q <= TRI_BS_MAX; ++q) p[q] = __ldg(ptr + q0 + (q < bs ? q : bs));
+  bool ok = r0 >= 0 && r0 + bs <= n;
+#pragma unroll
+  for (int q = 0; q < TRI_BS_MAX; ++q)
+    if (q < bs) ok = ok && p[q + 1] - p[q] >= q;
+  if (!ok && (threadIdx.x & 31) == 0) atomicExch(err, (int)EGPU_ERR_ARG);
+  return ok;
+}
+
+template <typename VT, typename RHS>
+__device__ __forceinline__ void lower_solve_blk(const KArgs<VT> &a, VT *y, RHS &rhs) {
+  const int lane = threadIdx.x & 31;
+  int gsub, nsub;
+  if (!tri_participant<32>(a.tri_per_block, gsub, nsub)) return;
+  const int bs = a.tri_bs, nblk = a.n / bs;
+  for (int sb = gsub; sb < nblk; sb += nsub) {
+    int r0, p[TRI_BS_MAX + 1];
+    if (!blk_fetch(sb * bs, bs, a.lower_order, a.lo_ptr, a.n, 1, r0, p, a.err)) continue;
+    // lane k < bs: right-hand side of row k; lane t < bs(bs-1)/2: in-block coefficient
+    // L_kj with t = k(k-1)/2 + j (the j-th of row k's last k entries)
+    VT rl = 0, cl = 0;
+    if (lane < bs) rl = rhs(r0 + lane);
+    if (lane < bs * (bs - 1) / 2) {
+      int k = 1;
+      while (k * (k + 1) / 2 <= lane) ++k;
+      const int j = lane - k * (k - 1) / 2;
+      cl = __ldg(a.lo_vals + blk_at(p, k + 1) - k + j);
+    }
+    VT acc[TRI_BS_MAX];
+    blk_dot<VT, true>(acc, p, bs, y, a.lo_cols, a.lo_vals, lane, a.n, a.err);
+    VT yk[TRI_BS_MAX], mine = 0;
+#pragma unroll
+    for (int k = 0; k < TRI_BS_MAX; ++k) {
+      if (k >= bs) break;
+      VT t = __shfl_sync(0xffffffffu, rl, k) - acc[k];
+#pragma unroll
+      for (int j = 0; j < k; ++j) t -= __shfl_sync(0xffffffffu, cl, k * (k - 1) / 2 + j) * yk[j];
+      yk[k] = t;
+      if (lane == k) mine = t;
+    }
+    if (lane < bs) Sentinel<VT>::publish(y + r0 + lane, mine);
+  }
+}
+
+template <typename VT, typename OUT>
+__device__ __forceinline__ void upper_solve_blk(const KArgs<VT> &a, const VT *y, VT *z, OUT &out) {
+  const int lane = threadIdx.x & 31;
+  int gsub, nsub;
+  if (!tri_participant<32>(a.tri_per_block, gsub, nsub)) return;
+  const int bs = a.tri_bs, nblk = a.n / bs;
+  for (int sb = gsub; sb < nblk; sb += nsub) {
+    const int q0 = sb * bs;
+    int r0, p[TRI_BS_MAX + 1];
+    if (!blk_fetch(q0, bs, a.upper_order, a.up_ptr, a.n, 0, r0, p, a.err)) continue;
+    // slot k of the block is row r0 + bs - 1 - k; its first k packed entries are the
+    // in-block ones (rows of slots k-1 .. 0).  Lane t < bs(bs-1)/2: U for slot k, entry j.
+    VT dl = 0, cl = 0;
+    if (lane < bs) dl = __ldg(a.up_dinv + q0 + lane);
+    if (lane < bs * (bs - 1) / 2) {
+      int k = 1;
+      while (k * (k + 1) / 2 <= lane) ++k;
+      const int j = lane - k * (k - 1) / 2;
+      cl = __ldg(a.up_vals + blk_at(p, k) + j);
+    }
+    VT acc[TRI_BS_MAX];
+    blk_dot<VT, false>(acc, p, bs, z, a.up_cols, a.up_vals, lane, a.n, a.err);
+    VT yl = 0;
+    if (lane < bs) yl = Sentinel<VT>::wait(y + r0 + bs - 1 - lane, a.err);
+    VT zk[TRI_BS_MAX], mine = 0;
+#pragma unroll
+    for (int k = 0; k < TRI_BS_MAX; ++k) {
+      if (k >= bs) break;
+      VT t = __shfl_sync(0xffffffffu, yl, k) - acc[k];
+      // entry j of slot k is column r0 + bs - k + j, i.e. slot k - 1 - j
+#pragma unroll
+      for (int j = 0; j < k; ++j) t -= __shfl_sync(0xffffffffu, cl, k * (k - 1) / 2 + j) * zk[k - 1 - j];
+      zk[k] = __shfl_sync(0xffffffffu, dl, k) * t;
+      if (lane == k) mine = zk[k];
+    }
+    if (lane < bs) {
+      Sentinel<VT>::publish(z + r0 + bs - 1 - lane, mine);
+      out(r0 + bs - 1 - lane, mine);
+    }
+  }
+}
+
 // lower: y_i = rhs_i - sum_{j<i} L_ij y_j (CRS_LUSolve forward, CRSMatrix.src:3346-3352).
 // One warp per slot; the next slot's row and entries are fetched while this slot waits.
 template <typename VT, int TS, typename RHS>
 __device__ __forceinline__ void lower_solve(const KArgs<VT> &a, VT *y, RHS &&rhs) {
   static_assert(TS == 32, "one warp per row");
+  if (a.tri_bs > 1) {
+    lower_solve_blk<VT>(a, y, rhs);
+    return;
+  }
   const int lane = threadIdx.x & 31;
   int gsub, nsub;
   if (!tri_participant<TS>(a.tri_per_block, gsub, nsub)) return;
@@ -320,6 +544,10 @@ __device__ __forceinline__ void lower_solve(const KArgs<VT> &a, VT *y, RHS &&rhs
 template <typename VT, int TS, typename OUT>
 __device__ __forceinline__ void upper_solve(const KArgs<VT> &a, const VT *y, VT *z, OUT &&out) {
   static_assert(TS == 32, "one warp per row");
+  if (a.tri_bs > 1) {
+    upper_solve_blk<VT>(a, y, z, out);
+    return;
+  }
   const int lane = threadIdx.x & 31;
   int gsub, nsub;
   if (!tri_participant<TS>(a.tri_per_block, gsub, nsub)) return;

@@ -48,6 +48,7 @@ int build_cta_schedule(egpu_mat *A, const std::vector<int> &rows, const std::vec
                        const std::vector<int> &lp, const std::vector<int> &lc, const std::vector<int> &upp,
                        const std::vector<int> &uc);
 int cta_fill_values(egpu_mat *A);
+bool tri_prefer_node_blocks(int nlo, int nup, int bl, int bu, int n);
 bool cta_use(const egpu_mat *A, int v);
 int cta_threads(const egpu_mat *A);
 

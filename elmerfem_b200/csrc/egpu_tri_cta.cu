@@ -33,14 +33,30 @@ int tri_mode_env() {
   return 0;
 }
 
-// Estimated seconds of one M^-1 application, from B200 measurements of both solves on hex
-// meshes: sync-free, about 2 us per dependency level (a cross-SM publish/observe round
-// trip); single block, about 0.6 us per level plus 4 ns per row (its entries streamed and
-// summed by one SM), plus the extra grid barrier.
-double est_syncfree(int nlev_lo, int nlev_up) { return 2.0e-6 * (nlev_lo + nlev_up); }
+// Estimated seconds of one M^-1 application, from B200 measurements of the solves on hex
+// meshes (Poisson and 3-DOF elasticity): sync-free, about 0.9 us per dependency level (a
+// cross-SM publish/observe round trip) plus 0.8 ns per row; node-block sync-free, about
+// 1.7 us per block level plus 0.65 ns per row; single block, about 0.6 us per level plus
+// 4 ns per row (its entries streamed and summed by one SM), plus the extra grid barrier.
+double est_syncfree(int nlev_lo, int nlev_up, int n) { return 0.9e-6 * (nlev_lo + nlev_up) + 0.8e-9 * 2.0 * n; }
+double est_nodeblock(int nlev_lo, int nlev_up, int n) { return 1.7e-6 * (nlev_lo + nlev_up) + 0.65e-9 * 2.0 * n; }
 double est_block(int nlev_lo, int nlev_up, int n) { return 0.6e-6 * (nlev_lo + nlev_up) + 4e-9 * 2.0 * n + 3e-6; }
 
 }  // namespace
+
+// node-block sync-free solve (bl / bu block levels) instead of the row schedule (nlo / nup
+// row levels, sync-free or single block)?  EGPU_TRI_NODE_BLOCKS=0 never, =1 always.
+bool tri_prefer_node_blocks(int nlo, int nup, int bl, int bu, int n) {
+  if (const char *e = std::getenv("EGPU_TRI_NODE_BLOCKS")) {
+    if (!std::strcmp(e, "0")) return false;
+    if (!std::strcmp(e, "1")) return true;
+  }
+  const int mode = tri_mode_env();
+  if (mode == 2) return false;
+  const double blk = est_nodeblock(bl, bu, n);
+  if (blk >= est_syncfree(nlo, nup, n)) return false;
+  return mode == 1 || blk < est_block(nlo, nup, n);
+}
 
 __global__ void k_cta_fill(long long nl, long long nu, const int *__restrict__ lsrc, const int *__restrict__ usrc,
                            const double *__restrict__ lo, const double *__restrict__ up,
@@ -78,7 +94,7 @@ int build_cta_schedule(egpu_mat *A, const std::vector<int> &rows, const std::vec
   if (!P.ok) return EGPU_OK;
   bool any = false;
   for (int v = 0; v < 2; ++v)
-    if (P.fits[v] && (mode == 2 || est_block(P.lo.nlev, P.up.nlev, n) < est_syncfree(P.lo.nlev, P.up.nlev)))
+    if (P.fits[v] && (mode == 2 || est_block(P.lo.nlev, P.up.nlev, n) < est_syncfree(P.lo.nlev, P.up.nlev, n)))
       any = true;
   if (!any) return EGPU_OK;
   if (!plan::plan_arrays(P, n, lo, up, lp, lc, upp, uc)) {
@@ -154,7 +170,7 @@ bool cta_use(const egpu_mat *A, int v) {
   const int mode = tri_mode_env();
   if (mode == 1) return false;
   if (mode == 2) return true;
-  return est_block(S.cta_lo.nlev, S.cta_up.nlev, A->n) < est_syncfree(S.cta_lo.nlev, S.cta_up.nlev);
+  return est_block(S.cta_lo.nlev, S.cta_up.nlev, A->n) < est_syncfree(S.cta_lo.nlev, S.cta_up.nlev, A->n);
 }
 
 }  // namespace egpu

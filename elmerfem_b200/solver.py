@@ -272,6 +272,13 @@ class Matrix:
               self.ctx.handle, "egpu_ilu_download")
         return r, c, d, v
 
+    def tri_info(self) -> dict:
+        """The triangular-solve schedule of the matrix's ILU structure (after a factorisation)."""
+        info = np.zeros(6, np.int32)
+        check(lib().egpu_tri_info(self._h, info.ctypes.data), self.ctx.handle, "egpu_tri_info")
+        return {"node_block": int(info[0]), "lower_levels": int(info[1]), "upper_levels": int(info[2]),
+                "max_width": int(info[3]), "single_block_fp64": bool(info[4]), "single_block_fp32": bool(info[5])}
+
     def ilu0(self, scale_system: bool = True):
         """Factor ILU0 on the device; returns (ILUValues with inverted U diagonal, DiagScaling)."""
         check(lib().egpu_ilu0_build(self._h, int(scale_system)), self.ctx.handle, "egpu_ilu0_build")

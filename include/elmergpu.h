@@ -155,6 +155,12 @@ long long egpu_ilu_pattern(int n, const int *rows, const int *cols, const int *d
 int egpu_ilu_download(egpu_mat *A, int *ilu_rows, int *ilu_cols, int *ilu_diag, double *ilu_values);
 int egpu_ilu0_download(egpu_mat *A, double *ilu_values, double *diag_scaling);
 int egpu_lu_precondition(egpu_mat *A, const double *v, double *u);
+/* The triangular-solve schedule built for the matrix's ILU structure (diagnostics): info[0]
+ * rows per sync-free slot group (> 1: node-block solve), [1] / [2] lower / upper dependency
+ * levels (of slot groups), [3] most rows in one level, [4] / [5] single-block schedule usable
+ * for FP64 / FP32.  EGPU_ERR_STATE before the first factorisation.  No reference
+ * counterpart (the reference's CRS_LUSolve has no schedule). */
+int egpu_tri_info(egpu_mat *A, int info[6]);
 
 /* ---- Matrix Vector Proc hook (CRSMatrix.src:3555-3559, Load.c:734-747) ----------- */
 int egpu_mv(egpu_mat *A, const double *u, double *v);
