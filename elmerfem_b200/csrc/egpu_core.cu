@@ -151,13 +151,13 @@ __global__ void k_backscale_x(int n, const double *__restrict__ xs, const double
 }
 
 // CRS_IncompleteLU(A,0), CRSMatrix.src:2312-2356, one warp per row in a dependency order
-// (every row after the rows of its strictly lower part).  The warp first waits (bounded,
-// all lanes polling together) until every row k of its strictly lower part is done, then
-// runs the IKJ loop over those k in ascending column order: S_m /= u_kk, then
-// S_j -= S_m * U_kj for the U entries of row k that fall in the row's pattern (found by
-// binary search in the row's columns).  Row k+1's U entries and u_kk are loaded while row
-// k's update runs.  Every entry of the row sees its updates in the reference's order, so
-// the factor is bit-identical to the sequential routine.  The U diagonal stays un-inverted.
+// (every row after the rows of its strictly lower part).  The warp runs the IKJ loop over
+// the rows k of its strictly lower part in ascending column order, each once it is done:
+// S_m /= u_kk, then S_j -= S_m * U_kj for the U entries of row k that fall in the row's
+// pattern (found by binary search in the row's columns).  Row k+1's U entries and u_kk are
+// loaded while row k's update runs.  Every entry of the row sees its updates in the
+// reference's order, so the factor is bit-identical to the sequential routine.  The U
+// diagonal stays un-inverted.
 struct IluDep {
   int dk, kend;
   int c0, c1;
@@ -222,52 +222,59 @@ __global__ void __launch_bounds__(256) k_ilu0_factor(int n, const int *__restric
       Cc[t] = cols[beg + t];
     }
     __syncwarp();
-    // every row of the strictly lower part done (acquire), all lanes polling together
-    {
-      bool pend = false;
-      for (int m = lane; m < nl; m += 32) pend |= ld_acquire_s32(done + Cc[m]) == 0;
-      if (__any_sync(0xffffffffu, pend)) {
-        const unsigned long long t0 = egpu_globaltimer();
-        for (unsigned int spin = 1;; ++spin) {
-          pend = false;
-          for (int m = lane; m < nl; m += 32) pend |= ld_acquire_s32(done + Cc[m]) == 0;
-          if (!__any_sync(0xffffffffu, pend)) break;
-          if ((spin & 31u) == 0) {
-            int stop = 0;
-            if (lane == 0) stop = egpu_globaltimer() - t0 > EGPU_WAIT_NS ? 1 : (*(volatile int *)err ? 2 : 0);
-            stop = __shfl_sync(0xffffffffu, stop, 0);
-            if (stop) {
-              if (stop == 1 && lane == 0) atomicExch(err, (int)EGPU_ERR_TIMEOUT);
-              return;
-            }
+    // The dependencies are taken in rounds: the 32 lanes poll the done flags of the next 32
+    // rows of the strictly lower part at once (acquire), and the leading run of finished
+    // ones is processed while the rest may still be in progress (typically the row's own
+    // node-block predecessors, the last entries).  A round that finds nothing is a bounded
+    // wait.
+    unsigned long long t0 = 0;
+    unsigned int spin = 0;
+    for (int m0 = 0; m0 < nl;) {
+      const int mp = m0 + lane;
+      const bool ok = mp >= nl || ld_acquire_s32(done + Cc[mp]) != 0;
+      const unsigned int mask = __ballot_sync(0xffffffffu, ok);
+      __syncwarp();
+      const int ready = mask == 0xffffffffu ? 32 : __ffs(~mask) - 1;
+      if (ready == 0) {
+        if (t0 == 0) t0 = egpu_globaltimer();
+        if ((++spin & 31u) == 0) {
+          int stop = 0;
+          if (lane == 0) stop = egpu_globaltimer() - t0 > EGPU_WAIT_NS ? 1 : (*(volatile int *)err ? 2 : 0);
+          stop = __shfl_sync(0xffffffffu, stop, 0);
+          if (stop) {
+            if (stop == 1 && lane == 0) atomicExch(err, (int)EGPU_ERR_TIMEOUT);
+            return;
           }
         }
+        continue;
       }
-    }
-    __syncwarp();
-    IluDep nxt;
-    if (nl > 0) ilu_dep_fetch(nxt, Cc[0], rows, cols, diag, ilu, lane);
-    for (int m = 0; m < nl; ++m) {
-      const IluDep cur = nxt;
-      if (m + 1 < nl) ilu_dep_fetch(nxt, Cc[m + 1], rows, cols, diag, ilu, lane);
-      double sk = S[m];
-      if (sk == 0.0) continue;
-      if (fabs(cur.ukk) > EGPU_AEPS) sk = sk / cur.ukk;
+      const int m1 = min(nl, m0 + ready);
+      IluDep nxt;
+      ilu_dep_fetch(nxt, Cc[m0], rows, cols, diag, ilu, lane);
+      for (int m = m0; m < m1; ++m) {
+        const IluDep cur = nxt;
+        if (m + 1 < m1) ilu_dep_fetch(nxt, Cc[m + 1], rows, cols, diag, ilu, lane);
+        double sk = S[m];
+        if (sk == 0.0) continue;
+        if (fabs(cur.ukk) > EGPU_AEPS) sk = sk / cur.ukk;
+        __syncwarp();
+        if (lane == 0) S[m] = sk;
+        if (cur.c0 >= 0) {
+          const int pos = ilu_find(Cc, len, cur.c0);
+          if (pos >= 0) S[pos] = __dsub_rn(S[pos], __dmul_rn(sk, cur.v0));
+        }
+        if (cur.c1 >= 0) {
+          const int pos = ilu_find(Cc, len, cur.c1);
+          if (pos >= 0) S[pos] = __dsub_rn(S[pos], __dmul_rn(sk, cur.v1));
+        }
+        for (int l = cur.dk + 65 + lane; l < cur.kend; l += 32) {
+          const int pos = ilu_find(Cc, len, cols[l]);
+          if (pos >= 0) S[pos] = __dsub_rn(S[pos], __dmul_rn(sk, __ldcg(ilu + l)));
+        }
+        __syncwarp();
+      }
       __syncwarp();
-      if (lane == 0) S[m] = sk;
-      if (cur.c0 >= 0) {
-        const int pos = ilu_find(Cc, len, cur.c0);
-        if (pos >= 0) S[pos] = __dsub_rn(S[pos], __dmul_rn(sk, cur.v0));
-      }
-      if (cur.c1 >= 0) {
-        const int pos = ilu_find(Cc, len, cur.c1);
-        if (pos >= 0) S[pos] = __dsub_rn(S[pos], __dmul_rn(sk, cur.v1));
-      }
-      for (int l = cur.dk + 65 + lane; l < cur.kend; l += 32) {
-        const int pos = ilu_find(Cc, len, cols[l]);
-        if (pos >= 0) S[pos] = __dsub_rn(S[pos], __dmul_rn(sk, __ldcg(ilu + l)));
-      }
-      __syncwarp();
+      m0 = m1;
     }
     for (int t = lane; t < len; t += 32) ilu[beg + t] = S[t];
     __syncwarp();
