@@ -230,16 +230,15 @@ __device__ __forceinline__ void spmv_phase(const KArgs<VT> &a, const VT *x0, con
 }
 
 // -------------------------------------------------------------------------------------
-// Sync-free triangular solves.  Rows are taken in ascending dependency level
-// (lower_order / upper_order); slot s is handled by sub-warp s mod nsub in increasing s,
-// so every dependency of a row sits in an earlier slot of a running sub-warp.  Each
-// produced value is published as itself; consumers spin (bounded) until the entry no
+// Sync-free triangular solves.  Rows are taken in a dependency order (lower_order /
+// upper_order: ascending dependency level); slot s is handled by sub-warp s mod nsub in
+// increasing s, so every dependency of a row sits in an earlier slot of a running sub-warp.
+// Each produced value is published as itself; consumers poll (bounded) until the entry no
 // longer holds the sentinel.
 //
 // lower: y_i = rhs_i - sum_{j<i} L_ij y_j            (CRS_LUSolve forward, CRSMatrix.src:3346-3352)
 // upper: z_i = u_ii^-1 (y_i - sum_{j>i} U_ij z_j)     (backward, :3355-3362)
-// One slot's packed entries held by a warp: lane t has entries t and t+32 (rows with more
-// than 64 strictly-lower / upper entries finish the rest with a plain loop).
+//
 // Warp-collective bounded wait: every lane re-polls all of its unproduced entries (c[u] >= 0
 // and x[u] still the sentinel) in one round, all loads in flight together, until no lane of
 // the warp has one left.  No lane spins alone, so a warp costs one L2 round trip per round
@@ -273,6 +272,8 @@ __device__ __forceinline__ void warp_wait_all(VT (&xv)[E], const int (&c)[E], co
   }
 }
 
+// One slot's packed entries held by a warp: lane t has entries t and t+32 (rows with more
+// than 64 strictly-lower / upper entries finish the rest with a plain loop).
 template <typename VT>
 struct TriRow {
   int row, beg, end;
