@@ -253,14 +253,24 @@ def cpu_solve_rate(p, values, rhs, solve_kw, full_iters, threads, target_s=10.0)
         return 1.0 / t, {"seconds_per_iter": t / max(1, full_iters), "setup_seconds": None,
                          "sample_iters": full_iters * len(times), "sample_seconds": sum(times),
                          "sample": f"{len(times)} complete oracle solves ({sum(times):.1f} s), median"}
+    # t_lo includes the solve's set-up, so the first sample undershoots: a second one sized
+    # from the measured per-iteration time brings the total near target_s
     hi = min(full_iters, lo + max(8, int(target_s / max(1e-9, t_lo / lo))))
     t_hi = run(hi)
+    spent, iters_run = t_lo + t_hi, lo + hi
     per_iter = max(1e-9, (t_hi - t_lo) / (hi - lo))
+    if spent < 0.6 * target_s and hi < full_iters:
+        hi2 = min(full_iters, hi + int((target_s - spent) / per_iter))
+        if hi2 > hi:
+            t_hi2 = run(hi2)
+            spent += t_hi2
+            iters_run += hi2
+            per_iter = max(1e-9, (t_hi2 - t_lo) / (hi2 - lo))
     setup = max(0.0, t_lo - lo * per_iter)
     t_full = setup + per_iter * full_iters
-    return 1.0 / t_full, {"seconds_per_iter": per_iter, "setup_seconds": setup, "sample_iters": lo + hi,
-                          "sample_seconds": t_lo + t_hi,
-                          "sample": f"{lo + hi} oracle iterations on the full system ({t_lo + t_hi:.1f} s), "
+    return 1.0 / t_full, {"seconds_per_iter": per_iter, "setup_seconds": setup, "sample_iters": iters_run,
+                          "sample_seconds": spent,
+                          "sample": f"{iters_run} oracle iterations on the full system ({spent:.1f} s), "
                                     f"extrapolated to the FP64 iteration count {full_iters}"}
 
 

@@ -192,6 +192,123 @@ __device__ __forceinline__ void batch_tri(const BatchArgs &a, const BatchShared 
   }
 }
 
+// The same with G rows per warp (TS = 32 / G lanes each), the G consecutive slots of a slot
+// group.  Consecutive slots belong to different systems when at least G systems are active,
+// and every dependency of a row lies at least nact slots back, so all dependencies of a
+// group lie in earlier groups: a warp can wait for its G rows together (one collective poll)
+// without ever waiting on itself.  With many systems each warp would otherwise take its
+// slots one after another, each a full publish/observe round trip; G rows in flight per
+// warp divide that chain by G.
+template <bool LOWER, int G, typename RHS, typename OUT>
+__device__ __forceinline__ void batch_tri_group(const BatchArgs &a, const BatchShared &sh, int yoff, int zoff,
+                                                RHS &&rhs, OUT &&out) {
+  constexpr int TS = 32 / G;
+  constexpr int E = G >= 8 ? 4 : 2;  // entries per lane held in registers
+  const int local = threadIdx.x >> 5;
+  if (local >= a.tri_warps_per_block || sh.nact < G) return;
+  const int lane = threadIdx.x & 31, sub = lane / TS, sl = lane % TS;
+  const int P = a.tri_warps_per_block * gridDim.x;
+  int maxn = 0;
+  for (int t = 0; t < sh.nact; ++t)
+    if (sh.status[sh.act[t]] == ST_RUN) maxn = max(maxn, a.sys[sh.act[t]].n);
+  const long long nslot = (long long)maxn * sh.nact;
+  const long long ngrp = (nslot + G - 1) / G;
+  for (long long g = (long long)local * gridDim.x + blockIdx.x; g < ngrp; g += P) {
+    const long long q = g * G + sub;
+    int ai = 0, pos = 0;
+    bool valid = q < nslot && batch_slot(a, sh, q, ai, pos);
+    if (!__any_sync(0xffffffffu, valid)) continue;
+    const int s = valid ? sh.act[ai] : 0;
+    const SysDesc &d = a.sys[s];
+    int row = -1, beg = 0, end = 0;
+    int c[E];
+    float v[E], dinv = 0.f;
+#pragma unroll
+    for (int u = 0; u < E; ++u) {
+      c[u] = -1;
+      v[u] = 0.f;
+    }
+    if (valid) {
+      const int *order = LOWER ? d.lower_order : d.upper_order;
+      const int *ptr = LOWER ? d.lo_ptr : d.up_ptr;
+      const int *cols = LOWER ? d.lo_cols : d.up_cols;
+      const float *vals = LOWER ? d.lo_vals : d.up_vals;
+      row = __ldg(order + pos);
+      beg = __ldg(ptr + pos);
+      end = __ldg(ptr + pos + 1);
+      if (row < 0 || row >= d.n || end < beg) {
+        if (sl == 0) atomicExch(a.err, (int)EGPU_ERR_ARG);
+        valid = false;
+        row = -1;
+      } else {
+#pragma unroll
+        for (int u = 0; u < E; ++u) {
+          const int e = beg + sl + TS * u;
+          if (e < end) {
+            c[u] = __ldg(cols + e);
+            v[u] = __ldg(vals + e);
+            if (c[u] < 0 || c[u] >= d.n) {
+              atomicExch(a.err, (int)EGPU_ERR_ARG);
+              c[u] = -1;
+            }
+          }
+        }
+        if (!LOWER) dinv = __ldg(d.up_dinv + pos);
+      }
+    }
+    float *y = valid ? d.w + yoff * d.ldw : nullptr, *z = valid ? d.w + zoff * d.ldw : nullptr;
+    const float *x = LOWER ? y : z;
+    float r = 0.f;
+    if (LOWER && valid && sl == 0) r = rhs(ai, s, d, row);
+    float xv[E];
+#pragma unroll
+    for (int u = 0; u < E; ++u) xv[u] = c[u] >= 0 ? Sentinel<float>::peek(x + c[u]) : 0.f;
+    warp_wait_all<float, E>(xv, c, x, a.err);
+    float acc = 0.f;
+#pragma unroll
+    for (int u = 0; u < E; ++u)
+      if (c[u] >= 0) acc += v[u] * xv[u];
+    if (valid) {  // rows longer than E TS entries
+      const int *cols = LOWER ? d.lo_cols : d.up_cols;
+      const float *vals = LOWER ? d.lo_vals : d.up_vals;
+      for (int e = beg + E * TS + sl; e < end; e += TS) {
+        const int cc = __ldg(cols + e);
+        if (cc < 0 || cc >= d.n) {
+          atomicExch(a.err, (int)EGPU_ERR_ARG);
+          continue;
+        }
+        acc += __ldg(vals + e) * Sentinel<float>::wait(x + cc, a.err);
+      }
+    }
+#pragma unroll
+    for (int off = TS / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if (valid && sl == 0) {
+      if (LOWER) {
+        Sentinel<float>::publish(y + row, r - acc);
+      } else {
+        const float yi = Sentinel<float>::wait(y + row, a.err);
+        const float zi = dinv * (yi - acc);
+        Sentinel<float>::publish(z + row, zi);
+        out(ai, s, d, row, zi);
+      }
+    }
+  }
+}
+
+// G rows per warp when the batch allows it (a.tri_group) and enough systems are active
+template <bool LOWER, typename RHS, typename OUT>
+__device__ __forceinline__ void batch_tri_any(const BatchArgs &a, const BatchShared &sh, int yoff, int zoff, RHS &&rhs,
+                                              OUT &&out) {
+  if (a.tri_group >= 8 && sh.nact >= 8)
+    batch_tri_group<LOWER, 8>(a, sh, yoff, zoff, rhs, out);
+  else if (a.tri_group >= 4 && sh.nact >= 4)
+    batch_tri_group<LOWER, 4>(a, sh, yoff, zoff, rhs, out);
+  else if (a.tri_group >= 2 && sh.nact >= 2)
+    batch_tri_group<LOWER, 2>(a, sh, yoff, zoff, rhs, out);
+  else
+    batch_tri<LOWER>(a, sh, yoff, zoff, rhs, out);
+}
+
 // ------------------------------------------------------------------------------------
 // the kernel
 
@@ -357,13 +474,13 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       batch_clear(a, BA_TS);
       batch_clear(a, BA_TT);
       if (ilu) {
-        batch_tri<true>(a, sh, 8, 6, [&](int, int s, const SysDesc &d, int i) {
+        batch_tri_any<true>(a, sh, 8, 6, [&](int, int s, const SysDesc &d, int i) {
           float *R = d.w, *P = d.w + 2 * d.ldw, *V = d.w + 3 * d.ldw;
           const float p = R[i] + sh.sb[s] * (P[i] - sh.sa[s] * V[i]);
           P[i] = p;
           return p;
         }, [&](int, int, const SysDesc &, int, float) {});
-        batch_tri<false>(a, sh, 8, 6, [&](int, int, const SysDesc &, int) { return 0.f; },
+        batch_tri_any<false>(a, sh, 8, 6, [&](int, int, const SysDesc &, int) { return 0.f; },
                          [&](int, int, const SysDesc &, int, float) {});
       } else {
         batch_slices(sh, [&](int, int s, int slice) {
@@ -409,14 +526,14 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       }
       __syncthreads();
       if (ilu) {
-        batch_tri<true>(a, sh, 9, 7, [&](int ai, int s, const SysDesc &d, int i) {
+        batch_tri_any<true>(a, sh, 9, 7, [&](int ai, int s, const SysDesc &d, int i) {
           float *R = d.w, *V = d.w + 3 * d.ldw, *S = d.w + 5 * d.ldw;
           const float sv = R[i] - (float)rho_s[s] * V[i];
           S[i] = sv;
           atomicAdd(&sh.red[2 * ai], (double)sv * (double)sv);
           return sv;
         }, [&](int, int, const SysDesc &, int, float) {});
-        batch_tri<false>(a, sh, 9, 7, [&](int, int, const SysDesc &, int) { return 0.f; },
+        batch_tri_any<false>(a, sh, 9, 7, [&](int, int, const SysDesc &, int) { return 0.f; },
                          [&](int, int, const SysDesc &, int, float) {});
       } else {
         batch_slices(sh, [&](int ai, int s, int slice) {
@@ -998,6 +1115,21 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
     a.tri_warps_per_block = std::max((nrun + grid - 1) / grid,
                                      std::min(EGPU_BLOCK / 32, (B->tri_mult * maxw * nrun + grid - 1) / grid));
     a.tri_warps_per_block = std::max(1, std::min(EGPU_BLOCK / 32, a.tri_warps_per_block));
+    // rows per warp in the sync-free solves: up to 4 (8 lanes, 16 entries in registers; fewer
+    // when fewer systems run) or 2 (16 lanes, 32 entries) when the longest strictly-lower /
+    // upper row part fits, else 1.  EGPU_BATCH_TRI_GROUP overrides (1, 2, 4 or 8; 8 rows of 4
+    // lanes measured slower than 4 on eight 96^3 systems)
+    {
+      int maxpart = 0;
+      for (int i = 0; i < ns; ++i)
+        if (B->sys[i] && B->sys[i]->phase == 2)
+          maxpart = std::max(maxpart, std::max(B->sys[i]->A->tri.max_lower, B->sys[i]->A->tri.max_upper));
+      a.tri_group = maxpart <= 16 ? 4 : maxpart <= 32 ? 2 : 1;
+      if (const char *e = std::getenv("EGPU_BATCH_TRI_GROUP")) {
+        const int g = std::atoi(e);
+        if (g == 1 || g == 2 || g == 4 || g == 8) a.tri_group = g;
+      }
+    }
     a.bar = ctx->sync.p;
     a.err = (int *)(ctx->sync.p + 1);
     a.it_done = B->d_it.p;

@@ -68,6 +68,7 @@ struct BatchArgs {
   double tol;
   int maxit;
   int tri_warps_per_block;
+  int tri_group;            // rows per warp in the sync-free solves (1, 2, 4 or 8)
   unsigned int *bar;
   int *err;
   int *it_done;             // iterations run by this launch (written by block 0)
