@@ -23,7 +23,7 @@ HUTI = {1: "HUTI_CONVERGENCE", 2: "HUTI_MAXITER", 3: "HUTI_DIVERGENCE", 20: "HUT
         36: "HUTI_BICGSTAB_SNORM", 37: "HUTI_BICGSTAB_OMEGA"}
 
 CG, BICGSTAB, GCR, BICGSTABL = 1, 2, 3, 4
-PREC_NONE, PREC_DIAGONAL, PREC_ILU0 = 0, 1, 2
+PREC_NONE, PREC_DIAGONAL, PREC_ILU0, PREC_ILUT = 0, 1, 2, 3
 FP64, MIXED = 0, 1
 
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -35,7 +35,8 @@ class Params(C.Structure):
     _fields_ = [("method", C.c_int), ("precond", C.c_int), ("max_iter", C.c_int), ("tol", C.c_double),
                 ("scale_system", C.c_int), ("precision", C.c_int), ("refactorize", C.c_int),
                 ("precond_recompute", C.c_int), ("inner_tol", C.c_double), ("inner_max_iter", C.c_int),
-                ("max_refinements", C.c_int), ("ilu_order", C.c_int), ("restart", C.c_int)]
+                ("max_refinements", C.c_int), ("ilu_order", C.c_int), ("restart", C.c_int),
+                ("ilut_tol", C.c_double)]
 
 
 class Result(C.Structure):
@@ -90,6 +91,7 @@ PROTOTYPES = {
     "egpu_ilu_pattern": (C.c_longlong, [C.c_int, _i32p, _i32p, _i32p, C.c_int, C.c_longlong, _vp, _vp, _vp]),
     "egpu_ilu_download": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "egpu_tri_info": (C.c_int, [_vp, _vp]),
+    "egpu_ilut_build": (C.c_int, [_vp, C.c_int, C.c_double]),
     "egpu_iter_solve": (C.c_int, [_vp, _f64p, _f64p, C.POINTER(Params), C.POINTER(Result)]),
     "egpu_iter_solve_dev": (C.c_int, [_vp, _vp, _vp, C.POINTER(Params), C.POINTER(Result)]),
     "egpu_mv": (C.c_int, [_vp, _f64p, _f64p]),

@@ -797,6 +797,8 @@ __global__ void k_ilu_scatter(long long nnz, const int *__restrict__ pos, const 
     out[pos[e]] = v[e];
 }
 
+static int ilu_pack(egpu_mat *A);
+
 // ILU(order) of the scaled matrix (IterSolve.src:420-575 -> CRS_IncompleteLU(A, order))
 int ilu_factor(egpu_mat *A, int order) {
   egpu_ctx *ctx = A->ctx;
@@ -843,6 +845,14 @@ int ilu_factor(egpu_mat *A, int order) {
                                   : (const void *)k_ilu0_factor<256>;
   EGPU_CUDA_TRY(ctx, cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(256), args, 0, ctx->stream));
   k_ilu_invdiag<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, A->ilu_diag.p, A->ilu.p);
+  ctx->launches += 2;
+  return ilu_pack(A);
+}
+
+// the factors (A->ilu, inverted U diagonal) packed in both solves' layouts, FP64 and FP32
+static int ilu_pack(egpu_mat *A) {
+  egpu_ctx *ctx = A->ctx;
+  const int n = A->n;
   const long long nl = A->tri.lo_cols.n, nu = A->tri.up_cols.n;
   EGPU_CUDA_TRY(ctx, A->lo_vals.alloc(nl));
   EGPU_CUDA_TRY(ctx, A->up_vals.alloc(nu));
@@ -853,12 +863,69 @@ int ilu_factor(egpu_mat *A, int order) {
   k_pack_tri<<<grid_for(ctx, nl + nu + n), 256, 0, ctx->stream>>>(
       nl, nu, n, A->tri.lo_src.p, A->tri.up_src.p, A->tri.up_dsrc.p, A->ilu.p, A->lo_vals.p, A->up_vals.p,
       A->up_dinv.p, A->lo_vals32.p, A->up_vals32.p, A->up_dinv32.p);
-  ctx->launches += 3;
+  ctx->launches++;
   EGPU_CUDA_TRY(ctx, cudaGetLastError());
-  rc = cta_fill_values(A);
+  const int rc = cta_fill_values(A);
   if (rc) return rc;
   A->ilu_valid = true;
   return EGPU_OK;
+}
+
+// ILUT of the scaled matrix (IterSolve.src:577-578 -> CRS_ILUT(A, ILUT_TOL)).  The factor's
+// structure depends on its values, so the factorisation runs on the host as the reference's
+// does (egpu_ilut_host); its structure then gets the level schedules of ILU(n), rebuilt with
+// every factorisation, and the device applies it.
+int ilut_factor(egpu_mat *A, double tol) {
+  egpu_ctx *ctx = A->ctx;
+  if (A->parent || A->clones > 0) {
+    egpu_set_error(ctx, "ILUT: the factor's structure depends on the values, so cloned matrices (batches, the "
+                        "server) cannot share it; use ILU(n)");
+    return EGPU_ERR_STATE;
+  }
+  if (!(tol >= 0.0)) return EGPU_ERR_ARG;
+  const int n = A->n;
+  const long long z = A->nnz;
+  std::vector<int> rows(n + 1), cols(z);
+  std::vector<double> vals(z);
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(rows.data(), A->rows.p, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(cols.data(), A->cols.p, z * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(vals.data(), A->scaled.p, z * sizeof(double), cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  std::vector<int> ir, ic, id;
+  std::vector<double> iv;
+  if (!::egpu_ilut_host(n, rows, cols, vals, tol, ir, ic, id, iv)) {
+    egpu_set_error(ctx, "ILUT: a row has no diagonal entry");
+    return EGPU_ERR_ARG;
+  }
+  const long long nz = (long long)ic.size();
+  int maxrow = 0;
+  for (int i = 0; i < n; ++i) maxrow = std::max(maxrow, ir[i + 1] - ir[i]);
+  EGPU_CUDA_TRY(ctx, A->ilu_rows.alloc(n + 1));
+  EGPU_CUDA_TRY(ctx, A->ilu_cols.alloc(nz));
+  EGPU_CUDA_TRY(ctx, A->ilu_diag.alloc(n));
+  EGPU_CUDA_TRY(ctx, A->ilu.alloc(nz));
+  EGPU_CUDA_TRY(ctx, cudaMemcpy(A->ilu_rows.p, ir.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  EGPU_CUDA_TRY(ctx, cudaMemcpy(A->ilu_cols.p, ic.data(), nz * sizeof(int), cudaMemcpyHostToDevice));
+  EGPU_CUDA_TRY(ctx, cudaMemcpy(A->ilu_diag.p, id.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+  EGPU_CUDA_TRY(ctx, cudaMemcpy(A->ilu.p, iv.data(), nz * sizeof(double), cudaMemcpyHostToDevice));
+  A->ilu_scatter.release();
+  A->ilu_in.release();
+  A->ilu_nnz = nz;
+  A->ilu_max_row = maxrow;
+  A->ilu_order = ILU_ORDER_T;
+  A->ilut_tol = tol;
+  A->ilu_valid = false;
+  A->tri_built = false;
+  const int rc = ensure_tri_schedule(A);
+  if (rc) return rc;
+  return ilu_pack(A);
+}
+
+int precond_factor(egpu_mat *A, const egpu_params *p) {
+  if (p->precond == EGPU_PREC_ILUT) return ilut_factor(A, p->ilut_tol);
+  return ilu_factor(A, p->ilu_order);
 }
 
 static void set_tri_vals(KArgs<double> &a, const egpu_mat *A) {
@@ -1011,11 +1078,13 @@ int solve_fp64(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_param
   ctx->launches += 2;
   // preconditioner (Linear System Refactorize / Precondition Recompute, IterSolve.src:413-421)
   A->solve_count++;
-  if (prm->precond == EGPU_PREC_ILU0) {
+  if (is_ilu(prm->precond)) {
     const int every = prm->precond_recompute > 0 ? prm->precond_recompute : 1;
-    if (!A->ilu_valid || A->ilu_order != prm->ilu_order ||
+    const bool ilut = prm->precond == EGPU_PREC_ILUT;
+    const int code = ilut ? ILU_ORDER_T : prm->ilu_order;
+    if (!A->ilu_valid || A->ilu_order != code || (ilut && A->ilut_tol != prm->ilut_tol) ||
         (prm->refactorize && (A->solve_count - 1) % every == 0)) {
-      rc = ilu_factor(A, prm->ilu_order);
+      rc = precond_factor(A, prm);
       if (rc) return rc;
     } else {
       rc = ensure_tri_schedule(A);
@@ -1037,7 +1106,7 @@ int solve_fp64(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_param
   a.ilu = A->ilu.p;
   a.dvals = dvals;
   set_tri(a, A);
-  a.precond = prm->precond;
+  a.precond = is_ilu(prm->precond) ? EGPU_PREC_ILU0 : prm->precond;  // ILUT applies like ILU(n)
   a.maxit = prm->max_iter;
   a.true_residual = 1;
   a.tol = prm->tol;
@@ -1194,7 +1263,7 @@ int krylov_fp64_scaled(egpu_mat *A, const double *bs, double *xs, const egpu_par
   a.ilu = A->ilu.p;
   a.dvals = A->work.p + (size_t)11 * A->ldw;
   set_tri(a, A);
-  a.precond = prm->precond;
+  a.precond = is_ilu(prm->precond) ? EGPU_PREC_ILU0 : prm->precond;  // ILUT applies like ILU(n)
   a.maxit = prm->max_iter;
   a.true_residual = 1;
   a.tol = prm->tol;
@@ -1272,9 +1341,9 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
                                                             xs, flags, sc ? 1 : 0);
   ctx->launches += 2;
   A->solve_count++;
-  const bool ilu = prm->precond == EGPU_PREC_ILU0;
+  const bool ilu = is_ilu(prm->precond);
   if (ilu) {
-    rc = ilu_factor(A, prm->ilu_order);
+    rc = precond_factor(A, prm);
     if (rc) return rc;
   }
   rc = prepare_fp32(A, ilu);
@@ -1356,7 +1425,7 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
       a.ilu = A->ilu32.p;
       a.dvals = dv32;
       set_tri(a, A);
-      a.precond = prm->precond;
+      a.precond = is_ilu(prm->precond) ? EGPU_PREC_ILU0 : prm->precond;  // ILUT applies like ILU(n)
       a.maxit = std::max(1, std::min(prm->inner_max_iter, prm->max_iter - r.iters));
       a.true_residual = 0;
       a.tol = inner_tol_of(prm);
@@ -1824,9 +1893,9 @@ extern "C" int egpu_matrix_clone(egpu_mat *proto, egpu_mat **out) {
 // the preconditioner's one-time structures ahead of the first solve (ILU0 level schedules,
 // shared with every clone of the prototype)
 extern "C" int egpu_matrix_prepare(egpu_mat *A, const egpu_params *prm) {
-  if (!A || !prm || prm->precond < EGPU_PREC_NONE || prm->precond > EGPU_PREC_ILU0) return EGPU_ERR_ARG;
+  if (!A || !prm || prm->precond < EGPU_PREC_NONE || prm->precond > EGPU_PREC_ILUT) return EGPU_ERR_ARG;
   cudaSetDevice(A->ctx->device);
-  if (prm->precond != EGPU_PREC_ILU0) return EGPU_OK;
+  if (prm->precond != EGPU_PREC_ILU0) return EGPU_OK;  // ILUT: its structure needs the values
   const int rc = egpu::ensure_ilu_structure(A, prm->ilu_order);
   if (rc) return rc;
   return egpu::ensure_tri_schedule(A);
@@ -1841,8 +1910,8 @@ extern "C" long long egpu_matrix_footprint(const egpu_mat *A, int precond) {
   b += 8 * z + 8 * zs + 4 * zs;             // scaled CRS, SELL FP64, SELL FP32
   b += 8 * n + 13 * 8 * l + 14 * 4 * l;     // DiagScaling, work vectors
   const long long zi = std::max(z, A->ilu_nnz);   // ILU structure (ILU(n) fill included once built)
-  if (precond == EGPU_PREC_ILU0) b += 8 * zi + 4 * zi + 4 * n + (zi > z ? 8 * zi : 0);  // factors, flags, scatter
-  if (precond == EGPU_PREC_ILU0) b += 12 * (A->tri.cta_lo.nent + A->tri.cta_up.nent);  // single-block layout
+  if (is_ilu(precond)) b += 8 * zi + 4 * zi + 4 * n + (zi > z ? 8 * zi : 0);  // factors, flags, scatter
+  if (is_ilu(precond)) b += 12 * (A->tri.cta_lo.nent + A->tri.cta_up.nent);  // single-block layout
   return b + 8 * n;                         // back-scaled solution
 }
 
@@ -1850,7 +1919,8 @@ static int check_params(const egpu_params *p) {
   if (!p) return EGPU_ERR_ARG;
   if (p->method < EGPU_CG || p->method > EGPU_BICGSTABL) return EGPU_ERR_ARG;
   if (p->restart < 0) return EGPU_ERR_ARG;
-  if (p->precond < EGPU_PREC_NONE || p->precond > EGPU_PREC_ILU0) return EGPU_ERR_ARG;
+  if (p->precond < EGPU_PREC_NONE || p->precond > EGPU_PREC_ILUT) return EGPU_ERR_ARG;
+  if (p->precond == EGPU_PREC_ILUT && !(p->ilut_tol >= 0.0 && p->ilut_tol < 1e300)) return EGPU_ERR_ARG;
   if (p->max_iter < 1) return EGPU_ERR_ARG;
   if (p->precision != EGPU_FP64 && p->precision != EGPU_MIXED) return EGPU_ERR_ARG;
   if (p->ilu_order < 0 || p->ilu_order > 9) return EGPU_ERR_ARG;
@@ -1973,6 +2043,21 @@ extern "C" int egpu_ilu_build(egpu_mat *A, int scale_system, int order) {
 }
 
 extern "C" int egpu_ilu0_build(egpu_mat *A, int scale_system) { return egpu_ilu_build(A, scale_system, 0); }
+
+extern "C" int egpu_ilut_build(egpu_mat *A, int scale_system, double tol) {
+  if (!A || !A->has_values) return EGPU_ERR_STATE;
+  if (!(tol >= 0.0)) return EGPU_ERR_ARG;
+  egpu_ctx *ctx = A->ctx;
+  cudaSetDevice(ctx->device);
+  int rc = egpu::reset_sync(ctx);
+  if (rc) return rc;
+  rc = egpu::scale_matrix(A, scale_system != 0);
+  if (rc) return rc;
+  rc = egpu::ilut_factor(A, tol);
+  if (rc) return rc;
+  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return EGPU_OK;
+}
 
 // the current factors on their structure, 1-based; returns the number of entries
 extern "C" int egpu_ilu_download(egpu_mat *A, int *ilu_rows, int *ilu_cols, int *ilu_diag, double *ilu_values) {

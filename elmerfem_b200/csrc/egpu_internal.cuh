@@ -189,7 +189,8 @@ struct egpu_mat {
   DevBuf<float> sell_vals32;     // scaled values (FP32)
   // ILU structure: the matrix's own pattern for ILU0, the ILU(n) fill structure otherwise
   // (0-based); the triangular-solve schedules in tri are built on it
-  int ilu_order = -1;            // order the structure was built for (-1: not yet)
+  int ilu_order = -1;            // order the structure was built for (-1: not yet, ILU_ORDER_T: ILUT)
+  double ilut_tol = 0.0;         // drop tolerance of the current ILUT factor
   long long ilu_nnz = 0;
   int ilu_max_row = 0;
   DevBuf<int> ilu_rows, ilu_cols, ilu_diag;

@@ -9,6 +9,8 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <cmath>
+#include <functional>
 #include <cstdint>
 #include <cstring>
 #include <mutex>
@@ -396,6 +398,88 @@ void egpu_ilu_structure(int n, const std::vector<int> &rows, const std::vector<i
     ocols.swap(c);
     odiag.swap(d);
   }
+}
+
+// Threshold ILU (CRS_ILUT, CRSMatrix.src:2849-3044), 0-based, on the host: the factor's
+// pattern depends on its values, so it is computed row after row as the reference does and
+// the device then runs the triangular solves on the result.  Row i: the matrix row is
+// scattered into the dense row w; its flagged columns left of the diagonal are eliminated in
+// ascending order (a min-heap holds them, fill included), w_k /= u_kk (U diagonals are
+// still un-inverted here), then w_j -= w_k * U_kj over ILU row k's U part, flagging new fill
+// whether or not w_k is zero, as the reference does.  The finished row keeps the entries
+// with |w_k| >= tol * ||A(i,:)||_2, and the diagonal, in ascending column order.  Finally the
+// U diagonal is inverted (1 where |u_ii| < AEPS).  Each entry sees the reference's updates
+// in the reference's order with separately rounded products (built with
+// -ffp-contract=off), so the factor is bit-identical.  False if a row's diagonal is absent.
+bool egpu_ilut_host(int n, const std::vector<int> &rows, const std::vector<int> &cols,
+                    const std::vector<double> &vals, double tol, std::vector<int> &ir, std::vector<int> &ic,
+                    std::vector<int> &id, std::vector<double> &iv) {
+  constexpr double AEPS = 10.0 * 2.220446049250313e-16;  // the reference's AEPS (EGPU_AEPS)
+  std::vector<double> w(n, 0.0);
+  std::vector<char> flag(n, 0);
+  std::vector<int> touched, heap;
+  ir.assign(n + 1, 0);
+  id.assign(n, -1);
+  ic.clear();
+  iv.clear();
+  ic.reserve((size_t)rows[n] * 2);
+  iv.reserve((size_t)rows[n] * 2);
+  auto push = [&](int k) {
+    heap.push_back(k);
+    std::push_heap(heap.begin(), heap.end(), std::greater<int>());
+  };
+  for (int i = 0; i < n; ++i) {
+    touched.clear();
+    for (int e = rows[i]; e < rows[i + 1]; ++e) {
+      const int c = cols[e];
+      flag[c] = 1;
+      w[c] = vals[e];
+      touched.push_back(c);
+      if (c < i) push(c);
+    }
+    while (!heap.empty()) {
+      std::pop_heap(heap.begin(), heap.end(), std::greater<int>());
+      const int k = heap.back();
+      heap.pop_back();
+      const double ukk = iv[id[k]];
+      if (std::fabs(ukk) > AEPS) w[k] = w[k] / ukk;
+      const double mk = w[k];
+      for (int l = id[k] + 1; l < ir[k + 1]; ++l) {
+        const int j = ic[l];
+        if (!flag[j]) {
+          flag[j] = 1;
+          touched.push_back(j);
+          if (j < i) push(j);
+        }
+        const double prod = mk * iv[l];
+        w[j] = w[j] - prod;
+      }
+    }
+    double sq = 0.0;
+    for (int e = rows[i]; e < rows[i + 1]; ++e) {
+      const double a = std::fabs(vals[e]);
+      const double a2 = a * a;
+      sq = sq + a2;
+    }
+    const double drop = tol * std::sqrt(sq);
+    std::sort(touched.begin(), touched.end());
+    for (int k : touched) {
+      if (std::fabs(w[k]) >= drop || k == i) {
+        if (k == i) id[i] = (int)ic.size();
+        ic.push_back(k);
+        iv.push_back(w[k]);
+      }
+      w[k] = 0.0;
+      flag[k] = 0;
+    }
+    if (id[i] < 0) return false;
+    ir[i + 1] = (int)ic.size();
+  }
+  for (int i = 0; i < n; ++i) {
+    double &d = iv[id[i]];
+    d = std::fabs(d) < AEPS ? 1.0 : 1.0 / d;
+  }
+  return true;
 }
 
 extern "C" long long egpu_ilu_pattern(int n, const int *rows, const int *cols, const int *diag, int order,

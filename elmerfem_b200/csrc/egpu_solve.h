@@ -8,6 +8,11 @@ void egpu_ilu_structure(int n, const std::vector<int> &rows, const std::vector<i
                         const std::vector<int> &diag, int order, std::vector<int> &orows, std::vector<int> &ocols,
                         std::vector<int> &odiag);
 
+// threshold ILU factors on the host (egpu_pattern.cpp), 0-based, inverted U diagonal
+bool egpu_ilut_host(int n, const std::vector<int> &rows, const std::vector<int> &cols,
+                    const std::vector<double> &vals, double tol, std::vector<int> &ir, std::vector<int> &ic,
+                    std::vector<int> &id, std::vector<double> &iv);
+
 namespace egpu {
 
 // inner tolerance of one FP32 segment of the mixed-precision solve; 0 picks it by
@@ -17,7 +22,7 @@ namespace egpu {
 // FP64) and 3e-2 with ILU0 (BiCGStab 32^3: 19 against 19).
 inline double inner_tol_of(const egpu_params *p) {
   if (p->inner_tol > 0) return p->inner_tol;
-  return p->precond == EGPU_PREC_ILU0 ? 3e-2 : 1e-2;
+  return (p->precond == EGPU_PREC_ILU0 || p->precond == EGPU_PREC_ILUT) ? 3e-2 : 1e-2;
 }
 
 int ensure_ctx_scratch(egpu_ctx *ctx);
@@ -26,6 +31,12 @@ int scale_matrix(egpu_mat *A, bool scale_system);
 int ensure_ilu_structure(egpu_mat *A, int order);
 int ensure_tri_schedule(egpu_mat *A);
 int ilu_factor(egpu_mat *A, int order);
+// the ILU structure code of threshold ILU (A->ilu_order; ILU(n) uses 0..9)
+constexpr int ILU_ORDER_T = 100;
+inline bool is_ilu(int precond) { return precond == EGPU_PREC_ILU0 || precond == EGPU_PREC_ILUT; }
+int ilut_factor(egpu_mat *A, double tol);
+// the factor the parameters ask for: ILU(n) or ILUT
+int precond_factor(egpu_mat *A, const egpu_params *p);
 int solve_fp64(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_params *prm,
                egpu_result *res);
 int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_params *prm,

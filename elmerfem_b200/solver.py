@@ -16,7 +16,8 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from ._lib import BICGSTAB, BICGSTABL, CG, FP64, GCR, MIXED, PREC_DIAGONAL, PREC_ILU0, PREC_NONE, LibError, check, lib
+from ._lib import (BICGSTAB, BICGSTABL, CG, FP64, GCR, MIXED, PREC_DIAGONAL, PREC_ILU0, PREC_ILUT, PREC_NONE, LibError,
+                   check, lib)
 
 
 class NotConverged(RuntimeError):
@@ -106,11 +107,13 @@ class SolverParams:
     symmetric: bool = False
     ilu_order: int = 0            # ILU(n) with precond PREC_ILU0 (Linear System ILU Order)
     restart: int = 0              # GCR restart (0: max_iter) / BiCGStab(l) degree (0: 2)
+    ilut_tol: float = 0.0         # drop tolerance with precond PREC_ILUT (Linear System ILUT Tolerance)
 
     def to_c(self) -> _lib.Params:
         return _lib.Params(self.method, self.precond, self.max_iter, self.tol, int(self.scale_system),
                            self.precision, int(self.refactorize), self.precond_recompute, self.inner_tol,
-                           self.inner_max_iter, self.max_refinements, self.ilu_order, self.restart)
+                           self.inner_max_iter, self.max_refinements, self.ilu_order, self.restart,
+                           float(self.ilut_tol))
 
     @classmethod
     def from_sif(cls, keywords) -> "SolverParams":
@@ -125,11 +128,18 @@ class SolverParams:
             raise NotImplementedError(f"Linear System Iterative Method = {meth}")
         prec = str(kw.get("linear system preconditioning", "none")).lower()
         ilu_n = 0
+        ilut_tol = 0.0
         if prec.startswith("none"):
             pc = PREC_NONE
         elif prec.startswith("diagonal"):
             pc = PREC_DIAGONAL
-        elif prec.startswith("ilu") and not prec.startswith("ilut"):
+        elif prec.startswith("ilut"):
+            # IterSolve.src:384-388: ListGetCReal returns 0 when the keyword is absent
+            ilut_tol = float(kw.get("linear system ilut tolerance", 0.0))
+            if not ilut_tol >= 0.0:
+                raise ValueError(f"Linear System ILUT Tolerance {ilut_tol} < 0")
+            pc = PREC_ILUT
+        elif prec.startswith("ilu"):
             # IterSolve.src: "ILU<n>" or "ILU" with Linear System ILU Order
             order = kw.get("linear system ilu order")
             ilu_n = int(round(float(order))) if order is not None else (int(prec[3]) if len(prec) > 3 and prec[3].isdigit() else 0)
@@ -150,7 +160,7 @@ class SolverParams:
             if restart < 2:
                 raise ValueError("BiCGstabl polynomial degree < 2")
         p = cls(method=methods[meth], precond=pc, restart=restart,
-                ilu_order=ilu_n if pc == PREC_ILU0 else 0,
+                ilu_order=ilu_n if pc == PREC_ILU0 else 0, ilut_tol=ilut_tol,
                 max_iter=int(kw["linear system max iterations"]),
                 tol=float(kw["linear system convergence tolerance"]),
                 scale_system=_bool(kw.get("linear system scaling", True)),
@@ -278,6 +288,11 @@ class Matrix:
         check(lib().egpu_tri_info(self._h, info.ctypes.data), self.ctx.handle, "egpu_tri_info")
         return {"node_block": int(info[0]), "lower_levels": int(info[1]), "upper_levels": int(info[2]),
                 "max_width": int(info[3]), "single_block_fp64": bool(info[4]), "single_block_fp32": bool(info[5])}
+
+    def ilut(self, tol: float, scale_system: bool = True):
+        """CRS_ILUT on the (scaled) matrix: (rows, cols, diag 1-based, values with inverted U diagonal)."""
+        check(lib().egpu_ilut_build(self._h, int(scale_system), float(tol)), self.ctx.handle, "egpu_ilut_build")
+        return self.ilu_factors()
 
     def ilu0(self, scale_system: bool = True):
         """Factor ILU0 on the device; returns (ILUValues with inverted U diagonal, DiagScaling)."""

@@ -44,7 +44,9 @@ extern "C" {
 
 /* ---- keyword surface (IterSolve.src:221-420) ------------------------------------ */
 enum { EGPU_CG = 1, EGPU_BICGSTAB = 2, EGPU_GCR = 3, EGPU_BICGSTABL = 4 }; /* Linear System Iterative Method */
-enum { EGPU_PREC_NONE = 0, EGPU_PREC_DIAGONAL = 1, EGPU_PREC_ILU0 = 2 }; /* Linear System Preconditioning */
+/* Linear System Preconditioning: None, Diagonal, ILU0 / ILUn (with ilu_order), ILUT (with
+ * ilut_tol; IterSolve.src:384-388, CRS_ILUT CRSMatrix.src:2849-3044) */
+enum { EGPU_PREC_NONE = 0, EGPU_PREC_DIAGONAL = 1, EGPU_PREC_ILU0 = 2, EGPU_PREC_ILUT = 3 };
 enum { EGPU_FP64 = 0, EGPU_MIXED = 1 };  /* FP64 drop-in | FP32 inner Krylov in FP64 refinement */
 
 typedef struct {
@@ -70,6 +72,12 @@ typedef struct {
    * EGPU_BICGSTABL: BiCGstabl polynomial degree (0: 2, :306-310).  Both run in FP64 whatever
    * the precision, stopping on the recursive residual as the reference's internal methods do. */
   int restart;
+  /* EGPU_PREC_ILUT: Linear System ILUT Tolerance (0 when absent, as in the reference: no entry
+   * dropped).  Entries with |ILU(i,j)| < tol * ||A(i,:)||_2 are dropped after the row's full
+   * elimination.  The factor's structure depends on the values, so it is computed on the host
+   * (as the reference does) and applied on the device; not available to cloned matrices
+   * (batches, the server). */
+  double ilut_tol;
 } egpu_params;
 
 typedef struct {
@@ -150,6 +158,10 @@ int egpu_ilu_build(egpu_mat *A, int scale_system, int order);
  * entries; ilu_rows (n+1), ilu_cols and ilu_diag (n) are written when cap >= it. */
 long long egpu_ilu_pattern(int n, const int *rows, const int *cols, const int *diag, int order, long long cap,
                            int *ilu_rows, int *ilu_cols, int *ilu_diag);
+/* threshold ILU (CRS_ILUT, CRSMatrix.src:2849-3044) of the (optionally scaled) matrix: host
+ * factorisation, device schedules and packed factors as for ILU(n); egpu_ilu_download reads
+ * the result */
+int egpu_ilut_build(egpu_mat *A, int scale_system, double tol);
 /* the matrix's current ILU factors on their structure (1-based, as egpu_ilu_pattern
  * returns it), inverted U diagonal; NULL arrays are skipped.  Returns the number of entries. */
 int egpu_ilu_download(egpu_mat *A, int *ilu_rows, int *ilu_cols, int *ilu_diag, double *ilu_values);

@@ -18,7 +18,7 @@ _LIB_PATH = os.path.join(_HERE, "_build", "libelmer_oracle.so")
 _lib = None
 
 CG, BICGSTAB, GCR, BICGSTABL = 1, 2, 3, 4
-PREC_NONE, PREC_DIAGONAL, PREC_ILU0 = 0, 1, 2
+PREC_NONE, PREC_DIAGONAL, PREC_ILU0, PREC_ILUT = 0, 1, 2, 3
 
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -27,7 +27,7 @@ _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 class _Params(C.Structure):
     _fields_ = [("method", C.c_int), ("precond", C.c_int), ("max_iter", C.c_int),
                 ("tol", C.c_double), ("scale_system", C.c_int), ("omp_threads", C.c_int),
-                ("ilu_order", C.c_int), ("restart", C.c_int)]
+                ("ilu_order", C.c_int), ("restart", C.c_int), ("ilut_tol", C.c_double)]
 
 
 class _Result(C.Structure):
@@ -69,6 +69,9 @@ def lib():
         L.orc_ilu_pattern.argtypes = [C.c_int, _i32p, _i32p, _i32p, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p,
                                       C.c_void_p]
         L.orc_iluk.argtypes = [C.c_int, _i32p, _i32p, _f64p, _i32p, _i32p, _i32p, _f64p]
+        L.orc_ilut.restype = C.c_longlong
+        L.orc_ilut.argtypes = [C.c_int, _i32p, _i32p, _f64p, C.c_double, C.c_longlong, C.c_void_p, C.c_void_p,
+                               C.c_void_p, C.c_void_p]
         L.orc_scale.argtypes = [C.c_int, _i32p, _i32p, _i32p, _f64p, C.c_void_p, C.c_void_p,
                                 _f64p, C.POINTER(C.c_double), C.c_int]
         L.orc_compute_norm.restype = C.c_double
@@ -149,9 +152,9 @@ def dirichlet(pat: Pattern, values, rhs, con_rows, con_vals=None, symmetric=Fals
 
 
 def solve(pat: Pattern, values, b, method=BICGSTAB, precond=PREC_ILU0, max_iter=1000, tol=1e-10,
-          x0=None, scale=True, threads=0, ilu_order=0, restart=0):
+          x0=None, scale=True, threads=0, ilu_order=0, restart=0, ilut_tol=0.0):
     x = np.zeros(pat.n) if x0 is None else np.array(x0, dtype=np.float64)
-    p = _Params(method, precond, max_iter, tol, int(scale), threads, ilu_order, restart)
+    p = _Params(method, precond, max_iter, tol, int(scale), threads, ilu_order, restart, ilut_tol)
     r = _Result()
     lib().orc_solve(pat.n, pat.rows, pat.cols, pat.diag, np.ascontiguousarray(values, np.float64),
                     np.ascontiguousarray(b, np.float64), x, C.byref(p), C.byref(r))
@@ -187,6 +190,26 @@ def iluk(pat: Pattern, values, order: int):
     out = np.zeros(c.size)
     lib().orc_iluk(pat.n, pat.rows, pat.cols, np.ascontiguousarray(values, np.float64), r, c, d, out)
     return r, c, d, out
+
+
+def ilut(pat: Pattern, values, tol: float):
+    """CRS_ILUT factors (threshold ILU): (rows, cols, diag, values), 1-based, inverted U diagonal."""
+    v = np.ascontiguousarray(values, np.float64)
+    nz = lib().orc_ilut(pat.n, pat.rows, pat.cols, v, float(tol), 0, None, None, None, None)
+    if nz < 0:
+        raise ValueError("ILUT: a row's diagonal is missing")
+    r, c, d, out = np.zeros(pat.n + 1, np.int32), np.zeros(nz, np.int32), np.zeros(pat.n, np.int32), np.zeros(nz)
+    lib().orc_ilut(pat.n, pat.rows, pat.cols, v, float(tol), nz, r.ctypes.data, c.ctypes.data, d.ctypes.data,
+                   out.ctypes.data)
+    return r, c, d, out
+
+
+def lusolve_on(rows, cols, diag, ilu, b):
+    """CRS_LUPrecondition on a factor with its own structure (ILU(n), ILUT), 1-based arrays."""
+    x = np.array(b, dtype=np.float64)
+    lib().orc_lusolve(len(diag), np.ascontiguousarray(rows, np.int32), np.ascontiguousarray(cols, np.int32),
+                      np.ascontiguousarray(diag, np.int32), np.ascontiguousarray(ilu, np.float64), x)
+    return x
 
 
 def lusolve(pat: Pattern, ilu, b):

@@ -984,6 +984,85 @@ extern "C" void orc_iluk(int n, const int *rows, const int *cols, const double *
   }
 }
 
+// CRS_ILUT / ComputeILUT, CRSMatrix.src:2849-3044.  Row i: the matrix row enters the dense
+// row S with its flags C; k runs from the row's first column RowMin to i-1 over the flagged
+// entries (fill included): S(k) /= u_kk (the U diagonal is still un-inverted while rows are
+// factored), then every U entry j of ILU row k is flagged and S(j) -= S(k) * U(k,j)
+// (:2944-2959: flags and updates do not test S(k) for zero).  The finished row keeps, in
+// ascending column order, the entries with |S(k)| >= TOL * ||A(i,:)||_2 and the diagonal
+// (:2961-2979).  Afterwards every U diagonal is inverted (1 if |u_ii| < AEPS, :3023-3030).
+// Output 1-based; returns false if a row's diagonal never enters the factor.
+static bool ilut_rows(int n, const int *rows, const int *cols, const double *values, double tol,
+                      std::vector<int> &ir, std::vector<int> &ic, std::vector<int> &id, std::vector<double> &iv) {
+  std::vector<double> S(n + 1, 0.0);
+  std::vector<char> C(n + 1, 0);
+  ir.assign(n + 1, 0);
+  id.assign(n, 0);
+  ic.clear();
+  iv.clear();
+  ir[0] = 1;
+  for (int i = 1; i <= n; ++i) {
+    for (int k = rows[i - 1]; k <= rows[i] - 1; ++k) {
+      C[cols[k - 1]] = 1;
+      S[cols[k - 1]] = values[k - 1];
+    }
+    const int rowmin = cols[rows[i - 1] - 1];
+    int rowmax = cols[rows[i] - 2];
+    for (int k = rowmin; k <= i - 1; ++k) {
+      if (!C[k]) continue;
+      const double ukk = iv[id[k - 1] - 1];
+      if (std::fabs(ukk) > AEPS) S[k] = S[k] / ukk;
+      for (int l = id[k - 1] + 1; l <= ir[k] - 1; ++l) {
+        const int j = ic[l - 1];
+        if (!C[j]) {
+          C[j] = 1;
+          rowmax = std::max(rowmax, j);
+        }
+        S[j] = S[j] - S[k] * iv[l - 1];
+      }
+    }
+    double sq = 0.0;
+    for (int k = rows[i - 1]; k <= rows[i] - 1; ++k) sq = sq + std::fabs(values[k - 1]) * std::fabs(values[k - 1]);
+    const double norma = std::sqrt(sq);
+    bool has_diag = false;
+    for (int k = rowmin; k <= rowmax; ++k) {
+      if (!C[k]) continue;
+      if (std::fabs(S[k]) >= tol * norma || k == i) {
+        ic.push_back(k);
+        iv.push_back(S[k]);
+        if (k == i) {
+          id[i - 1] = (int)ic.size();
+          has_diag = true;
+        }
+      }
+      S[k] = 0.0;
+      C[k] = 0;
+    }
+    if (!has_diag) return false;
+    ir[i] = (int)ic.size() + 1;
+  }
+  for (int i = 1; i <= n; ++i) {
+    double &dv = iv[id[i - 1] - 1];
+    dv = std::fabs(dv) < AEPS ? 1.0 : 1.0 / dv;
+  }
+  return true;
+}
+
+extern "C" long long orc_ilut(int n, const int *rows, const int *cols, const double *values, double tol,
+                              long long cap, int *ilu_rows, int *ilu_cols, int *ilu_diag, double *ilu_values) {
+  std::vector<int> ir, ic, id;
+  std::vector<double> iv;
+  if (!ilut_rows(n, rows, cols, values, tol, ir, ic, id, iv)) return -1;
+  const long long nz = (long long)ic.size();
+  if (cap >= nz && ilu_rows) {
+    std::copy(ir.begin(), ir.end(), ilu_rows);
+    std::copy(ic.begin(), ic.end(), ilu_cols);
+    std::copy(id.begin(), id.end(), ilu_diag);
+    std::copy(iv.begin(), iv.end(), ilu_values);
+  }
+  return nz;
+}
+
 extern "C" int orc_lower_levels(int n, const int *rows, const int *cols, const int *diag, int *level) {
   int maxl = 0;
   for (int i = 1; i <= n; ++i) {
@@ -1425,9 +1504,16 @@ extern "C" int orc_solve(int n, const int *rows, const int *cols, const int *dia
   } else if (prm->precond == ORC_PREC_ILU0) {
     ilu.assign(values.size(), 0.0);
     orc_ilu0(n, rows, cols, diag, values.data(), ilu.data());
+  } else if (prm->precond == ORC_PREC_ILUT) {  // CRS_ILUT(A, Linear System ILUT Tolerance)
+    if (!ilut_rows(n, rows, cols, values.data(), prm->ilut_tol, ir, ic, id, ilu)) return -1;
+    irows = ir.data();
+    icols = ic.data();
+    idiag = id.data();
   }
   r.seconds_precond_setup = now() - tp;
-  Ctx c{n, rows, cols, diag, values.data(), ilu.empty() ? nullptr : ilu.data(), prm->precond,
+  // ILUT is applied by the same CRS_LUPrecondition as ILU(n), on its own structure
+  const int apply = prm->precond == ORC_PREC_ILUT ? ORC_PREC_ILU0 : prm->precond;
+  Ctx c{n, rows, cols, diag, values.data(), ilu.empty() ? nullptr : ilu.data(), apply,
         prm->omp_threads, irows, icols, idiag};
   if (prm->method == ORC_CG)
     r.info = huti_cg(c, x, b.data(), prm->max_iter, prm->tol, &r.iters, &r.residual);

@@ -46,7 +46,7 @@ void orc_dirichlet(int n, const int *rows, const int *cols, const int *diag, dou
 
 /* ---- linear solve (SolveLinearSystem -> IterSolver -> HUTI) */
 enum { ORC_CG = 1, ORC_BICGSTAB = 2, ORC_GCR = 3, ORC_BICGSTABL = 4 };
-enum { ORC_PREC_NONE = 0, ORC_PREC_DIAGONAL = 1, ORC_PREC_ILU0 = 2 };
+enum { ORC_PREC_NONE = 0, ORC_PREC_DIAGONAL = 1, ORC_PREC_ILU0 = 2, ORC_PREC_ILUT = 3 };
 typedef struct {
   int method;          /* ORC_CG | ORC_BICGSTAB */
   int precond;         /* ORC_PREC_* */
@@ -56,6 +56,7 @@ typedef struct {
   int omp_threads;     /* threads for the SpMV loop (CRSMatrix.src:3565), <=0: all */
   int ilu_order;       /* ORC_PREC_ILU0 with ilu_order n > 0: ILU(n) (Linear System ILU Order) */
   int restart;         /* GCR: Linear System GCR Restart (0: Max Iterations); BiCGStab(l): degree l */
+  double ilut_tol;     /* ORC_PREC_ILUT: Linear System ILUT Tolerance (0 when absent, as ListGetCReal) */
 } orc_params;
 typedef struct {
   int info;            /* HUTI status code (huti_fdefs.h) */
@@ -87,6 +88,11 @@ long long orc_ilu_pattern(int n, const int *rows, const int *cols, const int *di
  * kept; inverted U diagonal (:2359-2366). */
 void orc_iluk(int n, const int *rows, const int *cols, const double *values, const int *ilu_rows,
               const int *ilu_cols, const int *ilu_diag, double *ilu_values);
+/* CRS_ILUT (CRSMatrix.src:2849-3044): threshold ILU with the drop test
+ * |ILU(i,j)| >= tol * ||A(i,:)||_2 after the row's full elimination; inverted U diagonal.
+ * 1-based output, written when cap >= the returned entry count; -1 if a row has no diagonal. */
+long long orc_ilut(int n, const int *rows, const int *cols, const double *values, double tol, long long cap,
+                   int *ilu_rows, int *ilu_cols, int *ilu_diag, double *ilu_values);
 void orc_scale(int n, const int *rows, const int *cols, const int *diag, double *values,
                double *b, double *x, double *diag_scaling, double *rhs_scaling, int rhs_scale);
 double orc_compute_norm(int n, const double *x);

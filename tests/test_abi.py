@@ -84,8 +84,21 @@ def test_sif_ilu_order():
     assert eg.SolverParams.from_sif(dict(base, **{"Linear System Preconditioning": "ILU0"})).ilu_order == 0
 
 
+def test_sif_ilut():
+    base = {"Linear System Max Iterations": 10, "Linear System Convergence Tolerance": 1e-6}
+    p = eg.SolverParams.from_sif(dict(base, **{"Linear System Preconditioning": "ILUT",
+                                               "Linear System ILUT Tolerance": 1e-3}))
+    assert (p.precond, p.ilut_tol, p.ilu_order) == (eg.PREC_ILUT, 1e-3, 0)
+    # absent tolerance: 0 (ListGetCReal's default), nothing dropped
+    assert eg.SolverParams.from_sif(dict(base, **{"Linear System Preconditioning": "ILUT"})).ilut_tol == 0.0
+    assert p.to_c().ilut_tol == 1e-3
+    with pytest.raises(ValueError):
+        eg.SolverParams.from_sif(dict(base, **{"Linear System Preconditioning": "ILUT",
+                                               "Linear System ILUT Tolerance": -1}))
+
+
 @pytest.mark.parametrize("bad", [{"Linear System Solver": "Direct"}, {"Linear System Iterative Method": "GMRES"},
-                                 {"Linear System Preconditioning": "ILUT"}])
+                                 {"Linear System Preconditioning": "BILU1"}])
 def test_sif_outside_the_path(bad):
     kw = {"Linear System Max Iterations": 10, "Linear System Convergence Tolerance": 1e-6}
     kw.update(bad)
