@@ -1219,7 +1219,7 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstab_kernel(KArgs<VT> a) {
           vld<W>(V, i, v);
 #pragma unroll
           for (int q = 0; q < W; ++q) {
-            sv[q] = r[q] - al * v[q];
+            sv[q] = row_msub(r[q], al, v[q]);  // S = R - alpha V, rounded as HUTI
             acc[0] += (double)sv[q] * (double)sv[q];
             SLO[a.pos_lo[i + q]] = sv[q];
           }
@@ -1232,7 +1232,7 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstab_kernel(KArgs<VT> a) {
       } else {
         if (ilu) {
           lower_solve<VT, LPR>(a, Y2, [&](int i) {
-            const VT s = R[i] - al * V[i];
+            const VT s = row_msub(R[i], al, V[i]);
             S[i] = s;
             acc[0] += (double)s * (double)s;
             return s;
@@ -1247,7 +1247,7 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstab_kernel(KArgs<VT> a) {
             if (jac) vld<W>(a.dvals, i, d);
 #pragma unroll
             for (int q = 0; q < W; ++q) {
-              sv[q] = r[q] - al * v[q];
+              sv[q] = row_msub(r[q], al, v[q]);  // S = R - alpha V, rounded as HUTI
               acc[0] += (double)sv[q] * (double)sv[q];
               t[q] = jac ? diag_prec(sv[q], d[q]) : sv[q];
             }

@@ -174,3 +174,21 @@ def test_node_block_solves(ctx, monkeypatch, name, method, precision):
     if precision == "fp64":
         assert abs(r["iters"] - r_ref["iters"]) <= 1, (r["iters"], r_ref["iters"])
     assert rel(x, x_ref) < 1e-8
+
+
+def test_node_block_lu_precondition_elastic32(ctx, monkeypatch):
+    """3-DOF elasticity 32^3 (107,811 rows) on the schedule the cost model picks by itself (node
+    blocks); also the case the node-block apply profile is captured on."""
+    monkeypatch.delenv("EGPU_TRI_NODE_BLOCKS", raising=False)
+    monkeypatch.delenv("EGPU_TRI_MODE", raising=False)
+    p, _, _, v, _, _ = elastic_problem(meshgen.hex_cube(32))
+    A = eg.Matrix(ctx, _pat(p), v)
+    ilu, _ = A.ilu0(scale_system=True)
+    assert A.tri_info()["node_block"] == 3
+    vs = v.copy()
+    oracle.scale(p, vs)
+    ref = oracle.ilu0(p, vs)
+    assert np.array_equal(ilu, ref)
+    b = np.random.default_rng(7).standard_normal(p.n)
+    u = A.lu_precondition(b)
+    assert rel(u, oracle.lusolve(p, ref, b)) < 1e-13
