@@ -1291,6 +1291,14 @@ int krylov_fp64_scaled(egpu_mat *A, const double *bs, double *xs, const egpu_par
 
 // FP32 copies of the scaled matrix, its diagonal and the ILU0 factors; int16 column
 // offsets when every |col - row| < 32768.
+// entries of d that are not exactly 1.0f (the scaled matrix's diagonal in FP32)
+__global__ void k_count_not_one(const float *__restrict__ d, int n, unsigned int *cnt) {
+  unsigned int c = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) c += d[i] != 1.0f;
+  for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(cnt, c);
+}
+
 static int prepare_fp32(egpu_mat *A, bool with_ilu) {
   egpu_ctx *ctx = A->ctx;
   const int n = A->n;
@@ -1348,13 +1356,21 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
   }
   rc = prepare_fp32(A, ilu);
   if (rc) return rc;
-  EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
-  unsigned int hflags = 0;
-  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(&hflags, flags, sizeof(hflags), cudaMemcpyDeviceToHost, ctx->stream));
-  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-  egpu_result r{};
   float *W32 = A->work32.p;
   float *r32 = W32 + (size_t)10 * ldw, *d32 = W32 + (size_t)11 * ldw, *dv32 = W32 + (size_t)13 * ldw;
+  // Jacobi on a diagonal that is 1.0f everywhere (the symmetric scaling makes |a_ii| one up to
+  // rounding) is the identity in FP32: the inner CG then keeps no separate Z (bit-identical)
+  if (prm->precond == EGPU_PREC_DIAGONAL) {
+    k_count_not_one<<<std::min(grid_for(ctx, n), 1024), 256, 0, ctx->stream>>>(dv32, n, flags + 1);
+    ctx->launches++;
+  }
+  EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+  unsigned int hf[2] = {0, 1};
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  const unsigned int hflags = hf[0];
+  const bool unit_diag = prm->precond == EGPU_PREC_DIAGONAL && hf[1] == 0;
+  egpu_result r{};
   double *norms = (double *)(ctx->sync.p + 32);
   const int lpr = pick_lpr(A);
   const int rgrid = std::min(1024, (int)std::min<long long>(((long long)n * lpr + EGPU_BLOCK - 1) / EGPU_BLOCK,
@@ -1424,6 +1440,7 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
       set_sell(a, A, A->sell_vals32.p, A->sell_c16.p != nullptr);
       a.ilu = A->ilu32.p;
       a.dvals = dv32;
+      a.unit_diag = unit_diag ? 1 : 0;
       set_tri(a, A);
       a.precond = is_ilu(prm->precond) ? EGPU_PREC_ILU0 : prm->precond;  // ILUT applies like ILU(n)
       a.maxit = std::max(1, std::min(prm->inner_max_iter, prm->max_iter - r.iters));

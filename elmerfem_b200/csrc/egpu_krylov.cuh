@@ -56,6 +56,8 @@ struct KArgs {
   const unsigned int *skip;       // bit 1 set: zero right-hand side, return at once
   int tri_per_block;              // sub-warps per block taking part in the triangular solves
   int tri_bs;                     // rows per sync-free slot group (node blocks; 1 = row per slot)
+  int unit_diag;                  // FP32 inner CG: every diagonal of the scaled matrix is 1.0f, so the
+                                  // Jacobi step is the identity (Z is R, no diagonal loads)
   // ILU0 factors packed in solve order (see TriSchedule)
   const int *lo_ptr, *lo_cols, *up_ptr, *up_cols;
   const VT *lo_vals, *up_vals, *up_dinv;
@@ -788,10 +790,12 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) cg_kernel(KArgs<VT> a) {
   const int n = a.n;
 
   const int nb = gridDim.x;
-  VT *X = a.x, *R = a.w, *Z = a.w + a.ldw, *P = a.w + 2 * a.ldw, *Q = a.w + 3 * a.ldw,
+  const bool ilu = a.precond == EGPU_PREC_ILU0;
+  // FP32 inner solve with M = I (no preconditioner, or Jacobi on a unit diagonal): Z is R
+  const bool zr = sizeof(VT) == 4 && !a.true_residual && !ilu && (a.precond == EGPU_PREC_NONE || a.unit_diag);
+  VT *X = a.x, *R = a.w, *Z = zr ? a.w : a.w + a.ldw, *P = a.w + 2 * a.ldw, *Q = a.w + 3 * a.ldw,
      *Y = a.w + 4 * a.ldw;
   const VT *B = a.b;
-  const bool ilu = a.precond == EGPU_PREC_ILU0;
   const bool cta = ilu && a.tri_cta;  // block 0 runs the ILU0 solves level-synchronously
   const VT SENT = Sentinel<VT>::value();
   // level-synchronous mode: R in lower / upper slot order, y in upper slot order
@@ -852,7 +856,7 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) cg_kernel(KArgs<VT> a) {
       lower_solve<VT, LPR>(a, Y, [&](int i) { return R[i]; });
       upper_solve<VT, LPR>(a, Y, Z, [&](int i, VT zi) { acc[0] += (double)R[i] * (double)zi; });
     } else {
-      const bool jac = a.precond == EGPU_PREC_DIAGONAL;
+      const bool jac = a.precond == EGPU_PREC_DIAGONAL && !zr;
       vec_loop<VT>(n, [&](int i, auto w) {
         constexpr int W = decltype(w)::value;
         VT r[W], d[W], z[W];
@@ -863,7 +867,7 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) cg_kernel(KArgs<VT> a) {
           z[k] = jac ? diag_prec(r[k], d[k]) : r[k];
           acc[0] += (double)r[k] * (double)z[k];
         }
-        vst<W>(Z, i, z);
+        if (!zr) vst<W>(Z, i, z);
       });
     }
     block_sum<1>(acc, sm);
@@ -978,7 +982,7 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) cg_kernel(KArgs<VT> a) {
             acc[1] += (double)r * (double)r;
           });
         } else {
-          const bool jac = a.precond == EGPU_PREC_DIAGONAL;
+          const bool jac = a.precond == EGPU_PREC_DIAGONAL && !zr;
           vec_loop<VT>(n, [&](int i, auto w) {
             constexpr int W = decltype(w)::value;
             VT x[W], p[W], r[W], q[W], d[W], z[W];
@@ -997,7 +1001,7 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) cg_kernel(KArgs<VT> a) {
             }
             vst<W>(X, i, x);
             vst<W>(R, i, r);
-            vst<W>(Z, i, z);
+            if (!zr) vst<W>(Z, i, z);
           });
         }
         block_sum<2>(acc, sm);
