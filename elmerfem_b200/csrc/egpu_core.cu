@@ -1302,14 +1302,12 @@ __global__ void k_count_not_one(const float *__restrict__ d, int n, unsigned int
 static int prepare_fp32(egpu_mat *A, bool with_ilu) {
   egpu_ctx *ctx = A->ctx;
   const int n = A->n;
-  EGPU_CUDA_TRY(ctx, A->scaled32.alloc(A->nnz));
-  k_to_f32<<<grid_for(ctx, A->nnz), 256, 0, ctx->stream>>>(A->scaled.p, A->scaled32.p, A->nnz);
   EGPU_CUDA_TRY(ctx, A->work32.alloc((size_t)14 * A->ldw));
   k_to_f32<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(A->work.p + (size_t)11 * A->ldw,
                                                        A->work32.p + (size_t)13 * A->ldw, n);
   EGPU_CUDA_TRY(ctx, A->sell_vals32.alloc(A->sell_nnz));
   k_to_f32<<<grid_for(ctx, A->sell_nnz), 256, 0, ctx->stream>>>(A->sell_vals.p, A->sell_vals32.p, A->sell_nnz);
-  ctx->launches += 3;
+  ctx->launches += 2;
   if (with_ilu) {
     EGPU_CUDA_TRY(ctx, A->ilu32.alloc(A->ilu_nnz));
     k_to_f32<<<grid_for(ctx, A->ilu_nnz), 256, 0, ctx->stream>>>(A->ilu.p, A->ilu32.p, A->ilu_nnz);
@@ -1436,7 +1434,7 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
       a.cols = A->cols.p;
       a.diag = A->diag.p;
       a.cols16 = A->cols16.p;
-      a.vals = A->scaled32.p;
+      a.vals = nullptr;  // the FP32 kernels read the SELL copy only
       set_sell(a, A, A->sell_vals32.p, A->sell_c16.p != nullptr);
       a.ilu = A->ilu32.p;
       a.dvals = dv32;

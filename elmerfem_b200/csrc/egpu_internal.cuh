@@ -167,7 +167,7 @@ struct egpu_mat {
   DevBuf<double> scaled;         // D A D
   DevBuf<double> dscale;         // DiagScaling (times the rhs norm during a solve)
   DevBuf<double> ilu;            // ILU0 values on the scaled matrix, inverted U diagonal
-  DevBuf<float> scaled32, ilu32; // FP32 copies for the mixed-precision inner solver
+  DevBuf<float> ilu32;           // FP32 factor copy for the mixed-precision inner solver
   DevBuf<double> lo_vals, up_vals, up_dinv;        // ILU0 factors packed in solve order
   DevBuf<float> lo_vals32, up_vals32, up_dinv32;
   DevBuf<double> cta_lo_vals, cta_up_vals;        // the factors in the level-synchronous ELL layout
