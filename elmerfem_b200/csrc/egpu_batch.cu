@@ -73,6 +73,68 @@ __device__ __forceinline__ void batch_slices(const BatchShared &sh, F &&f) {
   }
 }
 
+// batch_slices for the SpMV phases: lane 0 also prefetches into L2 the values and column
+// offsets of the slice this warp takes next (one bulk request each; slices start at
+// multiples of 32 entries, so both requests are 16-byte aligned and sized), while the
+// current one is summed.  The next slice's position is loaded one slice earlier still, so
+// the request never waits for it.  Slices of systems that do not run are not prefetched.
+struct SliceMeta {
+  const void *vals, *cols;
+  unsigned vbytes, cbytes;
+};
+
+__device__ __forceinline__ int batch_locate(const BatchShared &sh, int q) {
+  int l = 0, r = sh.nact - 1;
+  while (l < r) {
+    const int m = (l + r + 1) >> 1;
+    if (sh.pre[m] <= q)
+      l = m;
+    else
+      r = m - 1;
+  }
+  return l;
+}
+
+__device__ __forceinline__ SliceMeta batch_slice_meta(const BatchArgs &ba, const BatchShared &sh, int q, int hi) {
+  SliceMeta m{nullptr, nullptr, 0u, 0u};
+  if (q >= hi) return m;
+  const int a = batch_locate(sh, q);
+  const int s = sh.act[a];
+  if (sh.status[s] != ST_RUN) return m;
+  const SysDesc &d = ba.sys[s];
+  const int sl = q - sh.pre[a];
+  if (sl < 0 || sl >= d.nslices) return m;
+  const int p = __ldg(d.sell_ptr + sl), w = __ldg(d.sell_w + sl);
+  if (w <= 0) return m;
+  m.vals = d.svals + p;
+  m.vbytes = (unsigned)(32 * w * (int)sizeof(float));
+  if (d.scols16) {
+    m.cols = d.scols16 + p;
+    m.cbytes = (unsigned)(32 * w * (int)sizeof(int16_t));
+  } else {
+    m.cols = d.scols + p;
+    m.cbytes = (unsigned)(32 * w * (int)sizeof(int));
+  }
+  return m;
+}
+
+template <typename F>
+__device__ __forceinline__ void batch_slices_spmv(const BatchArgs &ba, const BatchShared &sh, F &&f) {
+  const int total = sh.total, nb = gridDim.x;
+  const int lo = (int)((long long)total * blockIdx.x / nb), hi = (int)((long long)total * (blockIdx.x + 1) / nb);
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, lane = threadIdx.x & 31;
+  SliceMeta next = batch_slice_meta(ba, sh, lo + warp + nw, hi);
+  for (int q = lo + warp; q < hi; q += nw) {
+    const int a = batch_locate(sh, q);
+    if (lane == 0 && next.vbytes) {
+      prefetch_l2_bulk(next.vals, next.vbytes);
+      prefetch_l2_bulk(next.cols, next.cbytes);
+    }
+    next = batch_slice_meta(ba, sh, q + 2 * nw, hi);
+    f(a, sh.act[a], q - sh.pre[a]);
+  }
+}
+
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
@@ -419,7 +481,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       // S: Q = A P; PQ;  clear RHO, RR
       batch_clear(a, BA_RHO);
       batch_clear(a, BA_RR);
-      batch_slices(sh, [&](int ai, int s, int slice) {
+      batch_slices_spmv(a, sh, [&](int ai, int s, int slice) {
         if (sh.status[s] != ST_RUN) return;
         const SysDesc &d = a.sys[s];
         const int r = (slice << 5) + lane;
@@ -499,7 +561,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       batch_clear(a, BA_RHO);
       batch_clear(a, BA_RR);
       batch_clear(a, BA_SS);
-      batch_slices(sh, [&](int ai, int s, int slice) {
+      batch_slices_spmv(a, sh, [&](int ai, int s, int slice) {
         if (sh.status[s] != ST_RUN) return;
         const SysDesc &d = a.sys[s];
         const int r = (slice << 5) + lane;
@@ -556,7 +618,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       if (!grid_barrier(a.bar, a.err, epoch)) return;
       // 4: T = A T2; TS, TT;  clear PQ
       batch_clear(a, BA_PQ);
-      batch_slices(sh, [&](int ai, int s, int slice) {
+      batch_slices_spmv(a, sh, [&](int ai, int s, int slice) {
         if (sh.status[s] != ST_RUN) return;
         const SysDesc &d = a.sys[s];
         const int r = (slice << 5) + lane;
