@@ -1,0 +1,90 @@
+// egpu_devmem.h -- device memory blocks for the library's buffers (host-only header).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <map>
+#include <mutex>
+
+namespace egpu {
+
+// device memory: a per-device cache of freed blocks
+//
+// Requests of the serving engine and the batched solver clone, fill and free a matrix's
+// device objects (twenty-odd buffers) per request.  cudaMalloc / cudaFree of large blocks
+// cost milliseconds each and vary with the driver's state (measured on B200: 1 to 5 s of
+// allocation and free per 48-request serving stream, varying from run to run).  Freed blocks therefore
+// stay in a process-wide cache, by device, and are handed out again to requests of a size
+// between the block's half and its full size.  A release first synchronises the device,
+// as cudaFree does implicitly, so no queued kernel can still use a block when it is reused.
+// At most DEVCACHE_MAX bytes are kept; an allocation that fails empties the device's cache
+// and retries.
+constexpr size_t DEVCACHE_GRAIN = (size_t)1 << 16;   // blocks are multiples of 64 KB
+constexpr size_t DEVCACHE_MAX = (size_t)24 << 30;    // bytes kept in the cache per device
+
+struct DevCache {
+  std::mutex mu;
+  std::map<int, std::multimap<size_t, void *>> free_blocks;  // device -> size -> block
+  std::map<int, size_t> cached;                                 // device -> bytes held
+};
+inline DevCache &devcache() {
+  static DevCache *c = new DevCache;  // never destroyed: blocks go back with the process
+  return *c;
+}
+inline size_t devcache_round(size_t bytes) { return (bytes + DEVCACHE_GRAIN - 1) / DEVCACHE_GRAIN * DEVCACHE_GRAIN; }
+
+// a block of at least `bytes` on the current device; *cap receives its size
+inline cudaError_t dev_alloc(void **p, size_t bytes, size_t *cap, int *dev) {
+  cudaError_t e = cudaGetDevice(dev);
+  if (e != cudaSuccess) return e;
+  const size_t want = devcache_round(bytes);
+  DevCache &c = devcache();
+  {
+    std::lock_guard<std::mutex> g(c.mu);
+    auto &fb = c.free_blocks[*dev];
+    auto it = fb.lower_bound(want);
+    if (it != fb.end() && it->first <= 2 * want) {
+      *p = it->second;
+      *cap = it->first;
+      c.cached[*dev] -= it->first;
+      fb.erase(it);
+      return cudaSuccess;
+    }
+  }
+  e = cudaMalloc(p, want);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();  // clear the sticky-free allocation error before retrying
+    std::lock_guard<std::mutex> g(c.mu);
+    auto &fb = c.free_blocks[*dev];
+    for (auto &kv : fb) cudaFree(kv.second);
+    fb.clear();
+    c.cached[*dev] = 0;
+    e = cudaMalloc(p, want);
+  }
+  if (e == cudaSuccess) *cap = want;
+  return e;
+}
+
+// return a block (allocated on device dev) to the cache, or to the driver past the cap
+inline void dev_free(void *p, size_t cap, int dev) {
+  if (!p) return;
+  int cur = -1;
+  cudaGetDevice(&cur);
+  if (cur != dev) cudaSetDevice(dev);
+  cudaDeviceSynchronize();
+  DevCache &c = devcache();
+  bool keep = false;
+  {
+    std::lock_guard<std::mutex> g(c.mu);
+    if (c.cached[dev] + cap <= DEVCACHE_MAX) {
+      c.free_blocks[dev].emplace(cap, p);
+      c.cached[dev] += cap;
+      keep = true;
+    }
+  }
+  if (!keep) cudaFree(p);
+  if (cur != dev && cur >= 0) cudaSetDevice(cur);
+}
+
+}  // namespace egpu

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/elmergpu.h"
+#include "egpu_devmem.h"
 #include "egpu_tri_plan.h"
 
 // ------------------------------------------------------------------------------------
@@ -58,14 +59,17 @@ struct DevBuf {
   T *p = nullptr;
   size_t n = 0;
   bool owned = true;  // false: a view of another object's buffer (matrix clones)
+  size_t cap = 0;     // bytes of the owned block (at least n elements)
+  int dev = 0;        // device of the owned block
   DevBuf() = default;
   DevBuf(const DevBuf &) = delete;
   DevBuf &operator=(const DevBuf &) = delete;
   ~DevBuf() { release(); }
   void release() {
-    if (p && owned) cudaFree(p);
+    if (p && owned) egpu::dev_free(p, cap, dev);
     p = nullptr;
     n = 0;
+    cap = 0;
     owned = true;
   }
   void view(const DevBuf &o) {
@@ -80,8 +84,12 @@ struct DevBuf {
     if (count == n && p && owned) return cudaSuccess;
     release();
     if (count == 0) return cudaSuccess;
-    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
-    if (e == cudaSuccess) n = count;
+    void *q = nullptr;
+    cudaError_t e = egpu::dev_alloc(&q, count * sizeof(T), &cap, &dev);
+    if (e == cudaSuccess) {
+      p = (T *)q;
+      n = count;
+    }
     return e;
   }
   size_t bytes() const { return n * sizeof(T); }

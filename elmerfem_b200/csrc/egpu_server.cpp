@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "../../include/elmergpu.h"
+#include "egpu_devmem.h"
 
 namespace {
 
@@ -59,6 +60,8 @@ struct Request {
   // device state while resident (touched by the worker only)
   egpu_mat *A = nullptr;
   double *rhs_dev = nullptr;
+  size_t rhs_cap = 0;
+  int rhs_devid = 0;
   int slot = -1;
   // result
   std::vector<double> x;
@@ -86,6 +89,7 @@ struct egpu_server {
   std::unordered_map<int, Request *> by_slot;  // written by the worker under mu
   long long next_id = 1, steps = 0, done = 0;
   double used = 0;
+  double t_prepare = 0, t_step = 0, t_retire = 0;  // worker wall time per activity (under mu)
   bool stop = false;
   std::thread worker;
 };
@@ -107,7 +111,9 @@ int prepare(egpu_server *S, Request *r) {
   }
   rc = egpu_matrix_update_values(r->A, r->values.data());
   if (rc) return rc;
-  if (cudaMalloc(&r->rhs_dev, sizeof(double) * r->n) != cudaSuccess ||
+  void *q = nullptr;
+  if (egpu::dev_alloc(&q, sizeof(double) * r->n, &r->rhs_cap, &r->rhs_devid) != cudaSuccess ||
+      !(r->rhs_dev = (double *)q) ||
       cudaMemcpy(r->rhs_dev, r->rhs.data(), sizeof(double) * r->n, cudaMemcpyHostToDevice) != cudaSuccess)
     return EGPU_ERR_ALLOC;
   return egpu_batch_add_matrix(S->batch, r->A, r->rhs_dev);
@@ -115,7 +121,7 @@ int prepare(egpu_server *S, Request *r) {
 
 // device and input memory of a request (under gpu_mu)
 void release(Request *r) {
-  if (r->rhs_dev) cudaFree(r->rhs_dev);
+  if (r->rhs_dev) egpu::dev_free(r->rhs_dev, r->rhs_cap, r->rhs_devid);
   r->rhs_dev = nullptr;
   if (r->A) egpu_matrix_free(r->A);
   r->A = nullptr;
@@ -159,8 +165,10 @@ void work(egpu_server *S) {
     std::vector<std::pair<Request *, int>> added;
     std::vector<Request *> retired;
     int step_rc = 0;
+    Clock::time_point c0, c1, c2, c3;
     {
       std::lock_guard<std::mutex> g(S->gpu_mu);
+      c0 = Clock::now();
       for (Request *r : admit) {
         const int slot = prepare(S, r);
         if (slot < 0) {
@@ -171,7 +179,9 @@ void work(egpu_server *S) {
         added.push_back({r, slot});
       }
       int nf = 0;
+      c1 = Clock::now();
       if (egpu_batch_pending(S->batch) > 0) step_rc = egpu_batch_step(S->batch, fin.data(), &nf);
+      c2 = Clock::now();
       std::vector<int> done_slots;
       if (step_rc < 0) {  // the batch failed: every resident request ends with the error code
         for (auto &kv : S->by_slot) done_slots.push_back(kv.first);
@@ -199,8 +209,12 @@ void work(egpu_server *S) {
         release(r);
         retired.push_back(r);
       }
+      c3 = Clock::now();
     }
     lk.lock();
+    S->t_prepare += std::chrono::duration<double>(c1 - c0).count();
+    S->t_step += std::chrono::duration<double>(c2 - c1).count();
+    S->t_retire += std::chrono::duration<double>(c3 - c2).count();
     const auto now = Clock::now();
     for (auto &[r, slot] : added) {
       if (slot < 0) {
@@ -388,6 +402,9 @@ extern "C" int egpu_server_info(egpu_server *S, egpu_server_stats *st) {
   st->done = S->done;
   st->steps = S->steps;
   st->used_bytes = S->used;
+  st->seconds_prepare = S->t_prepare;
+  st->seconds_step = S->t_step;
+  st->seconds_retire = S->t_retire;
   return EGPU_OK;
 }
 

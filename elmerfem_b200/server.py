@@ -262,6 +262,7 @@ class NativeSolveServer:
             self.mesh_prototype(r.m)
             r.material(self.patterns[r.m][1][0])
         ids = []
+        w0 = self.info()
         t0 = clock()
         for r in reqs:
             now = clock() - t0
@@ -282,7 +283,9 @@ class NativeSolveServer:
         makespan = max(r.finished for r in reqs) - min(r.arrival for r in reqs)
         return {"solves": len(reqs), "makespan_s": makespan, "solves_per_s": len(reqs) / makespan,
                 "p50_ms": 1000 * float(np.percentile(lat, 50)), "p99_ms": 1000 * float(np.percentile(lat, 99)),
-                "steps": self.info()["steps"], "converged": sum(1 for r in reqs if r.result.get("info") == 1)}
+                "steps": self.info()["steps"], "converged": sum(1 for r in reqs if r.result.get("info") == 1),
+                "worker_seconds": {k: round(self.info()[k] - w0[k], 4) for k in ("seconds_prepare", "seconds_step",
+                                                                                 "seconds_retire")}}
 
 
 def run_one_at_a_time(ctx: Context, params: SolverParams, requests: list[Request], protos: dict,

@@ -283,6 +283,10 @@ typedef struct egpu_server egpu_server;
 typedef struct {
   long long queued, resident, done, steps;
   double used_bytes;
+  /* worker thread's wall time so far: preparing admitted requests (clone, device assembly,
+   * scaling, factorisation), batch steps, retiring finished requests (results, solution
+   * copies, device memory returned) */
+  double seconds_prepare, seconds_step, seconds_retire;
 } egpu_server_stats;
 int egpu_server_create(int device, const egpu_params *prm, double hbm_budget_bytes, int chunk_iters,
                        int max_resident, egpu_server **out);
