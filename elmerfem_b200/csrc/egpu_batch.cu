@@ -473,7 +473,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
         const SysDesc &d = a.sys[s];
         const int r = (slice << 5) + lane;
         if (r >= d.n) return;
-        float *Z = d.w + d.ldw, *P = d.w + 2 * d.ldw;
+        float *Z = d.unit_diag ? d.w : d.w + d.ldw, *P = d.w + 2 * d.ldw;
         const float z = Z[r];
         P[r] = (sh.kk[s] == 1 && sh.fresh[s]) ? z : z + sh.sb[s] * P[r];
       });
@@ -516,8 +516,11 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
             d.x[r] = 0.f;
           }
           R[r] = rv;
-          const float z = bprec(rv, dv[r], a.precond);
-          Z[r] = z;
+          float z = rv;  // the identity on a unit diagonal: Z is R, not stored
+          if (!d.unit_diag) {
+            z = bprec(rv, dv[r], a.precond);
+            Z[r] = z;
+          }
           rz = (double)rv * (double)z;
           rr = (double)rv * (double)rv;
         }
@@ -936,6 +939,11 @@ static int batch_prepare(egpu_batch *B, int slot, const double *b_dev) {
   }
   rc = prepare_fp32_public(A, B->prm.precond == EGPU_PREC_ILU0);
   if (rc) return rc;
+  int unit = 0;
+  if (B->prm.method == EGPU_CG && B->prm.precond == EGPU_PREC_DIAGONAL) {
+    rc = unit_diagonal_fp32(A, &unit);
+    if (rc) return rc;
+  }
   S->phase = S->bnorm_s < 0 ? 3 : 1;  // negative: zero right-hand side, x = 0
   if (S->bnorm_s < 0) {
     S->info = EGPU_HUTI_CONVERGENCE;
@@ -944,6 +952,7 @@ static int batch_prepare(egpu_batch *B, int slot, const double *b_dev) {
   const long long ldw32 = A->ldw;
   SysDesc d{};
   d.n = n;
+  d.unit_diag = unit;
   d.nslices = A->nslices;
   d.sell_ptr = A->sell_ptr.p;
   d.sell_w = A->sell_w.p;

@@ -32,6 +32,7 @@ enum { ST_IDLE = 0, ST_INIT = 1, ST_RUN = 2, ST_DONE = 3 };
 
 struct SysDesc {
   int n, nslices;
+  int unit_diag;           // CG + Jacobi on a scaled diagonal that is 1.0f everywhere: Z is R
   const int *sell_ptr, *sell_w;
   const int16_t *scols16;  // col - row
   const int *scols;        // absolute column (when scols16 is null)

@@ -1597,6 +1597,23 @@ int rhs_scale(egpu_mat *A, const double *b_dev, const double *x_dev, double *bs,
 
 int prepare_fp32_public(egpu_mat *A, bool with_ilu) { return prepare_fp32(A, with_ilu); }
 
+// *unit = 1 when the FP32 copy of the scaled diagonal (work32 vector 13, written by
+// prepare_fp32) is 1.0f in every row; synchronises the stream
+int unit_diagonal_fp32(egpu_mat *A, int *unit) {
+  egpu_ctx *ctx = A->ctx;
+  const int n = A->n;
+  unsigned int *cnt = ctx->sync.p + 3;
+  EGPU_CUDA_TRY(ctx, cudaMemsetAsync(cnt, 0, sizeof(unsigned int), ctx->stream));
+  k_count_not_one<<<std::min(grid_for(ctx, n), 1024), 256, 0, ctx->stream>>>(A->work32.p + (size_t)13 * A->ldw, n,
+                                                                              cnt);
+  ctx->launches++;
+  unsigned int h = 1;
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(&h, cnt, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  *unit = h == 0 ? 1 : 0;
+  return EGPU_OK;
+}
+
 }  // namespace egpu
 
 // =====================================================================================

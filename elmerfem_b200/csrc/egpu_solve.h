@@ -52,6 +52,7 @@ int rhs_scale(egpu_mat *A, const double *b_dev, const double *x_dev, double *bs,
               double *bnorm_s);
 // FP32 SELL values, diagonal and (optionally) ILU0 factors for the inner solver
 int prepare_fp32_public(egpu_mat *A, bool with_ilu);
+int unit_diagonal_fp32(egpu_mat *A, int *unit);
 
 // level-synchronous single-block ILU0 solves (egpu_tri_cta.cu)
 int build_cta_schedule(egpu_mat *A, const std::vector<int> &rows, const std::vector<int> &cols,
