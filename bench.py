@@ -467,6 +467,30 @@ def run_gpu(args, rank, world, local, pg):
     te = reduce_max(pg, te, dev)
     e2e = world * args.steps / te
 
+    # ---- element assembly (not part of the step): device time of one egpu_assemble_poisson
+    # (element conductivity upload, zeroing, the colour launches), per element.  Estimated work
+    # per 8-node element (2x2x2 Gauss points): Jacobian 72 FMA, its inverse ~40 FLOP,
+    # dN/dx 72 FMA, the 8x8 stiffness 192 FMA and the load 8 FMA per point, about 5.6 kFLOP;
+    # bytes: 8 nodes x (24 B coordinates + 4 B index), the element's k, 64 slot indices and
+    # read-modify-writes of 64 values and 8 right-hand-side entries (1,640 B).
+    assembly = None
+    if not w.get("elastic") and m.elem_code == 808:
+        ta = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(ext)
+            A.assemble_poisson(elem_k=w["elem_k"], nodal_k=nodal_k, load=w["load"])
+            a1.record(ext)
+            torch.cuda.synchronize()
+            ta.append(a0.elapsed_time(a1) / 1000.0)
+            A.dirichlet(con, symmetric=w["symmetric"])
+        t_as = statistics.median(ta)
+        ne = m.nelem
+        assembly = {"ms": 1000 * t_as, "elements": ne, "elements_per_s": ne / t_as,
+                    "gflops_fp64_est": 5600.0 * ne / t_as / 1e9, "gbs_est": 1640.0 * ne / t_as / 1e9,
+                    "hbm_frac_est": 1640.0 * ne / t_as / 1e9 / peak}
+
     # ---- CPU baseline (rank 0, N=1 only)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -501,7 +525,8 @@ def run_gpu(args, rank, world, local, pg):
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 8 * n},
                 "gpu_launches": launches,
                 "clocks": clk.summary(),
-                "cpu_baseline": cpu}
+                "cpu_baseline": cpu,
+                "assembly": assembly}
         print(json.dumps(line), flush=True)
     A.free()
     ctx.close()
