@@ -179,7 +179,7 @@ constexpr int ASM_WARPS = 8;
 // Diffusion: K_pq = sum_t s_t k_t dN_q.dN_p, f_p = sum_t s_t (sum_m load_m N_m) N_p
 // (DiffuseConvectiveAnisotropic.src:334-344, 515-561, 569-612)
 template <int CODE>
-__global__ void __launch_bounds__(ASM_WARPS * 32) k_assemble_poisson(
+__global__ void __launch_bounds__(ASM_WARPS * 32, 3) k_assemble_poisson(
     int ne, const int *__restrict__ elist, const int *__restrict__ enodes, const double *__restrict__ xyz,
     int cdim, const double *__restrict__ elem_k, const double *__restrict__ nodal_k,
     const double *__restrict__ load, const int *__restrict__ perm, const int *__restrict__ slots,
@@ -189,38 +189,30 @@ __global__ void __launch_bounds__(ASM_WARPS * 32) k_assemble_poisson(
   __shared__ double sh_dB[ASM_WARPS][NGP][NEN][3];
   __shared__ double sh_N[ASM_WARPS][NGP][NEN];
   __shared__ double sh_s[ASM_WARPS][NGP], sh_k[ASM_WARPS][NGP], sh_f[ASM_WARPS][NGP];
+  // the element's node coordinates and nodal k / load, staged once per warp (lane p holds
+  // node p's) instead of in every lane's registers
+  __shared__ double sh_X[ASM_WARPS][NEN][3], sh_kn[ASM_WARPS][NEN], sh_ln[ASM_WARPS][NEN];
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int w = blockIdx.x * ASM_WARPS + wib;
   if (w >= ne) return;
   const int e = elist[w];
   int node = 0;
-  double X[NEN][3];
-  double kn = 1.0, ln = 0.0;
   if (lane < NEN) {
     node = enodes[(size_t)e * NEN + lane];
-    kn = elem_k ? elem_k[e] : (nodal_k ? nodal_k[node] : 1.0);
-    ln = load ? load[node] : 0.0;
-  }
+    sh_kn[wib][lane] = elem_k ? elem_k[e] : (nodal_k ? nodal_k[node] : 1.0);
+    sh_ln[wib][lane] = load ? load[node] : 0.0;
 #pragma unroll
-  for (int p = 0; p < NEN; ++p) {
-    const int np = __shfl_sync(0xffffffffu, node, p);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) X[p][c] = xyz[(size_t)np * 3 + c];
+    for (int c = 0; c < 3; ++c) sh_X[wib][lane][c] = xyz[(size_t)node * 3 + c];
   }
-  double kn_all[NEN], ln_all[NEN];
-#pragma unroll
-  for (int p = 0; p < NEN; ++p) {
-    kn_all[p] = __shfl_sync(0xffffffffu, kn, p);
-    ln_all[p] = __shfl_sync(0xffffffffu, ln, p);
-  }
+  __syncwarp();
   if (lane < NGP) {
     double N[NEN], dB[NEN][3], s;
-    const bool ok = gp_geometry<CODE>(lane, X, cdim, N, dB, s);
+    const bool ok = gp_geometry<CODE>(lane, sh_X[wib], cdim, N, dB, s);
     double kk = 0.0, ff = 0.0;
 #pragma unroll
     for (int p = 0; p < NEN; ++p) {
-      kk += kn_all[p] * N[p];
-      ff += ln_all[p] * N[p];
+      kk += sh_kn[wib][p] * N[p];
+      ff += sh_ln[wib][p] * N[p];
     }
     sh_s[wib][lane] = ok ? s : 0.0;
     sh_k[wib][lane] = kk;
@@ -270,22 +262,21 @@ __global__ void __launch_bounds__(ASM_WARPS * 32) k_assemble_elastic(
   __shared__ double sh_dB[ASM_WARPS][NGP][NEN][3];
   __shared__ double sh_N[ASM_WARPS][NGP][NEN];
   __shared__ double sh_s[ASM_WARPS][NGP], sh_sn[ASM_WARPS][NGP];
+  __shared__ double sh_X[ASM_WARPS][NEN][3];  // node coordinates, staged once per warp
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int w = blockIdx.x * ASM_WARPS + wib;
   if (w >= ne) return;
   const int e = elist[w];
   int node = 0;
-  double X[NEN][3];
-  if (lane < NEN) node = enodes[(size_t)e * NEN + lane];
+  if (lane < NEN) {
+    node = enodes[(size_t)e * NEN + lane];
 #pragma unroll
-  for (int p = 0; p < NEN; ++p) {
-    const int np = __shfl_sync(0xffffffffu, node, p);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) X[p][c] = xyz[(size_t)np * 3 + c];
+    for (int c = 0; c < 3; ++c) sh_X[wib][lane][c] = xyz[(size_t)node * 3 + c];
   }
+  __syncwarp();
   if (lane < NGP) {
     double N[NEN], dB[NEN][3], s;
-    const bool ok = gp_geometry<CODE>(lane, X, 3, N, dB, s);
+    const bool ok = gp_geometry<CODE>(lane, sh_X[wib], 3, N, dB, s);
     double sn = 0.0;
 #pragma unroll
     for (int p = 0; p < NEN; ++p) sn += N[p];
