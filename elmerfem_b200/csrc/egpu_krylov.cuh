@@ -196,14 +196,20 @@ __device__ __forceinline__ void spmv_phase(const KArgs<VT> &a, const VT *x0, con
     VT s0 = 0, s1 = 0;
     if (OFFS && a.scolsc) {
       const int cp = __ldg(a.sell_cptr + s);
-      if (cp < 0) {  // one offset list for the whole slice: a broadcast load per entry
+      if (cp < 0) {  // one offset list for the whole slice
+        // lane k holds offset k of each chunk of 32 (one coalesced load per chunk) and the
+        // warp broadcasts it with a shuffle, so no gather waits on an offset load
         const int16_t *co = a.scolsc + (-cp - 1);
+        for (int k0 = 0; k0 < w; k0 += 32) {
+          const int kn = min(32, w - k0);
+          const int offl = lane < kn ? (int)__ldg(co + k0 + lane) : 0;
 #pragma unroll 8
-        for (int k = 0; k < w; ++k) {
-          const VT v = ld_stream(a.svals + base + (k << 5));
-          const int c = r + (int)__ldg(co + k);
-          s0 = row_madd(s0, v, ld_l2(x0 + c));
-          if (TWO) s1 = row_madd(s1, v, ld_l2(x1 + c));
+          for (int k = 0; k < kn; ++k) {
+            const VT v = ld_stream(a.svals + base + ((k0 + k) << 5));
+            const int c = r + __shfl_sync(0xffffffffu, offl, k);
+            s0 = row_madd(s0, v, ld_l2(x0 + c));
+            if (TWO) s1 = row_madd(s1, v, ld_l2(x1 + c));
+          }
         }
       } else {
         const int16_t *co = a.scolsc + cp + lane;
