@@ -1,6 +1,6 @@
 """GPU parity through the C ABI against the oracle (needs a B200).
 
-Tolerances: CRS pattern bit-exact; Values within 1e-13 of the row
+Tolerances of the path: CRS pattern bit-exact; Values within 1e-13 of the row
 scale; SpMV within 1e-14 of the row's |a||x| scale; converged solutions within 1e-8
 relative of the oracle's at the same tolerance.  ILU0 factors are bit-exact.
 """
