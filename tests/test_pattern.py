@@ -66,3 +66,25 @@ def test_ilu_structure_matches_oracle(mk, order):
     assert np.array_equal(r, ref[0]) and np.array_equal(c, ref[1]) and np.array_equal(d, ref[2])
     # the structure contains the matrix pattern and grows with the order
     assert nz >= p.nnz
+
+
+@pytest.mark.parametrize("order", [1, 2, 3])
+@pytest.mark.parametrize("mk", [lambda: meshgen.hex_cube(5), lambda: meshgen.tet_cube(5), lambda: _heateq()],
+                         ids=["hex5", "tet5", "heateq"])
+def test_ilu_structure_is_the_symbolic_product(mk, order):
+    """Pins the oracle's ILU(n) structure by an independent construction: one InitializeILU1
+    step (CRSMatrix.src:2391-2497) adds to the pattern S every (i, j) reached through some
+    k < i with s_ik in S and j in the strictly upper part of S's row k, i.e. S | tril(S) @ triu(S)
+    as boolean sparse matrices; ILU(n) applies the step n times."""
+    import scipy.sparse as sp
+
+    mesh = mk()
+    p = oracle.create_pattern(mesh)
+    S = sp.csr_matrix((np.ones(p.nnz), p.cols - 1, p.rows - 1), shape=(p.n, p.n))
+    for _ in range(order):
+        L, U = sp.tril(S, -1, format="csr"), sp.triu(S, 1, format="csr")
+        S = ((S + L @ U) != 0).astype(np.float64).tocsr()
+    S.sort_indices()
+    r, c, d = oracle.ilu_pattern(p, order)
+    assert np.array_equal(r - 1, S.indptr) and np.array_equal(c - 1, S.indices)
+    assert np.all(c[d - 1] - 1 == np.arange(p.n))
