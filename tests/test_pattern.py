@@ -88,3 +88,34 @@ def test_ilu_structure_is_the_symbolic_product(mk, order):
     r, c, d = oracle.ilu_pattern(p, order)
     assert np.array_equal(r - 1, S.indptr) and np.array_equal(c - 1, S.indices)
     assert np.all(c[d - 1] - 1 == np.arange(p.n))
+
+
+@pytest.mark.parametrize("mk,dofs", [(lambda: meshgen.hex_cube(4), 1), (lambda: meshgen.tet_cube(4), 1),
+                                     (lambda: meshgen.hex_cube(3), 3), (lambda: _heateq(), 1)],
+                         ids=["hex4", "tet4", "hex3x3", "heateq"])
+def test_pattern_is_the_element_adjacency(mk, dofs):
+    """Pins the oracle's CRS creation (MakeListMatrix, CRS_CreateMatrix, CRS_SortMatrix) by an
+    independent construction: under its own Perm, row (Perm(a)-1)*DOFs+i holds the columns
+    (Perm(b)-1)*DOFs+j of every node b sharing an element with node a (a itself included), all
+    DOFs coupled, sorted ascending, Diag pointing at the row's own column; Perm is a
+    permutation of the nodes, and the optimised bandwidth never exceeds the original one."""
+    mesh = mk()
+    p = oracle.create_pattern(mesh, dofs=dofs)
+    nn = mesh.nnodes
+    assert sorted(p.perm.tolist()) == list(range(1, nn + 1))
+    assert p.hbw_after <= p.hbw_before
+    adj = [set() for _ in range(nn)]
+    for el in mesh.elements:
+        nodes = [int(q) - 1 for q in el]
+        for a in nodes:
+            adj[a].update(nodes)
+    rows, cols = [0], []
+    order = np.argsort(p.perm)  # node of each row block
+    for a in order:
+        bl = sorted((int(p.perm[b]) - 1) for b in adj[a])
+        for i in range(dofs):
+            for bb in bl:
+                cols.extend(bb * dofs + j for j in range(dofs))
+            rows.append(len(cols))
+    assert np.array_equal(p.rows - 1, np.array(rows)) and np.array_equal(p.cols - 1, np.array(cols))
+    assert np.all(p.cols[p.diag - 1] - 1 == np.arange(p.n))
