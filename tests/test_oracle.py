@@ -99,3 +99,62 @@ def test_zero_rhs_short_cut():
     p, _, _, v, _, _ = poisson_problem(m)
     x, r = oracle.solve(p, v, np.zeros(p.n), method=oracle.CG, precond=oracle.PREC_DIAGONAL, max_iter=10)
     assert r["info"] == 1 and not np.any(x)
+
+
+@pytest.mark.parametrize("mk", [lambda: meshgen.hex_cube(4), lambda: meshgen.tet_cube(4)], ids=["hex", "tet"])
+def test_poisson_patch_and_load_integral(mk):
+    """Pins the restated diffusion compose by properties of the exact Galerkin matrix: a linear
+    field is reproduced exactly by trilinear hexes and linear tets (the patch test: K u = 0 at
+    every interior node, for k constant), the energy u^T K u of u = x equals k * volume, and a
+    unit load integrates to the volume (sum of the load vector = 1 on the unit cube)."""
+    m = mk()
+    p = oracle.create_pattern(m)
+    k = 2.5
+    vals, rhs = oracle.assemble_poisson(m, p, nodal_k=np.full(m.nnodes, k), load=np.ones(m.nnodes))
+    xyz = m.coords
+    row_of = p.perm - 1  # node -> row
+    bnd = set((m.boundary_nodes(range(1, 7)) - 1).tolist())
+    interior_rows = np.array([row_of[a] for a in range(m.nnodes) if a not in bnd])
+    for c in range(3):
+        u = np.zeros(p.n)
+        u[row_of] = 0.3 + 1.7 * xyz[:, c]
+        Ku = oracle.spmv(p, vals, u)
+        assert np.max(np.abs(Ku[interior_rows])) < 1e-12
+        ux = np.zeros(p.n)
+        ux[row_of] = xyz[:, c]
+        assert abs(ux @ oracle.spmv(p, vals, ux) - k * 1.0) < 1e-12
+    assert abs(rhs.sum() - 1.0) < 1e-13
+
+
+@pytest.mark.parametrize("mk", [lambda: meshgen.hex_cube(3), lambda: meshgen.tet_cube(3)], ids=["hex", "tet"])
+def test_elastic_rigid_body_modes_and_load(mk):
+    """Pins the restated StressCompose: the three translations and three infinitesimal
+    rotations of the body are strain-free, so K u = 0 in every row; a uniform stretch
+    u = e x along x has energy u^T K u = C11 e^2 * volume with C11 = E(1-nu)/((1+nu)(1-2nu));
+    and a body force b integrates to b * volume per component."""
+    m = mk()
+    p = oracle.create_pattern(m, dofs=3)
+    E, nu, bf = 200e9, 0.3, (1.0, -2.0, 3.0)
+    vals, rhs = oracle.assemble_elastic(m, p, E, nu, bf)
+    xyz = m.coords
+    base = (p.perm - 1) * 3
+    scale = np.abs(vals).max()
+    modes = []
+    for d in range(3):
+        u = np.zeros(p.n)
+        u[base + d] = 1.0
+        modes.append(u)
+    for (i, j) in ((0, 1), (1, 2), (2, 0)):
+        u = np.zeros(p.n)
+        u[base + i] = -xyz[:, j]
+        u[base + j] = xyz[:, i]
+        modes.append(u)
+    for u in modes:
+        assert np.max(np.abs(oracle.spmv(p, vals, u))) < 1e-12 * scale
+    e = 1e-3
+    u = np.zeros(p.n)
+    u[base] = e * xyz[:, 0]
+    c11 = E * (1 - nu) / ((1 + nu) * (1 - 2 * nu))
+    assert abs(u @ oracle.spmv(p, vals, u) / (c11 * e * e) - 1.0) < 1e-12
+    for d in range(3):
+        assert abs(rhs[np.arange(p.n) % 3 == d].sum() - bf[d]) < 1e-12 * abs(bf[d])
