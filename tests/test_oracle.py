@@ -158,3 +158,31 @@ def test_elastic_rigid_body_modes_and_load(mk):
     assert abs(u @ oracle.spmv(p, vals, u) / (c11 * e * e) - 1.0) < 1e-12
     for d in range(3):
         assert abs(rhs[np.arange(p.n) % 3 == d].sum() - bf[d]) < 1e-12 * abs(bf[d])
+
+
+def test_dirichlet_variants_agree_and_reproduce_linear_fields():
+    """Pins the restated DefaultDirichletBCs: with the boundary values of a linear field and no
+    load, both variants (row replacement, symmetric elimination) give the linear field itself
+    (the discrete solution is exact for it); the symmetric variant leaves a symmetric matrix."""
+    m = meshgen.hex_cube(5)
+    p = oracle.create_pattern(m)
+    vals, rhs = oracle.assemble_poisson(m, p, nodal_k=np.ones(m.nnodes), load=None)
+    nodes = m.boundary_nodes(range(1, 7)) - 1
+    con = (p.perm[nodes]).astype(np.int32)  # 1-based rows
+    order = np.argsort(con)
+    con, nodes = con[order], nodes[order]
+    field = 1.0 + 2.0 * m.coords[:, 0] - 0.5 * m.coords[:, 1] + 0.25 * m.coords[:, 2]
+    exact = np.zeros(p.n)
+    exact[p.perm - 1] = field
+    for sym in (False, True):
+        v, b = vals.copy(), rhs.copy()
+        oracle.dirichlet(p, v, b, con, field[nodes], symmetric=sym)
+        x, r = oracle.solve(p, v, b, method=oracle.BICGSTAB, precond=oracle.PREC_ILU0, max_iter=500, tol=1e-12)
+        assert r["info"] == 1
+        assert np.max(np.abs(x - exact)) < 1e-9
+        if sym:
+            A = np.zeros((p.n, p.n))
+            for i in range(p.n):
+                for kk in range(p.rows[i] - 1, p.rows[i + 1] - 1):
+                    A[i, p.cols[kk] - 1] = v[kk]
+            assert np.max(np.abs(A - A.T)) < 1e-14 * np.abs(A).max()
