@@ -245,3 +245,38 @@ def test_ilu0_spmv_lusolve_match_transcriptions(mk):
     x = oracle.lusolve(p, ilu, u)
     ref = np.linalg.solve(U, np.linalg.solve(L, u))
     assert np.linalg.norm(x - ref) <= 1e-12 * np.linalg.norm(ref)
+
+
+def test_scaling_matches_transcription():
+    """ScaleLinearSystem (SolverUtils.src:6470-6640) transcribed: D_i = 1/sqrt|a_ii| (a zero
+    diagonal takes the row's absolute sum first), values a_ij (D_i D_j) bit-identical; b D
+    normalised by its 2-norm, DiagScaling multiplied by that norm, x divided by it (rounding
+    of the norm's summation order aside)."""
+    p = oracle.create_pattern(meshgen.hex_cube(3))
+    rng = np.random.default_rng(6)
+    v = rng.uniform(-1.0, 1.0, p.nnz)
+    v[p.diag - 1] = rng.uniform(0.5, 3.0, p.n) * rng.choice([-1, 1], p.n)
+    v[p.diag[5] - 1] = 0.0  # one vanishing diagonal
+    b = rng.standard_normal(p.n)
+    x = rng.standard_normal(p.n)
+    rows, cols = p.rows - 1, p.cols - 1
+    d = v[p.diag - 1].copy()
+    if np.any(np.abs(d) <= np.finfo(float).tiny):
+        for i in range(p.n):
+            if abs(d[i]) <= np.finfo(float).tiny:
+                d[i] = np.abs(v[rows[i]:rows[i + 1]]).sum()
+    D = np.where(np.abs(d) > np.finfo(float).tiny, 1.0 / np.sqrt(np.abs(d)), 1.0)
+    vr = v.copy()
+    for i in range(p.n):
+        for e in range(rows[i], rows[i + 1]):
+            vr[e] = v[e] * (D[i] * D[cols[e]])
+    bd = b * D
+    bnorm = np.sqrt(np.sum(bd ** 2))
+    Dn = D * bnorm
+    vs, bs, xs = v.copy(), b.copy(), x.copy()
+    Do, rs = oracle.scale(p, vs, bs, xs)
+    assert np.array_equal(vs, vr)
+    assert abs(rs / bnorm - 1) < 1e-14
+    assert np.allclose(Do, Dn, rtol=1e-14, atol=0)
+    assert np.allclose(bs, bd / bnorm, rtol=1e-14, atol=0)
+    assert np.allclose(xs, x / Dn, rtol=1e-14, atol=0)
