@@ -119,3 +119,127 @@ def test_pattern_is_the_element_adjacency(mk, dofs):
             rows.append(len(cols))
     assert np.array_equal(p.rows - 1, np.array(rows)) and np.array_equal(p.cols - 1, np.array(cols))
     assert np.all(p.cols[p.diag - 1] - 1 == np.arange(p.n))
+
+
+def _python_optimize_bandwidth(nn, lists, use_always=False):
+    """OptimizeBandwidth (BandwidthOptimize.src:108-355) transcribed with the list pointers as
+    (row, position) pairs: minimum-degree start, the depth-first Levelize with its explicit
+    stack, the pseudo-peripheral search (with its `StartNode = j` assignment as written), the
+    Cuthill-McKee numbering in list order from StartNode, reversed, and the rejection when the
+    half bandwidth grows.  lists[i] (1-based nodes) are sorted and hold i itself."""
+    deg = [0] + [len(lists[i]) for i in range(1, nn + 1)]
+
+    def bandwidth(perm):
+        return max(abs(perm[i] - perm[k]) for i in range(1, nn + 1) for k in lists[i])
+
+    hb_before = bandwidth(list(range(nn + 1))) + 1
+    level = [0] * (nn + 1)
+    done = [False] * (nn + 1)
+    state = {"max": 0}
+
+    def levelize(nin, lev):
+        n, L = nin, lev
+        stack = []
+        p = (n, 0) if lists[n] else None
+        while p is not None:
+            stack.append(p)
+            level[n] = L
+            done[n] = True
+            state["max"] = max(state["max"], L)
+            p = (n, 0) if lists[n] else None
+            while True:
+                if p is not None:
+                    nn_ = lists[p[0]][p[1]]
+                    if not done[nn_]:
+                        n = nn_
+                        L += 1
+                        break
+                elif stack:
+                    p = stack.pop()
+                    L -= 1
+                else:
+                    break
+                p = (p[0], p[1] + 1) if p[1] + 1 < len(lists[p[0]]) else None
+
+    start, mindeg = 1, deg[1]
+    for i in range(1, nn + 1):
+        if deg[i] < mindeg:
+            start, mindeg = i, deg[i]
+        level[i] = 0
+    levelize(start, 0)
+    newroot = True
+    while newroot:
+        newroot = False
+        mindeg, k = deg[start], start
+        for i in range(1, nn + 1):
+            if level[i] == state["max"] and deg[i] < mindeg:
+                k, mindeg = i, deg[i]
+        if k != start:
+            j = state["max"]
+            state["max"] = 0
+            for i in range(nn + 1):
+                done[i] = False
+            levelize(k, 0)
+            if j > state["max"]:
+                newroot = True
+                start = j
+    permlocal = [0] * (nn + 2)
+    doneidx = [0] * (nn + 1)
+    indx = 1
+    permlocal[indx] = start
+    doneidx[start] = indx
+    indx += 1
+    for i in range(1, nn + 1):
+        if permlocal[i] == 0:
+            for j in range(1, nn + 1):
+                if doneidx[j] == 0:
+                    permlocal[indx] = j
+                    doneidx[j] = indx
+                    indx += 1
+                    break
+        for k in lists[permlocal[i]]:
+            if doneidx[k] == 0:
+                permlocal[indx] = k
+                doneidx[k] = indx
+                indx += 1
+    perm = [0] * (nn + 1)
+    for i in range(1, nn + 1):
+        perm[permlocal[i]] = nn - i + 1
+    hb_after = bandwidth(perm) + 1
+    rejected = hb_before < hb_after and not use_always
+    if rejected:  # the routine then returns the original half bandwidth and ordering
+        perm = list(range(nn + 1))
+        hb_after = hb_before
+    return perm[1:], hb_before, hb_after, start, rejected
+
+
+def _shuffled(mesh, seed):
+    rng = np.random.default_rng(seed)
+    new = rng.permutation(mesh.nnodes)  # old node -> new node (0-based)
+    coords = np.empty_like(mesh.coords)
+    coords[new] = mesh.coords
+    return meshgen.Mesh(coords, mesh.elem_code, (new[mesh.elements - 1] + 1).astype(np.int32), mesh.bnd_code,
+                        (new[mesh.bnd_elements - 1] + 1).astype(np.int32), mesh.bnd_ids)
+
+
+@pytest.mark.parametrize("mk", [lambda: meshgen.hex_cube(4), lambda: meshgen.tet_cube(4), lambda: _heateq(),
+                                lambda: _shuffled(meshgen.hex_cube(4), 1), lambda: _shuffled(meshgen.tet_cube(3), 2),
+                                lambda: _shuffled(_heateq(), 3)],
+                         ids=["hex4", "tet4", "heateq", "hex4-shuffled", "tet3-shuffled", "heateq-shuffled"])
+def test_bandwidth_optimisation_matches_transcription(mk):
+    """The oracle's OptimizeBandwidth against a Python transcription of the reference's routine
+    (structured meshes: rejected; shuffled node numbering and the heateq mesh: accepted)."""
+    mesh = mk()
+    nn = mesh.nnodes
+    lists = [[] for _ in range(nn + 1)]
+    adj = [set() for _ in range(nn + 1)]
+    for el in mesh.elements:
+        nodes = [int(q) for q in el]
+        for a in nodes:
+            adj[a].update(nodes)
+    for a in range(1, nn + 1):
+        lists[a] = sorted(adj[a])
+    perm, hb, ha, start, rej = _python_optimize_bandwidth(nn, lists)
+    p = oracle.create_pattern(mesh)
+    assert (p.hbw_before, p.hbw_after, p.start_node, bool(p.rejected)) == (hb, ha, start, rej)
+    assert np.array_equal(p.perm, np.array(perm, np.int32))
