@@ -17,7 +17,9 @@ def _heateq():
 
 
 @pytest.mark.parametrize("mesh", [lambda: meshgen.hex_cube(5), lambda: meshgen.hex_cube(3, 4, 7),
-                                  lambda: meshgen.tet_cube(4), _heateq])
+                                  lambda: meshgen.tet_cube(4), _heateq,
+                                  lambda: _shuffled(meshgen.hex_cube(4), 1), lambda: _shuffled(meshgen.tet_cube(3), 2)],
+                         ids=["hex5", "hex3x4x7", "tet4", "heateq", "hex4-shuffled", "tet3-shuffled"])
 @pytest.mark.parametrize("dofs", [1, 3])
 @pytest.mark.parametrize("opt", [True, False])
 def test_pattern_bit_exact(mesh, dofs, opt):
