@@ -40,3 +40,15 @@ def row_rel_max(pat, a, b):
     scale = np.maximum.reduceat(np.abs(b), rows[:-1])
     per = np.repeat(scale, np.diff(rows))
     return float(np.max(np.abs(a - b) / np.maximum(per, 1e-300)))
+
+
+def renumbered(mesh, seed):
+    """The same mesh with its nodes numbered in a random order (boundary elements follow)."""
+    from elmerfem_b200 import meshgen
+
+    rng = np.random.default_rng(seed)
+    new = rng.permutation(mesh.nnodes)  # old node -> new node (0-based)
+    coords = np.empty_like(mesh.coords)
+    coords[new] = mesh.coords
+    return meshgen.Mesh(coords, mesh.elem_code, (new[mesh.elements - 1] + 1).astype(np.int32), mesh.bnd_code,
+                        (new[mesh.bnd_elements - 1] + 1).astype(np.int32), mesh.bnd_ids)

@@ -14,7 +14,7 @@ import pytest
 import elmerfem_b200 as eg
 import oracle
 from elmerfem_b200 import _lib, meshgen
-from helpers import elastic_problem, poisson_problem, rel, row_rel_max
+from helpers import renumbered, elastic_problem, poisson_problem, rel, row_rel_max
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
@@ -81,11 +81,15 @@ def test_ilu0_elastic_bit_exact(ctx):
     assert np.array_equal(ilu, oracle.ilu0(p, vs))
 
 
-@pytest.mark.parametrize("kind", ["hex", "tet", "heateq", "hex_lognormal"])
+@pytest.mark.parametrize("kind", ["hex", "tet", "heateq", "hex_lognormal", "hex_renumbered", "tet_renumbered"])
 @pytest.mark.parametrize("sym", [False, True])
 def test_assembly_and_dirichlet(ctx, kind, sym):
     if kind == "heateq":
         m, k, load = _heateq(), None, None
+    elif kind == "hex_renumbered":  # random node numbering: the bandwidth optimisation is accepted
+        m, k, load = renumbered(meshgen.hex_cube(6), 1), None, None
+    elif kind == "tet_renumbered":
+        m, k, load = renumbered(meshgen.tet_cube(5), 2), None, None
     elif kind == "hex":
         m, k, load = meshgen.hex_cube(7), None, None
     elif kind == "tet":
@@ -130,6 +134,10 @@ CASES = [
     ("tet8_bicgstab_none", lambda: poisson_problem(meshgen.tet_cube(8)), eg.BICGSTAB, eg.PREC_NONE),
     ("tet8_bicgstab_jacobi", lambda: poisson_problem(meshgen.tet_cube(8)), eg.BICGSTAB, eg.PREC_DIAGONAL),
     ("elastic5_bicgstab_ilu0", lambda: elastic_problem(meshgen.hex_cube(5)), eg.BICGSTAB, eg.PREC_ILU0),
+    ("hex9_renumbered_bicgstab_ilu0", lambda: poisson_problem(renumbered(meshgen.hex_cube(9), 3)), eg.BICGSTAB,
+     eg.PREC_ILU0),
+    ("tet7_renumbered_cg_jacobi", lambda: poisson_problem(renumbered(meshgen.tet_cube(7), 4), sym=True), eg.CG,
+     eg.PREC_DIAGONAL),
 ]
 
 

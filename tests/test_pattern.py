@@ -216,12 +216,9 @@ def _python_optimize_bandwidth(nn, lists, use_always=False):
 
 
 def _shuffled(mesh, seed):
-    rng = np.random.default_rng(seed)
-    new = rng.permutation(mesh.nnodes)  # old node -> new node (0-based)
-    coords = np.empty_like(mesh.coords)
-    coords[new] = mesh.coords
-    return meshgen.Mesh(coords, mesh.elem_code, (new[mesh.elements - 1] + 1).astype(np.int32), mesh.bnd_code,
-                        (new[mesh.bnd_elements - 1] + 1).astype(np.int32), mesh.bnd_ids)
+    from helpers import renumbered
+
+    return renumbered(mesh, seed)
 
 
 @pytest.mark.parametrize("mk", [lambda: meshgen.hex_cube(4), lambda: meshgen.tet_cube(4), lambda: _heateq(),
