@@ -79,6 +79,8 @@ PROTOTYPES = {
     "egpu_last_error": (C.c_char_p, [_vp]),
     "egpu_kernel_launches": (C.c_longlong, [_vp]),
     "egpu_stream": (C.c_void_p, [_vp]),
+    "egpu_cached_bytes": (C.c_longlong, [C.c_int]),
+    "egpu_release_cached_memory": (C.c_longlong, [C.c_int]),
     "egpu_pattern_create": (C.c_int, [C.c_int, C.c_int, C.c_int, _i32p, C.c_int, C.c_int, C.POINTER(C.c_int),
                                       C.POINTER(C.c_longlong), _vp, _vp, _vp, _vp]),
     "egpu_matrix_bind": (C.c_int, [_vp, C.c_int, _i32p, _i32p, _i32p, _vp, C.POINTER(_vp)]),

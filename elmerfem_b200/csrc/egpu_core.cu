@@ -1686,6 +1686,10 @@ extern "C" long long egpu_kernel_launches(const egpu_ctx *ctx) { return ctx ? ct
 
 extern "C" void *egpu_stream(const egpu_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
+extern "C" long long egpu_cached_bytes(int device) { return egpu::devcache_bytes(device); }
+
+extern "C" long long egpu_release_cached_memory(int device) { return egpu::devcache_release(device); }
+
 extern "C" int egpu_matrix_bind(egpu_ctx *ctx, int n, const int *rows, const int *cols, const int *diag,
                                 const double *values, egpu_mat **out) {
   if (!ctx || !out || n <= 0 || !rows || !cols || !diag) return EGPU_ERR_ARG;

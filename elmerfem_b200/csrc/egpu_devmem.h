@@ -87,4 +87,40 @@ inline void dev_free(void *p, size_t cap, int dev) {
   if (cur != dev && cur >= 0) cudaSetDevice(cur);
 }
 
+// bytes held in the cache for device dev (every device if dev < 0)
+inline long long devcache_bytes(int dev) {
+  DevCache &c = devcache();
+  std::lock_guard<std::mutex> g(c.mu);
+  long long t = 0;
+  for (auto &kv : c.cached)
+    if (dev < 0 || kv.first == dev) t += (long long)kv.second;
+  return t;
+}
+
+// give the cached blocks of device dev (every device if dev < 0) back to the driver
+inline long long devcache_release(int dev) {
+  DevCache &c = devcache();
+  std::lock_guard<std::mutex> g(c.mu);
+  long long t = 0;
+  bool any = false;
+  for (auto &kv : c.free_blocks) any = any || ((dev < 0 || kv.first == dev) && !kv.second.empty());
+  if (!any) return 0;
+  int cur = -1;
+  cudaGetDevice(&cur);
+  for (auto &kv : c.free_blocks) {
+    if (dev >= 0 && kv.first != dev) continue;
+    if (kv.second.empty()) continue;
+    cudaSetDevice(kv.first);
+    cudaDeviceSynchronize();
+    for (auto &b : kv.second) {
+      cudaFree(b.second);
+      t += (long long)b.first;
+    }
+    kv.second.clear();
+    c.cached[kv.first] = 0;
+  }
+  if (cur >= 0) cudaSetDevice(cur);
+  return t;
+}
+
 }  // namespace egpu

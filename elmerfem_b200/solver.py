@@ -370,6 +370,16 @@ def iter_solver(A: Matrix, b, x, params: SolverParams):
     return res
 
 
+def cached_bytes(device: int = -1) -> int:
+    """Bytes of freed device blocks the library keeps for reuse (egpu_cached_bytes); all devices if device < 0."""
+    return int(lib().egpu_cached_bytes(device))
+
+
+def release_cached_memory(device: int = -1) -> int:
+    """Frees the library's cached device blocks (egpu_release_cached_memory); returns the bytes released."""
+    return int(lib().egpu_release_cached_memory(device))
+
+
 def compute_norm(x) -> float:
     """ComputeNorm default (SolverUtils.src:4983-4988): sqrt(sum(x^2)/n)."""
     x = np.asarray(x, np.float64)

@@ -105,6 +105,13 @@ const char *egpu_last_error(const egpu_ctx *ctx);
 long long egpu_kernel_launches(const egpu_ctx *ctx);
 /* the cudaStream_t every call of this context runs on (for callers' CUDA events) */
 void *egpu_stream(const egpu_ctx *ctx);
+/* Device blocks freed by the library (matrix copies, work vectors, factors) stay in a
+ * process-wide cache per device, at most 24 GB each, for the next matrix of a similar size.
+ * egpu_cached_bytes: bytes held for `device` (all devices if device < 0).
+ * egpu_release_cached_memory: synchronises and frees them (all devices if device < 0);
+ * returns the bytes given back to the driver. */
+long long egpu_cached_bytes(int device);
+long long egpu_release_cached_memory(int device);
 
 /* ---- sparsity pattern: CreateMatrix (ElementUtils.src:698-930) -------------------
  * MakeListMatrix + OptimizeBandwidth (BandwidthOptimize.src:108-355) +

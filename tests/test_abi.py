@@ -109,3 +109,9 @@ def test_sif_outside_the_path(bad):
 def test_sif_required_keywords():
     with pytest.raises(KeyError):
         eg.SolverParams.from_sif({"Linear System Convergence Tolerance": 1e-6})
+
+
+def test_cache_queries_without_gpu():
+    """The cache queries need no device while nothing is cached (no CUDA call is made)."""
+    assert eg.cached_bytes() == 0 and eg.cached_bytes(0) == 0
+    assert eg.release_cached_memory() == 0

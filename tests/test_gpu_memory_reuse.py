@@ -39,3 +39,22 @@ def test_solves_on_recycled_blocks(ctx):
                     assert abs(r["iters"] - r_ref["iters"]) <= 1
                 assert rel(x, x_ref) < 1e-8
                 A.free()
+
+
+def test_release_cached_memory(ctx):
+    """Freed blocks are counted in the cache; releasing gives them back and empties it, and the
+    next matrix allocates afresh and still solves like the oracle."""
+    p, _, _, v, b, _ = poisson_problem(meshgen.hex_cube(9))
+    A = eg.Matrix(ctx, _pat(p), v)
+    A.solve(b, params=eg.SolverParams(method=eg.BICGSTAB, precond=eg.PREC_ILU0, tol=1e-10))
+    A.free()
+    held = eg.cached_bytes(ctx.device)
+    assert held > 0 and held % (1 << 16) == 0
+    assert eg.cached_bytes(-1) >= held
+    assert eg.release_cached_memory(ctx.device) == held
+    assert eg.cached_bytes(ctx.device) == 0 and eg.release_cached_memory(ctx.device) == 0
+    A = eg.Matrix(ctx, _pat(p), v)
+    x, r = A.solve(b, params=eg.SolverParams(method=eg.BICGSTAB, precond=eg.PREC_ILU0, tol=1e-10))
+    x_ref, r_ref = oracle.solve(p, v, b, method=eg.BICGSTAB, precond=eg.PREC_ILU0, tol=1e-10)
+    assert r["info"] == 1 and abs(r["iters"] - r_ref["iters"]) <= 1 and rel(x, x_ref) < 1e-8
+    A.free()
