@@ -700,9 +700,13 @@ def run_serve(args, rank, world, local, pg):
                 "latency_ms": {"p50": stats["p50_ms"], "p99": stats["p99_ms"]},
                 "serving": stats, "fp64_one_at_a_time": stats64,
                 "speedup_vs_fp64_one_at_a_time": stats["solves_per_s"] / stats64["solves_per_s"],
-                "rel_err_vs_fp64_max": max(errs), "e2e": {"value": stats["solves_per_s"] * world, "unit": UNIT,
-                                                         "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
-                "gpu_launches": None, "clocks": clk.summary(), "cpu_baseline": None}
+                "rel_err_vs_fp64_max": max(errs),
+                "e2e": ({"value": stats["solves_per_s"] * world, "unit": UNIT,
+                         "h2d_bytes_per_step": stats["bytes_h2d"] / len(reqs),
+                         "d2h_bytes_per_step": stats["bytes_d2h"] / len(reqs)} if "bytes_h2d" in stats else
+                        {"value": stats["solves_per_s"] * world, "unit": UNIT, "h2d_bytes_per_step": None,
+                         "d2h_bytes_per_step": None}),
+                "gpu_launches": stats.get("kernel_launches"), "clocks": clk.summary(), "cpu_baseline": None}
         print(json.dumps(line), flush=True)
     ctx.close()
 

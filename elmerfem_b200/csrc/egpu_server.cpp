@@ -90,6 +90,8 @@ struct egpu_server {
   long long next_id = 1, steps = 0, done = 0;
   double used = 0;
   double t_prepare = 0, t_step = 0, t_retire = 0;  // worker wall time per activity (under mu)
+  long long launches = 0;                           // kernel launches of ctx (under mu)
+  double bytes_h2d = 0, bytes_d2h = 0;              // request inputs uploaded, solutions read back (under mu)
   bool stop = false;
   std::thread worker;
 };
@@ -130,6 +132,14 @@ void release(Request *r) {
   std::vector<double>().swap(r->elem_k);
   std::vector<double>().swap(r->nodal_k);
   std::vector<double>().swap(r->load);
+  std::vector<int>().swap(r->con);
+}
+
+// host bytes a request's preparation copies to the device
+double input_bytes(const Request *r) {
+  return (double)sizeof(double) * (r->values.size() + r->rhs.size() + r->elem_k.size() + r->nodal_k.size() +
+                                   r->load.size()) +
+         (double)sizeof(int) * r->con.size();
 }
 
 // (under mu)
@@ -166,10 +176,13 @@ void work(egpu_server *S) {
     std::vector<Request *> retired;
     int step_rc = 0;
     Clock::time_point c0, c1, c2, c3;
+    double h2d = 0, d2h = 0;
+    long long nl = 0;
     {
       std::lock_guard<std::mutex> g(S->gpu_mu);
       c0 = Clock::now();
       for (Request *r : admit) {
+        h2d += input_bytes(r);
         const int slot = prepare(S, r);
         if (slot < 0) {
           r->res = egpu_result{};
@@ -204,14 +217,19 @@ void work(egpu_server *S) {
           egpu_batch_result(S->batch, slot, &r->res);
           r->x.resize(r->n);
           egpu_batch_solution(S->batch, slot, r->x.data());
+          d2h += (double)sizeof(double) * r->n;
         }
         egpu_batch_remove(S->batch, slot);
         release(r);
         retired.push_back(r);
       }
       c3 = Clock::now();
+      nl = egpu_kernel_launches(S->ctx);
     }
     lk.lock();
+    S->launches = nl;
+    S->bytes_h2d += h2d;
+    S->bytes_d2h += d2h;
     S->t_prepare += std::chrono::duration<double>(c1 - c0).count();
     S->t_step += std::chrono::duration<double>(c2 - c1).count();
     S->t_retire += std::chrono::duration<double>(c3 - c2).count();
@@ -405,6 +423,9 @@ extern "C" int egpu_server_info(egpu_server *S, egpu_server_stats *st) {
   st->seconds_prepare = S->t_prepare;
   st->seconds_step = S->t_step;
   st->seconds_retire = S->t_retire;
+  st->kernel_launches = S->launches;
+  st->bytes_h2d = S->bytes_h2d;
+  st->bytes_d2h = S->bytes_d2h;
   return EGPU_OK;
 }
 

@@ -281,11 +281,14 @@ class NativeSolveServer:
             r.finished = r.admitted + res["seconds"]
         lat = np.array([r.latency for r in reqs])
         makespan = max(r.finished for r in reqs) - min(r.arrival for r in reqs)
+        w1 = self.info()
         return {"solves": len(reqs), "makespan_s": makespan, "solves_per_s": len(reqs) / makespan,
                 "p50_ms": 1000 * float(np.percentile(lat, 50)), "p99_ms": 1000 * float(np.percentile(lat, 99)),
-                "steps": self.info()["steps"], "converged": sum(1 for r in reqs if r.result.get("info") == 1),
-                "worker_seconds": {k: round(self.info()[k] - w0[k], 4) for k in ("seconds_prepare", "seconds_step",
-                                                                                 "seconds_retire")}}
+                "steps": w1["steps"], "converged": sum(1 for r in reqs if r.result.get("info") == 1),
+                "worker_seconds": {k: round(w1[k] - w0[k], 4) for k in ("seconds_prepare", "seconds_step",
+                                                                        "seconds_retire")},
+                "kernel_launches": int(w1["kernel_launches"] - w0["kernel_launches"]),
+                "bytes_h2d": w1["bytes_h2d"] - w0["bytes_h2d"], "bytes_d2h": w1["bytes_d2h"] - w0["bytes_d2h"]}
 
 
 def run_one_at_a_time(ctx: Context, params: SolverParams, requests: list[Request], protos: dict,

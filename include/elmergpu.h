@@ -294,6 +294,10 @@ typedef struct {
    * scaling, factorisation), batch steps, retiring finished requests (results, solution
    * copies, device memory returned) */
   double seconds_prepare, seconds_step, seconds_retire;
+  /* kernel launches of the server's context so far; request inputs copied host -> device
+   * (Values, RHS, conductivities, loads, Dirichlet rows) and solutions device -> host, bytes */
+  long long kernel_launches;
+  double bytes_h2d, bytes_d2h;
 } egpu_server_stats;
 int egpu_server_create(int device, const egpu_params *prm, double hbm_budget_bytes, int chunk_iters,
                        int max_resident, egpu_server **out);

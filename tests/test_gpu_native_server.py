@@ -45,6 +45,10 @@ def test_native_server_host_values(method, prec):
         info = srv.info()
         assert info["done"] == 5 and info["resident"] == 0 and info["queued"] == 0 and info["steps"] >= 1
         assert info["used_bytes"] == pytest.approx(0.0, abs=1.0)
+        # transfers: every request's Values and RHS up, its solution down; the batch launched kernels
+        n, nnz = systems[0][0].n, systems[0][0].nnz
+        assert info["bytes_h2d"] == 5 * 8 * (nnz + n) and info["bytes_d2h"] == 5 * 8 * n
+        assert info["kernel_launches"] >= info["steps"]
         with pytest.raises(Exception):
             srv.poll(ids[0])  # released by wait
     finally:
@@ -63,6 +67,8 @@ def test_native_server_stream_equals_alone(ctx):
         srv.close()
     assert stats["solves"] == 12 and stats["converged"] == 12
     assert stats["p99_ms"] >= stats["p50_ms"] > 0
+    assert stats["kernel_launches"] > 0 and stats["bytes_h2d"] > 0
+    assert stats["bytes_d2h"] == 8 * sum((r.m + 1) ** 3 for r in reqs)  # one solution of n = (m+1)^3 each
     protos = {m: server.MeshPrototype(ctx, m, eg.PREC_ILU0) for m in sorted({r.m for r in reqs})}
     alone = [server.Request(r.rid, r.m, r.seed, 0.0) for r in reqs]
     server.run_one_at_a_time(ctx, eg.SolverParams(method=eg.BICGSTAB, precond=eg.PREC_ILU0, tol=1e-12,
