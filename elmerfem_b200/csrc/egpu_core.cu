@@ -593,6 +593,10 @@ int ensure_ilu_structure(egpu_mat *A, int order) {
     egpu_set_error(ctx, "clones of one pattern share its ILU structure: use one ILU order for all of them");
     return EGPU_ERR_STATE;
   }
+  if (!A->sorted_rows) {
+    egpu_set_error(ctx, "ILU needs the columns of every row in ascending order (CRS_SortMatrix)");
+    return EGPU_ERR_ARG;
+  }
   const int n = A->n;
   if (order == 0) {
     A->ilu_rows.view(A->rows);
@@ -883,6 +887,10 @@ int ilut_factor(egpu_mat *A, double tol) {
     return EGPU_ERR_STATE;
   }
   if (!(tol >= 0.0)) return EGPU_ERR_ARG;
+  if (!A->sorted_rows) {
+    egpu_set_error(ctx, "ILUT needs the columns of every row in ascending order (CRS_SortMatrix)");
+    return EGPU_ERR_ARG;
+  }
   const int n = A->n;
   const long long z = A->nnz;
   std::vector<int> rows(n + 1), cols(z);
@@ -1706,6 +1714,7 @@ extern "C" int egpu_matrix_bind(egpu_ctx *ctx, int n, const int *rows, const int
   A->n = n;
   A->nnz = nnz;
   int maxrow = 0, maxbw = 0;
+  bool sorted = true;
   for (int i = 0; i < n; ++i) {
     const int len = rows[i + 1] - rows[i];
     if (len < 0) {
@@ -1720,11 +1729,20 @@ extern "C" int egpu_matrix_bind(egpu_ctx *ctx, int n, const int *rows, const int
         egpu_set_error(ctx, "Cols out of range");
         return EGPU_ERR_ARG;
       }
+      if (k > rows[i] - 1 && cols[k] <= cols[k - 1]) sorted = false;
       maxbw = std::max(maxbw, std::abs(cols[k] - 1 - i));
+    }
+    // every kernel that reads the diagonal (scaling, Jacobi, ILU) indexes Values by Diag
+    const int d = diag[i];
+    if (d != 0 && (d < rows[i] || d >= rows[i + 1] || cols[d - 1] != i + 1)) {
+      delete A;
+      egpu_set_error(ctx, "Diag(i) must index row i's diagonal entry in Cols (0: the row stores none)");
+      return EGPU_ERR_ARG;
     }
   }
   A->max_row = maxrow;
   A->max_bandwidth = maxbw;
+  A->sorted_rows = sorted;
   auto fail = [&](cudaError_t e) {
     egpu_set_error(ctx, std::string("egpu_matrix_bind: ") + cudaGetErrorString(e));
     delete A;
@@ -1882,6 +1900,7 @@ extern "C" int egpu_matrix_clone(egpu_mat *proto, egpu_mat **out) {
   A->nnz = proto->nnz;
   A->max_row = proto->max_row;
   A->max_bandwidth = proto->max_bandwidth;
+  A->sorted_rows = proto->sorted_rows;
   A->rows.view(proto->rows);
   A->cols.view(proto->cols);
   A->diag.view(proto->diag);

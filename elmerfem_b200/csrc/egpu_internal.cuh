@@ -171,6 +171,7 @@ struct egpu_mat {
   bool has_values = false, has_rhs = false;
   int max_row = 0;               // longest row
   int max_bandwidth = 0;         // max |col - row|
+  bool sorted_rows = true;       // columns strictly ascending in every row (CRS_SortMatrix); ILU needs it
   // solve state
   DevBuf<double> scaled;         // D A D
   DevBuf<double> dscale;         // DiagScaling (times the rhs norm during a solve)

@@ -160,3 +160,49 @@ def test_ilu0_row_longer_than_the_factor_kernel_takes(ctx):
     oracle.scale(op, vs)
     rr, cc, dd, vv = oracle.ilut(op, vs, 0.0)
     assert np.array_equal(c, cc) and np.array_equal(val, vv)
+
+
+def _descending(gp, v):
+    """The same matrix with every row's columns stored in descending order (Diag follows)."""
+    n, rows = gp.n, gp.rows
+    cols, vals, diag = gp.cols.copy(), v.copy(), np.zeros(n, np.int32)
+    for i in range(n):
+        a, b = rows[i] - 1, rows[i + 1] - 1
+        cols[a:b], vals[a:b] = gp.cols[a:b][::-1], v[a:b][::-1]
+        k = np.nonzero(cols[a:b] == i + 1)[0]
+        diag[i] = a + k[0] + 1 if k.size else 0
+    op = oracle.Pattern(n, len(cols), 1, gp.perm, rows, cols, diag, 0, 0, 0, 0)
+    return op, eg.CRSPattern(n, len(cols), 1, gp.perm, rows, cols, diag), vals
+
+
+def test_unsorted_rows_solve_without_ilu_and_refuse_it(ctx):
+    """Rows whose columns are not ascending still multiply and solve with Jacobi like the oracle
+    (the SpMV keeps the stored order); ILU, which splits each row at Diag, refuses them."""
+    _, gp, v = _crs(200, _banded(200, 3))
+    op, gq, w = _descending(gp, v)
+    A = eg.Matrix(ctx, gq, w)
+    u = np.random.default_rng(3).random(gp.n)
+    assert rel(A.mv(u), oracle.spmv(op, w, u)) < 1e-14
+    b = np.random.default_rng(4).random(gp.n)
+    x, r = A.solve(b, params=eg.SolverParams(method=eg.BICGSTAB, precond=eg.PREC_DIAGONAL, tol=1e-10))
+    x_ref, r_ref = oracle.solve(op, w, b, method=eg.BICGSTAB, precond=eg.PREC_DIAGONAL, tol=1e-10)
+    assert r["info"] == 1 and r_ref["info"] == 1 and abs(r["iters"] - r_ref["iters"]) <= 1
+    assert rel(x, x_ref) < 1e-8
+    with pytest.raises(eg.LibError, match="ascending"):
+        A.solve(b, params=eg.SolverParams(method=eg.BICGSTAB, precond=eg.PREC_ILU0, tol=1e-10))
+    with pytest.raises(eg.LibError, match="ascending"):
+        A.ilut(0.0)
+
+
+def test_diag_not_at_the_diagonal_is_refused(ctx):
+    """Diag must index the row's own diagonal entry (or be 0): one outside its row or on an
+    off-diagonal column is refused before anything reads Values through it."""
+    _, gp, v = _crs(10, _banded(10, 1))
+    for bad in (int(gp.rows[1]) + 5, int(gp.diag[0]) + 1, -3):
+        d = gp.diag.copy()
+        d[0] = bad
+        with pytest.raises(eg.LibError, match="Diag"):
+            eg.Matrix(ctx, eg.CRSPattern(gp.n, gp.nnz, 1, gp.perm, gp.rows, gp.cols, d), v)
+    d = gp.diag.copy()
+    d[0] = 0  # no stored diagonal: accepted (scaling falls back to the row sum)
+    eg.Matrix(ctx, eg.CRSPattern(gp.n, gp.nnz, 1, gp.perm, gp.rows, gp.cols, d), v).free()
