@@ -1,0 +1,49 @@
+"""The size-independent property checks (tests/properties.py) on the oracle's own systems at
+small sizes: they must hold there before they are used to check the device path at the full
+workload sizes."""
+import numpy as np
+import pytest
+
+import oracle
+import properties as P
+from elmerfem_b200 import meshgen
+from helpers import elastic_problem
+
+
+@pytest.mark.parametrize("mk", [lambda: meshgen.hex_cube(10), lambda: meshgen.tet_cube(8)], ids=["hex10", "tet8"])
+def test_poisson_properties_on_oracle_systems(mk):
+    m = mk()
+    p = oracle.create_pattern(m)
+    k = meshgen.lognormal_conductivity(m.nelem, 1.0, 1)
+    vals, rhs = oracle.assemble_poisson(m, p, elem_k=k, load=np.ones(m.nnodes))
+    assert P.row_sum_defect(p, vals) < 1e-12
+    assert P.symmetry_defect(p, vals) < 1e-14
+    assert P.linear_field_energy_defect(m, p, vals, k) < 1e-12
+    assert abs(rhs.sum() - 1.0) < 1e-12
+    # a wrong conductivity or a lost element shows
+    assert P.linear_field_energy_defect(m, p, vals, k * 1.001) > 5e-4
+
+
+def test_rigid_modes_on_oracle_elasticity():
+    m = meshgen.hex_cube(6)
+    p, vals, rhs, v, b, con = elastic_problem(m)
+    assert P.rigid_mode_defect(m, p, vals) < 1e-12
+    assert P.symmetry_defect(p, vals) < 1e-14
+    # after the clamped rows are set, the translations are no longer in the kernel
+    assert P.rigid_mode_defect(m, p, v) > 1e-3
+
+
+@pytest.mark.parametrize("method,prec,tol", [(oracle.CG, oracle.PREC_DIAGONAL, 1e-10),
+                                             (oracle.BICGSTAB, oracle.PREC_ILU0, 1e-10)], ids=["cg-diag", "bicgstab-ilu0"])
+def test_scaled_residual_meets_the_stopping_test(method, prec, tol):
+    m = meshgen.hex_cube(12)
+    p = oracle.create_pattern(m)
+    k = meshgen.lognormal_conductivity(m.nelem, 1.0, 1)
+    vals, rhs = oracle.assemble_poisson(m, p, elem_k=k, load=meshgen.sine_source(m.coords))
+    con = np.sort(p.perm[m.boundary_nodes(range(1, 7)) - 1]).astype(np.int32)
+    oracle.dirichlet(p, vals, rhs, con, symmetric=True)
+    x, r = oracle.solve(p, vals, rhs, method=method, precond=prec, max_iter=5000, tol=tol)
+    assert r["info"] == 1
+    res = P.scaled_residual(p, vals, rhs, x)
+    assert res < tol * (1 + 1e-3)
+    assert res == pytest.approx(r["residual"], rel=1e-3, abs=1e-3 * tol)
