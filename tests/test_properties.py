@@ -1,6 +1,8 @@
 """The size-independent property checks (tests/properties.py) on the oracle's own systems at
 small sizes: they must hold there before they are used to check the device path at the full
 workload sizes."""
+import os
+
 import numpy as np
 import pytest
 
@@ -47,3 +49,36 @@ def test_scaled_residual_meets_the_stopping_test(method, prec, tol):
     res = P.scaled_residual(p, vals, rhs, x)
     assert res < tol * (1 + 1e-3)
     assert res == pytest.approx(r["residual"], rel=1e-3, abs=1e-3 * tol)
+
+
+@pytest.mark.skipif(os.environ.get("EGPU_FULL_SIZE_ORACLE") != "1",
+                    reason="about three minutes of CPU: set EGPU_FULL_SIZE_ORACLE=1")
+@pytest.mark.parametrize("case", ["poisson128", "elastic64"])
+def test_full_size_properties_on_oracle_systems(case):
+    """The oracle's own full-size systems meet the checks that tests/test_gpu_full_size.py
+    applies to the device's (measured here: CG + Diagonal on Poisson 128^3 takes 378
+    iterations to a scaled residual of 9.87e-11; BiCGStab + ILU0 on elasticity 64^3 takes 179
+    to 9.62e-9)."""
+    if case == "poisson128":
+        m = meshgen.hex_cube(128)
+        k = meshgen.lognormal_conductivity(m.nelem, 1.0, 1)
+        p = oracle.create_pattern(m)
+        vals, rhs = oracle.assemble_poisson(m, p, elem_k=k, load=np.ones(m.nnodes))
+        assert P.row_sum_defect(p, vals) < 1e-12 and P.symmetry_defect(p, vals) < 1e-13
+        assert P.linear_field_energy_defect(m, p, vals, k) < 1e-11 and abs(rhs.sum() - 1.0) < 1e-11
+        vals, rhs = oracle.assemble_poisson(m, p, elem_k=k, load=meshgen.sine_source(m.coords))
+        con = np.sort(p.perm[m.boundary_nodes(range(1, 7)) - 1]).astype(np.int32)
+        oracle.dirichlet(p, vals, rhs, con, symmetric=True)
+        method, prec, tol = oracle.CG, oracle.PREC_DIAGONAL, 1e-10
+    else:
+        m = meshgen.hex_cube(64)
+        p = oracle.create_pattern(m, dofs=3)
+        vals, rhs = oracle.assemble_elastic(m, p, 200e9, 0.3, (0.0, 0.0, -1e4))
+        assert P.rigid_mode_defect(m, p, vals) < 1e-10 and P.symmetry_defect(p, vals) < 1e-13
+        assert abs(rhs[2::3].sum() + 1e4) < 1e-6
+        nodes = p.perm[m.boundary_nodes([1]) - 1]
+        con = np.sort(np.concatenate([3 * (nodes - 1) + d for d in (1, 2, 3)])).astype(np.int32)
+        oracle.dirichlet(p, vals, rhs, con, symmetric=False)
+        method, prec, tol = oracle.BICGSTAB, oracle.PREC_ILU0, 1e-8
+    x, r = oracle.solve(p, vals, rhs, method=method, precond=prec, max_iter=20000, tol=tol)
+    assert r["info"] == 1 and P.scaled_residual(p, vals, rhs, x) < 1.5 * tol
