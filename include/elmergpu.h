@@ -50,7 +50,7 @@ enum { EGPU_PREC_NONE = 0, EGPU_PREC_DIAGONAL = 1, EGPU_PREC_ILU0 = 2, EGPU_PREC
 enum { EGPU_FP64 = 0, EGPU_MIXED = 1 };  /* FP64 drop-in | FP32 inner Krylov in FP64 refinement */
 
 typedef struct {
-  int method;             /* EGPU_CG | EGPU_BICGSTAB */
+  int method;             /* EGPU_CG | EGPU_BICGSTAB | EGPU_GCR | EGPU_BICGSTABL */
   int precond;            /* EGPU_PREC_* */
   int max_iter;           /* Linear System Max Iterations (required, >= 1) */
   double tol;             /* Linear System Convergence Tolerance (true residual / ||b||) */
