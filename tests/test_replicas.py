@@ -40,3 +40,26 @@ def test_two_rank_timing_is_max_over_ranks():
         p.join(timeout=60)
         assert p.exitcode == 0
     assert got == {0: 2.0, 1: 2.0}
+
+
+def test_reference_arm_under_two_ranks_prints_one_line():
+    """`bench.py --impl reference` launched like a 2-GPU run: rank 0 alone times the CPU
+    reference (the oracle on every host thread) and prints the one JSON line; the other rank
+    exits 0 without work."""
+    import json
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, BENCH_BACKEND="gloo")
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
+           "127.0.0.1", "--master-port", str(_free_port()), "bench.py", "--impl", "reference", "--workload",
+           "poisson32_bicgstab_ilu0", "--gpus", "2", "--steps", "1", "--warmup", "1"]
+    out = subprocess.run(cmd, cwd=root, env=env, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [json.loads(s) for s in out.stdout.splitlines() if s.startswith("{")]
+    assert len(lines) == 1
+    d = lines[0]
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
