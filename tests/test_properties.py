@@ -93,3 +93,26 @@ def test_full_size_properties_on_oracle_systems(case):
         ilu = oracle.ilu0(p, vs)
         _, it_np, info_np = _huti_bicgstab(P.csr(p, vs), bs, lambda q: oracle.lusolve(p, ilu, q), tol, 20000)
         assert info_np == 1 and abs(it_np - r["iters"]) <= 0.05 * r["iters"]
+
+
+@pytest.mark.skipif(os.environ.get("EGPU_FULL_SIZE_ORACLE") != "1",
+                    reason="about two minutes of CPU: set EGPU_FULL_SIZE_ORACLE=1")
+def test_fp32_representation_floor_of_the_scaled_systems():
+    """How far one FP32 inner solve can take the FP64 residual: with the scaled matrix's values
+    rounded to FP32, ||(A - A32) x|| / ||b|| at the FP64 solution x.  It grows as h^-2 with
+    ||A| |x|| / ||b||: elasticity 16^3 / 32^3 / 64^3 give 1.7e-5 / 7.2e-5 / 3.0e-4 (amplification
+    2.8e3 / 1.1e4 / 4.5e4), Poisson 64^3 with log-normal conductivity 3.1e-6 (840).  So a
+    refinement step gains at most about 3e-4 on elasticity 64^3, and its mixed solve needs
+    several refinements and more inner iterations than the FP64 drop-in."""
+    floors = {}
+    for nx in (16, 32, 64):
+        m = meshgen.hex_cube(nx)
+        p, vals, rhs, v, b, con = elastic_problem(m)
+        oracle.scale(p, v, b)
+        x, r = oracle.solve(p, v, b, method=oracle.BICGSTAB, precond=oracle.PREC_ILU0, max_iter=20000, tol=1e-10,
+                            scale=False)
+        assert r["info"] == 1
+        S, S32 = P.csr(p, v), P.csr(p, v.astype(np.float32).astype(np.float64))
+        floors[nx] = np.linalg.norm((S - S32) @ x) / np.linalg.norm(b)
+    assert 1e-5 < floors[16] < floors[32] < floors[64] and floors[64] > 1e-4
+    assert 2.5 < floors[64] / floors[32] < 6 and 2.5 < floors[32] / floors[16] < 6
