@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <mutex>
 #include <numeric>
 
@@ -2052,28 +2053,33 @@ static std::mutex g_hook_mu;
 
 extern "C" void egpu_matvec_subr(void **spmv, int *n, int *rows, int *cols, double *values, double *u,
                                  double *v, int *reinit) {
+  if (!spmv || !n || *n <= 0 || !rows || !cols || !values || !u || !v) return;
+  // the hook has no status argument: a failed product leaves v = NaN, so the Krylov method
+  // that called it stops on a NaN residual instead of iterating on a stale vector
+  const int nn = *n;
+  auto fail = [&] { std::fill(v, v + nn, std::numeric_limits<double>::quiet_NaN()); };
   std::lock_guard<std::mutex> lk(g_hook_mu);
-  if (!g_hook_ctx && egpu_create(0, &g_hook_ctx) != EGPU_OK) return;
+  if (!g_hook_ctx && egpu_create(0, &g_hook_ctx) != EGPU_OK) return fail();
   egpu_mat *A = (egpu_mat *)*spmv;
-  if (A && ((reinit && *reinit) || A->n != *n)) {
+  if (A && ((reinit && *reinit) || A->n != nn)) {
     egpu_matrix_free(A);
     A = nullptr;
     *spmv = nullptr;
   }
   if (!A) {
-    std::vector<int> diag(*n, 0);
-    for (int i = 0; i < *n; ++i)
+    std::vector<int> diag(nn, 0);
+    for (int i = 0; i < nn; ++i)
       for (int k = rows[i]; k < rows[i + 1]; ++k)
         if (cols[k - 1] == i + 1) {
           diag[i] = k;
           break;
         }
-    if (egpu_matrix_bind(g_hook_ctx, *n, rows, cols, diag.data(), values, &A) != EGPU_OK) return;
+    if (egpu_matrix_bind(g_hook_ctx, nn, rows, cols, diag.data(), values, &A) != EGPU_OK) return fail();
     *spmv = A;
   } else if (egpu_matrix_update_values(A, values) != EGPU_OK) {
-    return;
+    return fail();
   }
-  egpu_mv(A, u, v);
+  if (egpu_mv(A, u, v) != EGPU_OK) fail();
 }
 
 extern "C" int egpu_ilu_build(egpu_mat *A, int scale_system, int order) {

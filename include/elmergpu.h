@@ -185,7 +185,8 @@ int egpu_tri_info(egpu_mat *A, int info[6]);
 int egpu_mv(egpu_mat *A, const double *u, double *v);
 int egpu_mv_dev(egpu_mat *A, const double *u_dev, double *v_dev);
 /* exact MatVecSubr signature; *spmv is the per-matrix handle slot A%SpMV; the
- * matrix is (re)uploaded when *reinit != 0 or *spmv == NULL */
+ * matrix is (re)uploaded when *reinit != 0 or *spmv == NULL.  The signature has no status:
+ * when the product cannot be formed (no device, rejected arrays) v is filled with NaN. */
 void egpu_matvec_subr(void **spmv, int *n, int *rows, int *cols, double *values, double *u,
                       double *v, int *reinit);
 

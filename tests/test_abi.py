@@ -1,6 +1,7 @@
 """C-ABI surface: the library loads and exports every declared symbol; keyword parsing (CPU)."""
 import ctypes as C
 
+import numpy as np
 import pytest
 
 import elmerfem_b200 as eg
@@ -115,3 +116,24 @@ def test_cache_queries_without_gpu():
     """The cache queries need no device while nothing is cached (no CUDA call is made)."""
     assert eg.cached_bytes() == 0 and eg.cached_bytes(0) == 0
     assert eg.release_cached_memory() == 0
+
+
+def test_matvec_hook_without_a_device_returns_nan():
+    """The Matrix Vector Proc hook has no status argument: when no device can take the product
+    it fills v with NaN (the caller's Krylov method then stops) and leaves the handle slot empty.
+    Where a device exists the same call must give the product itself."""
+    n = 3
+    rows = np.array([1, 3, 6, 8], np.int32)
+    cols = np.array([1, 2, 1, 2, 3, 2, 3], np.int32)
+    vals = np.array([4.0, -1.0, -1.0, 4.0, -1.0, -1.0, 4.0])
+    u = np.array([1.0, 2.0, 3.0])
+    v = np.zeros(n)
+    h = C.c_void_p()
+    nn, zero = C.c_int(n), C.c_int(0)
+    _lib.lib().egpu_matvec_subr(C.byref(h), C.byref(nn), rows, cols, vals, u, v, C.byref(zero))
+    import torch
+
+    if torch.cuda.is_available():
+        assert np.allclose(v, [2.0, 4.0, 10.0])
+    else:
+        assert np.all(np.isnan(v)) and not h.value
