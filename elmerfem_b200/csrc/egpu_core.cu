@@ -2055,7 +2055,7 @@ extern "C" void egpu_matvec_subr(void **spmv, int *n, int *rows, int *cols, doub
                                  double *v, int *reinit) {
   if (!spmv || !n || *n <= 0 || !rows || !cols || !values || !u || !v) return;
   // the hook has no status argument: a failed product leaves v = NaN, so the Krylov method
-  // that called it stops on a NaN residual instead of iterating on a stale vector
+  // that called it cannot converge instead of returning a solution built on a stale vector
   const int nn = *n;
   auto fail = [&] { std::fill(v, v + nn, std::numeric_limits<double>::quiet_NaN()); };
   std::lock_guard<std::mutex> lk(g_hook_mu);

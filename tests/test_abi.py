@@ -120,7 +120,8 @@ def test_cache_queries_without_gpu():
 
 def test_matvec_hook_without_a_device_returns_nan():
     """The Matrix Vector Proc hook has no status argument: when no device can take the product
-    it fills v with NaN (the caller's Krylov method then stops) and leaves the handle slot empty.
+    it fills v with NaN (the caller's Krylov method then cannot converge) and leaves the handle
+    slot empty.
     Where a device exists the same call must give the product itself."""
     n = 3
     rows = np.array([1, 3, 6, 8], np.int32)
