@@ -138,3 +138,13 @@ def test_matvec_hook_without_a_device_returns_nan():
         assert np.allclose(v, [2.0, 4.0, 10.0])
     else:
         assert np.all(np.isnan(v)) and not h.value
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    """No fallback: without the built library every entry point raises."""
+    monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "libelmergpu.so"))
+    monkeypatch.setattr(_lib, "_lib", None)
+    with pytest.raises(eg.LibError, match="missing"):
+        eg.Context(0)
+    with pytest.raises(eg.LibError, match="missing"):
+        eg.cached_bytes()
