@@ -10,8 +10,8 @@ solver is timed on the same system in the same run.  Inputs are synthetic (no da
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload NAME]
 
-Workloads: poisson128_cg_jacobi (default), poisson32_bicgstab_ilu0, elastic64_bicgstab_ilu0
-(single systems: mixed solve timed, FP64 drop-in beside it), batch512_tet_cg_jacobi (one
+Workloads: poisson128_cg_jacobi (default), poisson96_cg_jacobi, poisson32_bicgstab_ilu0,
+elastic64_bicgstab_ilu0 (single systems: mixed solve timed, FP64 drop-in beside it), batch512_tet_cg_jacobi (one
 batched mixed solve of 512 tet systems against the FP64 drop-in one at a time),
 serve_hex_bicgstab_ilu0 (a 200/s Poisson request stream through the native server against the
 FP64 drop-in one request at a time).
