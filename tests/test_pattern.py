@@ -7,6 +7,7 @@ import pytest
 import elmerfem_b200 as eg
 import oracle
 from elmerfem_b200 import _lib, meshgen
+from helpers import renumbered
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
@@ -18,7 +19,7 @@ def _heateq():
 
 @pytest.mark.parametrize("mesh", [lambda: meshgen.hex_cube(5), lambda: meshgen.hex_cube(3, 4, 7),
                                   lambda: meshgen.tet_cube(4), _heateq,
-                                  lambda: _shuffled(meshgen.hex_cube(4), 1), lambda: _shuffled(meshgen.tet_cube(3), 2)],
+                                  lambda: renumbered(meshgen.hex_cube(4), 1), lambda: renumbered(meshgen.tet_cube(3), 2)],
                          ids=["hex5", "hex3x4x7", "tet4", "heateq", "hex4-shuffled", "tet3-shuffled"])
 @pytest.mark.parametrize("dofs", [1, 3])
 @pytest.mark.parametrize("opt", [True, False])
@@ -215,15 +216,9 @@ def _python_optimize_bandwidth(nn, lists, use_always=False):
     return perm[1:], hb_before, hb_after, start, rejected
 
 
-def _shuffled(mesh, seed):
-    from helpers import renumbered
-
-    return renumbered(mesh, seed)
-
-
 @pytest.mark.parametrize("mk", [lambda: meshgen.hex_cube(4), lambda: meshgen.tet_cube(4), lambda: _heateq(),
-                                lambda: _shuffled(meshgen.hex_cube(4), 1), lambda: _shuffled(meshgen.tet_cube(3), 2),
-                                lambda: _shuffled(_heateq(), 3)],
+                                lambda: renumbered(meshgen.hex_cube(4), 1), lambda: renumbered(meshgen.tet_cube(3), 2),
+                                lambda: renumbered(_heateq(), 3)],
                          ids=["hex4", "tet4", "heateq", "hex4-shuffled", "tet3-shuffled", "heateq-shuffled"])
 def test_bandwidth_optimisation_matches_transcription(mk):
     """The oracle's OptimizeBandwidth against a Python transcription of the reference's routine
