@@ -1,5 +1,6 @@
 """C-ABI surface: the library loads and exports every declared symbol; keyword parsing (CPU)."""
 import ctypes as C
+import os
 
 import numpy as np
 import pytest
@@ -148,3 +149,27 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
         eg.Context(0)
     with pytest.raises(eg.LibError, match="missing"):
         eg.cached_bytes()
+
+
+def test_plain_c_host_links_and_calls(tmp_path):
+    """The ABI is plain C: a C99 program includes the header, links the library and calls it."""
+    import shutil
+    import subprocess
+
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "host.c"
+    src.write_text('#include "elmergpu.h"\n'
+                   "int main(void) {\n"
+                   "  egpu_params p;\n"
+                   "  egpu_params_default(&p, EGPU_BICGSTAB, EGPU_PREC_ILU0);\n"
+                   "  if (p.method != EGPU_BICGSTAB || p.precond != EGPU_PREC_ILU0) return 2;\n"
+                   "  if (egpu_iter_solve(0, 0, 0, &p, 0) != EGPU_ERR_ARG) return 3;\n"
+                   "  return egpu_cached_bytes(-1) == 0 ? 0 : 4;\n"
+                   "}\n")
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    exe = tmp_path / "host"
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(root, "include"), str(src), "-o", str(exe),
+                    "-L", libdir, "-lelmergpu", "-Wl,-rpath," + libdir], check=True, capture_output=True)
+    assert subprocess.run([str(exe)]).returncode == 0
