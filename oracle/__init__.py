@@ -3,6 +3,11 @@
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the CPU
 baseline leg of bench.py as the checker.  The product library never loads it.
 All index arrays are 1-based int32, as in Elmer's Matrix_t.
+
+Pinned to the reference's own regression targets (the heateq and linearsolvers NRM values
+on their committed 2D mesh, tests/golden/) and to independent transcriptions of the
+reference's loops; not pinned against a built ElmerSolver, which is Fortran and cannot be
+built here.
 """
 from __future__ import annotations
 

@@ -6,6 +6,8 @@
 // reference's gfortran -O2 x86-64 build does.
 //
 // Every routine names the Fortran it restates (paths relative to the Elmer tree).
+// Pinned to the reference's regression targets (heateq / linearsolvers NRM values on their
+// committed mesh) and to independent transcriptions; not to a built ElmerSolver (Fortran).
 // Indices are 1-based like Matrix_t; arrays below are addressed with a -1 shift.
 
 #include "elmer_oracle.h"
