@@ -282,11 +282,88 @@ def cpu_solve_rate(p, values, rhs, solve_kw, full_iters, threads, target_s=10.0)
                                     f"extrapolated to the FP64 iteration count {full_iters}"}
 
 
+def run_reference_systems(args, world):
+    """Reference arm of the batched and serving workloads: the oracle solves the workload's own
+    systems one at a time in FP64 (the reference's only mode; SpMV on every host thread) in
+    their seeded order, until about target seconds of solve time per step, and reports systems
+    per second.  Sizes are drawn independently, so the prefix is a random sample of the mix.
+    Assembly and Dirichlet rows are set up outside the timing, as in the GPU arms."""
+    import oracle
+    from elmerfem_b200 import meshgen, server
+
+    threads = os.cpu_count() or 1
+    if args.workload == "batch512_tet_cg_jacobi":
+        rng = np.random.Generator(np.random.PCG64(1))
+        ms = np.clip(np.floor(np.exp(rng.uniform(np.log(8), np.log(61), size=args.systems))).astype(int), 8, 60)
+        method, prec, target = oracle.CG, oracle.PREC_DIAGONAL, 8.0
+        cfg = {"workload": "batched_tet_poisson_512_cg_jacobi", "systems": int(args.systems), "m_range": [8, 60],
+               "method": "CG", "preconditioner": "Diagonal", "tol": args.tol, "precision": "fp64"}
+
+        def system(i):
+            mesh = meshgen.tet_cube(int(ms[i]))
+            p = oracle.create_pattern(mesh)
+            k = meshgen.lognormal_conductivity(mesh.nelem, 0.5, 1000 + i)
+            vals, rhs = oracle.assemble_poisson(mesh, p, elem_k=k, load=np.zeros(mesh.nnodes))
+            con = np.sort(p.perm[mesh.boundary_nodes(range(1, 7)) - 1]).astype(np.int32)
+            oracle.dirichlet(p, vals, rhs, con, symmetric=True)
+            b = np.random.Generator(np.random.PCG64(5000 + i)).random(p.n)
+            b[con - 1] = 0.0
+            return p, vals, b
+        count = args.systems
+    else:
+        reqs = server.poisson_stream(args.requests, rate=args.rate, m_lo=16, m_hi=128, seed=1, sigma=1.0)
+        method, prec, target = oracle.BICGSTAB, oracle.PREC_ILU0, 20.0
+        cfg = {"workload": "serving_hex_poisson_bicgstab_ilu0", "requests": len(reqs), "m_range": [16, 128],
+               "method": "BiCGStab", "preconditioner": "ILU0", "tol": args.tol, "precision": "fp64",
+               "served": "one request at a time, arrival order"}
+
+        def system(i):
+            r = reqs[i]
+            mesh = meshgen.hex_cube(r.m)
+            p = oracle.create_pattern(mesh)
+            k, load = r.material(mesh)
+            vals, rhs = oracle.assemble_poisson(mesh, p, elem_k=k, load=load)
+            con = np.sort(p.perm[mesh.boundary_nodes(range(1, 7)) - 1]).astype(np.int32)
+            oracle.dirichlet(p, vals, rhs, con, symmetric=False)
+            return p, vals, rhs
+        count = len(reqs)
+    cache = {}
+
+    def step(target_s):
+        t, n = 0.0, 0
+        while t < target_s and n < count:
+            if n not in cache:
+                cache[n] = system(n)
+            p, vals, b = cache[n]
+            _, r = oracle.solve(p, vals, b, method=method, precond=prec, max_iter=20000, tol=args.tol, threads=threads)
+            t += r["seconds"]
+            n += 1
+        return n / t, n, t
+
+    for _ in range(args.warmup):
+        step(min(2.0, target))
+    rates, n, t = [], 0, 0.0
+    for _ in range(args.steps):
+        r, n, t = step(target)
+        rates.append(r)
+    value = statistics.median(rates)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"per step: the first {n} systems in seeded order, whole oracle solves "
+                                       f"({t:.1f} s of solve time)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, world, pg):
     if rank != 0:
         return
     import oracle
 
+    if args.workload in ("batch512_tet_cg_jacobi", "serve_hex_bicgstab_ilu0"):
+        return run_reference_systems(args, world)
     build, solve_kw, cfg = workload_spec(args.workload)
     w = build()
     m = w["mesh"]
