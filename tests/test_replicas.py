@@ -63,3 +63,22 @@ def test_reference_arm_under_two_ranks_prints_one_line():
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_reference_arm_of_the_batched_workload():
+    """`--impl reference` on the batched workload: the oracle solves the seeded systems one at a
+    time and reports systems per second (a short run on 6 systems)."""
+    import json
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    cmd = [sys.executable, "bench.py", "--impl", "reference", "--workload", "batch512_tet_cg_jacobi", "--systems", "6",
+           "--steps", "1", "--warmup", "0"]
+    out = subprocess.run(cmd, cwd=root, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [json.loads(s) for s in out.stdout.splitlines() if s.startswith("{")]
+    assert len(lines) == 1
+    d = lines[0]
+    assert d["impl"] == "reference" and d["value"] > 0 and d["config"]["systems"] == 6
+    assert d["cpu_baseline"]["kind"] == "port" and "seeded order" in d["cpu_baseline"]["sample"]
