@@ -1,5 +1,6 @@
 """Multi-GPU runs are replicas (independent systems per rank, no data-path collective):
-the bench's rendezvous, barrier and max-over-ranks timing on 2 gloo ranks (CPU)."""
+the bench's rendezvous, barrier and max-over-ranks timing on 2 gloo ranks (CPU), and the
+reference arm's launch (rank 0 alone, one JSON line) on the CPU."""
 import os
 import socket
 
