@@ -18,7 +18,7 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "elmergpu.h")
 
 EGPU_OK = 0
 ERRORS = {-1: "EGPU_ERR_ARG", -2: "EGPU_ERR_CUDA", -3: "EGPU_ERR_ALLOC", -4: "EGPU_ERR_TIMEOUT",
-          -5: "EGPU_ERR_STATE", -6: "EGPU_ERR_BUDGET"}
+          -5: "EGPU_ERR_STATE", -6: "EGPU_ERR_BUDGET", -7: "EGPU_ERR_ABORT"}
 HUTI = {1: "HUTI_CONVERGENCE", 2: "HUTI_MAXITER", 3: "HUTI_DIVERGENCE", 20: "HUTI_CG_RHO", 35: "HUTI_BICGSTAB_RHO",
         36: "HUTI_BICGSTAB_SNORM", 37: "HUTI_BICGSTAB_OMEGA"}
 
@@ -67,7 +67,11 @@ class ServerStats(C.Structure):
 
 
 class LibError(RuntimeError):
-    pass
+    """A negative status from the library; .code holds it (EGPU_ERR_*)."""
+
+    def __init__(self, msg: str, code: int = 0):
+        super().__init__(msg)
+        self.code = code
 
 
 _lib = None
@@ -80,6 +84,9 @@ PROTOTYPES = {
     "egpu_last_error": (C.c_char_p, [_vp]),
     "egpu_kernel_launches": (C.c_longlong, [_vp]),
     "egpu_stream": (C.c_void_p, [_vp]),
+    "egpu_set_wait_limit": (C.c_int, [_vp, C.c_double]),
+    "egpu_abort": (C.c_int, [_vp, C.c_int]),
+    "egpu_wait_selftest": (C.c_int, [_vp, C.c_int]),
     "egpu_cached_bytes": (C.c_longlong, [C.c_int]),
     "egpu_release_cached_memory": (C.c_longlong, [C.c_int]),
     "egpu_pattern_create": (C.c_int, [C.c_int, C.c_int, C.c_int, _i32p, C.c_int, C.c_int, C.POINTER(C.c_int),
@@ -178,5 +185,5 @@ def check(rc: int, ctx=None, what: str = "") -> int:
             detail = lib().egpu_last_error(ctx)
             if detail:
                 msg += ": " + detail.decode(errors="replace")
-        raise LibError(f"{what}: {msg}")
+        raise LibError(f"{what}: {msg}", rc)
     return rc

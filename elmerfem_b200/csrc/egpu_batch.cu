@@ -1218,7 +1218,7 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
     EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(herr, ctx->sync.p, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
     EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     if (herr[1]) {
-      egpu_set_error(ctx, "device-side wait expired in the batched solver");
+      egpu_set_error(ctx, egpu_device_status_text((int)herr[1]) + " in the batched solver");
       return (int)herr[1];
     }
     B->parity = (B->parity + hit[0]) & 1;

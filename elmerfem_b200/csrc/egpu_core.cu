@@ -240,7 +240,10 @@ __global__ void __launch_bounds__(256) k_ilu0_factor(int n, const int *__restric
         if (t0 == 0) t0 = egpu_globaltimer();
         if ((++spin & 31u) == 0) {
           int stop = 0;
-          if (lane == 0) stop = egpu_globaltimer() - t0 > EGPU_WAIT_NS ? 1 : (*(volatile int *)err ? 2 : 0);
+          if (lane == 0) {
+            if ((spin & 1023u) == 0) egpu_poll_abort(err);
+            stop = egpu_globaltimer() - t0 > egpu_wait_limit(err) ? 1 : (*(volatile int *)err ? 2 : 0);
+          }
           stop = __shfl_sync(0xffffffffu, stop, 0);
           if (stop) {
             if (stop == 1 && lane == 0) atomicExch(err, (int)EGPU_ERR_TIMEOUT);
@@ -516,7 +519,23 @@ namespace egpu {
 
 int ensure_ctx_scratch(egpu_ctx *ctx) {
   if (!ctx->sync.p) {
-    EGPU_CUDA_TRY(ctx, ctx->sync.alloc(64));
+    EGPU_CUDA_TRY(ctx, ctx->sync.alloc(EGPU_SYNC_WORDS));
+    // the control words: default wait bound, and the host-mapped abort word (polled by the
+    // kernels, written by egpu_abort from any host thread)
+    EGPU_CUDA_TRY(ctx, cudaMemsetAsync(ctx->sync.p, 0, EGPU_SYNC_WORDS * sizeof(unsigned int), ctx->stream));
+    if (!ctx->abort_word) {
+      void *h = nullptr;
+      EGPU_CUDA_TRY(ctx, cudaHostAlloc(&h, 64, cudaHostAllocMapped));
+      ctx->abort_word = static_cast<volatile int *>(h);
+      *ctx->abort_word = 0;
+    }
+    void *dptr = nullptr;
+    EGPU_CUDA_TRY(ctx, cudaHostGetDevicePointer(&dptr, (void *)ctx->abort_word, 0));
+    // copied from a stack value: the copy is waited for before returning
+    const unsigned long long ctl_abort = (unsigned long long)(uintptr_t)dptr;
+    EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->sync.p + EGPU_CTL_WORD + 2, &ctl_abort, sizeof(ctl_abort),
+                                       cudaMemcpyHostToDevice, ctx->stream));
+    EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     // NUM_SLOTS partial slots and, from slot 16 on, BiCGStab(l)'s Gram matrix ((l+1)(l+2)/2 <= 45
     // slots), for up to two blocks per SM; the rest is the mixed path's residual partials
     EGPU_CUDA_TRY(ctx, ctx->partials.alloc((size_t)(16 + 45) * ctx->num_sms * 2 + 8192));
@@ -1173,7 +1192,7 @@ int solve_fp64(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_param
   }
   if (res) *res = r;
   if (err) {
-    egpu_set_error(ctx, "device-side wait expired (EGPU_ERR_TIMEOUT)");
+    egpu_set_error(ctx, egpu_device_status_text(err));
     return err;
   }
   return r.info;
@@ -1477,7 +1496,7 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
       EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(h, ctx->sync.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
       EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
       if (h[1]) {
-        egpu_set_error(ctx, "device-side wait expired in the FP32 inner solver");
+        egpu_set_error(ctx, egpu_device_status_text((int)h[1]) + " in the FP32 inner solver");
         return (int)h[1];
       }
       resume = allow_resume && ((const double *)(h + 16))[7] == 1.0;
@@ -1570,7 +1589,7 @@ int lu_apply(egpu_mat *A, const double *v_dev, double *u_dev) {
   EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(h, ctx->sync.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
   EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   if (h[1]) {
-    egpu_set_error(ctx, "device-side wait expired in the triangular solve");
+    egpu_set_error(ctx, egpu_device_status_text((int)h[1]) + " in the triangular solve");
     return (int)h[1];
   }
   return EGPU_OK;
@@ -1679,6 +1698,7 @@ extern "C" void egpu_destroy(egpu_ctx *ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   ctx->sync.release();
+  if (ctx->abort_word) cudaFreeHost((void *)ctx->abort_word);
   ctx->partials.release();
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -1687,6 +1707,61 @@ extern "C" void egpu_destroy(egpu_ctx *ctx) {
   if (ctx->ek1) cudaEventDestroy(ctx->ek1);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
+}
+
+extern "C" int egpu_set_wait_limit(egpu_ctx *ctx, double seconds) {
+  if (!ctx || !(seconds >= 0.0) || seconds > 3600.0) return EGPU_ERR_ARG;
+  EGPU_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const unsigned long long ns = (unsigned long long)(seconds * 1e9);
+  // copied from a stack value: wait for the copy before returning
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->sync.p + EGPU_CTL_WORD, &ns, sizeof(ns), cudaMemcpyHostToDevice,
+                                     ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return EGPU_OK;
+}
+
+extern "C" int egpu_abort(egpu_ctx *ctx, int raise) {
+  if (!ctx || !ctx->abort_word) return EGPU_ERR_ARG;
+  __atomic_store_n((int *)ctx->abort_word, raise ? 1 : 0, __ATOMIC_SEQ_CST);
+  return EGPU_OK;
+}
+
+namespace {
+
+// Self-test of the bounded waits: which = 0, block 1 never arrives at the grid barrier, so
+// the other block's wait runs out; which = 1, the block waits for a value that nothing
+// publishes (a word holding the sentinel).  Both end by the context's wait bound.
+__global__ void k_wait_selftest(unsigned int *bar, int *err, const double *never, int which) {
+  unsigned int epoch = 0;
+  if (which == 0) {
+    if (blockIdx.x == 1) return;
+    grid_barrier(bar, err, epoch);
+  } else if (threadIdx.x == 0) {
+    Sentinel<double>::wait(never, err);
+  }
+}
+
+}  // namespace
+
+extern "C" int egpu_wait_selftest(egpu_ctx *ctx, int which) {
+  if (!ctx || (which != 0 && which != 1)) return EGPU_ERR_ARG;
+  EGPU_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  if (egpu::reset_sync(ctx) != EGPU_OK) return EGPU_ERR_CUDA;
+  static const unsigned long long sentinel = EGPU_SENTINEL64;
+  unsigned int *never = ctx->sync.p + EGPU_SELFTEST_WORD;
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(never, &sentinel, sizeof(sentinel), cudaMemcpyHostToDevice, ctx->stream));
+  unsigned int *bar = ctx->sync.p;
+  int *err = (int *)(ctx->sync.p + 1);
+  const double *nv = (const double *)never;
+  void *kargs[] = {&bar, &err, &nv, &which};
+  EGPU_CUDA_TRY(ctx, cudaLaunchCooperativeKernel((const void *)k_wait_selftest, dim3(2), dim3(32), kargs, 0,
+                                                 ctx->stream));
+  ctx->launches++;
+  int e = 0;
+  if (egpu::read_err(ctx, &e) != EGPU_OK) return EGPU_ERR_CUDA;
+  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (egpu::reset_sync(ctx) != EGPU_OK) return EGPU_ERR_CUDA;
+  return e;
 }
 
 extern "C" const char *egpu_last_error(const egpu_ctx *ctx) { return ctx ? ctx->last_error.c_str() : ""; }
@@ -2097,7 +2172,7 @@ extern "C" int egpu_ilu_build(egpu_mat *A, int scale_system, int order) {
   EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(h, ctx->sync.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
   EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   if (h[1]) {
-    egpu_set_error(ctx, "device-side wait expired in the ILU0 factorisation");
+    egpu_set_error(ctx, egpu_device_status_text((int)h[1]) + " in the ILU0 factorisation");
     return (int)h[1];
   }
   return EGPU_OK;

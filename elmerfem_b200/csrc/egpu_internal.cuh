@@ -19,10 +19,20 @@
 #define EGPU_TINY_DP 2.2250738585072014e-308
 #define EGPU_HUTI_EPSILON 1.17549435E-38
 
-// Upper bound on any device-side spin (grid barrier, sync-free dependency wait):
-// after this many nanoseconds the waiting thread records EGPU_ERR_TIMEOUT and the
-// kernel unwinds.
+// Default upper bound on any device-side spin (grid barrier, sync-free dependency wait):
+// after this many nanoseconds the waiting thread records EGPU_ERR_TIMEOUT and the kernel
+// unwinds.  A context can set its own bound (egpu_set_wait_limit).
 #define EGPU_WAIT_NS 2000000000ull
+
+// The context's device control block is its sync buffer of EGPU_SYNC_WORDS 32-bit words:
+// word 0 the grid-barrier counter, word 1 the error word every kernel reports to, words
+// 2..63 per-solve scratch (cleared before each solve), and from EGPU_CTL_WORD on the words
+// that persist across solves: the wait bound in ns (u64, 0 = EGPU_WAIT_NS) and the device
+// address of the host-mapped abort word (u64, 0 = none).  Kernels receive a pointer to the
+// error word and find the control words at a fixed distance from it.
+#define EGPU_SYNC_WORDS 128
+#define EGPU_CTL_WORD 64
+#define EGPU_SELFTEST_WORD 96
 
 // Bit patterns that mark "not yet produced" in the sync-free triangular solves and the
 // ILU factorisation.  They are NaNs with a payload that arithmetic never produces
@@ -50,6 +60,16 @@
 
 struct egpu_ctx;
 void egpu_set_error(const egpu_ctx *ctx, const std::string &msg);
+
+// text for a status a kernel recorded in the context's error word
+inline std::string egpu_device_status_text(int err) {
+  switch (err) {
+    case EGPU_ERR_TIMEOUT: return "device-side wait expired (EGPU_ERR_TIMEOUT)";
+    case EGPU_ERR_ABORT: return "cancelled through the abort word (EGPU_ERR_ABORT)";
+    case EGPU_ERR_ARG: return "invalid data found on the device (EGPU_ERR_ARG)";
+    default: return "device-side error " + std::to_string(err);
+  }
+}
 
 // ------------------------------------------------------------------------------------
 // device memory owner
@@ -109,6 +129,8 @@ struct egpu_ctx {
   DevBuf<unsigned int> sync;    // [0] barrier counter, [1] error flag, [2..] misc
   DevBuf<double> partials;      // per-block partial sums
   unsigned int *sync_host_err = nullptr;
+  // host-mapped abort word (egpu_abort): written by any host thread, polled by the kernels
+  volatile int *abort_word = nullptr;
 };
 
 // One triangle of the level-synchronous solve that a single block runs (CtaTri in
@@ -266,6 +288,22 @@ __device__ __forceinline__ void st_relaxed_u32(void *p, unsigned int v) {
   asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// the context's wait bound (ns), read next to its error word
+__device__ __forceinline__ unsigned long long egpu_wait_limit(const int *err) {
+  const unsigned long long v =
+      *(const volatile unsigned long long *)((const unsigned int *)err + (EGPU_CTL_WORD - 1));
+  return v ? v : EGPU_WAIT_NS;
+}
+
+// Reads the context's host-mapped abort word (one load over the host link) and, when the host
+// has raised it, records EGPU_ERR_ABORT unless another error is already recorded; every
+// block then leaves at its next grid barrier or bounded wait.
+__device__ __forceinline__ void egpu_poll_abort(int *err) {
+  const unsigned long long a =
+      *(const volatile unsigned long long *)((const unsigned int *)err + (EGPU_CTL_WORD + 1));
+  if (a && *(const volatile int *)a) atomicCAS(err, 0, (int)EGPU_ERR_ABORT);
+}
+
 // value type traits for the sync-free solves
 template <typename T>
 struct Sentinel;
@@ -279,12 +317,13 @@ struct Sentinel<double> {
   __device__ __forceinline__ static double wait(const double *p, int *err) {
     unsigned long long v = ld_relaxed_u64(p);
     if (v != EGPU_SENTINEL64) return __longlong_as_double((long long)v);
-    unsigned long long t0 = egpu_globaltimer();
+    const unsigned long long t0 = egpu_globaltimer(), lim = egpu_wait_limit(err);
     for (unsigned int spin = 1;; ++spin) {
       v = ld_relaxed_u64(p);
       if (v != EGPU_SENTINEL64) break;
       if ((spin & 31u) == 0) {
-        if (egpu_globaltimer() - t0 > EGPU_WAIT_NS) {
+        if ((spin & 4095u) == 0) egpu_poll_abort(err);
+        if (egpu_globaltimer() - t0 > lim) {
           atomicExch(err, (int)EGPU_ERR_TIMEOUT);
           break;
         }
@@ -308,12 +347,13 @@ struct Sentinel<float> {
   __device__ __forceinline__ static float wait(const float *p, int *err) {
     unsigned int v = ld_relaxed_u32(p);
     if (v != EGPU_SENTINEL32) return __uint_as_float(v);
-    unsigned long long t0 = egpu_globaltimer();
+    const unsigned long long t0 = egpu_globaltimer(), lim = egpu_wait_limit(err);
     for (unsigned int spin = 1;; ++spin) {
       v = ld_relaxed_u32(p);
       if (v != EGPU_SENTINEL32) break;
       if ((spin & 31u) == 0) {
-        if (egpu_globaltimer() - t0 > EGPU_WAIT_NS) {
+        if ((spin & 4095u) == 0) egpu_poll_abort(err);
+        if (egpu_globaltimer() - t0 > lim) {
           atomicExch(err, (int)EGPU_ERR_TIMEOUT);
           break;
         }
@@ -328,21 +368,25 @@ struct Sentinel<float> {
 
 // Grid-wide barrier for a cooperative (co-resident) launch.  count is a monotonically
 // increasing arrival counter reset to 0 before the launch; epoch is the per-block count
-// of barriers passed.  The wait is bounded by EGPU_WAIT_NS; on expiry the error flag is
-// set.  Returns false when the kernel must unwind (error flag set by anyone).
+// of barriers passed.  The wait is bounded by the context's wait limit; on expiry the error
+// flag is set.  Block 0 reads the host's abort word every 16th barrier (and every waiting
+// block during long waits).  Returns false when the kernel must unwind (error flag set by
+// anyone).
 __device__ __forceinline__ bool grid_barrier(unsigned int *count, int *err, unsigned int &epoch) {
   __syncthreads();
   epoch += 1;
   if (threadIdx.x == 0) {
+    if (blockIdx.x == 0 && (epoch & 15u) == 0) egpu_poll_abort(err);
     const unsigned int target = epoch * gridDim.x;
     red_release_add_u32(count, 1u);
     if (ld_acquire_u32(count) < target) {
-      unsigned long long t0 = egpu_globaltimer();
+      const unsigned long long t0 = egpu_globaltimer(), lim = egpu_wait_limit(err);
       unsigned int spins = 0;
       while (ld_acquire_u32(count) < target) {
         if ((++spins & 63u) == 0) {
+          if ((spins & 1023u) == 0) egpu_poll_abort(err);
           if (*(volatile int *)err) break;
-          if (egpu_globaltimer() - t0 > EGPU_WAIT_NS) {
+          if (egpu_globaltimer() - t0 > lim) {
             atomicExch(err, (int)EGPU_ERR_TIMEOUT);
             break;
           }

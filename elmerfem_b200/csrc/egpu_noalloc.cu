@@ -15,7 +15,11 @@
 //     by each call, everything else is overwritten before it is read.
 //   * the first call on a device looks up the array's device address (cudaGetSymbolAddress
 //     with that device current) and caches it; make that first call before any stream
-//     capture.
+//     capture.  The cached address is not looked up again, so after cudaDeviceReset on
+//     that device (which unloads the module and may place the array elsewhere) this entry
+//     point must not be called;
+//   * the caller's arrays are used in place and are checked on the device before any gather
+//     goes through them; the caller's current device is restored on return.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -28,7 +32,10 @@ namespace {
 constexpr int NA_MAXN = EGPU_NOALLOC_MAX_ROWS;
 constexpr int NA_NVEC = 9;          // D0 D dv bs xs R Z P Q
 constexpr int NA_PARTIALS = 8 * 1024;
-constexpr int NA_COUNTERS = 64;     // as unsigned ints at the tail
+// as unsigned ints at the tail, laid out as a context's control block (egpu_internal.cuh):
+// barrier counter, error word, then from EGPU_CTL_WORD the wait bound and abort address,
+// both kept at zero here (the default bound, no abort word)
+constexpr int NA_COUNTERS = EGPU_SYNC_WORDS;
 
 }  // namespace
 
@@ -81,6 +88,25 @@ __global__ void __launch_bounds__(256) k_cg_noalloc(NaArgs a) {
   int *out_i = reinterpret_cast<int *>(cnt + 8);
   double *out_d = reinterpret_cast<double *>(cnt + 16);
   unsigned int epoch = 0;
+
+  // The caller's Matrix_t arrays are used in place, so they are checked here before any
+  // gather goes through them (egpu_matrix_bind checks the same on the host): Rows(1) = 1 and
+  // non-decreasing, every Cols entry in 1..n, Diag either 0 (no stored diagonal) or inside its
+  // row at the column of the row itself.  A violation sets EGPU_ERR_ARG and every block leaves
+  // at the first grid barrier.  Only Rows(i), Rows(i+1) and entries they bound are read, and
+  // an entry is read only after its row's bounds passed.
+  for (int i = tid; i < n; i += nth) {
+    const int r0 = a.rows[i], r1 = a.rows[i + 1];
+    bool ok = r0 <= r1 && (i != 0 || r0 == 1) && r0 >= 1;
+    for (int k = r0 - 1; ok && k < r1 - 1; ++k) {
+      const int c = a.cols[k];
+      ok = c >= 1 && c <= n;
+    }
+    const int d = a.diag[i];
+    if (ok && d != 0) ok = d >= r0 && d < r1 && a.cols[d - 1] == i + 1;
+    if (!ok) atomicExch(err, (int)EGPU_ERR_ARG);
+  }
+  if (!grid_barrier(bar, err, epoch)) return;
 
   // ScaleLinearSystem (SolverUtils.src:6500-6636): D0 = 1/sqrt|a_ii|, ||b||, ||D0 b||, x != 0
   {
@@ -219,6 +245,10 @@ __global__ void __launch_bounds__(256) k_cg_noalloc(NaArgs a) {
 std::mutex g_mu;
 double *g_addr[64] = {nullptr};
 
+int noalloc_solve(int device, int n, const int *rows_dev, const int *cols_dev, const int *diag_dev,
+                  const double *values_dev, const double *b_dev, double *x_dev, const egpu_params *prm,
+                  egpu_result *res);
+
 }  // namespace
 
 extern "C" int egpu_cg_noalloc(int device, int n, const int *rows_dev, const int *cols_dev, const int *diag_dev,
@@ -230,7 +260,21 @@ extern "C" int egpu_cg_noalloc(int device, int n, const int *rows_dev, const int
       (prm->precond != EGPU_PREC_DIAGONAL && prm->precond != EGPU_PREC_NONE) || !prm->scale_system)
     return EGPU_ERR_ARG;
   if (device < 0 || device >= 64) return EGPU_ERR_ARG;
+  // the caller's current device is put back on every return: hosts that manage their own
+  // device (CUDA Fortran, OpenACC) keep it
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) return EGPU_ERR_CUDA;
   if (cudaSetDevice(device) != cudaSuccess) return EGPU_ERR_CUDA;
+  const int rc = noalloc_solve(device, n, rows_dev, cols_dev, diag_dev, values_dev, b_dev, x_dev, prm, res);
+  if (prev != device) cudaSetDevice(prev);
+  return rc;
+}
+
+namespace {
+
+int noalloc_solve(int device, int n, const int *rows_dev, const int *cols_dev, const int *diag_dev,
+                  const double *values_dev, const double *b_dev, double *x_dev, const egpu_params *prm,
+                  egpu_result *res) {
   double *scratch = nullptr;
   {
     // set-up, once per device, with that device current: the host-side name of the array is
@@ -243,9 +287,10 @@ extern "C" int egpu_cg_noalloc(int device, int n, const int *rows_dev, const int
     }
     scratch = g_addr[device];
   }
-  // counters that must start at zero: barrier count, error flag, x != 0 flag
+  // counters that must start at zero: barrier count, error flag, x != 0 flag, and the
+  // control words (default wait bound, no abort word)
   unsigned int *cnt = reinterpret_cast<unsigned int *>(scratch + NA_NVEC * NA_MAXN + NA_PARTIALS);
-  if (cudaMemsetAsync(cnt, 0, 8 * sizeof(unsigned int), 0) != cudaSuccess) return EGPU_ERR_CUDA;
+  if (cudaMemsetAsync(cnt, 0, (EGPU_CTL_WORD + 4) * sizeof(unsigned int), 0) != cudaSuccess) return EGPU_ERR_CUDA;
   int num_sms = 0, bps = 0;
   cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device);
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_cg_noalloc, 256, 0) != cudaSuccess || bps < 1)
@@ -270,3 +315,5 @@ extern "C" int egpu_cg_noalloc(int device, int n, const int *rows_dev, const int
   if (res) *res = r;
   return r.info;
 }
+
+}  // namespace

@@ -46,6 +46,19 @@ class Context:
     def kernel_launches(self) -> int:
         return int(lib().egpu_kernel_launches(self._h))
 
+    def set_wait_limit(self, seconds: float = 0.0):
+        """Bound of every device-side wait of this context's kernels (0: the default 2 s)."""
+        check(lib().egpu_set_wait_limit(self._h, float(seconds)), self._h, "egpu_set_wait_limit")
+
+    def abort(self, raise_: bool = True):
+        """Raise (or clear) the host-mapped abort word: the solve in flight and later ones
+        return EGPU_ERR_ABORT until it is cleared.  Safe from any thread."""
+        check(lib().egpu_abort(self._h, int(bool(raise_))), self._h, "egpu_abort")
+
+    def wait_selftest(self, which: int) -> int:
+        """Status recorded by a kernel whose bounded wait runs out by design (see the header)."""
+        return int(lib().egpu_wait_selftest(self._h, int(which)))
+
     def close(self):
         if self._h:
             for child in list(self._children):

@@ -33,6 +33,7 @@ extern "C" {
 #define EGPU_ERR_TIMEOUT (-4)  /* a bounded device-side wait expired (kernel returned) */
 #define EGPU_ERR_STATE (-5)    /* call out of order (e.g. solve before values exist) */
 #define EGPU_ERR_BUDGET (-6)   /* admission refused: footprint exceeds the HBM budget */
+#define EGPU_ERR_ABORT (-7)    /* the host raised the context's abort word (egpu_abort) */
 
 /* HUTI status values returned by the solve calls (huti_fdefs.h:18-52) */
 #define EGPU_HUTI_CONVERGENCE 1
@@ -105,6 +106,22 @@ const char *egpu_last_error(const egpu_ctx *ctx);
 long long egpu_kernel_launches(const egpu_ctx *ctx);
 /* the cudaStream_t every call of this context runs on (for callers' CUDA events) */
 void *egpu_stream(const egpu_ctx *ctx);
+/* Failure detection, no counterpart in the reference (whose IterSolver has only its status
+ * exits, IterSolve.src:784-792).  Every device-side wait of this context's kernels (grid
+ * barriers, sync-free dependency waits, factorisation flags) is bounded: after `seconds`
+ * (0: the default of 2 s) the kernel records EGPU_ERR_TIMEOUT, unwinds and the call returns
+ * it; the context stays usable. */
+int egpu_set_wait_limit(egpu_ctx *ctx, double seconds);
+/* Cancellation: raise != 0 sets the context's host-mapped abort word, which the running
+ * kernels poll (block 0 every 16th grid barrier, and every long wait); the call in flight
+ * and every later call return EGPU_ERR_ABORT until egpu_abort(ctx, 0).  Makes no CUDA call
+ * and may be called from any host thread while a solve runs. */
+int egpu_abort(egpu_ctx *ctx, int raise);
+/* Self-test of the bounded waits: which = 0 launches two blocks of which one never arrives at
+ * the grid barrier; which = 1 waits for a value that nothing publishes.  Returns the status
+ * the kernel recorded: EGPU_ERR_TIMEOUT once the wait bound has passed (EGPU_ERR_ABORT if the
+ * abort word is raised). */
+int egpu_wait_selftest(egpu_ctx *ctx, int which);
 /* Device blocks freed by the library (matrix copies, work vectors, factors) stay in a
  * process-wide cache per device, at most 24 GB each, for the next matrix of a similar size.
  * egpu_cached_bytes: bytes held for `device` (all devices if device < 0).
@@ -219,8 +236,12 @@ int egpu_dirichlet(egpu_mat *A, int ncon, const int *con_rows, const double *con
  * (about 2.4 MB, held by every GPU that loads the library until the process exits), so:
  * n is limited to EGPU_NOALLOC_MAX_ROWS (larger n returns EGPU_ERR_ARG); calls that
  * overlap on the GPU race on that array; the first call on a device looks up the array's
- * device address and should come before any stream capture.  Runs on the legacy default
- * stream and returns when the solve has finished. */
+ * device address and should come before any stream capture.  That address is kept for the
+ * life of the process: after cudaDeviceReset on the device this entry point must not be
+ * called again.  The Matrix_t arrays are checked on the device before use (Rows(1) = 1 and
+ * non-decreasing, Cols in 1..n, Diag 0 or the row's own diagonal entry); a violation returns
+ * EGPU_ERR_ARG.  Runs on the legacy default stream, returns when the solve has finished and
+ * leaves the caller's current device as it found it. */
 #define EGPU_NOALLOC_MAX_ROWS 32768
 int egpu_cg_noalloc(int device, int n, const int *rows_dev, const int *cols_dev, const int *diag_dev,
                     const double *values_dev, const double *b_dev, double *x_dev, const egpu_params *prm,

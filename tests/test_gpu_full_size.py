@@ -1,69 +1,114 @@
-"""The two single-system workloads at their full sizes on the device, checked through
-size-independent properties (tests/properties.py) where the oracle would take minutes:
+"""The two single-system workloads at their full sizes on the device, against the oracle on the
+same seeded systems, plus the size-independent properties of tests/properties.py:
 
 * Poisson on the 128^3 hex mesh (2,146,689 rows, 57.1 M nonzeros), log-normal element
-  conductivity (sigma 1, seed 1): the assembled matrix annihilates constants, is symmetric and
-  integrates the energy of a linear field to sum_e k_e vol_e; a unit load integrates to the
-  volume; the device SpMV agrees with a host product; with the sine source and symmetric zero
-  Dirichlet conditions, CG + Diagonal in FP64 and in mixed precision both meet the scaled
-  stopping test (1e-10) and agree within 1e-8.
-* Elasticity on the 64^3 hex mesh (823,875 rows, 64.7 M nonzeros): the matrix annihilates the
-  six rigid-body modes and is symmetric, the body force integrates to force x volume; clamped
-  at x = 0, BiCGStab + ILU0 in FP64 and mixed precision meet the stopping test (1e-8) and agree
-  within 1e-8.
+  conductivity (sigma 1, seed 1), source sin(pi x) sin(pi y) sin(pi z), symmetric zero Dirichlet
+  conditions, CG + Diagonal to 1e-10.
+* Elasticity on the 64^3 hex mesh (823,875 rows, 64.7 M nonzeros), E = 200e9, nu = 0.3, body
+  force -1e4 in z, clamped at x = 0, BiCGStab + ILU0 to 1e-8.
+
+Against the oracle (the CPU restatement of the reference path, about a minute of host time
+each): Rows/Cols/Diag/Perm bit-exact; device-assembled Values and RHS, before and after the
+Dirichlet conditions, within 1e-13 of the row scale; the device SpMV within 1e-14 of the row's
+|a||x| scale; ILU0 factors (elasticity) bit-exact; FP64 and mixed solutions within 1e-8 relative
+of the oracle's solution at the same tolerance.
+
+Iteration counts: CG + Diagonal matches the oracle within one.  BiCGStab on the elasticity
+operator is held to 4% of the oracle's count: its iterates depend on the summation order of the
+dot products (the device sums in a fixed tree, the oracle serially), and on this stiff operator
+(scaled condition number ~1e7) that alone moves the count by a few percent: a numpy
+transcription of the same loop on the oracle's own scaled system and ILU0 factors, differing
+only in summing the dot products pairwise, takes 184 iterations against the oracle's 179.  All
+counts end below the tolerance, which the test recomputes on the host from each solution.
 """
 import numpy as np
 import pytest
 
 import elmerfem_b200 as eg
+import oracle
 import properties as P
 from elmerfem_b200 import meshgen
-from helpers import rel
+from helpers import elastic_problem, poisson_problem, rel, row_rel_max
 
 pytestmark = pytest.mark.gpu
+
+
+def _same_pattern(pat, p):
+    assert (pat.n, pat.nnz) == (p.n, p.nnz)
+    for f in ("rows", "cols", "diag", "perm"):
+        assert np.array_equal(getattr(pat, f), getattr(p, f)), f
+
+
+def _spmv_rel(A, p, vals, seed):
+    u = np.random.default_rng(seed).standard_normal(p.n)
+    ref = oracle.spmv(p, vals, u)
+    scale = oracle.spmv(p, np.abs(vals), np.abs(u))
+    return float(np.max(np.abs(A.mv(u) - ref) / scale))
 
 
 def test_poisson_hex128_lognormal(ctx):
     m = meshgen.hex_cube(128)
     k = meshgen.lognormal_conductivity(m.nelem, 1.0, 1)
+    load = meshgen.sine_source(m.coords)
+    tol = 1e-10
+    p, vals0, rhs0, v, b, con = poisson_problem(m, elem_k=k, load=load, sym=True)
+    x_orc, r_orc = oracle.solve(p, v, b, method=oracle.CG, precond=oracle.PREC_DIAGONAL, max_iter=20000, tol=tol)
+    assert r_orc["info"] == 1
+
     pat = eg.create_matrix(m)
     assert (pat.n, pat.nnz) == (129 ** 3, 385 ** 3)
+    _same_pattern(pat, p)
     A = eg.Matrix(ctx, pat)
     try:
         A.bind_assembly(m)
+        # properties of the assembled operator (unit load)
         A.assemble_poisson(elem_k=k, load=np.ones(m.nnodes))
-        vals, rhs = A.values(), A.rhs()
-        assert P.row_sum_defect(pat, vals) < 1e-12
-        assert P.symmetry_defect(pat, vals) < 1e-13
-        assert P.linear_field_energy_defect(m, pat, vals, k) < 1e-11
-        assert abs(rhs.sum() - 1.0) < 1e-11
-        u = np.random.default_rng(5).standard_normal(pat.n)
-        assert rel(A.mv(u), P.csr(pat, vals) @ u) < 1e-14
+        pv, prhs = A.values(), A.rhs()
+        assert P.row_sum_defect(pat, pv) < 1e-12
+        assert P.symmetry_defect(pat, pv) < 1e-13
+        assert P.linear_field_energy_defect(m, pat, pv, k) < 1e-11
+        assert abs(prhs.sum() - 1.0) < 1e-11
 
-        A.assemble_poisson(elem_k=k, load=meshgen.sine_source(m.coords))
-        con = np.sort(pat.perm[m.boundary_nodes(range(1, 7)) - 1]).astype(np.int32)
+        # the workload's system against the oracle's
+        A.assemble_poisson(elem_k=k, load=load)
+        assert row_rel_max(p, A.values(), vals0) < 1e-13
+        assert rel(A.rhs(), rhs0) < 1e-13
+        assert _spmv_rel(A, p, vals0, 5) < 1e-14
         A.dirichlet(con, symmetric=True)
-        v, b = A.values(), A.rhs()
-        assert P.symmetry_defect(pat, v) < 1e-13
-        tol = 1e-10
+        dv, db = A.values(), A.rhs()
+        assert row_rel_max(p, dv, v) < 1e-13
+        assert np.max(np.abs(db - b)) <= 1e-13 * np.max(np.abs(b))
+        assert P.symmetry_defect(pat, dv) < 1e-13
+
         x64, r64 = A.solve(b, params=eg.SolverParams(method=eg.CG, precond=eg.PREC_DIAGONAL, tol=tol,
                                                      max_iter=20000))
         xm, rm = A.solve(b, params=eg.SolverParams(method=eg.CG, precond=eg.PREC_DIAGONAL, tol=tol,
                                                    max_iter=20000, precision=eg.MIXED))
         assert r64["info"] == 1 and rm["info"] == 1
+        assert abs(r64["iters"] - r_orc["iters"]) <= 1
+        assert rel(x64, x_orc) < 1e-8
+        assert rel(xm, x_orc) < 1e-8
         assert P.scaled_residual(pat, v, b, x64) < 1.5 * tol
         assert P.scaled_residual(pat, v, b, xm) < 1.5 * tol
-        assert rel(xm, x64) < 1e-8
     finally:
         A.free()
 
 
 def test_elasticity_hex64(ctx):
     m = meshgen.hex_cube(64)
+    force = (0.0, 0.0, -1e4)
+    tol = 1e-8
+    p, vals0, rhs0, v, b, con = elastic_problem(m, bf=force)
+    vs = v.copy()
+    oracle.scale(p, vs)
+    ilu_orc = oracle.ilu0(p, vs)
+    x_orc, r_orc = oracle.solve(p, v, b, method=oracle.BICGSTAB, precond=oracle.PREC_ILU0, max_iter=20000, tol=tol)
+    assert r_orc["info"] == 1
+
     pat = eg.create_matrix(m, dofs=3)
     assert (pat.n, pat.nnz) == (3 * 65 ** 3, 9 * 193 ** 3)
+    _same_pattern(pat, p)
     A = eg.Matrix(ctx, pat)
-    force = (0.0, 0.0, -1e4)
     try:
         A.bind_assembly(m)
         A.assemble_elastic(200e9, 0.3, force)
@@ -72,19 +117,25 @@ def test_elasticity_hex64(ctx):
         assert P.symmetry_defect(pat, vals) < 1e-13
         for d in range(3):  # row 3 (Perm(node) - 1) + d holds component d
             assert abs(rhs[d::3].sum() - force[d]) < 1e-10 * 1e4
+        assert row_rel_max(p, vals, vals0) < 1e-13
+        assert rel(rhs, rhs0) < 1e-13
+        assert _spmv_rel(A, p, vals0, 6) < 1e-14
 
-        nodes = pat.perm[m.boundary_nodes([1]) - 1]
-        con = np.sort(np.concatenate([3 * (nodes - 1) + d for d in (1, 2, 3)])).astype(np.int32)
         A.dirichlet(con, symmetric=False)
-        v, b = A.values(), A.rhs()
-        tol = 1e-8
+        assert row_rel_max(p, A.values(), v) < 1e-13
+        assert np.max(np.abs(A.rhs() - b)) <= 1e-13 * np.max(np.abs(b))
+        ilu, _ = A.ilu0(scale_system=True)
+        assert np.array_equal(ilu, ilu_orc)
+
         x64, r64 = A.solve(b, params=eg.SolverParams(method=eg.BICGSTAB, precond=eg.PREC_ILU0, tol=tol,
                                                      max_iter=20000))
         xm, rm = A.solve(b, params=eg.SolverParams(method=eg.BICGSTAB, precond=eg.PREC_ILU0, tol=tol,
                                                    max_iter=20000, precision=eg.MIXED))
         assert r64["info"] == 1 and rm["info"] == 1
+        assert abs(r64["iters"] - r_orc["iters"]) <= max(1, int(0.04 * r_orc["iters"]))
+        assert rel(x64, x_orc) < 1e-8
+        assert rel(xm, x_orc) < 1e-8
         assert P.scaled_residual(pat, v, b, x64) < 1.5 * tol
         assert P.scaled_residual(pat, v, b, xm) < 1.5 * tol
-        assert rel(xm, x64) < 1e-8
     finally:
         A.free()

@@ -58,3 +58,33 @@ def test_noalloc_rejects_systems_beyond_its_limit():
     assert rc == -1
     bad = eg.SolverParams(method=eg.BICGSTAB, precond=eg.PREC_ILU0).to_c()
     assert _lib.lib().egpu_cg_noalloc(0, 10, one, one, one, one, one, one, C.byref(bad), None) == -1
+
+
+def test_noalloc_refuses_malformed_arrays(ctx):
+    """The caller's arrays are used in place, so the entry point checks them on the device before
+    any gather: a Cols entry of n + 1 (one past the last row) and a Diag that does not point at
+    its row's diagonal each return EGPU_ERR_ARG, and x is left untouched.  A well-formed call
+    afterwards still solves (the error flag does not stick)."""
+    torch = pytest.importorskip("torch")
+    m = meshgen.hex_cube(5)
+    p, _, _, v, b, _ = poisson_problem(m, sym=True)
+    prm = eg.SolverParams(method=eg.CG, precond=eg.PREC_DIAGONAL, max_iter=500, tol=1e-10)
+    rows, vals, bd = _dev(torch, p.rows), _dev(torch, v), _dev(torch, b)
+    bad_cols = p.cols.copy()
+    bad_cols[p.rows[3] - 1] = p.n + 1
+    bad_diag = p.diag.copy()
+    bad_diag[4] += 1
+    cases = [(_dev(torch, bad_cols), _dev(torch, p.diag)), (_dev(torch, p.cols), _dev(torch, bad_diag))]
+    for cols, diag in cases:
+        x = torch.full((p.n,), 7.0, dtype=torch.float64, device="cuda")
+        cp = prm.to_c()
+        rc = _lib.lib().egpu_cg_noalloc(0, p.n, rows.data_ptr(), cols.data_ptr(), diag.data_ptr(), vals.data_ptr(),
+                                        bd.data_ptr(), x.data_ptr(), C.byref(cp), None)
+        assert rc == -1
+        assert bool((x == 7.0).all())
+    cols, diag = _dev(torch, p.cols), _dev(torch, p.diag)
+    x = torch.zeros(p.n, dtype=torch.float64, device="cuda")
+    cp = prm.to_c()
+    rc = _lib.lib().egpu_cg_noalloc(0, p.n, rows.data_ptr(), cols.data_ptr(), diag.data_ptr(), vals.data_ptr(),
+                                    bd.data_ptr(), x.data_ptr(), C.byref(cp), None)
+    assert rc == 1
