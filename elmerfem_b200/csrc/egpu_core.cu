@@ -193,6 +193,10 @@ __device__ __forceinline__ int ilu_find(const int *Cc, int len, int j) {
   return -1;
 }
 
+// MAXROW > 0: the row's values and columns are staged in shared memory (rows of at most
+// MAXROW entries).  MAXROW == 0: rows of any length; the row is updated in place in its own
+// slots of the output (private to the warp until its done flag is published) and the
+// binary searches run over its columns in global memory.
 template <int MAXROW>
 __global__ void __launch_bounds__(256) k_ilu0_factor(int n, const int *__restrict__ rows,
                                                      const int *__restrict__ cols,
@@ -200,11 +204,10 @@ __global__ void __launch_bounds__(256) k_ilu0_factor(int n, const int *__restric
                                                      const int *__restrict__ order,
                                                      const double *__restrict__ A, double *ilu,
                                                      int *done, int *err) {
-  __shared__ double S_all[8][MAXROW];
-  __shared__ int C_all[8][MAXROW];
+  constexpr int SR = MAXROW > 0 ? MAXROW : 1;
+  __shared__ double S_all[8][SR];
+  __shared__ int C_all[8][SR];
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double *S = S_all[wib];
-  int *Cc = C_all[wib];
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int s = gw; s < n; s += nw) {
@@ -214,13 +217,15 @@ __global__ void __launch_bounds__(256) k_ilu0_factor(int n, const int *__restric
       return;
     }
     const int beg = rows[i], len = rows[i + 1] - beg, nl = diag[i] - beg;
-    if (len > MAXROW || nl < 0 || nl > len) {
+    if ((MAXROW > 0 && len > MAXROW) || nl < 0 || nl > len) {
       if (lane == 0) atomicExch(err, (int)EGPU_ERR_ARG);
       return;
     }
+    double *S = MAXROW > 0 ? S_all[wib] : ilu + beg;
+    const int *Cc = MAXROW > 0 ? C_all[wib] : cols + beg;
     for (int t = lane; t < len; t += 32) {
       S[t] = A[beg + t];
-      Cc[t] = cols[beg + t];
+      if (MAXROW > 0) C_all[wib][t] = cols[beg + t];
     }
     __syncwarp();
     // The dependencies are taken in rounds: the 32 lanes poll the done flags of the next 32
@@ -280,7 +285,8 @@ __global__ void __launch_bounds__(256) k_ilu0_factor(int n, const int *__restric
       __syncwarp();
       m0 = m1;
     }
-    for (int t = lane; t < len; t += 32) ilu[beg + t] = S[t];
+    if (MAXROW > 0)
+      for (int t = lane; t < len; t += 32) ilu[beg + t] = S[t];
     __syncwarp();
     if (lane == 0) {
       __threadfence();
@@ -836,10 +842,6 @@ int ilu_factor(egpu_mat *A, int order) {
   EGPU_CUDA_TRY(ctx, cudaMemsetAsync(A->ilu_done.p, 0, n * sizeof(int), ctx->stream));
   EGPU_CUDA_TRY(ctx, cudaMemsetAsync(ctx->sync.p + 1, 0, sizeof(int), ctx->stream));
   int *err = (int *)(ctx->sync.p + 1);
-  if (A->ilu_max_row > 256) {
-    egpu_set_error(ctx, "ILU: rows of the ILU structure longer than 256 entries are not supported");
-    return EGPU_ERR_ARG;
-  }
   const double *input = A->scaled.p;
   if (order > 0) {
     EGPU_CUDA_TRY(ctx, A->ilu_in.alloc(A->ilu_nnz));
@@ -856,17 +858,20 @@ int ilu_factor(egpu_mat *A, int order) {
     EGPU_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_ilu0_factor<32>, 256, 0));
   } else if (mr <= 128) {
     EGPU_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_ilu0_factor<128>, 256, 0));
-  } else {
+  } else if (mr <= 256) {
     EGPU_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_ilu0_factor<256>, 256, 0));
+  } else {  // rows longer than the shared-memory window: the in-place variant
+    EGPU_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_ilu0_factor<0>, 256, 0));
   }
   // enough warps for about twice the widest level, never more than fit at once
   const int want_blocks = (2 * std::max(1, A->tri.max_width) + 7) / 8;
   int grid = std::max(1, std::min(std::min(bps, 4) * ctx->num_sms, std::max(ctx->num_sms, want_blocks)));
   void *args[] = {(void *)&n, &A->ilu_rows.p, &A->ilu_cols.p, &A->ilu_diag.p, &A->tri.lower_order.p, &input,
                   &A->ilu.p, &A->ilu_done.p, &err};
-  const void *kern = mr <= 32 ? (const void *)k_ilu0_factor<32>
+  const void *kern = mr <= 32    ? (const void *)k_ilu0_factor<32>
                      : mr <= 128 ? (const void *)k_ilu0_factor<128>
-                                  : (const void *)k_ilu0_factor<256>;
+                     : mr <= 256 ? (const void *)k_ilu0_factor<256>
+                                 : (const void *)k_ilu0_factor<0>;
   EGPU_CUDA_TRY(ctx, cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(256), args, 0, ctx->stream));
   k_ilu_invdiag<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, A->ilu_diag.p, A->ilu.p);
   ctx->launches += 2;
@@ -1138,6 +1143,7 @@ int solve_fp64(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_param
   a.maxit = prm->max_iter;
   a.true_residual = 1;
   a.tol = prm->tol;
+  a.divtol = prm->divtol;
   a.b = bs;
   a.x = xs;
   a.w = W;
@@ -1295,6 +1301,7 @@ int krylov_fp64_scaled(egpu_mat *A, const double *bs, double *xs, const egpu_par
   a.maxit = prm->max_iter;
   a.true_residual = 1;
   a.tol = prm->tol;
+  a.divtol = prm->divtol;
   a.b = bs;
   a.x = xs;
   a.w = A->work.p;

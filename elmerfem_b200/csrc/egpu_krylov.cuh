@@ -44,6 +44,7 @@ struct KArgs {
   const int *lower_order, *upper_order;
   int precond, maxit, true_residual;
   double tol;
+  double divtol;                  // Linear System Divergence Tolerance (<= 0: none); GCR, BiCGStab(l)
   const VT *b;
   VT *x;
   VT *w;                          // work vectors, stride ldw
@@ -1419,8 +1420,10 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) gcr_kernel(KArgs<double> a) {
   const double bnorm = sqrt(reduce_partials(a.partials + SLOT_BB * nb, nb, sm));
   double residual = sqrt(reduce_partials(a.partials + SLOT_RR * nb, nb, sm)) / bnorm;
   int info = 0, iters = 0;
+  // IterativeMethods.src:959-961: Converged = Residual < MinTolerance; Diverged = Residual >
+  // MaxTolerance (Linear System Divergence Tolerance) or NaN
   if (residual < a.tol) info = EGPU_HUTI_CONVERGENCE;
-  if (residual != residual) info = 3;  // HUTI_DIVERGENCE
+  if (residual != residual || (a.divtol > 0.0 && residual > a.divtol)) info = 3;  // HUTI_DIVERGENCE
   for (int k = 1; info == 0; ++k) {
     if (k > a.maxit) {
       info = EGPU_HUTI_MAXITER;
@@ -1543,7 +1546,7 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) gcr_kernel(KArgs<double> a) {
     residual = sqrt(reduce_partials(a.partials + SLOT_RR * nb, nb, sm)) / bnorm;
     iters = k;
     if (residual < a.tol) info = EGPU_HUTI_CONVERGENCE;
-    else if (residual != residual) info = 3;  // HUTI_DIVERGENCE
+    else if (residual != residual || (a.divtol > 0.0 && residual > a.divtol)) info = 3;  // :1047-1048
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.out_i[0] = info;
@@ -1689,7 +1692,8 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstabl_kernel(KArgs<double>
   double alpha = 0.0, omega = 1.0, sigma = 1.0, rho0 = 1.0, rho1 = 0.0;
   int info = 0, round = 0, rounds = 0;
   if (errorind < a.tol) info = EGPU_HUTI_CONVERGENCE;
-  bool done_x = info != 0;  // converged at the initial guess: x unchanged
+  else if (a.divtol > 0.0 && errorind > a.divtol) info = 3;  // IterativeMethods.src:626-629
+  bool done_x = info != 0;  // converged or diverged at the initial guess: x unchanged
   for (round = 1; info == 0 && round <= a.maxit; ++round) {
     // --------------------------------------------------------------- the BiCG part
     rounds = round;
@@ -1939,7 +1943,7 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstabl_kernel(KArgs<double>
     if (!grid_barrier(a.bar, a.err, epoch)) return;
     errorind = rnrm / bnrm;
     if (errorind < a.tol) info = EGPU_HUTI_CONVERGENCE;
-    else if (errorind != errorind) info = 3;
+    else if (errorind != errorind || (a.divtol > 0.0 && errorind > a.divtol)) info = 3;  // :817-819
   }
   if (info == 0) info = EGPU_HUTI_MAXITER;
   const int iters = rounds;

@@ -121,12 +121,13 @@ class SolverParams:
     ilu_order: int = 0            # ILU(n) with precond PREC_ILU0 (Linear System ILU Order)
     restart: int = 0              # GCR restart (0: max_iter) / BiCGStab(l) degree (0: 2)
     ilut_tol: float = 0.0         # drop tolerance with precond PREC_ILUT (Linear System ILUT Tolerance)
+    divtol: float = 0.0           # Linear System Divergence Tolerance (0: none); GCR and BiCGStab(l)
 
     def to_c(self) -> _lib.Params:
         return _lib.Params(self.method, self.precond, self.max_iter, self.tol, int(self.scale_system),
                            self.precision, int(self.refactorize), self.precond_recompute, self.inner_tol,
                            self.inner_max_iter, self.max_refinements, self.ilu_order, self.restart,
-                           float(self.ilut_tol))
+                           float(self.ilut_tol), float(self.divtol))
 
     @classmethod
     def from_sif(cls, keywords) -> "SolverParams":
@@ -174,6 +175,7 @@ class SolverParams:
                 raise ValueError("BiCGstabl polynomial degree < 2")
         p = cls(method=methods[meth], precond=pc, restart=restart,
                 ilu_order=ilu_n if pc == PREC_ILU0 else 0, ilut_tol=ilut_tol,
+                divtol=float(kw.get("linear system divergence tolerance", 0.0)),
                 max_iter=int(kw["linear system max iterations"]),
                 tol=float(kw["linear system convergence tolerance"]),
                 scale_system=_bool(kw.get("linear system scaling", True)),

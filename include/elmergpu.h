@@ -38,6 +38,7 @@ extern "C" {
 /* HUTI status values returned by the solve calls (huti_fdefs.h:18-52) */
 #define EGPU_HUTI_CONVERGENCE 1
 #define EGPU_HUTI_MAXITER 2
+#define EGPU_HUTI_DIVERGENCE 3
 #define EGPU_HUTI_CG_RHO 20
 #define EGPU_HUTI_BICGSTAB_RHO 35
 #define EGPU_HUTI_BICGSTAB_SNORM 36
@@ -79,6 +80,11 @@ typedef struct {
    * (as the reference does) and applied on the device; not available to cloned matrices
    * (batches, the server). */
   double ilut_tol;
+  /* Linear System Divergence Tolerance (IterSolve.src:364-366; 0 when absent: no bound, as the
+   * reference's HUGE).  EGPU_GCR and EGPU_BICGSTABL stop with HUTI_DIVERGENCE (3) when the
+   * residual ratio exceeds it (IterativeMethods.src:626-629, 817-819, 959-961, 1047-1048);
+   * HUTI's CG and BiCGStab do not read it, as in the reference. */
+  double divtol;
 } egpu_params;
 
 typedef struct {

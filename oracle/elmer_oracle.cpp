@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -1240,7 +1241,8 @@ int huti_bicgstab(const Ctx &c, double *X, const double *B, int maxit, double to
 // GCR with restart m, IterativeMethods.src:919-1055 (preconditioned search directions
 // T1 = M^-1 r, modified Gram-Schmidt of A T1 against the stored ones, recursive residual
 // stopping test ||r|| / ||b|| < tol)
-int gcr(const Ctx &c, double *x, const double *b, int rounds, double tol, int m, int *iters, double *resid) {
+int gcr(const Ctx &c, double *x, const double *b, int rounds, double tol, double maxtol, int m, int *iters,
+        double *resid) {
   const int n = c.n;
   std::vector<double> r(n), T1(n), T2(n);
   std::vector<std::vector<double>> S(std::max(0, m - 1), std::vector<double>(n, 0.0)),
@@ -1253,7 +1255,7 @@ int gcr(const Ctx &c, double *x, const double *b, int rounds, double tol, int m,
   *iters = 0;
   *resid = residual;
   if (residual < tol) return HUTI_CONVERGENCE;
-  if (residual != residual) return HUTI_DIVERGENCE;
+  if (residual > maxtol || residual != residual) return HUTI_DIVERGENCE;  // :959-961
   for (int k = 1; k <= rounds; ++k) {
     int j;
     if (k % m == 0) {
@@ -1287,7 +1289,7 @@ int gcr(const Ctx &c, double *x, const double *b, int rounds, double tol, int m,
     *iters = k;
     *resid = residual;
     if (residual < tol) return HUTI_CONVERGENCE;
-    if (residual != residual) return HUTI_DIVERGENCE;
+    if (residual > maxtol || residual != residual) return HUTI_DIVERGENCE;  // :1047-1048
   }
   return HUTI_MAXITER;
 }
@@ -1321,7 +1323,7 @@ void small_lu_solve(int m, const double *a, int lda, const int *piv, double *bv)
 
 // BiCGStab(l), IterativeMethods.src:559-834 (right preconditioned, convex polynomial part,
 // reliable residual / solution updates with delta = 1e-2; stop on the recursive residual)
-int bicgstabl(const Ctx &c, double *x_out, const double *b, int max_rounds, double tol, int l, int *iters,
+int bicgstabl(const Ctx &c, double *x_out, const double *b, int max_rounds, double tol, double maxtol, int l, int *iters,
               double *resid) {
   const int n = c.n;
   const double delta = 1.0e-2;
@@ -1339,6 +1341,7 @@ int bicgstabl(const Ctx &c, double *x_out, const double *b, int max_rounds, doub
   *iters = 0;
   *resid = errorind;
   if (errorind < tol) return HUTI_CONVERGENCE;
+  if (errorind > maxtol) return HUTI_DIVERGENCE;  // IterativeMethods.src:626-629
   rr = r[0];
   bp = r[0];
   xp = x;
@@ -1445,7 +1448,7 @@ int bicgstabl(const Ctx &c, double *x_out, const double *b, int max_rounds, doub
     }
     errorind = rnrm / bnrm;
     if (errorind < tol) { info = HUTI_CONVERGENCE; break; }
-    if (errorind != errorind) { info = HUTI_DIVERGENCE; break; }
+    if (errorind > maxtol || errorind != errorind) { info = HUTI_DIVERGENCE; break; }  // :817-819
   }
   *iters = std::min(round, max_rounds);
   *resid = errorind;
@@ -1517,14 +1520,16 @@ extern "C" int orc_solve(int n, const int *rows, const int *cols, const int *dia
   const int apply = prm->precond == ORC_PREC_ILUT ? ORC_PREC_ILU0 : prm->precond;
   Ctx c{n, rows, cols, diag, values.data(), ilu.empty() ? nullptr : ilu.data(), apply,
         prm->omp_threads, irows, icols, idiag};
+  // HUTI_MAXTOLERANCE: Linear System Divergence Tolerance, HUGE when absent (IterSolve.src:364-366)
+  const double maxtol = prm->divtol > 0.0 ? prm->divtol : std::numeric_limits<double>::max();
   if (prm->method == ORC_CG)
     r.info = huti_cg(c, x, b.data(), prm->max_iter, prm->tol, &r.iters, &r.residual);
   else if (prm->method == ORC_GCR)  // restart: Linear System GCR Restart, else Max Iterations
-    r.info = gcr(c, x, b.data(), prm->max_iter, prm->tol, prm->restart > 0 ? prm->restart : prm->max_iter,
+    r.info = gcr(c, x, b.data(), prm->max_iter, prm->tol, maxtol, prm->restart > 0 ? prm->restart : prm->max_iter,
                  &r.iters, &r.residual);
   else if (prm->method == ORC_BICGSTABL)  // BiCGstabl polynomial degree, default 2
-    r.info = bicgstabl(c, x, b.data(), prm->max_iter, prm->tol, prm->restart >= 2 ? prm->restart : 2, &r.iters,
-                       &r.residual);
+    r.info = bicgstabl(c, x, b.data(), prm->max_iter, prm->tol, maxtol, prm->restart >= 2 ? prm->restart : 2,
+                       &r.iters, &r.residual);
   else
     r.info = huti_bicgstab(c, x, b.data(), prm->max_iter, prm->tol, &r.iters, &r.residual);
   if (prm->scale_system) backscale(n, rows, cols, values.data(), b.data(), x, D.data(), rs);

@@ -57,6 +57,7 @@ typedef struct {
   int ilu_order;       /* ORC_PREC_ILU0 with ilu_order n > 0: ILU(n) (Linear System ILU Order) */
   int restart;         /* GCR: Linear System GCR Restart (0: Max Iterations); BiCGStab(l): degree l */
   double ilut_tol;     /* ORC_PREC_ILUT: Linear System ILUT Tolerance (0 when absent, as ListGetCReal) */
+  double divtol;       /* GCR / BiCGStab(l): Linear System Divergence Tolerance (<= 0: HUGE, as when absent) */
 } orc_params;
 typedef struct {
   int info;            /* HUTI status code (huti_fdefs.h) */

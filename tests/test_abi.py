@@ -72,6 +72,11 @@ def test_sif_gcr_bicgstabl():
                                                "BiCGstabl polynomial degree": 4}))
     assert (q.method, q.restart) == (eg.BICGSTABL, 4)
     assert eg.SolverParams.from_sif(dict(base, **{"Linear System Iterative Method": "BiCGStabl"})).restart == 0
+    # Linear System Divergence Tolerance (IterSolve.src:364-366): absent -> no bound (0 here, HUGE there)
+    assert p.divtol == 0.0 and p.to_c().divtol == 0.0
+    d = eg.SolverParams.from_sif(dict(base, **{"Linear System Iterative Method": "GCR",
+                                               "Linear System Divergence Tolerance": 1e4}))
+    assert d.divtol == 1e4 and d.to_c().divtol == 1e4
     with pytest.raises(ValueError):
         eg.SolverParams.from_sif(dict(base, **{"Linear System Iterative Method": "BiCGStabl",
                                                "BiCGstabl polynomial degree": 1}))

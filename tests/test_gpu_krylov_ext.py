@@ -86,3 +86,29 @@ def test_gcr_maxiter_status(ctx):
     x, r = A.solve(b, params=eg.SolverParams(method=eg.GCR, precond=eg.PREC_NONE, max_iter=3, tol=1e-14,
                                              abort_not_converged=False))
     assert r["info"] == 2 and r["iters"] == 3
+
+
+@pytest.mark.parametrize("method", [eg.GCR, eg.BICGSTABL], ids=["gcr", "bicgstabl"])
+def test_divergence_tolerance(ctx, method):
+    """Linear System Divergence Tolerance (IterSolve.src:364-366): GCR and BiCGStab(l) stop with
+    HUTI_DIVERGENCE (3) when the residual ratio exceeds it (IterativeMethods.src:626-629,
+    959-961).  A far-off initial guess exceeds a bound of 10 before the first iteration, as in the
+    oracle; a bound the decreasing residual never reaches leaves the solve as it was."""
+    p, _, _, v, b, _ = PROBLEMS["hex8"]()
+    omethod = oracle.GCR if method == eg.GCR else oracle.BICGSTABL
+    A = eg.Matrix(ctx, _pat(p), v)
+    x0 = np.full(p.n, 100.0)
+    x_ref, r_ref = oracle.solve(p, v, b, method=omethod, precond=eg.PREC_DIAGONAL, max_iter=3000, tol=1e-10,
+                                x0=x0, divtol=10.0)
+    assert r_ref["info"] == 3 and r_ref["iters"] == 0
+    x, r = A.solve(b, x0=x0, params=eg.SolverParams(method=method, precond=eg.PREC_DIAGONAL, max_iter=3000, tol=1e-10,
+                                                    divtol=10.0, abort_not_converged=False))
+    assert r["info"] == 3 and r["iters"] == 0
+    assert rel(x, x_ref) < 1e-12
+    x_ref, r_ref = oracle.solve(p, v, b, method=omethod, precond=eg.PREC_DIAGONAL, max_iter=3000, tol=1e-10,
+                                divtol=1e3)
+    x, r = A.solve(b, params=eg.SolverParams(method=method, precond=eg.PREC_DIAGONAL, max_iter=3000, tol=1e-10,
+                                             divtol=1e3))
+    assert r_ref["info"] == 1 and r["info"] == 1
+    assert abs(r["iters"] - r_ref["iters"]) <= 1
+    assert rel(x, x_ref) < 1e-8
