@@ -63,14 +63,34 @@ def poisson_stream(n: int, rate: float, m_lo: int, m_hi: int, seed: int, sigma: 
     return [Request(i, int(ms[i]), seed * 100003 + i, float(t[i]), sigma) for i in range(n)]
 
 
+def build_meshes(ms, threads: int = 0) -> dict:
+    """{m: (hex mesh, CRS pattern)} for every distinct m, built on host threads (CreateMatrix
+    runs in the library without the interpreter lock); a start-up cost of the serving loops."""
+    import concurrent.futures as cf
+    import os
+
+    ms = sorted(set(int(m) for m in ms))
+
+    def one(m):
+        mesh = meshgen.hex_cube(m)
+        return m, (mesh, create_matrix(mesh))
+
+    nt = threads if threads > 0 else min(16, os.cpu_count() or 1)
+    with cf.ThreadPoolExecutor(max_workers=nt) as ex:
+        return dict(ex.map(one, sorted(ms, reverse=True)))
+
+
 class MeshPrototype:
     """Resident pattern + bound mesh of one mesh size (built once, cloned per request); with a
-    preconditioner given, its one-time structures are built here too."""
+    preconditioner given, its one-time structures are built here too.  built: (mesh, pattern)
+    from build_meshes, else both are made here."""
 
-    def __init__(self, ctx: Context, m: int, precond: int | None = None):
+    def __init__(self, ctx: Context, m: int, precond: int | None = None, built: tuple | None = None):
         self.m = m
-        self.mesh = meshgen.hex_cube(m)
-        self.pattern = create_matrix(self.mesh)
+        if built is None:
+            built = (meshgen.hex_cube(m), None)
+        self.mesh = built[0]
+        self.pattern = built[1] if built[1] is not None else create_matrix(self.mesh)
         self.A = Matrix(ctx, self.pattern)
         self.A.bind_assembly(self.mesh)
         if precond is not None:
@@ -187,12 +207,14 @@ class NativeSolveServer:
                     "egpu_server_pattern")
         return pid.value
 
-    def mesh_prototype(self, m: int) -> int:
-        """Pattern of the m^3 hex mesh with the mesh bound for device assembly (once per m)."""
+    def mesh_prototype(self, m: int, built: tuple | None = None) -> int:
+        """Pattern of the m^3 hex mesh with the mesh bound for device assembly (once per m);
+        built: (mesh, pattern) from build_meshes."""
         if m in self.patterns:
             return self.patterns[m][0]
-        mesh = meshgen.hex_cube(m)
-        pat = create_matrix(mesh)
+        mesh, pat = built if built is not None else (meshgen.hex_cube(m), None)
+        if pat is None:
+            pat = create_matrix(mesh)
         pid = self.pattern(pat)
         self._check(self._lib.lib().egpu_server_pattern_mesh(
             self._h, pid, mesh.nnodes, np.ascontiguousarray(mesh.coords, np.float64), 3, mesh.nelem,

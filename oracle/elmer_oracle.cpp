@@ -1096,15 +1096,42 @@ struct Ctx {
   const int *irows, *icols, *idiag;  // ILU structure (the matrix's for ILU0)
 };
 
+// Threads for the vector operations (BLAS-1 and the elementwise updates) of the solve in
+// flight: 0 runs them serially, as the vendored netlib BLAS does (the checker's setting);
+// t > 0 splits every loop into t static chunks, as a threaded BLAS would (the timed CPU
+// baseline's setting).  Dot products then sum each chunk serially and the chunk sums in chunk
+// order, so the result is deterministic for a given t.
+thread_local int t_blas_threads = 0;
+
 double dot(int n, const double *x, const double *y) {  // ddot, restated as a plain sum
+  const int t = t_blas_threads;
+  if (t <= 1) {
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s = s + x[i] * y[i];
+    return s;
+  }
+  std::vector<double> part(t, 0.0);
+#pragma omp parallel for num_threads(t) schedule(static, 1)
+  for (int c = 0; c < t; ++c) {
+    const long long lo = (long long)n * c / t, hi = (long long)n * (c + 1) / t;
+    double s = 0.0;
+    for (long long i = lo; i < hi; ++i) s = s + x[i] * y[i];
+    part[c] = s;
+  }
   double s = 0.0;
-  for (int i = 0; i < n; ++i) s = s + x[i] * y[i];
+  for (int c = 0; c < t; ++c) s = s + part[c];
   return s;
 }
 double nrm2(int n, const double *x) {  // dnrm2, restated as sqrt of the plain sum of squares
-  double s = 0.0;
-  for (int i = 0; i < n; ++i) s = s + x[i] * x[i];
-  return std::sqrt(s);
+  return std::sqrt(dot(n, x, x));
+}
+
+// an elementwise vector update f(i) for i in [0, n), on t_blas_threads threads
+template <typename F>
+void vec_loop(int n, F &&f) {
+  const int t = t_blas_threads;
+#pragma omp parallel for num_threads(t > 1 ? t : 1) schedule(static) if (t > 1)
+  for (int i = 0; i < n; ++i) f(i);
 }
 
 void matvec(const Ctx &c, const double *u, double *v) {
@@ -1116,15 +1143,15 @@ void matvec(const Ctx &c, const double *u, double *v) {
 void pcond(const Ctx &c, double *u, const double *v) {
   const int n = c.n;
   if (c.precond == ORC_PREC_ILU0) {
-    for (int i = 0; i < n; ++i) u[i] = v[i];
+    vec_loop(n, [&](int i) { u[i] = v[i]; });
     orc_lusolve(n, c.irows, c.icols, c.idiag, c.ilu, u);
   } else if (c.precond == ORC_PREC_DIAGONAL) {
-    for (int i = 1; i <= n; ++i) {
-      double d = c.values[c.diag[i - 1] - 1];
-      u[i - 1] = std::fabs(d) > AEPS ? v[i - 1] / d : v[i - 1];
-    }
+    vec_loop(n, [&](int i) {
+      double d = c.values[c.diag[i] - 1];
+      u[i] = std::fabs(d) > AEPS ? v[i] / d : v[i];
+    });
   } else {
-    for (int i = 0; i < n; ++i) u[i] = v[i];
+    vec_loop(n, [&](int i) { u[i] = v[i]; });
   }
 }
 
@@ -1138,27 +1165,27 @@ int huti_cg(const Ctx &c, double *X, const double *B, int maxit, double tol, int
   double rho = 0, oldrho = 1, alpha, beta, residual = 0;
   int info = 0;
   matvec(c, X, R.data());
-  for (int i = 0; i < n; ++i) R[i] = B[i] - R[i];
+  vec_loop(n, [&](int i) { R[i] = B[i] - R[i]; });
   while (true) {
     pcond(c, Q.data(), R.data());
-    for (int i = 0; i < n; ++i) Z[i] = Q[i];  // pcondrsubr = dummy copy
+    vec_loop(n, [&](int i) { Z[i] = Q[i]; });  // pcondrsubr = dummy copy
     rho = dot(n, R.data(), Z.data());
     if (rho == 0) {
       info = HUTI_CG_RHO;
       break;
     }
     if (iter_count == 1) {
-      for (int i = 0; i < n; ++i) P[i] = Z[i];
+      vec_loop(n, [&](int i) { P[i] = Z[i]; });
     } else {
       beta = rho / oldrho;
-      for (int i = 0; i < n; ++i) P[i] = Z[i] + beta * P[i];
+      vec_loop(n, [&](int i) { P[i] = Z[i] + beta * P[i]; });
     }
     matvec(c, P.data(), Q.data());
     alpha = rho / dot(n, P.data(), Q.data());
-    for (int i = 0; i < n; ++i) X[i] = X[i] + alpha * P[i];
-    for (int i = 0; i < n; ++i) R[i] = R[i] - alpha * Q[i];
+    vec_loop(n, [&](int i) { X[i] = X[i] + alpha * P[i]; });
+    vec_loop(n, [&](int i) { R[i] = R[i] - alpha * Q[i]; });
     matvec(c, X, Z.data());
-    for (int i = 0; i < n; ++i) Z[i] = Z[i] - B[i];
+    vec_loop(n, [&](int i) { Z[i] = Z[i] - B[i]; });
     residual = nrm2(n, Z.data()) / rhsnorm;
     if (residual < tol) {
       info = HUTI_CONVERGENCE;
@@ -1186,7 +1213,7 @@ int huti_bicgstab(const Ctx &c, double *X, const double *B, int maxit, double to
   double rho, oldrho = 1, omega = 1, alpha = 0, beta, residual = 0;
   int info = 0;
   matvec(c, X, R.data());
-  for (int i = 0; i < n; ++i) R[i] = B[i] - R[i];
+  vec_loop(n, [&](int i) { R[i] = B[i] - R[i]; });
   RTLD = R;
   std::fill(P.begin(), P.end(), 0.0);
   std::fill(V.begin(), V.end(), 0.0);
@@ -1197,26 +1224,26 @@ int huti_bicgstab(const Ctx &c, double *X, const double *B, int maxit, double to
       break;
     }
     beta = (rho * alpha) / (oldrho * omega);
-    for (int i = 0; i < n; ++i) P[i] = R[i] + beta * (P[i] - omega * V[i]);
+    vec_loop(n, [&](int i) { P[i] = R[i] + beta * (P[i] - omega * V[i]); });
     pcond(c, V.data(), P.data());
-    for (int i = 0; i < n; ++i) T1V[i] = V[i];
+    vec_loop(n, [&](int i) { T1V[i] = V[i]; });
     matvec(c, T1V.data(), V.data());
     alpha = rho / dot(n, RTLD.data(), V.data());
-    for (int i = 0; i < n; ++i) S[i] = R[i] - alpha * V[i];
+    vec_loop(n, [&](int i) { S[i] = R[i] - alpha * V[i]; });
     residual = nrm2(n, S.data());
     if (residual < HUTI_EPSILON) {
-      for (int i = 0; i < n; ++i) X[i] = X[i] + alpha * T1V[i];
+      vec_loop(n, [&](int i) { X[i] = X[i] + alpha * T1V[i]; });
       info = HUTI_BICGSTAB_SNORM;
       break;
     }
     pcond(c, T.data(), S.data());
-    for (int i = 0; i < n; ++i) T2V[i] = T[i];
+    vec_loop(n, [&](int i) { T2V[i] = T[i]; });
     matvec(c, T2V.data(), T.data());
     omega = dot(n, T.data(), S.data()) / dot(n, T.data(), T.data());
-    for (int i = 0; i < n; ++i) X[i] = X[i] + alpha * T1V[i] + omega * T2V[i];
-    for (int i = 0; i < n; ++i) R[i] = S[i] - omega * T[i];
+    vec_loop(n, [&](int i) { X[i] = X[i] + alpha * T1V[i] + omega * T2V[i]; });
+    vec_loop(n, [&](int i) { R[i] = S[i] - omega * T[i]; });
     matvec(c, X, T2V.data());
-    for (int i = 0; i < n; ++i) T1V[i] = T2V[i] - B[i];
+    vec_loop(n, [&](int i) { T1V[i] = T2V[i] - B[i]; });
     residual = nrm2(n, T1V.data()) / rhsnorm;
     if (residual < tol) {
       info = HUTI_CONVERGENCE;
@@ -1520,6 +1547,11 @@ extern "C" int orc_solve(int n, const int *rows, const int *cols, const int *dia
   const int apply = prm->precond == ORC_PREC_ILUT ? ORC_PREC_ILU0 : prm->precond;
   Ctx c{n, rows, cols, diag, values.data(), ilu.empty() ? nullptr : ilu.data(), apply,
         prm->omp_threads, irows, icols, idiag};
+  struct BlasThreads {  // the vector operations' thread count for this solve only
+    int saved;
+    explicit BlasThreads(int t) : saved(t_blas_threads) { t_blas_threads = t > 0 ? t : 0; }
+    ~BlasThreads() { t_blas_threads = saved; }
+  } blas_threads_scope(prm->blas_threads);
   // HUTI_MAXTOLERANCE: Linear System Divergence Tolerance, HUGE when absent (IterSolve.src:364-366)
   const double maxtol = prm->divtol > 0.0 ? prm->divtol : std::numeric_limits<double>::max();
   if (prm->method == ORC_CG)

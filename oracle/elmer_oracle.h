@@ -58,6 +58,8 @@ typedef struct {
   int restart;         /* GCR: Linear System GCR Restart (0: Max Iterations); BiCGStab(l): degree l */
   double ilut_tol;     /* ORC_PREC_ILUT: Linear System ILUT Tolerance (0 when absent, as ListGetCReal) */
   double divtol;       /* GCR / BiCGStab(l): Linear System Divergence Tolerance (<= 0: HUGE, as when absent) */
+  int blas_threads;    /* threads for the vector operations: 0 serial (netlib BLAS, the checker's
+                          setting), t > 0 t static chunks (a threaded BLAS; the timed baseline) */
 } orc_params;
 typedef struct {
   int info;            /* HUTI status code (huti_fdefs.h) */

@@ -56,12 +56,25 @@ def test_reference_arm_under_two_ranks_prints_one_line():
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
            "127.0.0.1", "--master-port", str(_free_port()), "bench.py", "--impl", "reference", "--workload",
            "poisson32_bicgstab_ilu0", "--gpus", "2", "--steps", "1", "--warmup", "1"]
+    import time
+
+    t0 = time.perf_counter()
     out = subprocess.run(cmd, cwd=root, env=env, capture_output=True, text=True, timeout=600)
+    wall = time.perf_counter() - t0
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [json.loads(s) for s in out.stdout.splitlines() if s.startswith("{")]
     assert len(lines) == 1
     d = lines[0]
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+    # every step is one whole oracle solve: ms_per_step is a time a step took, and the steps fit
+    # in the run's own wall time
+    assert abs(d["value"] * d["ms_per_step"] / 1000.0 - 1.0) < 1e-9
+    assert d["steps"] * d["ms_per_step"] / 1000.0 < wall
+    # the same config as the GPU arm's line (bench.headline_config)
+    import bench
+
+    _, _, cfg = bench.workload_spec("poisson32_bicgstab_ilu0")
+    assert d["config"] == bench.headline_config(cfg, 33 ** 3, 97 ** 3, 2)
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
 
