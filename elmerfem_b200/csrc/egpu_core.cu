@@ -1845,6 +1845,7 @@ extern "C" int egpu_matrix_bind(egpu_ctx *ctx, int n, const int *rows, const int
   if (values) {
     cudaMemcpyAsync(A->values.p, values, nnz * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
     A->has_values = true;
+  A->t_fp64 = A->t_mixed = 0.0;
   } else {
     cudaMemsetAsync(A->values.p, 0, nnz * sizeof(double), ctx->stream);
   }
@@ -1937,6 +1938,7 @@ extern "C" int egpu_matrix_update_values(egpu_mat *A, const double *values) {
                                      ctx->stream));
   EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   A->has_values = true;
+  A->t_fp64 = A->t_mixed = 0.0;
   return EGPU_OK;
 }
 
@@ -2074,8 +2076,28 @@ extern "C" int egpu_iter_solve_dev(egpu_mat *A, const double *b_dev, double *x_d
   }
   cudaSetDevice(A->ctx->device);
   if (!b_dev) b_dev = A->rhs.p;
-  if (prm->precision == EGPU_MIXED) return egpu::solve_mixed(A, b_dev, x_dev, prm, res);
-  return egpu::solve_fp64(A, b_dev, x_dev, prm, res);
+  egpu_result r{};
+  int rc;
+  // Mixed precision is a request for the faster of the two paths at the same tolerance: on
+  // operators where rounding the scaled matrix to FP32 costs more refinements than the FP32
+  // iterations save (latency-bound triangular solves, stiff elasticity), the FP64 drop-in is
+  // faster.  Once both have solved the current values, a mixed request takes the one measured
+  // faster (EGPU_MIXED_AUTO=0 keeps mixed).  CG / BiCGStab only; GCR and BiCGStab(l) are FP64.
+  const char *aenv = std::getenv("EGPU_MIXED_AUTO");
+  const bool auto_ok = !(aenv && aenv[0] == '0');
+  const bool krylov32 = prm->method == EGPU_CG || prm->method == EGPU_BICGSTAB;
+  if (prm->precision == EGPU_MIXED && krylov32 &&
+      !(auto_ok && A->t_fp64 > 0.0 && A->t_mixed > 0.0 && A->t_fp64 < A->t_mixed)) {
+    rc = egpu::solve_mixed(A, b_dev, x_dev, prm, &r);
+    r.precision_used = EGPU_MIXED;
+    if (rc > 0) A->t_mixed = r.seconds;
+  } else {
+    rc = egpu::solve_fp64(A, b_dev, x_dev, prm, &r);
+    r.precision_used = EGPU_FP64;
+    if (rc > 0) A->t_fp64 = r.seconds;
+  }
+  if (res) *res = r;
+  return rc;
 }
 
 extern "C" int egpu_iter_solve(egpu_mat *A, const double *b, double *x, const egpu_params *prm,
