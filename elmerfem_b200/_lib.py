@@ -117,6 +117,7 @@ PROTOTYPES = {
     "egpu_ilu_build": (C.c_int, [_vp, C.c_int, C.c_int]),
     "egpu_ilu0_download": (C.c_int, [_vp, _vp, _vp]),
     "egpu_lu_precondition": (C.c_int, [_vp, _f64p, _f64p]),
+    "egpu_lu_precondition_dev": (C.c_int, [_vp, _vp, _vp]),
     "egpu_cg_noalloc": (C.c_int, [C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, C.POINTER(Params),
                                   C.POINTER(Result)]),
     "egpu_batch_create": (C.c_int, [_vp, C.POINTER(Params), C.POINTER(_vp)]),

@@ -2282,6 +2282,12 @@ extern "C" int egpu_ilu0_download(egpu_mat *A, double *ilu_values, double *diag_
   return EGPU_OK;
 }
 
+extern "C" int egpu_lu_precondition_dev(egpu_mat *A, const double *v_dev, double *u_dev) {
+  if (!A || !A->ilu_valid || !v_dev || !u_dev || v_dev == u_dev) return EGPU_ERR_STATE;
+  cudaSetDevice(A->ctx->device);
+  return egpu::lu_apply(A, v_dev, u_dev);
+}
+
 extern "C" int egpu_lu_precondition(egpu_mat *A, const double *v, double *u) {
   if (!A || !A->ilu_valid || !v || !u) return EGPU_ERR_STATE;
   egpu_ctx *ctx = A->ctx;

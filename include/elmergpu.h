@@ -201,6 +201,9 @@ int egpu_ilut_build(egpu_mat *A, int scale_system, double tol);
 int egpu_ilu_download(egpu_mat *A, int *ilu_rows, int *ilu_cols, int *ilu_diag, double *ilu_values);
 int egpu_ilu0_download(egpu_mat *A, double *ilu_values, double *diag_scaling);
 int egpu_lu_precondition(egpu_mat *A, const double *v, double *u);
+/* the same on device vectors (v_dev != u_dev), on the context's stream; returns when applied.
+ * ParLUPrec (SParIterPrecond.src:86-146) of a rank's block in the row-sharded solve */
+int egpu_lu_precondition_dev(egpu_mat *A, const double *v_dev, double *u_dev);
 /* The triangular-solve schedule built for the matrix's ILU structure (diagnostics): info[0]
  * rows per sync-free slot group (> 1: node-block solve), [1] / [2] lower / upper dependency
  * levels (of slot groups), [3] most rows in one level, [4] / [5] single-block schedule usable

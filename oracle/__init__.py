@@ -33,7 +33,7 @@ class _Params(C.Structure):
     _fields_ = [("method", C.c_int), ("precond", C.c_int), ("max_iter", C.c_int),
                 ("tol", C.c_double), ("scale_system", C.c_int), ("omp_threads", C.c_int),
                 ("ilu_order", C.c_int), ("restart", C.c_int), ("ilut_tol", C.c_double), ("divtol", C.c_double),
-                ("blas_threads", C.c_int)]
+                ("blas_threads", C.c_int), ("block_starts", C.c_void_p), ("nblocks", C.c_int)]
 
 
 class _Result(C.Structure):
@@ -158,12 +158,15 @@ def dirichlet(pat: Pattern, values, rhs, con_rows, con_vals=None, symmetric=Fals
 
 
 def solve(pat: Pattern, values, b, method=BICGSTAB, precond=PREC_ILU0, max_iter=1000, tol=1e-10,
-          x0=None, scale=True, threads=0, ilu_order=0, restart=0, ilut_tol=0.0, divtol=0.0, blas_threads=0):
+          x0=None, scale=True, threads=0, ilu_order=0, restart=0, ilut_tol=0.0, divtol=0.0, blas_threads=0,
+          block_starts=None):
     """orc_solve.  threads: SpMV threads (0: all); blas_threads: threads for the vector operations
-    (0: serial as the reference's netlib BLAS, the checker's setting; > 0 for the timed baseline)."""
+    (0: serial as the reference's netlib BLAS, the checker's setting; > 0 for the timed baseline);
+    block_starts (0-based row offsets of a partition, nblocks + 1 entries): block-Jacobi ILU0."""
     x = np.zeros(pat.n) if x0 is None else np.array(x0, dtype=np.float64)
+    bst = None if block_starts is None else np.ascontiguousarray(block_starts, np.int32)
     p = _Params(method, precond, max_iter, tol, int(scale), threads, ilu_order, restart, ilut_tol, divtol,
-                blas_threads)
+                blas_threads, None if bst is None else bst.ctypes.data, 0 if bst is None else len(bst) - 1)
     r = _Result()
     lib().orc_solve(pat.n, pat.rows, pat.cols, pat.diag, np.ascontiguousarray(values, np.float64),
                     np.ascontiguousarray(b, np.float64), x, C.byref(p), C.byref(r))

@@ -1533,6 +1533,30 @@ extern "C" int orc_solve(int n, const int *rows, const int *cols, const int *dia
     idiag = id.data();
     ilu.assign(nz, 0.0);
     orc_iluk(n, rows, cols, values.data(), irows, icols, idiag, ilu.data());
+  } else if (prm->precond == ORC_PREC_ILU0 && prm->nblocks > 1 && prm->block_starts) {
+    // block-Jacobi ILU0: the matrix restricted to its diagonal blocks, factored whole (the
+    // blocks are independent, so this equals factoring each block on its own)
+    std::vector<int> blk(n);
+    for (int k = 0; k < prm->nblocks; ++k)
+      for (int i = prm->block_starts[k]; i < prm->block_starts[k + 1]; ++i) blk[i] = k;
+    ir.assign(n + 1, 1);
+    id.assign(n, 0);
+    std::vector<double> bv;
+    for (int i = 0; i < n; ++i) {
+      for (int j = rows[i] - 1; j < rows[i + 1] - 1; ++j) {
+        const int c = cols[j] - 1;
+        if (blk[c] != blk[i]) continue;
+        if (c == i) id[i] = (int)ic.size() + 1;
+        ic.push_back(c + 1);
+        bv.push_back(values[j]);
+      }
+      ir[i + 1] = (int)ic.size() + 1;
+    }
+    irows = ir.data();
+    icols = ic.data();
+    idiag = id.data();
+    ilu.assign(bv.size(), 0.0);
+    orc_ilu0(n, irows, icols, idiag, bv.data(), ilu.data());
   } else if (prm->precond == ORC_PREC_ILU0) {
     ilu.assign(values.size(), 0.0);
     orc_ilu0(n, rows, cols, diag, values.data(), ilu.data());

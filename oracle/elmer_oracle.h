@@ -60,6 +60,13 @@ typedef struct {
   double divtol;       /* GCR / BiCGStab(l): Linear System Divergence Tolerance (<= 0: HUGE, as when absent) */
   int blas_threads;    /* threads for the vector operations: 0 serial (netlib BLAS, the checker's
                           setting), t > 0 t static chunks (a threaded BLAS; the timed baseline) */
+  /* ORC_PREC_ILU0 with nblocks > 1: block-Jacobi ILU0 of a row partition (the parallel
+   * preconditioner, ParILU0 SParIterPrecond.src:234-301, which factors each partition's
+   * InsideMatrix): rows [block_starts[k], block_starts[k+1]) (0-based, nblocks + 1 entries)
+   * form block k, and the factor is CRS_IncompleteLU of the matrix with every entry coupling
+   * two blocks removed */
+  const int *block_starts;
+  int nblocks;
 } orc_params;
 typedef struct {
   int info;            /* HUTI status code (huti_fdefs.h) */
