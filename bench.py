@@ -109,24 +109,21 @@ def compact_offset_fraction(pat):
     return 1.0 - float((32 * wmax[:full][shared]).sum()) / float(tot)
 
 
-def algorithmic_bytes_per_iter(method, precond, precision, n, nnz, cols16, off_frac=1.0, unit_diag=False,
-                               single_reduction=True):
+def algorithmic_bytes_per_iter(method, precond, precision, n, nnz, cols16, off_frac=1.0, unit_diag=False):
     """Bytes one Krylov iteration must move (matrix streamed once per SpMV pass, vectors once).
 
     CG+Diagonal, FP32 inner (refinement): SpMV 4z values + 2z·off_frac offsets (int16 column
     offsets, stored once per slice where all rows share them) or 4z cols + 4n rowptr + P gather
-    4n + Q write 4n + epilogue P 4n; P update 12n; x/r/z update 32n: 60n of vectors.  When the
-    scaled diagonal is 1.0f everywhere (unit_diag) or there is no preconditioner, M = I and the
-    single-reduction kernel runs: SpMV of R (gather 4n, W write 4n) and one update pass reading
-    R W P S X and writing P S X R (36n): 44n of vectors (the batched kernel, which keeps HUTI's
-    three phases, moves 48n: single_reduction=False).
+    4n + Q write 4n + epilogue P 4n; P update 12n; x/r/z update 32n.  When the scaled diagonal
+    is 1.0f everywhere (unit_diag) the Jacobi step is the identity: no diagonal read and no Z
+    write, 48n of vectors instead of 60n.
     CG+Diagonal, FP64 drop-in (x_k residual fused in the next SpMV): SpMV 8z + the same offsets
     + 4n + 16n gathers + 8n write + 16n epilogue; P update 24n; update 64n.
     """
     cbytes = (2 * off_frac if cols16 else 4) * nnz
     if method == 1 and precond in (0, 1):
         if precision == "mixed":
-            return 4 * nnz + cbytes + ((44 if single_reduction else 48) if (unit_diag or precond == 0) else 60) * n
+            return 4 * nnz + cbytes + (48 if (unit_diag or precond == 0) else 60) * n
         return 8 * nnz + cbytes + 132 * n
     # BiCGStab: two SpMV passes (+x fused in FP64) and two preconditioner applications
     if precision == "mixed":
@@ -510,9 +507,7 @@ def run_gpu(args, rank, world, local, pg):
     achieved = bpi * iters / sec_k / 1e9
     traffic = read_traffic(cfg["workload"])
     if solve_kw["method"] == eg.CG:
-        kernel_name = ("cg1_kernel<LPR,int16 cols> (persistent single-reduction FP32 inner CG)"
-                       if (unit_diag or solve_kw["precond"] == eg.PREC_NONE) else
-                       "cg_kernel<float,LPR,int16 cols> (persistent FP32 inner CG)")
+        kernel_name = "cg_kernel<float,LPR,int16 cols> (persistent FP32 inner CG)"
     else:
         kernel_name = ("bicgstab_kernel<float,LPR,int16 cols> (persistent FP32 inner BiCGStab, "
                        + ("ILU0 triangular solves in the kernel)" if solve_kw["precond"] == eg.PREC_ILU0 else "no ILU)"))
@@ -772,7 +767,7 @@ def section_batched(args, rank, world, local, pg, nested=False):
         return bool(np.all((dv * dsc * dsc).astype(np.float32) == np.float32(1.0)))
 
     units = [unit_diag_of(A) for A in mats]
-    bpi = sum(algorithmic_bytes_per_iter(1, 1, "mixed", A.n, A.nnz, True, 1.0, u, single_reduction=False) * r["iters"]
+    bpi = sum(algorithmic_bytes_per_iter(1, 1, "mixed", A.n, A.nnz, True, 1.0, u) * r["iters"]
               for A, r, u in zip(mats, allres, units))
     # against the FP64 oracle: a seeded sample of systems (the smallest six and two more)
     out = None

@@ -1042,15 +1042,6 @@ static int run_krylov(egpu_mat *A, const KArgs<VT> &a0, int method, bool offs) {
   if (a.precond != EGPU_PREC_ILU0) a.tri_cta = 0;
   const size_t smem = a.tri_cta ? A->tri.cta_smem[sizeof(VT) == 8 ? 0 : 1] : 0;
   if (method == EGPU_CG) {
-    if constexpr (sizeof(VT) == 4) {
-      // FP32 inner solve with M = I: the single-reduction recurrence (EGPU_CG1=0 keeps HUTI's)
-      const char *e = std::getenv("EGPU_CG1");
-      const bool m_is_i = a.precond == EGPU_PREC_NONE || (a.precond == EGPU_PREC_DIAGONAL && a.unit_diag);
-      if (!a.true_residual && m_is_i && !(e && e[0] == '0')) {
-        if (offs) return launch_coop(ctx, cg1_kernel<TRI_TS, true>, a, nullptr, 0);
-        return launch_coop(ctx, cg1_kernel<TRI_TS, false>, a, nullptr, 0);
-      }
-    }
     if (offs) return launch_coop(ctx, cg_kernel<VT, TRI_TS, true>, a, nullptr, smem);
     return launch_coop(ctx, cg_kernel<VT, TRI_TS, false>, a, nullptr, smem);
   }

@@ -372,14 +372,16 @@ struct Sentinel<float> {
 // Grid-wide barrier for a cooperative (co-resident) launch.  count is a monotonically
 // increasing arrival counter reset to 0 before the launch; epoch is the per-block count
 // of barriers passed.  The wait is bounded by the context's wait limit; on expiry the error
-// flag is set.  Block 0 reads the host's abort word every 16th barrier (and every waiting
-// block during long waits).  Returns false when the kernel must unwind (error flag set by
-// anyone).
+// flag is set.  Block 0 reads the host's abort word every EGPU_ABORT_POLL-th barrier, before
+// it arrives (the read crosses the host link, so every other block waits for it: rare enough
+// to cost nothing measurable), and every waiting block reads it during long waits.  Returns
+// false when the kernel must unwind (error flag set by anyone).
+#define EGPU_ABORT_POLL 256u
 __device__ __forceinline__ bool grid_barrier(unsigned int *count, int *err, unsigned int &epoch) {
   __syncthreads();
   epoch += 1;
   if (threadIdx.x == 0) {
-    if (blockIdx.x == 0 && (epoch & 15u) == 0) egpu_poll_abort(err);
+    if (blockIdx.x == 0 && (epoch % EGPU_ABORT_POLL) == 0) egpu_poll_abort(err);
     const unsigned int target = epoch * gridDim.x;
     red_release_add_u32(count, 1u);
     if (ld_acquire_u32(count) < target) {

@@ -1036,144 +1036,6 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) cg_kernel(KArgs<VT> a) {
 }
 
 // =====================================================================================
-// Single-reduction CG for the FP32 inner solve with M = I (no preconditioner, or Jacobi on a
-// unit diagonal): the recurrence of Chronopoulos & Gear (1989).  W = A R is formed together
-// with both inner products (R,R) and (W,R) in the SpMV phase, and S = A P is carried by
-// recurrence (S = W + beta S), so an iteration is one elementwise phase and one SpMV phase:
-// two grid barriers instead of three, and 36n + 8n bytes of vectors instead of 48n.  The
-// inner solve is not bound to HUTI's operation order (it only has to reduce its residual by
-// inner_tol); the FP64 refinement around it keeps the reference's stopping test.
-//   alpha_k = gamma_k / (delta_k - beta_k gamma_k / alpha_{k-1}),  beta_k = gamma_k / gamma_{k-1}
-// The right-hand side buffer (the segment's normalised FP64 residual cast to FP32) is used as
-// R in place.  A resumed segment (reliable update) continues the previous one's directions P
-// and S = A P with beta = gamma / (gamma_prev * c) as the standard kernel does, and forms
-// (P, S) directly for that first step (the replaced residual breaks the recurrence's
-// orthogonality): one extra barrier per segment.
-// w layout: W P S (slots 1, 2, 3: the standard kernel's Z, P, Q)
-template <int LPR, bool OFFS>
-__global__ void __launch_bounds__(EGPU_KBLOCK, 1) cg1_kernel(KArgs<float> a) {
-  __shared__ double sm[32 * 4];
-  unsigned int epoch = 0;
-  const int n = a.n, nb = gridDim.x;
-  float *X = a.x, *R = const_cast<float *>(a.b), *W = a.w + a.ldw, *P = a.w + 2 * a.ldw, *S = a.w + 3 * a.ldw;
-  const bool resumed = a.resume != 0;
-  // W = A R with (R,R), (W,R); the first pass also clears X
-  auto spmv_dots = [&](bool clear_x) {
-    double acc[2] = {0.0, 0.0};
-    spmv_phase<float, LPR, OFFS, false>(a, R, R, [&](int i, float w, float) {
-      W[i] = w;
-      if (clear_x) X[i] = 0.0f;
-      const double r = (double)R[i];
-      acc[0] += r * r;
-      acc[1] += r * (double)w;
-    });
-    block_sum<2>(acc, sm);
-    store_partials(a, SLOT_RR, acc[0]);
-    store_partials(a, SLOT_PQ, acc[1]);
-  };
-  spmv_dots(true);
-  if (!grid_barrier(a.bar, a.err, epoch)) return;
-  double gamma = reduce_partials(a.partials + SLOT_RR * nb, nb, sm);
-  double delta = reduce_partials(a.partials + SLOT_PQ * nb, nb, sm);
-  const double rhsnorm = sqrt(gamma);
-  int k = 1, info = 0, iters = 0;
-  double residual = 1.0, gamma_prev = 0.0, alpha = 0.0, alpha_prev = 1.0;
-  while (true) {
-    if (k > 1) {  // recursive residual of x_{k-1}
-      residual = sqrt(gamma) / rhsnorm;
-      if (residual <= a.tol) { info = EGPU_HUTI_CONVERGENCE; iters = k - 1; break; }
-      if (k > a.maxit) { info = EGPU_HUTI_MAXITER; iters = k - 1; break; }
-    }
-    if (gamma == 0.0) { info = EGPU_HUTI_CG_RHO; iters = k; break; }
-    if (k == 1 && resumed) {
-      const float beta = (float)(gamma / (a.carry[0] * a.ru_c));
-      double acc[1] = {0.0};
-      vec_loop<float>(n, [&](int i, auto w) {
-        constexpr int V = decltype(w)::value;
-        float r[V], ww[V], p[V], sv[V];
-        vld<V>(R, i, r);
-        vld<V>(W, i, ww);
-        vld<V>(P, i, p);
-        vld<V>(S, i, sv);
-#pragma unroll
-        for (int q = 0; q < V; ++q) {
-          p[q] = r[q] + beta * p[q];
-          sv[q] = ww[q] + beta * sv[q];
-          acc[0] += (double)p[q] * (double)sv[q];
-        }
-        vst<V>(P, i, p);
-        vst<V>(S, i, sv);
-      });
-      block_sum<1>(acc, sm);
-      store_partials(a, SLOT_RR2, acc[0]);
-      if (!grid_barrier(a.bar, a.err, epoch)) return;
-      alpha = gamma / reduce_partials(a.partials + SLOT_RR2 * nb, nb, sm);
-      const float al = (float)alpha;
-      vec_loop<float>(n, [&](int i, auto w) {
-        constexpr int V = decltype(w)::value;
-        float x[V], p[V], r[V], sv[V];
-        vld<V>(X, i, x);
-        vld<V>(P, i, p);
-        vld<V>(R, i, r);
-        vld<V>(S, i, sv);
-#pragma unroll
-        for (int q = 0; q < V; ++q) {
-          x[q] = x[q] + al * p[q];
-          r[q] = r[q] - al * sv[q];
-        }
-        vst<V>(X, i, x);
-        vst<V>(R, i, r);
-      });
-    } else {
-      const bool first = k == 1;
-      const double beta_d = first ? 0.0 : gamma / gamma_prev;
-      alpha = first ? gamma / delta : gamma / (delta - beta_d * gamma / alpha_prev);
-      const float beta = (float)beta_d, al = (float)alpha;
-      vec_loop<float>(n, [&](int i, auto w) {
-        constexpr int V = decltype(w)::value;
-        float x[V], r[V], ww[V], p[V], sv[V];
-        vld<V>(R, i, r);
-        vld<V>(W, i, ww);
-        if (!first) {
-          vld<V>(P, i, p);
-          vld<V>(S, i, sv);
-        }
-        vld<V>(X, i, x);
-#pragma unroll
-        for (int q = 0; q < V; ++q) {
-          p[q] = first ? r[q] : r[q] + beta * p[q];
-          sv[q] = first ? ww[q] : ww[q] + beta * sv[q];
-          x[q] = x[q] + al * p[q];
-          r[q] = r[q] - al * sv[q];
-        }
-        vst<V>(P, i, p);
-        vst<V>(S, i, sv);
-        vst<V>(X, i, x);
-        vst<V>(R, i, r);
-      });
-    }
-    if (!grid_barrier(a.bar, a.err, epoch)) return;
-    spmv_dots(false);
-    if (!grid_barrier(a.bar, a.err, epoch)) return;
-    gamma_prev = gamma;
-    alpha_prev = alpha;
-    gamma = reduce_partials(a.partials + SLOT_RR * nb, nb, sm);
-    delta = reduce_partials(a.partials + SLOT_PQ * nb, nb, sm);
-    ++k;
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    a.out_i[0] = info;
-    a.out_i[1] = iters;
-    a.out_d[0] = residual;
-    a.out_d[1] = rhsnorm;
-    if (a.carry) {  // P (and S = A P) were built with gamma_prev
-      a.carry[0] = gamma_prev;
-      a.carry[3] = (info == EGPU_HUTI_CONVERGENCE && k > 1) ? 1.0 : 0.0;
-    }
-  }
-}
-
-// =====================================================================================
 // BiCGStab  (huti_dbicgstabsolv, hutiter/src/huti_bicgstab_D.F90:96-284)
 //
 // w layout: R RTLD P V T S T1V T2V Y1 Y2
