@@ -1041,16 +1041,30 @@ static int run_krylov(egpu_mat *A, const KArgs<VT> &a0, int method, bool offs) {
   a.tri_per_block = tri_per_block(A, TRI_TS, ctx->num_sms);
   if (a.precond != EGPU_PREC_ILU0) a.tri_cta = 0;
   const size_t smem = a.tri_cta ? A->tri.cta_smem[sizeof(VT) == 8 ? 0 : 1] : 0;
+  // the instantiation with the level-synchronous solves only when this matrix uses them
+  const bool cta = a.tri_cta != 0;
   if (method == EGPU_CG) {
-    if (offs) return launch_coop(ctx, cg_kernel<VT, TRI_TS, true>, a, nullptr, smem);
-    return launch_coop(ctx, cg_kernel<VT, TRI_TS, false>, a, nullptr, smem);
+    if (cta) {
+      if (offs) return launch_coop(ctx, cg_kernel<VT, TRI_TS, true, true>, a, nullptr, smem);
+      return launch_coop(ctx, cg_kernel<VT, TRI_TS, false, true>, a, nullptr, smem);
+    }
+    if (offs) return launch_coop(ctx, cg_kernel<VT, TRI_TS, true, false>, a, nullptr, smem);
+    return launch_coop(ctx, cg_kernel<VT, TRI_TS, false, false>, a, nullptr, smem);
   }
   if constexpr (sizeof(VT) == 8) {
-    if (method == EGPU_GCR) return launch_coop(ctx, gcr_kernel<TRI_TS>, a, nullptr, smem);
-    if (method == EGPU_BICGSTABL) return launch_coop(ctx, bicgstabl_kernel<TRI_TS>, a, nullptr, smem);
+    if (method == EGPU_GCR)
+      return cta ? launch_coop(ctx, gcr_kernel<TRI_TS, true>, a, nullptr, smem)
+                 : launch_coop(ctx, gcr_kernel<TRI_TS, false>, a, nullptr, smem);
+    if (method == EGPU_BICGSTABL)
+      return cta ? launch_coop(ctx, bicgstabl_kernel<TRI_TS, true>, a, nullptr, smem)
+                 : launch_coop(ctx, bicgstabl_kernel<TRI_TS, false>, a, nullptr, smem);
   }
-  if (offs) return launch_coop(ctx, bicgstab_kernel<VT, TRI_TS, true>, a, nullptr, smem);
-  return launch_coop(ctx, bicgstab_kernel<VT, TRI_TS, false>, a, nullptr, smem);
+  if (cta) {
+    if (offs) return launch_coop(ctx, bicgstab_kernel<VT, TRI_TS, true, true>, a, nullptr, smem);
+    return launch_coop(ctx, bicgstab_kernel<VT, TRI_TS, false, true>, a, nullptr, smem);
+  }
+  if (offs) return launch_coop(ctx, bicgstab_kernel<VT, TRI_TS, true, false>, a, nullptr, smem);
+  return launch_coop(ctx, bicgstab_kernel<VT, TRI_TS, false, false>, a, nullptr, smem);
 }
 
 // stored vectors of GCR (2 (m-1) directions) / BiCGStab(l) (r_0..r_l, u_0..u_l, shadow, x,
