@@ -246,6 +246,15 @@ def read_traffic(workload):
 
 
 # ------------------------------------------------------------------------------------- CPU arm
+def oracle_mod():
+    """The oracle, built for this host (-march=native) before its first use."""
+    import oracle
+
+    if oracle._lib is None:
+        oracle.use_native()
+    return oracle
+
+
 def host_threads():
     return os.cpu_count() or 1
 
@@ -266,7 +275,7 @@ def headline_config(cfg, n, nnz, world):
 
 def oracle_system(w):
     """(pattern, Values, RHS) of a single-system workload, assembled by the oracle."""
-    import oracle
+    oracle = oracle_mod()
 
     m = w["mesh"]
     if w.get("elastic"):
@@ -287,7 +296,7 @@ def oracle_solve_timed(p, values, rhs, method, precond, tol, threads, max_iter=2
     """One complete FP64 solve of the oracle (scaling, preconditioner, Krylov loop,
     back-scaling) with its SpMV and vector operations on `threads` host threads; the ILU
     triangular solves stay sequential, as in the reference.  Returns (x, result dict)."""
-    import oracle
+    oracle = oracle_mod()
 
     return oracle.solve(p, values, rhs, method=method, precond=precond, max_iter=max_iter, tol=tol,
                         threads=threads, blas_threads=threads)
@@ -300,7 +309,7 @@ def reference_systems_rate(kind, tol, systems, requests, rate, target_s, start=0
     systems solved, solve seconds, config).  Sizes are drawn independently, so the prefix is a
     random sample of the mix.  Assembly and Dirichlet rows are set up outside the timing, as in
     the GPU arms."""
-    import oracle
+    oracle = oracle_mod()
     from elmerfem_b200 import meshgen, server
 
     threads = host_threads()
@@ -574,7 +583,7 @@ def run_gpu(args, rank, world, local, pg):
     # N = 1): the CPU baseline, and the reference solution both GPU results are measured against
     cpu, err_oracle = None, None
     if rank == 0 and world == 1 and not args.no_cpu:
-        import oracle
+        oracle = oracle_mod()
 
         op = oracle.Pattern(n, nnz, dofs, pat.perm, pat.rows, pat.cols, pat.diag, 0, 0, 0, 0)
         threads = host_threads()
@@ -772,7 +781,7 @@ def section_batched(args, rank, world, local, pg, nested=False):
     # against the FP64 oracle: a seeded sample of systems (the smallest six and two more)
     out = None
     if rank == 0:
-        import oracle
+        oracle = oracle_mod()
 
         order = np.argsort(ms, kind="stable")
         rng = np.random.default_rng(17)
@@ -873,7 +882,7 @@ def section_serving(args, rank, world, local, pg, nested=False):
     errs = [rel(r.x, a.x) for r, a in zip(reqs, alone)]
     out = None
     if rank == 0:
-        import oracle
+        oracle = oracle_mod()
         from elmerfem_b200 import meshgen
 
         # against the FP64 oracle: the six smallest requests of the first stream

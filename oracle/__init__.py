@@ -46,6 +46,25 @@ def build() -> str:
     return _LIB_PATH
 
 
+def use_native() -> str:
+    """Switch to the -march=native build of the same source (the timed CPU baseline), built for
+    this host; call before the first oracle call.  Returns the library's path."""
+    global _LIB_PATH
+    if _lib is not None:
+        raise RuntimeError("oracle already loaded")
+    import hashlib
+
+    try:  # one directory per host CPU (model and feature flags)
+        info = [l for l in open("/proc/cpuinfo") if l.startswith(("model name", "flags"))][:2]
+    except OSError:
+        info = [os.uname().machine]
+    tag = hashlib.sha1("".join(info).encode()).hexdigest()[:12]
+    out = os.path.join(_HERE, "_build", "native_" + tag)
+    subprocess.run(["make", "-s", "-C", _HERE, "native", "NATIVE_OUT=" + out], check=True)
+    _LIB_PATH = os.path.join(out, "libelmer_oracle.so")
+    return _LIB_PATH
+
+
 def lib():
     global _lib
     if _lib is None:
