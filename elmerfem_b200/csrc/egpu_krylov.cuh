@@ -589,75 +589,24 @@ __device__ __forceinline__ void upper_solve(const KArgs<VT> &a, const VT *y, VT 
 // Level-synchronous triangular solves in one block.
 //
 // Every dependency of a row lies in an earlier level, and (for the meshes this is used on)
-// only a few levels back, so block 0 runs the levels in order with one named barrier per
+// only a few levels back, so block 0 runs the levels in order with one __syncthreads per
 // level and keeps the values of the recent slots in a shared-memory ring (slot s at
 // s mod cta_rs; the host sizes the ring so no slot is overwritten while a later row still
-// reads it).  A level's ELL block of factor entries and ring indices is contiguous in global
-// memory: thread 0 stages it into the shared-memory windows with bulk asynchronous copies
-// (cp.async.bulk, completion counted in bytes on one of cta_pd + 1 mbarriers), cta_pd levels
-// ahead; each row's right-hand side, inverted diagonal, auxiliary value and output position
-// are staged by the thread that will process the row (cp.async, its own commit groups).  One
-// thread per row sums its entries in CRS order with the reference's operation order:
+// reads it).  A level's ELL block of factor entries, and its rows' right-hand sides,
+// inverted diagonals and output positions, are contiguous in global memory; they are
+// staged into shared-memory windows with cp.async cta_pd levels ahead, so the copies of
+// later levels are in flight while the current one computes.  One thread per row sums its
+// entries in CRS order with the reference's operation order:
 //   lower  s = b_i;  s = s - L_ij y_j ...;  y_i = s                (CRS_LUSolve :3348-3353)
 //   upper  s = y_i;  s = s - U_ij z_j ...;  z_i = u_ii^-1 * s      (:3357-3363)
-// so the FP64 solve rounds exactly as CRS_LUSolve does.  A level costs the named barrier and
-// the dependent chain of its longest row: the copies of later levels are in flight, and a
-// row's ring indices and factor values are read a chunk at a time before its ring values, so
-// only the subtractions form a chain.
+// so the FP64 solve rounds exactly as CRS_LUSolve does.
 __device__ __forceinline__ double row_msub(double s, double a, double x) { return __dsub_rn(s, __dmul_rn(a, x)); }
 __device__ __forceinline__ float row_msub(float s, float a, float x) { return fmaf(-a, x, s); }
 __device__ __forceinline__ double cta_mul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ float cta_mul(float a, float b) { return a * b; }
 
-// mbarrier and bulk-copy primitives (shared::cta; the block is its own cluster)
-__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(unsigned long long *m, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-__device__ __forceinline__ void mbar_inval(unsigned long long *m) {
-  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(m)) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *m, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(m)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long *m, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(m)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// bounded wait for the phase with the given parity; on expiry the error flag is set
-__device__ __forceinline__ void mbar_wait(unsigned long long *m, unsigned parity, int *err) {
-  if (mbar_try_wait(m, parity)) return;
-  const unsigned long long t0 = egpu_globaltimer(), lim = egpu_wait_limit(err);
-  for (unsigned int spin = 1;; ++spin) {
-    if (mbar_try_wait(m, parity)) return;
-    if ((spin & 63u) == 0) {
-      if (*(volatile int *)err) return;
-      if (egpu_globaltimer() - t0 > lim) {
-        atomicExch(err, (int)EGPU_ERR_TIMEOUT);
-        return;
-      }
-    }
-  }
-}
-// global -> shared bulk copy (16-byte aligned ends, size a positive multiple of 16)
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *m) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(m))
-               : "memory");
-}
-// shared memory read through the generic proxy before being overwritten by a bulk copy
-__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
 template <typename VT>
 struct CtaSmem {
-  unsigned long long *mbar;  // cta_pd + 1 stage barriers
   int4 *lv;
   VT *sv;
   uint16_t *si;
@@ -670,8 +619,6 @@ __device__ __forceinline__ CtaSmem<VT> cta_smem(const KArgs<VT> &a, unsigned cha
   CtaSmem<VT> m;
   size_t o = 0;
   const int V = (int)sizeof(VT);
-  m.mbar = reinterpret_cast<unsigned long long *>(base + o);
-  o += cta_align16((size_t)8 * (plan::PD_MAX + 1));
   m.lv = reinterpret_cast<int4 *>(base + o);
   o += (size_t)a.cta_nl * 16;
   m.sv = reinterpret_cast<VT *>(base + o);
@@ -710,31 +657,20 @@ __device__ __forceinline__ int cta_wrap(int i, int n) { return i >= n ? i - n : 
 // barrier among the first nt threads of the block (named barrier 1; nt a multiple of 32)
 __device__ __forceinline__ void cta_bar(int nt) { asm volatile("bar.sync 1, %0;" ::"r"(nt) : "memory"); }
 
-// Thread 0: the bulk copies of level lv's ELL values and ring indices into the windows at
-// position p.sb (two pieces when the block wraps at the window's end), counted on mbar.
-// Offsets and sizes are multiples of 8 entries, so every piece is 16-byte aligned and sized.
-template <typename VT>
-__device__ __forceinline__ void cta_issue_bulk(const CtaSmem<VT> &m, const CtaTri<VT> &T, int4 lv, int sb, int SB,
-                                               unsigned long long *mbar) {
-  const int ne = (lv.y * lv.z + 7) & ~7;
-  const int n1 = min(ne, SB - sb), n2 = ne - n1;
-  mbar_arrive_expect_tx(mbar, (unsigned)ne * (unsigned)(sizeof(VT) + 2));
-  if (n1 > 0) {
-    bulk_g2s(m.sv + sb, T.vals + lv.w, (unsigned)n1 * sizeof(VT), mbar);
-    bulk_g2s(m.si + sb, T.ridx + lv.w, (unsigned)n1 * 2u, mbar);
-  }
-  if (n2 > 0) {
-    bulk_g2s(m.sv, T.vals + lv.w + n1, (unsigned)n2 * sizeof(VT), mbar);
-    bulk_g2s(m.si, T.ridx + lv.w + n1, (unsigned)n2 * 2u, mbar);
-  }
-}
-
-// the per-row data of level lv, staged by the thread that will process each row
+// issue the copies of level lv (window positions p) into the staging windows (threads
+// 0..nt-1)
 template <typename VT, bool UPPER>
-__device__ __forceinline__ void cta_issue_rows(const CtaTri<VT> &T, const CtaSmem<VT> &m, int4 lv, int rb, int SR,
-                                               int nt, const VT *rowv, const VT *dinv, const VT *aux) {
+__device__ __forceinline__ void cta_issue(const KArgs<VT> &a, const CtaTri<VT> &T, const CtaSmem<VT> &m, int4 lv,
+                                          CtaPos p, int nt, const VT *rowv, const VT *dinv, const VT *aux) {
+  constexpr int PV = 16 / sizeof(VT);
+  const int SB = a.cta_sb, SR = a.cta_sr;
+  const int ne = (lv.y * lv.z + 7) & ~7;
+  for (int c = threadIdx.x; c < ne / PV; c += nt)
+    cp_async16(m.sv + cta_wrap(p.sb + c * PV, SB), T.vals + lv.w + c * PV);
+  for (int c = threadIdx.x; c < ne / 8; c += nt)
+    cp_async16(m.si + cta_wrap(p.sb + c * 8, SB), T.ridx + lv.w + c * 8);
   for (int t = threadIdx.x; t < lv.y; t += nt) {
-    const int d = cta_wrap(rb + t, SR);
+    const int d = cta_wrap(p.rb + t, SR);
     cp_async_small<sizeof(VT)>(m.rr + d, rowv + lv.x + t);
     cp_async_small<4>(m.rm + d, T.map + lv.x + t);
     if (UPPER) {
@@ -744,10 +680,9 @@ __device__ __forceinline__ void cta_issue_rows(const CtaTri<VT> &T, const CtaSme
   }
 }
 
-// One level: the solve's thread t takes the level's rows t, t + nt, ...; a row's ring
-// indices and factor values are read CTA_CHUNK at a time, then their ring values, and the
-// entries are subtracted in CRS order, s = s - L_ij y_j as CRS_LUSolve does, so the FP64
-// result is the reference's to the bit.
+// One level: the solve's thread t takes the level's rows t, t + nt, ...; a row's entries
+// are read four at a time (ring indices, then ring values) and subtracted in CRS order,
+// s = s - L_ij y_j as CRS_LUSolve does, so the FP64 result is the reference's to the bit.
 template <typename VT, bool UPPER, typename OUT>
 __device__ __forceinline__ void cta_level(const KArgs<VT> &a, const CtaSmem<VT> &m, int4 lv, CtaPos p, int nt,
                                           VT *outv, OUT &&out) {
@@ -784,67 +719,43 @@ __device__ __forceinline__ void cta_level(const KArgs<VT> &a, const CtaSmem<VT> 
 // A whole triangle, run by the block's first a.cta_nt threads (the others go straight to
 // the closing __syncthreads).  rowv: right-hand side in this triangle's slot order; lower
 // results go to outv[map] (the upper slot order), upper results to outv[row] and
-// out(row, z, aux).  Level L uses stage barrier L mod (cta_pd + 1), phase L div (cta_pd + 1).
+// out(row, z, aux).
 template <typename VT, bool UPPER, typename OUT>
-__device__ __noinline__ void cta_tri_solve(const KArgs<VT> &a, const CtaTri<VT> &T, const CtaSmem<VT> &m,
+__device__ __forceinline__ void cta_tri_solve(const KArgs<VT> &a, const CtaTri<VT> &T, const CtaSmem<VT> &m,
                                               const VT *rowv, const VT *dinv, const VT *aux, VT *outv, OUT &&out) {
-  const int PD = a.cta_pd, nlev = T.nlev, nt = a.cta_nt, NST = a.cta_pd + 1;
+  const int PD = a.cta_pd, nlev = T.nlev, nt = a.cta_nt;
   const int SB = a.cta_sb, SR = a.cta_sr, RS = a.cta_rs;
   if (threadIdx.x < nt) {
-    // the level table, once per solve; the stage barriers
+    // the level table, once per solve
     for (int L = threadIdx.x; L < nlev; L += nt) cp_async16(m.lv + L, T.lev + L);
     cp_async_commit();
     cp_async_wait(0);
-    if (threadIdx.x == 0) {
-      m.ring[RS] = VT(0);
-      for (int q = 0; q < NST; ++q) mbar_init(m.mbar + q, 1);
-      mbar_init_fence();
-    }
+    if (threadIdx.x == 0) m.ring[RS] = VT(0);
     cta_bar(nt);
     CtaPos pi{0, 0, 0}, pp{0, 0, 0};  // issue / process positions
-    if (threadIdx.x == 0) fence_proxy_async_smem();  // the windows were read by an earlier solve
     for (int L = 0; L < PD; ++L) {
       if (L < nlev) {
         const int4 lv = m.lv[L];
-        if (threadIdx.x == 0) cta_issue_bulk(m, T, lv, pi.sb, SB, m.mbar + L);
-        cta_issue_rows<VT, UPPER>(T, m, lv, pi.rb, SR, nt, rowv, dinv, aux);
+        cta_issue<VT, UPPER>(a, T, m, lv, pi, nt, rowv, dinv, aux);
         pi.advance(lv, SB, SR, RS);
       }
       cp_async_commit();
     }
-    int q = 0;
-    unsigned ph = 0;
-    int qi = PD % NST;  // stage of the next level to issue (level PD)
     for (int L = 0; L < nlev; ++L) {
-      const int4 lv = m.lv[L];
       cp_async_wait(PD - 1);
-      if ((int)threadIdx.x < lv.y) mbar_wait(m.mbar + q, ph, a.err);
       cta_bar(nt);
-      cta_level<VT, UPPER>(a, m, lv, pp, nt, outv, out);
-      pp.advance(lv, SB, SR, RS);
       if (L + PD < nlev) {
-        const int4 ln = m.lv[L + PD];
-        if (threadIdx.x == 0) {
-          fence_proxy_async_smem();
-          cta_issue_bulk(m, T, ln, pi.sb, SB, m.mbar + qi);
-        }
-        cta_issue_rows<VT, UPPER>(T, m, ln, pi.rb, SR, nt, rowv, dinv, aux);
-        pi.advance(ln, SB, SR, RS);
+        const int4 lv = m.lv[L + PD];
+        cta_issue<VT, UPPER>(a, T, m, lv, pi, nt, rowv, dinv, aux);
+        pi.advance(lv, SB, SR, RS);
       }
       cp_async_commit();
-      if (++qi == NST) qi = 0;
-      if (++q == NST) {
-        q = 0;
-        ph ^= 1u;
-      }
+      const int4 lv = m.lv[L];
+      cta_level<VT, UPPER>(a, m, lv, pp, nt, outv, out);
+      pp.advance(lv, SB, SR, RS);
     }
     cp_async_wait(0);
   }
-  __syncthreads();
-  // every issued level has been waited for: the stage barriers can be dropped before the
-  // shared memory is used again
-  if (threadIdx.x == 0)
-    for (int st = 0; st < NST; ++st) mbar_inval(m.mbar + st);
   __syncthreads();
 }
 

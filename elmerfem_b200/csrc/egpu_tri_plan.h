@@ -25,13 +25,13 @@
 
 namespace egpu {
 
-// Shared-memory footprint of the level-synchronous solve: the stage barriers (PD_MAX + 1
-// mbarriers of 8 bytes), the level table (nl levels of 16 bytes), staged ELL values and ring indices (sb entries), the ring (rs slots + a zero
+// Shared-memory footprint of the level-synchronous solve: the level table (nl levels of
+// 16 bytes), staged ELL values and ring indices (sb entries), the ring (rs slots + a zero
 // slot), staged per-row data (sr rows: right-hand side, inverted diagonal, auxiliary
 // value, map).
 EGPU_HD constexpr size_t cta_align16(size_t b) { return (b + 15) & ~(size_t)15; }
 EGPU_HD constexpr size_t cta_smem_bytes(int sb, int rs, int sr, int vsize, int nl) {
-  return cta_align16((size_t)8 * (8 + 1)) + (size_t)nl * 16 + cta_align16((size_t)sb * vsize) + cta_align16((size_t)sb * 2) +
+  return (size_t)nl * 16 + cta_align16((size_t)sb * vsize) + cta_align16((size_t)sb * 2) +
          cta_align16((size_t)(rs + 1) * vsize) + 3 * cta_align16((size_t)sr * vsize) + cta_align16((size_t)sr * 4);
 }
 

@@ -7,8 +7,7 @@
 //   - every value a row reads was staged for its own level / produced by the slot the
 //     entry depends on, and padding entries read the zero slot,
 //   - no ring slot is written and read within one level,
-//   - every copy stays inside its global array, and the bulk copies that stage a level's
-//     block are 16-byte aligned and sized,
+//   - every copy stays inside its global array,
 // and returns the model's y / z next to a plain sequential CRS_LUSolve
 // (fem/src/CRSMatrix.src:3346-3363) with the same operation order, for a bit-exact
 // comparison.  Test infrastructure: built and called by tests/test_tri_plan.py.
@@ -95,16 +94,6 @@ struct Model {
     const int sb = lv.w % SB;
     if ((long long)lv.w + ne > T.nent) fail(10);
     if (sb % 8) fail(11);
-    // the kernel stages the block with bulk copies (cta_issue_bulk): at most two pieces, each
-    // 16-byte aligned at both ends and a positive multiple of 16 bytes, inside the window
-    {
-      const int n1 = ne < SB - sb ? ne : SB - sb, n2 = ne - n1;
-      if (SB % 8 || lv.w % 8 || n1 % 8 || n2 % 8 || n2 > sb) fail(16);
-      if (n1 > 0 && ((n1 * (int)sizeof(VT)) % 16 || (n1 * 2) % 16 || (sb * (int)sizeof(VT)) % 16 || (sb * 2) % 16))
-        fail(17);
-      if (n2 > 0 && (((long long)(lv.w + n1) * (long long)sizeof(VT)) % 16 || ((long long)(lv.w + n1) * 2) % 16))
-        fail(18);
-    }
     for (int c = 0; c < ne / PV; ++c) {
       int d = sb + c * PV;
       if (d >= SB) d -= SB;
