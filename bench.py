@@ -605,6 +605,9 @@ def run_gpu(args, rank, world, local, pg):
                 "latency_ms": {"p50": 1000 * lat[len(lat) // 2], "p99": 1000 * lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
                 "iterations": {"mixed_inner_total": rm["iters"], "refinements": rm["refinements"],
                                "fp64": r64["iters"]},
+                # a mixed request runs the FP64 drop-in on values it was measured faster on
+                "path_of_timed_steps": {"mixed": sum(1 for r in results if r.get("precision_used") == 1),
+                                        "fp64": sum(1 for r in results if r.get("precision_used") == 0)},
                 "fp64": {"solves_per_s": fp64_rate, "ms_per_solve": 1000 * statistics.median(t64),
                          "krylov_gbs": ach64},
                 "speedup_mixed_vs_fp64": value / world / fp64_rate,

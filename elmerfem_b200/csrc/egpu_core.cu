@@ -2099,16 +2099,18 @@ extern "C" int egpu_iter_solve_dev(egpu_mat *A, const double *b_dev, double *x_d
   // faster (EGPU_MIXED_AUTO=0 keeps mixed).  CG / BiCGStab only; GCR and BiCGStab(l) are FP64.
   const char *aenv = std::getenv("EGPU_MIXED_AUTO");
   const bool auto_ok = !(aenv && aenv[0] == '0');
+  // Each path keeps its fastest time on these values (a first solve carries one-time set-up),
+  // and FP64 is taken only with a clear margin.
   const bool krylov32 = prm->method == EGPU_CG || prm->method == EGPU_BICGSTAB;
   if (prm->precision == EGPU_MIXED && krylov32 &&
-      !(auto_ok && A->t_fp64 > 0.0 && A->t_mixed > 0.0 && A->t_fp64 < A->t_mixed)) {
+      !(auto_ok && A->t_fp64 > 0.0 && A->t_mixed > 0.0 && A->t_fp64 < 0.85 * A->t_mixed)) {
     rc = egpu::solve_mixed(A, b_dev, x_dev, prm, &r);
     r.precision_used = EGPU_MIXED;
-    if (rc > 0) A->t_mixed = r.seconds;
+    if (rc > 0) A->t_mixed = A->t_mixed > 0.0 ? std::min(A->t_mixed, r.seconds) : r.seconds;
   } else {
     rc = egpu::solve_fp64(A, b_dev, x_dev, prm, &r);
     r.precision_used = EGPU_FP64;
-    if (rc > 0) A->t_fp64 = r.seconds;
+    if (rc > 0) A->t_fp64 = A->t_fp64 > 0.0 ? std::min(A->t_fp64, r.seconds) : r.seconds;
   }
   if (res) *res = r;
   return rc;

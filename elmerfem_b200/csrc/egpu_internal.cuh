@@ -191,8 +191,9 @@ struct egpu_mat {
   DevBuf<double> values;         // as bound / assembled (unscaled)
   DevBuf<double> rhs;            // assembled right-hand side
   bool has_values = false, has_rhs = false;
-  // device seconds of the last FP64 and mixed-precision solve of the current values (0: none
-  // yet); a mixed request runs as the FP64 drop-in once both are known and FP64 was faster
+  // fastest device seconds of an FP64 and of a mixed-precision solve of the current values (0:
+  // none yet); a mixed request runs as the FP64 drop-in once both are known and FP64 took
+  // less than 0.85 of the mixed time
   double t_fp64 = 0.0, t_mixed = 0.0;
   int max_row = 0;               // longest row
   int max_bandwidth = 0;         // max |col - row|

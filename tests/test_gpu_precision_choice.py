@@ -1,0 +1,48 @@
+"""A mixed-precision request runs the faster of the two paths measured on the matrix's current
+values: once an FP64 solve and a mixed solve of those values have run, the FP64 drop-in is taken
+when its fastest time is below 0.85 of the mixed one (on stiff operators with latency-bound
+triangular solves, such as elasticity with ILU0, rounding the matrix to FP32 costs more
+refinements than FP32 saves).  Either way the solution meets 1e-8 against the oracle; new values
+reset the measurements; EGPU_MIXED_AUTO=0 keeps the mixed path."""
+import pytest
+
+import elmerfem_b200 as eg
+import oracle
+from elmerfem_b200 import meshgen
+from helpers import elastic_problem, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(precision):
+    return eg.SolverParams(method=eg.BICGSTAB, precond=eg.PREC_ILU0, tol=1e-8, max_iter=5000, precision=precision)
+
+
+def test_mixed_request_takes_the_measured_faster_path(ctx, monkeypatch):
+    p, _, _, v, b, _ = elastic_problem(meshgen.hex_cube(8))
+    x_orc, r_orc = oracle.solve(p, v, b, method=oracle.BICGSTAB, precond=oracle.PREC_ILU0, tol=1e-8, max_iter=5000)
+    A = eg.Matrix(ctx, eg.CRSPattern(p.n, p.nnz, 3, p.perm, p.rows, p.cols, p.diag), v)
+    try:
+        t64, tm = [], []
+        for _ in range(2):
+            x, r = A.solve(b, params=_params(eg.FP64))
+            assert r["precision_used"] == eg.FP64 and rel(x, x_orc) < 1e-8
+            t64.append(r["seconds"])
+        x, r = A.solve(b, params=_params(eg.MIXED))  # the first mixed solve is always mixed
+        assert r["precision_used"] == eg.MIXED and rel(x, x_orc) < 1e-8
+        tm.append(r["seconds"])
+        for _ in range(3):
+            expect = eg.FP64 if min(t64) < 0.85 * min(tm) else eg.MIXED
+            x, r = A.solve(b, params=_params(eg.MIXED))
+            assert r["precision_used"] == expect
+            assert r["info"] == 1 and rel(x, x_orc) < 1e-8
+            (t64 if expect == eg.FP64 else tm).append(r["seconds"])
+        monkeypatch.setenv("EGPU_MIXED_AUTO", "0")
+        x, r = A.solve(b, params=_params(eg.MIXED))
+        assert r["precision_used"] == eg.MIXED and rel(x, x_orc) < 1e-8
+        monkeypatch.delenv("EGPU_MIXED_AUTO")
+        A.update_values(v)  # new values: nothing measured on them yet
+        x, r = A.solve(b, params=_params(eg.MIXED))
+        assert r["precision_used"] == eg.MIXED and rel(x, x_orc) < 1e-8
+    finally:
+        A.free()
