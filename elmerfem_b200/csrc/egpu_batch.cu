@@ -73,11 +73,11 @@ __device__ __forceinline__ void batch_slices(const BatchShared &sh, F &&f) {
   }
 }
 
-// batch_slices for the SpMV phases: lane 0 also prefetches into L2 the values and column
-// offsets of the slice this warp takes next (one bulk request each; slices start at
-// multiples of 32 entries, so both requests are 16-byte aligned and sized), while the
-// current one is summed.  The next slice's position is loaded one slice earlier still, so
-// the request never waits for it.  Slices of systems that do not run are not prefetched.
+// For the SpMV phases, lane 0 of a warp prefetches into L2 the values and column offsets of
+// the slices the warp takes next (one bulk request each; slices start at multiples of 32
+// entries, so both requests are 16-byte aligned and sized) while the current ones are
+// summed; the next slices' positions are loaded a round earlier still, so the requests never
+// wait for them.  Slices of systems that do not run are not prefetched.
 struct SliceMeta {
   const void *vals, *cols;
   unsigned vbytes, cbytes;
@@ -118,23 +118,6 @@ __device__ __forceinline__ SliceMeta batch_slice_meta(const BatchArgs &ba, const
   return m;
 }
 
-template <typename F>
-__device__ __forceinline__ void batch_slices_spmv(const BatchArgs &ba, const BatchShared &sh, F &&f) {
-  const int total = sh.total, nb = gridDim.x;
-  const int lo = (int)((long long)total * blockIdx.x / nb), hi = (int)((long long)total * (blockIdx.x + 1) / nb);
-  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, lane = threadIdx.x & 31;
-  SliceMeta next = batch_slice_meta(ba, sh, lo + warp + nw, hi);
-  for (int q = lo + warp; q < hi; q += nw) {
-    const int a = batch_locate(sh, q);
-    if (lane == 0 && next.vbytes) {
-      prefetch_l2_bulk(next.vals, next.vbytes);
-      prefetch_l2_bulk(next.cols, next.cbytes);
-    }
-    next = batch_slice_meta(ba, sh, q + 2 * nw, hi);
-    f(a, sh.act[a], q - sh.pre[a]);
-  }
-}
-
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
@@ -166,20 +149,82 @@ __device__ __forceinline__ void batch_clear(const BatchArgs &a, int slot) {
     if (s % gridDim.x == (int)blockIdx.x) a.acc[slot * BATCH_MAX_SYS + s] = 0.0;
 }
 
-// SELL SpMV of one slice: lane's row sum of A x
-__device__ __forceinline__ float slice_spmv(const SysDesc &d, int slice, int lane, const float *x) {
-  const int r = (slice << 5) + lane;
-  const int w = __ldg(d.sell_w + slice);
-  const int base = __ldg(d.sell_ptr + slice) + lane;
-  float s = 0.f;
-#pragma unroll 8
-  for (int k = 0; k < w; ++k) {
-    const int e = base + (k << 5);
-    const float v = __ldcs(d.svals + e);
-    const int c = d.scols16 ? r + (int)__ldcs(d.scols16 + e) : __ldcs(d.scols + e);
-    s = fmaf(v, __ldca(x + c), s);
+// Two slices of (possibly) different systems summed in one interleaved loop: a tet row has
+// about 15 entries, so one slice alone gives each lane a short chain of dependent gathers and
+// leaves the warp waiting on memory; two slices double the loads in flight.  d0 / d1 null:
+// that slice does not run.  Each row sums in entry order.
+__device__ __forceinline__ void slice_spmv2(const SysDesc *d0, int sl0, const float *x0, const SysDesc *d1, int sl1,
+                                            const float *x1, int lane, float &y0, float &y1) {
+  int w0 = 0, w1 = 0, b0 = 0, b1 = 0;
+  if (d0) {
+    w0 = __ldg(d0->sell_w + sl0);
+    b0 = __ldg(d0->sell_ptr + sl0) + lane;
   }
-  return s;
+  if (d1) {
+    w1 = __ldg(d1->sell_w + sl1);
+    b1 = __ldg(d1->sell_ptr + sl1) + lane;
+  }
+  const int r0 = (sl0 << 5) + lane, r1 = (sl1 << 5) + lane;
+  const int wm = max(w0, w1);
+  float s0 = 0.f, s1 = 0.f;
+#pragma unroll 4
+  for (int k = 0; k < wm; ++k) {
+    if (k < w0) {
+      const int e = b0 + (k << 5);
+      const float v = __ldcs(d0->svals + e);
+      const int c = d0->scols16 ? r0 + (int)__ldcs(d0->scols16 + e) : __ldcs(d0->scols + e);
+      s0 = fmaf(v, __ldca(x0 + c), s0);
+    }
+    if (k < w1) {
+      const int e = b1 + (k << 5);
+      const float v = __ldcs(d1->svals + e);
+      const int c = d1->scols16 ? r1 + (int)__ldcs(d1->scols16 + e) : __ldcs(d1->scols + e);
+      s1 = fmaf(v, __ldca(x1 + c), s1);
+    }
+  }
+  y0 = s0;
+  y1 = s1;
+}
+
+// SpMV phase over this block's share of the active slices, two slices per warp at a time
+// (slice_spmv2); lane 0 prefetches the next pair into L2.  src(s): the
+// vector system s multiplies; epi(act_index, s, slice, y): once per running slice, y the
+// lane's row sum.  Slices of systems that do not run are skipped (warp-uniform).
+template <typename SRC, typename EPI>
+__device__ __forceinline__ void batch_spmv2(const BatchArgs &ba, const BatchShared &sh, SRC &&src, EPI &&epi) {
+  const int total = sh.total, nb = gridDim.x;
+  const int lo = (int)((long long)total * blockIdx.x / nb), hi = (int)((long long)total * (blockIdx.x + 1) / nb);
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, lane = threadIdx.x & 31;
+  SliceMeta n0 = batch_slice_meta(ba, sh, lo + warp + 2 * nw, hi), n1 = batch_slice_meta(ba, sh, lo + warp + 3 * nw, hi);
+  for (int q0 = lo + warp; q0 < hi; q0 += 2 * nw) {
+    const int q1 = q0 + nw;
+    if (lane == 0) {
+      if (n0.vbytes) {
+        prefetch_l2_bulk(n0.vals, n0.vbytes);
+        prefetch_l2_bulk(n0.cols, n0.cbytes);
+      }
+      if (n1.vbytes) {
+        prefetch_l2_bulk(n1.vals, n1.vbytes);
+        prefetch_l2_bulk(n1.cols, n1.cbytes);
+      }
+    }
+    n0 = batch_slice_meta(ba, sh, q0 + 4 * nw, hi);
+    n1 = batch_slice_meta(ba, sh, q1 + 4 * nw, hi);
+    const int a0 = batch_locate(sh, q0), s0 = sh.act[a0], sl0 = q0 - sh.pre[a0];
+    int a1 = -1, s1 = 0, sl1 = 0;
+    if (q1 < hi) {
+      a1 = batch_locate(sh, q1);
+      s1 = sh.act[a1];
+      sl1 = q1 - sh.pre[a1];
+    }
+    const bool run0 = sh.status[s0] == ST_RUN, run1 = a1 >= 0 && sh.status[s1] == ST_RUN;
+    if (!run0 && !run1) continue;
+    float y0, y1;
+    slice_spmv2(run0 ? &ba.sys[s0] : nullptr, sl0, run0 ? src(s0) : nullptr, run1 ? &ba.sys[s1] : nullptr, sl1,
+                run1 ? src(s1) : nullptr, lane, y0, y1);
+    if (run0) epi(a0, s0, sl0, y0);
+    if (run1) epi(a1, s1, sl1, y1);
+  }
 }
 
 // Sync-free ILU0 solves over the systems in RUN state, slots interleaved across systems:
@@ -481,13 +526,12 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       // S: Q = A P; PQ;  clear RHO, RR
       batch_clear(a, BA_RHO);
       batch_clear(a, BA_RR);
-      batch_slices_spmv(a, sh, [&](int ai, int s, int slice) {
-        if (sh.status[s] != ST_RUN) return;
+      batch_spmv2(a, sh, [&](int s) -> const float * { return a.sys[s].w + 2 * a.sys[s].ldw; },
+                  [&](int ai, int s, int slice, float q) {
         const SysDesc &d = a.sys[s];
         const int r = (slice << 5) + lane;
         const float *P = d.w + 2 * d.ldw;
         float *Q = d.w + 3 * d.ldw;
-        const float q = slice_spmv(d, slice, lane, P);
         double pq = 0.0;
         if (r < d.n) {
           Q[r] = q;
@@ -564,13 +608,12 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       batch_clear(a, BA_RHO);
       batch_clear(a, BA_RR);
       batch_clear(a, BA_SS);
-      batch_slices_spmv(a, sh, [&](int ai, int s, int slice) {
-        if (sh.status[s] != ST_RUN) return;
+      batch_spmv2(a, sh, [&](int s) -> const float * { return a.sys[s].w + 6 * a.sys[s].ldw; },
+                  [&](int ai, int s, int slice, float v) {
         const SysDesc &d = a.sys[s];
         const int r = (slice << 5) + lane;
-        const float *RT = d.w + d.ldw, *T1 = d.w + 6 * d.ldw;
+        const float *RT = d.w + d.ldw;
         float *V = d.w + 3 * d.ldw;
-        const float v = slice_spmv(d, slice, lane, T1);
         double rv = 0.0;
         if (r < d.n) {
           V[r] = v;
@@ -621,13 +664,12 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       if (!grid_barrier(a.bar, a.err, epoch)) return;
       // 4: T = A T2; TS, TT;  clear PQ
       batch_clear(a, BA_PQ);
-      batch_slices_spmv(a, sh, [&](int ai, int s, int slice) {
-        if (sh.status[s] != ST_RUN) return;
+      batch_spmv2(a, sh, [&](int s) -> const float * { return a.sys[s].w + 7 * a.sys[s].ldw; },
+                  [&](int ai, int s, int slice, float t) {
         const SysDesc &d = a.sys[s];
         const int r = (slice << 5) + lane;
-        const float *S = d.w + 5 * d.ldw, *T2 = d.w + 7 * d.ldw;
+        const float *S = d.w + 5 * d.ldw;
         float *T = d.w + 4 * d.ldw;
-        const float t = slice_spmv(d, slice, lane, T2);
         double ts = 0.0, tt = 0.0;
         if (r < d.n) {
           T[r] = t;
