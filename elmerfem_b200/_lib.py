@@ -50,7 +50,7 @@ class Result(C.Structure):
 
 class BatchConfig(C.Structure):
     _fields_ = [("chunk_iters", C.c_int), ("blocks_per_sm", C.c_int), ("tri_mult", C.c_int),
-                ("candidates", C.c_int), ("rate", C.c_double)]
+                ("candidates", C.c_int), ("rate", C.c_double), ("slices_per_warp", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

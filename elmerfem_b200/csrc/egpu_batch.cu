@@ -186,8 +186,8 @@ __device__ __forceinline__ void slice_spmv2(const SysDesc *d0, int sl0, const fl
   y1 = s1;
 }
 
-// SpMV phase over this block's share of the active slices, two slices per warp at a time
-// (slice_spmv2); lane 0 prefetches the next pair into L2.  src(s): the
+// SpMV phase over this block's share of the active slices, ba.spw (1 or 2, chosen by the
+// autotuner) slices per warp at a time (slice_spmv2); lane 0 prefetches the next ones into L2.  src(s): the
 // vector system s multiplies; epi(act_index, s, slice, y): once per running slice, y the
 // lane's row sum.  Slices of systems that do not run are skipped (warp-uniform).
 template <typename SRC, typename EPI>
@@ -195,9 +195,11 @@ __device__ __forceinline__ void batch_spmv2(const BatchArgs &ba, const BatchShar
   const int total = sh.total, nb = gridDim.x;
   const int lo = (int)((long long)total * blockIdx.x / nb), hi = (int)((long long)total * (blockIdx.x + 1) / nb);
   const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, lane = threadIdx.x & 31;
-  SliceMeta n0 = batch_slice_meta(ba, sh, lo + warp + 2 * nw, hi), n1 = batch_slice_meta(ba, sh, lo + warp + 3 * nw, hi);
-  for (int q0 = lo + warp; q0 < hi; q0 += 2 * nw) {
-    const int q1 = q0 + nw;
+  const int g = ba.spw == 2 ? 2 : 1, step = g * nw;  // slices a warp takes at once, and its stride
+  SliceMeta n0 = batch_slice_meta(ba, sh, lo + warp + step, hi),
+            n1 = batch_slice_meta(ba, sh, g == 2 ? lo + warp + step + nw : hi, hi);
+  for (int q0 = lo + warp; q0 < hi; q0 += step) {
+    const int q1 = g == 2 ? q0 + nw : hi;
     if (lane == 0) {
       if (n0.vbytes) {
         prefetch_l2_bulk(n0.vals, n0.vbytes);
@@ -208,8 +210,8 @@ __device__ __forceinline__ void batch_spmv2(const BatchArgs &ba, const BatchShar
         prefetch_l2_bulk(n1.cols, n1.cbytes);
       }
     }
-    n0 = batch_slice_meta(ba, sh, q0 + 4 * nw, hi);
-    n1 = batch_slice_meta(ba, sh, q1 + 4 * nw, hi);
+    n0 = batch_slice_meta(ba, sh, q0 + 2 * step, hi);
+    n1 = batch_slice_meta(ba, sh, g == 2 ? q1 + 2 * step : hi, hi);
     const int a0 = batch_locate(sh, q0), s0 = sh.act[a0], sl0 = q0 - sh.pre[a0];
     int a1 = -1, s1 = 0, sl1 = 0;
     if (q1 < hi) {
@@ -904,6 +906,7 @@ struct egpu_batch {
   int chunk = 64;
   int tri_mult = 2;       // sync-free participants: tri_mult x widest level x running systems
   int bps = 2;            // blocks of the persistent inner kernel per SM (1 or 2)
+  int spw = 2;            // SELL slices a warp sums at once in the SpMV phases (1 or 2: 32 or 64 rows)
   bool resume_ok = true;  // reliable updating between segments (EGPU_MIXED_RESTART=1: off)
   bool exit_on_done = false;  // latency mode (egpu_batch_set_latency_mode)
   long long launches = 0;
@@ -1208,6 +1211,7 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
     a.method = B->prm.method;
     a.precond = B->prm.precond;
     a.kmax = B->chunk;
+    a.spw = B->spw;
     a.exit_on_done = B->exit_on_done ? 1 : 0;
     a.tol = inner_tol_of(&B->prm);
     a.maxit = B->prm.inner_max_iter;
@@ -1305,11 +1309,13 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
 }
 
 extern "C" int egpu_batch_set_config(egpu_batch *B, const egpu_batch_config *cfg) {
-  if (!B || !cfg || cfg->chunk_iters < 1 || cfg->blocks_per_sm < 1 || cfg->blocks_per_sm > 2 || cfg->tri_mult < 1)
+  if (!B || !cfg || cfg->chunk_iters < 1 || cfg->blocks_per_sm < 1 || cfg->blocks_per_sm > 2 || cfg->tri_mult < 1 ||
+      cfg->slices_per_warp < 0 || cfg->slices_per_warp > 2)
     return EGPU_ERR_ARG;
   B->chunk = cfg->chunk_iters;
   B->bps = cfg->blocks_per_sm;
   B->tri_mult = cfg->tri_mult;
+  if (cfg->slices_per_warp) B->spw = cfg->slices_per_warp;
   return EGPU_OK;
 }
 
@@ -1398,7 +1404,8 @@ extern "C" int egpu_batch_solve(egpu_batch *B, egpu_result *per_system) {
 
 // Autotuner.  Runs real steps of the resident systems (their progress is kept) with each
 // candidate configuration in turn: chunk length (inner iterations per launch), blocks of
-// the persistent kernel per SM, and, with ILU0, the sync-free participant multiplier.  The
+// the persistent kernel per SM, rows per warp in the SpMV phases (one or two SELL slices of
+// 32 rows), and, with ILU0, the sync-free participant multiplier.  The
 // rate of a step is inner iterations x nonzeros of the systems in the launch per device
 // second of the launch; the fastest configuration is kept.  Candidates are tried once each,
 // in a fixed order, while systems remain in inner solves; systems that finish meanwhile are
@@ -1406,17 +1413,18 @@ extern "C" int egpu_batch_solve(egpu_batch *B, egpu_result *per_system) {
 extern "C" int egpu_batch_tune(egpu_batch *B, egpu_batch_config *cfg) {
   if (!B) return EGPU_ERR_ARG;
   struct Cand {
-    int chunk, bps, tri_mult;
+    int chunk, bps, tri_mult, spw;
   };
   std::vector<Cand> cands;
   const bool ilu = B->prm.precond == EGPU_PREC_ILU0;
   for (int bps : {2, 1})
     for (int chunk : {16, 32, 64})
-      for (int tm : {1, 2, 4}) {
-        if (!ilu && tm != 2) continue;
-        cands.push_back({chunk, bps, tm});
-      }
-  Cand best{B->chunk, B->bps, B->tri_mult};
+      for (int tm : {1, 2, 4})
+        for (int spw : {2, 1}) {
+          if (!ilu && tm != 2) continue;
+          cands.push_back({chunk, bps, tm, spw});
+        }
+  Cand best{B->chunk, B->bps, B->tri_mult, B->spw};
   double best_rate = 0.0;
   int tried = 0;
   // a first step brings every system into its inner solve
@@ -1427,6 +1435,7 @@ extern "C" int egpu_batch_tune(egpu_batch *B, egpu_batch_config *cfg) {
     B->chunk = c.chunk;
     B->bps = c.bps;
     B->tri_mult = c.tri_mult;
+    B->spw = c.spw;
     B->last_iters = 0;
     B->last_ms = 0.f;
     rc = egpu_batch_step(B, nullptr, nullptr);
@@ -1442,10 +1451,12 @@ extern "C" int egpu_batch_tune(egpu_batch *B, egpu_batch_config *cfg) {
   B->chunk = best.chunk;
   B->bps = best.bps;
   B->tri_mult = best.tri_mult;
+  B->spw = best.spw;
   if (cfg) {
     cfg->chunk_iters = best.chunk;
     cfg->blocks_per_sm = best.bps;
     cfg->tri_mult = best.tri_mult;
+    cfg->slices_per_warp = best.spw;
     cfg->candidates = tried;
     cfg->rate = best_rate;
   }

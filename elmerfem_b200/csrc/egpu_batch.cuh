@@ -70,6 +70,7 @@ struct BatchArgs {
   int maxit;
   int tri_warps_per_block;
   int tri_group;            // rows per warp in the sync-free solves (1, 2, 4 or 8)
+  int spw;                  // SELL slices (of 32 rows) a warp sums at once in the SpMV phases (1 or 2)
   unsigned int *bar;
   int *err;
   int *it_done;             // iterations run by this launch (written by block 0)

@@ -443,8 +443,9 @@ class Batch:
         return check(lib().egpu_batch_pending(self._h), self.ctx.handle, "egpu_batch_pending")
 
     def tune(self) -> dict:
-        """egpu_batch_tune: picks chunk length, blocks per SM and triangular-solve participants
-        by timing real steps of the resident systems; returns the kept configuration."""
+        """egpu_batch_tune: picks chunk length, blocks per SM, rows per warp in the SpMV phases
+        and triangular-solve participants by timing real steps of the resident systems;
+        returns the kept configuration."""
         cfg = _lib.BatchConfig()
         check(lib().egpu_batch_tune(self._h, C.byref(cfg)), self.ctx.handle, "egpu_batch_tune")
         return cfg.as_dict()

@@ -288,12 +288,15 @@ int egpu_batch_result(egpu_batch *B, int sys, egpu_result *res);
 int egpu_batch_solution(egpu_batch *B, int sys, double *x);
 int egpu_batch_remove(egpu_batch *B, int sys);
 /* Autotuner: runs real steps of the resident systems with each candidate configuration
- * (inner iterations per launch, persistent-kernel blocks per SM, sync-free triangular-solve
- * participants) and keeps the fastest by nonzeros x iterations per device second.  Systems
- * that finish while tuning are listed by the next egpu_batch_step. */
+ * (inner iterations per launch, persistent-kernel blocks per SM, rows per warp in the SpMV
+ * phases, sync-free triangular-solve participants) and keeps the fastest by nonzeros x
+ * iterations per device second.  Systems that finish while tuning are listed by the next
+ * egpu_batch_step. */
 typedef struct {
   int chunk_iters, blocks_per_sm, tri_mult, candidates;
   double rate;  /* nonzeros x inner iterations per second of the kept configuration */
+  int slices_per_warp;  /* rows per warp in the SpMV phases: 1 or 2 SELL slices of 32 rows (0 in
+                           egpu_batch_set_config: keep) */
 } egpu_batch_config;
 int egpu_batch_tune(egpu_batch *B, egpu_batch_config *cfg);
 /* applies a configuration (e.g. one egpu_batch_tune chose for an earlier batch of the same kind) */

@@ -122,6 +122,7 @@ def test_autotuner_keeps_results_and_reports_every_system(ctx, method, prec, mak
     cfg = B.tune()
     assert cfg["candidates"] >= 1 and cfg["rate"] > 0
     assert cfg["chunk_iters"] in (16, 32, 64) and cfg["blocks_per_sm"] in (1, 2) and cfg["tri_mult"] in (1, 2, 4)
+    assert cfg["slices_per_warp"] in (1, 2)  # rows per warp in the SpMV phases: 32 or 64
     seen = []
     for _ in range(100000):
         seen += B.step()
