@@ -1860,6 +1860,7 @@ extern "C" int egpu_matrix_bind(egpu_ctx *ctx, int n, const int *rows, const int
     cudaMemcpyAsync(A->values.p, values, nnz * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
     A->has_values = true;
   A->t_fp64 = A->t_mixed = 0.0;
+  A->n_mixed = 0;
   } else {
     cudaMemsetAsync(A->values.p, 0, nnz * sizeof(double), ctx->stream);
   }
@@ -1953,6 +1954,7 @@ extern "C" int egpu_matrix_update_values(egpu_mat *A, const double *values) {
   EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   A->has_values = true;
   A->t_fp64 = A->t_mixed = 0.0;
+  A->n_mixed = 0;
   return EGPU_OK;
 }
 
@@ -2099,14 +2101,18 @@ extern "C" int egpu_iter_solve_dev(egpu_mat *A, const double *b_dev, double *x_d
   // faster (EGPU_MIXED_AUTO=0 keeps mixed).  CG / BiCGStab only; GCR and BiCGStab(l) are FP64.
   const char *aenv = std::getenv("EGPU_MIXED_AUTO");
   const bool auto_ok = !(aenv && aenv[0] == '0');
-  // Each path keeps its fastest time on these values (a first solve carries one-time set-up),
-  // and FP64 is taken only with a clear margin.
+  // Each path keeps its fastest time on these values, the mixed one over at least two solves
+  // (its first carries one-time set-up: the FP32 copies' allocations), and FP64 is taken only
+  // with a clear margin.
   const bool krylov32 = prm->method == EGPU_CG || prm->method == EGPU_BICGSTAB;
   if (prm->precision == EGPU_MIXED && krylov32 &&
-      !(auto_ok && A->t_fp64 > 0.0 && A->t_mixed > 0.0 && A->t_fp64 < 0.85 * A->t_mixed)) {
+      !(auto_ok && A->t_fp64 > 0.0 && A->n_mixed >= 2 && A->t_fp64 < 0.85 * A->t_mixed)) {
     rc = egpu::solve_mixed(A, b_dev, x_dev, prm, &r);
     r.precision_used = EGPU_MIXED;
-    if (rc > 0) A->t_mixed = A->t_mixed > 0.0 ? std::min(A->t_mixed, r.seconds) : r.seconds;
+    if (rc > 0) {
+      A->t_mixed = A->n_mixed > 0 ? std::min(A->t_mixed, r.seconds) : r.seconds;
+      A->n_mixed++;
+    }
   } else {
     rc = egpu::solve_fp64(A, b_dev, x_dev, prm, &r);
     r.precision_used = EGPU_FP64;

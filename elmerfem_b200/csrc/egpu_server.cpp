@@ -121,12 +121,17 @@ int prepare(egpu_server *S, Request *r) {
   return egpu_batch_add_matrix(S->batch, r->A, r->rhs_dev);
 }
 
-// device and input memory of a request (under gpu_mu)
-void release(Request *r) {
+// device memory of a request (under gpu_mu)
+void release_device(Request *r) {
   if (r->rhs_dev) egpu::dev_free(r->rhs_dev, r->rhs_cap, r->rhs_devid);
   r->rhs_dev = nullptr;
   if (r->A) egpu_matrix_free(r->A);
   r->A = nullptr;
+}
+
+// device and input memory of a request (under gpu_mu)
+void release(Request *r) {
+  release_device(r);
   std::vector<double>().swap(r->values);
   std::vector<double>().swap(r->rhs);
   std::vector<double>().swap(r->elem_k);
@@ -159,13 +164,24 @@ void work(egpu_server *S) {
   while (true) {
     S->cv_work.wait(lk, [&] { return S->stop || !S->queue.empty() || !S->by_slot.empty(); });
     if (S->stop) break;
-    // admission in arrival order: footprint within the budget and a free slot (a request
-    // larger than the whole budget still runs, alone)
+    // admission in arrival order: footprint within the budget, within the device memory that
+    // is free now (the registered patterns' resident prototypes and other users of the GPU
+    // take their share), and a free slot; a request larger than the whole budget still runs,
+    // alone
     std::vector<Request *> admit;
+    double avail = 0.0;
+    {
+      size_t fr = 0, tot = 0;
+      if (cudaMemGetInfo(&fr, &tot) == cudaSuccess)
+        avail = (double)fr + (double)egpu_cached_bytes(S->device) - 0.03 * (double)tot;
+    }
+    double adm_bytes = 0.0;
     while (!S->queue.empty() && (int)(S->by_slot.size() + admit.size()) < S->max_resident) {
       Request *r = S->queue.front();
-      if (S->used + r->footprint > S->budget && !(S->by_slot.empty() && admit.empty())) break;
+      const bool alone = S->by_slot.empty() && admit.empty();
+      if (!alone && (S->used + r->footprint > S->budget || adm_bytes + r->footprint > avail)) break;
       S->used += r->footprint;
+      adm_bytes += r->footprint;
       r->t_admit = Clock::now();
       admit.push_back(r);
       S->queue.pop_front();
@@ -173,7 +189,7 @@ void work(egpu_server *S) {
     lk.unlock();
     // GPU work: prepare the admitted systems, one step, collect the finished ones
     std::vector<std::pair<Request *, int>> added;
-    std::vector<Request *> retired;
+    std::vector<Request *> retired, requeue;
     int step_rc = 0;
     Clock::time_point c0, c1, c2, c3;
     double h2d = 0, d2h = 0;
@@ -181,13 +197,28 @@ void work(egpu_server *S) {
     {
       std::lock_guard<std::mutex> g(S->gpu_mu);
       c0 = Clock::now();
+      bool placed_any = !S->by_slot.empty();
       for (Request *r : admit) {
-        h2d += input_bytes(r);
+        // a device allocation that fails while other requests hold memory puts the request
+        // back in the queue, to be admitted again once some of them have retired
+        if (!requeue.empty()) {
+          requeue.push_back(r);
+          continue;
+        }
         const int slot = prepare(S, r);
+        if (slot < 0 && (slot == EGPU_ERR_ALLOC || slot == EGPU_ERR_CUDA) && placed_any) {
+          release_device(r);
+          cudaGetLastError();  // an out-of-memory allocation leaves a non-sticky error
+          requeue.push_back(r);
+          continue;
+        }
+        h2d += input_bytes(r);
         if (slot < 0) {
           r->res = egpu_result{};
           r->res.info = slot;
           release(r);
+        } else {
+          placed_any = true;
         }
         added.push_back({r, slot});
       }
@@ -227,6 +258,10 @@ void work(egpu_server *S) {
       nl = egpu_kernel_launches(S->ctx);
     }
     lk.lock();
+    for (auto it = requeue.rbegin(); it != requeue.rend(); ++it) {
+      S->used -= (*it)->footprint;
+      S->queue.push_front(*it);
+    }
     S->launches = nl;
     S->bytes_h2d += h2d;
     S->bytes_d2h += d2h;

@@ -304,9 +304,11 @@ class NativeSolveServer:
         lat = np.array([r.latency for r in reqs])
         makespan = max(r.finished for r in reqs) - min(r.arrival for r in reqs)
         w1 = self.info()
+        info = collections.Counter(int(r.result.get("info", 0)) for r in reqs)
         return {"solves": len(reqs), "makespan_s": makespan, "solves_per_s": len(reqs) / makespan,
                 "p50_ms": 1000 * float(np.percentile(lat, 50)), "p99_ms": 1000 * float(np.percentile(lat, 99)),
-                "steps": w1["steps"], "converged": sum(1 for r in reqs if r.result.get("info") == 1),
+                "steps": w1["steps"], "converged": info.get(1, 0),
+                "status_counts": {str(k): v for k, v in sorted(info.items())},
                 "worker_seconds": {k: round(w1[k] - w0[k], 4) for k in ("seconds_prepare", "seconds_step",
                                                                         "seconds_retire")},
                 "kernel_launches": int(w1["kernel_launches"] - w0["kernel_launches"]),

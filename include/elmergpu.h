@@ -97,8 +97,9 @@ typedef struct {
   double seconds_krylov;  /* device time inside the persistent Krylov kernels */
   int krylov_launches;    /* number of persistent Krylov kernel launches */
   /* the path that ran: EGPU_FP64, or EGPU_MIXED.  A mixed request on a matrix whose current
-   * values were solved clearly faster by the FP64 drop-in (both paths measured on them, fastest
-   * times, FP64 below 0.85 of mixed) runs the drop-in (EGPU_MIXED_AUTO=0 keeps mixed) */
+   * values were solved clearly faster by the FP64 drop-in (one FP64 and two mixed solves timed
+   * on them, fastest times, FP64 below 0.85 of mixed) runs the drop-in (EGPU_MIXED_AUTO=0 keeps
+   * mixed) */
   int precision_used;
 } egpu_result;
 

@@ -1,6 +1,6 @@
 """A mixed-precision request runs the faster of the two paths measured on the matrix's current
-values: once an FP64 solve and a mixed solve of those values have run, the FP64 drop-in is taken
-when its fastest time is below 0.85 of the mixed one (on stiff operators with latency-bound
+values: once an FP64 solve and two mixed solves of those values have run, the FP64 drop-in is
+taken when its fastest time is below 0.85 of the mixed one (on stiff operators with latency-bound
 triangular solves, such as elasticity with ILU0, rounding the matrix to FP32 costs more
 refinements than FP32 saves).  Either way the solution meets 1e-8 against the oracle; new values
 reset the measurements; EGPU_MIXED_AUTO=0 keeps the mixed path."""
@@ -28,9 +28,10 @@ def test_mixed_request_takes_the_measured_faster_path(ctx, monkeypatch):
             x, r = A.solve(b, params=_params(eg.FP64))
             assert r["precision_used"] == eg.FP64 and rel(x, x_orc) < 1e-8
             t64.append(r["seconds"])
-        x, r = A.solve(b, params=_params(eg.MIXED))  # the first mixed solve is always mixed
-        assert r["precision_used"] == eg.MIXED and rel(x, x_orc) < 1e-8
-        tm.append(r["seconds"])
+        for _ in range(2):  # the first two mixed requests are mixed (the first carries set-up)
+            x, r = A.solve(b, params=_params(eg.MIXED))
+            assert r["precision_used"] == eg.MIXED and rel(x, x_orc) < 1e-8
+            tm.append(r["seconds"])
         for _ in range(3):
             expect = eg.FP64 if min(t64) < 0.85 * min(tm) else eg.MIXED
             x, r = A.solve(b, params=_params(eg.MIXED))
