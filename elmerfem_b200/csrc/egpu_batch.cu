@@ -906,7 +906,7 @@ struct egpu_batch {
   int chunk = 64;
   int tri_mult = 2;       // sync-free participants: tri_mult x widest level x running systems
   int bps = 2;            // blocks of the persistent inner kernel per SM (1 or 2)
-  int spw = 2;            // SELL slices a warp sums at once in the SpMV phases (1 or 2: 32 or 64 rows)
+  int spw = 1;            // SELL slices a warp sums at once in the SpMV phases (1 or 2: 32 or 64 rows)
   bool resume_ok = true;  // reliable updating between segments (EGPU_MIXED_RESTART=1: off)
   bool exit_on_done = false;  // latency mode (egpu_batch_set_latency_mode)
   long long launches = 0;
@@ -1404,8 +1404,8 @@ extern "C" int egpu_batch_solve(egpu_batch *B, egpu_result *per_system) {
 
 // Autotuner.  Runs real steps of the resident systems (their progress is kept) with each
 // candidate configuration in turn: chunk length (inner iterations per launch), blocks of
-// the persistent kernel per SM, rows per warp in the SpMV phases (one or two SELL slices of
-// 32 rows), and, with ILU0, the sync-free participant multiplier.  The
+// the persistent kernel per SM, and, with ILU0, the sync-free participant multiplier; then
+// rows per warp in the SpMV phases (one or two SELL slices of 32 rows) by alternating steps.  The
 // rate of a step is inner iterations x nonzeros of the systems in the launch per device
 // second of the launch; the fastest configuration is kept.  Candidates are tried once each,
 // in a fixed order, while systems remain in inner solves; systems that finish meanwhile are
@@ -1419,11 +1419,10 @@ extern "C" int egpu_batch_tune(egpu_batch *B, egpu_batch_config *cfg) {
   const bool ilu = B->prm.precond == EGPU_PREC_ILU0;
   for (int bps : {2, 1})
     for (int chunk : {16, 32, 64})
-      for (int tm : {1, 2, 4})
-        for (int spw : {2, 1}) {
-          if (!ilu && tm != 2) continue;
-          cands.push_back({chunk, bps, tm, spw});
-        }
+      for (int tm : {1, 2, 4}) {
+        if (!ilu && tm != 2) continue;
+        cands.push_back({chunk, bps, tm, B->spw});
+      }
   Cand best{B->chunk, B->bps, B->tri_mult, B->spw};
   double best_rate = 0.0;
   int tried = 0;
@@ -1452,6 +1451,27 @@ extern "C" int egpu_batch_tune(egpu_batch *B, egpu_batch_config *cfg) {
   B->bps = best.bps;
   B->tri_mult = best.tri_mult;
   B->spw = best.spw;
+  // Rows per warp in the SpMV phases, with the rest fixed: steps alternate one and two slices
+  // per warp (A B A B ...), so the batch shrinking as systems converge biases neither, and the
+  // higher mean rate is kept.
+  {
+    double sum[2] = {0.0, 0.0};
+    int cnt[2] = {0, 0};
+    for (int t = 0; t < 6 && egpu_batch_pending(B) > 0; ++t) {
+      const int k = t & 1;
+      B->spw = k + 1;
+      B->last_iters = 0;
+      B->last_ms = 0.f;
+      rc = egpu_batch_step(B, nullptr, nullptr);
+      if (rc) return rc;
+      if (B->last_iters <= 0 || B->last_ms <= 0.f) continue;
+      sum[k] += (double)B->last_iters * (double)B->last_nnz / (B->last_ms * 1e-3);
+      cnt[k]++;
+      ++tried;
+    }
+    if (cnt[0] && cnt[1]) best.spw = sum[1] / cnt[1] > sum[0] / cnt[0] ? 2 : 1;
+    B->spw = best.spw;
+  }
   if (cfg) {
     cfg->chunk_iters = best.chunk;
     cfg->blocks_per_sm = best.bps;
