@@ -245,10 +245,7 @@ __global__ void __launch_bounds__(256) k_ilu0_factor(int n, const int *__restric
         if (t0 == 0) t0 = egpu_globaltimer();
         if ((++spin & 31u) == 0) {
           int stop = 0;
-          if (lane == 0) {
-            if ((spin & 1023u) == 0) egpu_poll_abort(err);
-            stop = egpu_globaltimer() - t0 > egpu_wait_limit(err) ? 1 : (*(volatile int *)err ? 2 : 0);
-          }
+          if (lane == 0) stop = egpu_globaltimer() - t0 > egpu_wait_limit(err) ? 1 : (*(volatile int *)err ? 2 : 0);
           stop = __shfl_sync(0xffffffffu, stop, 0);
           if (stop) {
             if (stop == 1 && lane == 0) atomicExch(err, (int)EGPU_ERR_TIMEOUT);

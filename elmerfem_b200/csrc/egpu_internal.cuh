@@ -327,7 +327,6 @@ struct Sentinel<double> {
       v = ld_relaxed_u64(p);
       if (v != EGPU_SENTINEL64) break;
       if ((spin & 31u) == 0) {
-        if ((spin & 4095u) == 0) egpu_poll_abort(err);
         if (egpu_globaltimer() - t0 > lim) {
           atomicExch(err, (int)EGPU_ERR_TIMEOUT);
           break;
@@ -357,7 +356,6 @@ struct Sentinel<float> {
       v = ld_relaxed_u32(p);
       if (v != EGPU_SENTINEL32) break;
       if ((spin & 31u) == 0) {
-        if ((spin & 4095u) == 0) egpu_poll_abort(err);
         if (egpu_globaltimer() - t0 > lim) {
           atomicExch(err, (int)EGPU_ERR_TIMEOUT);
           break;
@@ -376,8 +374,10 @@ struct Sentinel<float> {
 // of barriers passed.  The wait is bounded by the context's wait limit; on expiry the error
 // flag is set.  Block 0 reads the host's abort word every EGPU_ABORT_POLL-th barrier, before
 // it arrives (the read crosses the host link, so every other block waits for it: rare enough
-// to cost nothing measurable), and every waiting block reads it during long waits.  Returns
-// false when the kernel must unwind (error flag set by anyone).
+// to cost nothing measurable), and block 1 reads it during long waits.  Reads of host memory
+// are kept this rare on purpose: hundreds of warps polling it while they wait (the sync-free
+// solves, the ILU factorisation) doubled the set-up time of a large solve.  Returns false
+// when the kernel must unwind (error flag set by anyone).
 #define EGPU_ABORT_POLL 256u
 __device__ __forceinline__ bool grid_barrier(unsigned int *count, int *err, unsigned int &epoch) {
   __syncthreads();
@@ -391,7 +391,8 @@ __device__ __forceinline__ bool grid_barrier(unsigned int *count, int *err, unsi
       unsigned int spins = 0;
       while (ld_acquire_u32(count) < target) {
         if ((++spins & 63u) == 0) {
-          if ((spins & 1023u) == 0) egpu_poll_abort(err);
+          // one block polls during long waits (block 0 may be the one still working)
+          if ((spins & 1023u) == 0 && blockIdx.x == (gridDim.x > 1 ? 1u : 0u)) egpu_poll_abort(err);
           if (*(volatile int *)err) break;
           if (egpu_globaltimer() - t0 > lim) {
             atomicExch(err, (int)EGPU_ERR_TIMEOUT);

@@ -270,10 +270,8 @@ __device__ __forceinline__ void warp_wait_all(VT (&xv)[E], const int (&c)[E], co
     if (!__any_sync(0xffffffffu, pend)) return;
     if ((spin & 31u) == 0) {
       int stop = 0;
-      if ((threadIdx.x & 31) == 0) {
-        if ((spin & 1023u) == 0) egpu_poll_abort(err);
+      if ((threadIdx.x & 31) == 0)
         stop = egpu_globaltimer() - t0 > egpu_wait_limit(err) ? 1 : (*(volatile int *)err ? 2 : 0);
-      }
       stop = __shfl_sync(0xffffffffu, stop, 0);
       if (stop) {
         if (stop == 1 && (threadIdx.x & 31) == 0) atomicExch(err, (int)EGPU_ERR_TIMEOUT);

@@ -124,7 +124,7 @@ void *egpu_stream(const egpu_ctx *ctx);
  * it; the context stays usable. */
 int egpu_set_wait_limit(egpu_ctx *ctx, double seconds);
 /* Cancellation: raise != 0 sets the context's host-mapped abort word, which the running
- * kernels poll (block 0 every 256th grid barrier, and every long wait); the call in flight
+ * kernels poll (block 0 every 256th grid barrier, block 1 during long barrier waits); the call in flight
  * and every later call return EGPU_ERR_ABORT until egpu_abort(ctx, 0).  Makes no CUDA call
  * and may be called from any host thread while a solve runs. */
 int egpu_abort(egpu_ctx *ctx, int raise);
