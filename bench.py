@@ -452,13 +452,18 @@ def run_gpu(args, rank, world, local, pg):
             x.zero_()
         return A.solve_dev(None, x.data_ptr(), prm)
 
-    # warm-up (the FP64 drop-in's solution is kept for the error figures)
-    r64 = step(fp64)
+    # warm-up: two FP64 drop-in solves, then the mixed requests.  The library measures both
+    # paths on the matrix (each path's first solve carries one-time set-up) and, from the third
+    # mixed request on, runs the faster one; the second mixed request is always on the mixed
+    # path and its solution is kept for the error figures, as is the FP64 drop-in's.
+    for _ in range(2):
+        r64 = step(fp64)
     x64 = x.cpu().numpy()
-    for _ in range(max(0, args.warmup - 1)):
-        step(mixed)
-    rm = step(mixed)
-    xm = x.cpu().numpy()
+    for i in range(max(2, args.warmup)):
+        r = step(mixed)
+        if i == 1:
+            rm, xm = r, x.cpu().numpy()
+    assert rm["precision_used"] == eg.MIXED
 
     small, note = l2_note(n, nnz)
     flush_buf = torch.empty(64 * 2**20, dtype=torch.float32, device=dev) if small else None
@@ -498,10 +503,14 @@ def run_gpu(args, rank, world, local, pg):
     value = world * args.steps / t
     lat = sorted(r["seconds"] for r in results)
 
-    # ---- roofline of the dominant kernel (persistent FP32 inner Krylov kernel)
-    iters = sum(r["iters"] for r in results)
-    sec_k = sum(r["seconds_krylov"] for r in results)
-    nlaunch = sum(r["krylov_launches"] for r in results)
+    # ---- roofline of the dominant kernel: the persistent Krylov kernel of the path the timed
+    # requests took (FP32 inner for mixed, FP64 for the drop-in)
+    n_mixed_path = sum(1 for r in results if r.get("precision_used") == eg.MIXED)
+    path = "mixed" if 2 * n_mixed_path >= len(results) else "fp64"
+    on_path = [r for r in results if (r.get("precision_used") == eg.MIXED) == (path == "mixed")]
+    iters = sum(r["iters"] for r in on_path)
+    sec_k = sum(r["seconds_krylov"] for r in on_path)
+    nlaunch = sum(r["krylov_launches"] for r in on_path)
     off_frac = compact_offset_fraction(pat)
     # the library's FP32 inner CG drops the Jacobi step when the scaled diagonal rounds to 1.0f
     # everywhere (as it does after the symmetric scaling of a positive diagonal)
@@ -510,15 +519,16 @@ def run_gpu(args, rank, world, local, pg):
         dv = A.values()[pat.diag - 1]
         dsc = 1.0 / np.sqrt(np.abs(dv))
         unit_diag = bool(np.all((dv * dsc * dsc).astype(np.float32) == np.float32(1.0)))
-    bpi = algorithmic_bytes_per_iter(solve_kw["method"], solve_kw["precond"], "mixed", n, nnz, cols16, off_frac,
+    bpi = algorithmic_bytes_per_iter(solve_kw["method"], solve_kw["precond"], path, n, nnz, cols16, off_frac,
                                      unit_diag)
     peak, peak_kind = read_peaks()
     achieved = bpi * iters / sec_k / 1e9
     traffic = read_traffic(cfg["workload"])
+    ty, what = ("float", "FP32 inner") if path == "mixed" else ("double", "FP64 drop-in")
     if solve_kw["method"] == eg.CG:
-        kernel_name = "cg_kernel<float,LPR,int16 cols> (persistent FP32 inner CG)"
+        kernel_name = f"cg_kernel<{ty},LPR,int16 cols> (persistent {what} CG)"
     else:
-        kernel_name = ("bicgstab_kernel<float,LPR,int16 cols> (persistent FP32 inner BiCGStab, "
+        kernel_name = (f"bicgstab_kernel<{ty},LPR,int16 cols> (persistent {what} BiCGStab, "
                        + ("ILU0 triangular solves in the kernel)" if solve_kw["precond"] == eg.PREC_ILU0 else "no ILU)"))
 
     # ---- FP64 drop-in on the same system
@@ -600,7 +610,8 @@ def run_gpu(args, rank, world, local, pg):
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1000.0 * t / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 refinement", "data": "synthetic",
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 inner / f64 refinement" if path == "mixed" else "f64", "data": "synthetic",
                 "config": headline_config(cfg, n, nnz, world),
                 "latency_ms": {"p50": 1000 * lat[len(lat) // 2], "p99": 1000 * lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
                 "iterations": {"mixed_inner_total": rm["iters"], "refinements": rm["refinements"],

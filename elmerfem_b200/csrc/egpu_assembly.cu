@@ -537,8 +537,6 @@ extern "C" int egpu_assemble_poisson(egpu_mat *A, const double *elem_k, const do
   EGPU_CUDA_TRY(ctx, cudaGetLastError());
   EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   A->has_values = true;
-  A->t_fp64 = A->t_mixed = 0.0;
-  A->n_mixed = 0;
   A->has_rhs = true;
   A->ilu_valid = false;
   return EGPU_OK;
@@ -573,8 +571,6 @@ extern "C" int egpu_assemble_elastic(egpu_mat *A, double young, double poisson, 
   EGPU_CUDA_TRY(ctx, cudaGetLastError());
   EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   A->has_values = true;
-  A->t_fp64 = A->t_mixed = 0.0;
-  A->n_mixed = 0;
   A->has_rhs = true;
   A->ilu_valid = false;
   return EGPU_OK;

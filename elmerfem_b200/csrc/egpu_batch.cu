@@ -149,6 +149,22 @@ __device__ __forceinline__ void batch_clear(const BatchArgs &a, int slot) {
     if (s % gridDim.x == (int)blockIdx.x) a.acc[slot * BATCH_MAX_SYS + s] = 0.0;
 }
 
+// SELL SpMV of one slice: lane's row sum of A x
+__device__ __forceinline__ float slice_spmv(const SysDesc &d, int slice, int lane, const float *x) {
+  const int r = (slice << 5) + lane;
+  const int w = __ldg(d.sell_w + slice);
+  const int base = __ldg(d.sell_ptr + slice) + lane;
+  float s = 0.f;
+#pragma unroll 8
+  for (int k = 0; k < w; ++k) {
+    const int e = base + (k << 5);
+    const float v = __ldcs(d.svals + e);
+    const int c = d.scols16 ? r + (int)__ldcs(d.scols16 + e) : __ldcs(d.scols + e);
+    s = fmaf(v, __ldca(x + c), s);
+  }
+  return s;
+}
+
 // Two slices of (possibly) different systems summed in one interleaved loop: a tet row has
 // about 15 entries, so one slice alone gives each lane a short chain of dependent gathers and
 // leaves the warp waiting on memory; two slices double the loads in flight.  d0 / d1 null:
@@ -186,10 +202,31 @@ __device__ __forceinline__ void slice_spmv2(const SysDesc *d0, int sl0, const fl
   y1 = s1;
 }
 
-// SpMV phase over this block's share of the active slices, ba.spw (1 or 2, chosen by the
-// autotuner) slices per warp at a time (slice_spmv2); lane 0 prefetches the next ones into L2.  src(s): the
-// vector system s multiplies; epi(act_index, s, slice, y): once per running slice, y the
-// lane's row sum.  Slices of systems that do not run are skipped (warp-uniform).
+// SpMV phase over this block's share of the active slices, one slice per warp at a time;
+// lane 0 prefetches the next one into L2.  src(s): the vector system s multiplies;
+// epi(act_index, s, slice, y): once per running slice, y the lane's row sum.  Slices of
+// systems that do not run are skipped (warp-uniform).
+template <typename SRC, typename EPI>
+__device__ __forceinline__ void batch_spmv1(const BatchArgs &ba, const BatchShared &sh, SRC &&src, EPI &&epi) {
+  const int total = sh.total, nb = gridDim.x;
+  const int lo = (int)((long long)total * blockIdx.x / nb), hi = (int)((long long)total * (blockIdx.x + 1) / nb);
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, lane = threadIdx.x & 31;
+  SliceMeta next = batch_slice_meta(ba, sh, lo + warp + nw, hi);
+  for (int q = lo + warp; q < hi; q += nw) {
+    const int a = batch_locate(sh, q);
+    if (lane == 0 && next.vbytes) {
+      prefetch_l2_bulk(next.vals, next.vbytes);
+      prefetch_l2_bulk(next.cols, next.cbytes);
+    }
+    next = batch_slice_meta(ba, sh, q + 2 * nw, hi);
+    const int s = sh.act[a];
+    if (sh.status[s] != ST_RUN) continue;
+    const int slice = q - sh.pre[a];
+    epi(a, s, slice, slice_spmv(ba.sys[s], slice, lane, src(s)));
+  }
+}
+
+// The same phase with two slices per warp at a time (slice_spmv2).
 template <typename SRC, typename EPI>
 __device__ __forceinline__ void batch_spmv2(const BatchArgs &ba, const BatchShared &sh, SRC &&src, EPI &&epi) {
   const int total = sh.total, nb = gridDim.x;
@@ -227,6 +264,16 @@ __device__ __forceinline__ void batch_spmv2(const BatchArgs &ba, const BatchShar
     if (run0) epi(a0, s0, sl0, y0);
     if (run1) epi(a1, s1, sl1, y1);
   }
+}
+
+// SPW (1 or 2, chosen by the autotuner) slices per warp; each form is its own instantiation of
+// the inner kernel, so neither pays the other's registers
+template <int SPW, typename SRC, typename EPI>
+__device__ __forceinline__ void batch_spmv(const BatchArgs &ba, const BatchShared &sh, SRC &&src, EPI &&epi) {
+  if (SPW == 2)
+    batch_spmv2(ba, sh, src, epi);
+  else
+    batch_spmv1(ba, sh, src, epi);
 }
 
 // Sync-free ILU0 solves over the systems in RUN state, slots interleaved across systems:
@@ -421,6 +468,7 @@ __device__ __forceinline__ void batch_tri_any(const BatchArgs &a, const BatchSha
 // ------------------------------------------------------------------------------------
 // the kernel
 
+template <int SPW>
 __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int parity0) {
   __shared__ BatchShared sh;
   __shared__ double rho_s[BATCH_MAX_SYS];
@@ -528,7 +576,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       // S: Q = A P; PQ;  clear RHO, RR
       batch_clear(a, BA_RHO);
       batch_clear(a, BA_RR);
-      batch_spmv2(a, sh, [&](int s) -> const float * { return a.sys[s].w + 2 * a.sys[s].ldw; },
+      batch_spmv<SPW>(a, sh, [&](int s) -> const float * { return a.sys[s].w + 2 * a.sys[s].ldw; },
                   [&](int ai, int s, int slice, float q) {
         const SysDesc &d = a.sys[s];
         const int r = (slice << 5) + lane;
@@ -610,7 +658,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       batch_clear(a, BA_RHO);
       batch_clear(a, BA_RR);
       batch_clear(a, BA_SS);
-      batch_spmv2(a, sh, [&](int s) -> const float * { return a.sys[s].w + 6 * a.sys[s].ldw; },
+      batch_spmv<SPW>(a, sh, [&](int s) -> const float * { return a.sys[s].w + 6 * a.sys[s].ldw; },
                   [&](int ai, int s, int slice, float v) {
         const SysDesc &d = a.sys[s];
         const int r = (slice << 5) + lane;
@@ -666,7 +714,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       if (!grid_barrier(a.bar, a.err, epoch)) return;
       // 4: T = A T2; TS, TT;  clear PQ
       batch_clear(a, BA_PQ);
-      batch_spmv2(a, sh, [&](int s) -> const float * { return a.sys[s].w + 7 * a.sys[s].ldw; },
+      batch_spmv<SPW>(a, sh, [&](int s) -> const float * { return a.sys[s].w + 7 * a.sys[s].ldw; },
                   [&](int ai, int s, int slice, float t) {
         const SysDesc &d = a.sys[s];
         const int r = (slice << 5) + lane;
@@ -1218,8 +1266,9 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
     int maxw = 1;
     for (int i = 0; i < ns; ++i)
       if (B->sys[i] && B->sys[i]->phase == 2) maxw = std::max(maxw, B->sys[i]->A->tri.max_width);
+    const void *kern = a.spw == 2 ? (const void *)k_batch_inner<2> : (const void *)k_batch_inner<1>;
     int bps = 0;
-    EGPU_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_batch_inner, EGPU_BLOCK, 0));
+    EGPU_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, EGPU_BLOCK, 0));
     bps = std::max(1, std::min(bps, B->bps));
     const int grid = ctx->num_sms * bps;
     int nrun = 0;
@@ -1253,8 +1302,7 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
     int parity0 = B->parity;
     void *args[] = {&a, &parity0};
     EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ek0, ctx->stream));
-    EGPU_CUDA_TRY(ctx, cudaLaunchCooperativeKernel((const void *)k_batch_inner, dim3(grid), dim3(EGPU_BLOCK), args, 0,
-                                                   ctx->stream));
+    EGPU_CUDA_TRY(ctx, cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(EGPU_BLOCK), args, 0, ctx->stream));
     EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ek1, ctx->stream));
     ctx->launches++;
     B->launches++;

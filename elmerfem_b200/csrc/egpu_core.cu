@@ -1856,8 +1856,6 @@ extern "C" int egpu_matrix_bind(egpu_ctx *ctx, int n, const int *rows, const int
   if (values) {
     cudaMemcpyAsync(A->values.p, values, nnz * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
     A->has_values = true;
-  A->t_fp64 = A->t_mixed = 0.0;
-  A->n_mixed = 0;
   } else {
     cudaMemsetAsync(A->values.p, 0, nnz * sizeof(double), ctx->stream);
   }
@@ -1950,8 +1948,6 @@ extern "C" int egpu_matrix_update_values(egpu_mat *A, const double *values) {
                                      ctx->stream));
   EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   A->has_values = true;
-  A->t_fp64 = A->t_mixed = 0.0;
-  A->n_mixed = 0;
   return EGPU_OK;
 }
 
@@ -2094,26 +2090,26 @@ extern "C" int egpu_iter_solve_dev(egpu_mat *A, const double *b_dev, double *x_d
   // Mixed precision is a request for the faster of the two paths at the same tolerance: on
   // operators where rounding the scaled matrix to FP32 costs more refinements than the FP32
   // iterations save (latency-bound triangular solves, stiff elasticity), the FP64 drop-in is
-  // faster.  Once both have solved the current values, a mixed request takes the one measured
-  // faster (EGPU_MIXED_AUTO=0 keeps mixed).  CG / BiCGStab only; GCR and BiCGStab(l) are FP64.
+  // faster.  The library measures both on the matrix itself: the first two mixed requests run
+  // mixed, and while fewer than two FP64 solves have run (the caller's own included) the next
+  // run as the FP64 drop-in; each path's first solve carries one-time set-up and is not
+  // compared.  From then on a mixed request takes FP64 when its latest time is below 0.85 of
+  // the latest mixed one.  Both paths meet the same tolerance.  CG / BiCGStab only (GCR and
+  // BiCGStab(l) are FP64); EGPU_MIXED_AUTO=0 keeps every mixed request mixed.
   const char *aenv = std::getenv("EGPU_MIXED_AUTO");
   const bool auto_ok = !(aenv && aenv[0] == '0');
-  // Each path keeps its fastest time on these values, the mixed one over at least two solves
-  // (its first carries one-time set-up: the FP32 copies' allocations), and FP64 is taken only
-  // with a clear margin.
   const bool krylov32 = prm->method == EGPU_CG || prm->method == EGPU_BICGSTAB;
-  if (prm->precision == EGPU_MIXED && krylov32 &&
-      !(auto_ok && A->t_fp64 > 0.0 && A->n_mixed >= 2 && A->t_fp64 < 0.85 * A->t_mixed)) {
+  bool mixed = prm->precision == EGPU_MIXED && krylov32;
+  if (mixed && auto_ok && A->n_mixed >= 2)
+    mixed = A->n_fp64 >= 2 && !(A->t_fp64 < 0.85 * A->t_mixed);
+  if (mixed) {
     rc = egpu::solve_mixed(A, b_dev, x_dev, prm, &r);
     r.precision_used = EGPU_MIXED;
-    if (rc > 0) {
-      A->t_mixed = A->n_mixed > 0 ? std::min(A->t_mixed, r.seconds) : r.seconds;
-      A->n_mixed++;
-    }
+    if (rc > 0 && r.info == EGPU_HUTI_CONVERGENCE && A->n_mixed++ > 0) A->t_mixed = r.seconds;
   } else {
     rc = egpu::solve_fp64(A, b_dev, x_dev, prm, &r);
     r.precision_used = EGPU_FP64;
-    if (rc > 0) A->t_fp64 = A->t_fp64 > 0.0 ? std::min(A->t_fp64, r.seconds) : r.seconds;
+    if (krylov32 && rc > 0 && r.info == EGPU_HUTI_CONVERGENCE && A->n_fp64++ > 0) A->t_fp64 = r.seconds;
   }
   if (res) *res = r;
   return rc;

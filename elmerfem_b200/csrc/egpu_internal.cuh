@@ -191,11 +191,11 @@ struct egpu_mat {
   DevBuf<double> values;         // as bound / assembled (unscaled)
   DevBuf<double> rhs;            // assembled right-hand side
   bool has_values = false, has_rhs = false;
-  // fastest device seconds of an FP64 and of a mixed-precision solve of the current values (0:
-  // none yet) and the number of mixed solves timed; a mixed request runs as the FP64 drop-in
-  // once an FP64 solve and two mixed ones were timed and FP64 took less than 0.85 of mixed
+  // device seconds of the latest FP64 and mixed-precision solves of this matrix after each
+  // path's first (which carries one-time set-up), and the solves of each path so far; they
+  // outlive value updates (a time or nonlinear loop re-assembles the same operator)
   double t_fp64 = 0.0, t_mixed = 0.0;
-  int n_mixed = 0;
+  int n_fp64 = 0, n_mixed = 0;
   int max_row = 0;               // longest row
   int max_bandwidth = 0;         // max |col - row|
   bool sorted_rows = true;       // columns strictly ascending in every row (CRS_SortMatrix); ILU needs it

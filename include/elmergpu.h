@@ -96,10 +96,12 @@ typedef struct {
   double seconds_setup;   /* scaling + preconditioner construction part of seconds */
   double seconds_krylov;  /* device time inside the persistent Krylov kernels */
   int krylov_launches;    /* number of persistent Krylov kernel launches */
-  /* the path that ran: EGPU_FP64, or EGPU_MIXED.  A mixed request on a matrix whose current
-   * values were solved clearly faster by the FP64 drop-in (one FP64 and two mixed solves timed
-   * on them, fastest times, FP64 below 0.85 of mixed) runs the drop-in (EGPU_MIXED_AUTO=0 keeps
-   * mixed) */
+  /* the path that ran: EGPU_FP64, or EGPU_MIXED.  A CG / BiCGStab mixed request is a request
+   * for the faster path at the same tolerance: on each matrix the first two mixed requests run
+   * mixed, the next run the FP64 drop-in until two FP64 solves have run (the caller's own
+   * included), and after that the drop-in is taken when its latest time is below 0.85 of the
+   * latest mixed one.  Each path's first solve (one-time set-up) is not compared; the times
+   * outlive value updates.  EGPU_MIXED_AUTO=0 keeps every mixed request mixed. */
   int precision_used;
 } egpu_result;
 
