@@ -1041,6 +1041,17 @@ static int run_krylov(egpu_mat *A, const KArgs<VT> &a0, int method, bool offs) {
   // the instantiation with the level-synchronous solves only when this matrix uses them
   const bool cta = a.tri_cta != 0;
   if (method == EGPU_CG) {
+    if constexpr (sizeof(VT) == 4) {
+      // FP32 inner solves without ILU: single-reduction CG (EGPU_CG_SR=0 keeps cg_kernel)
+      const char *e = std::getenv("EGPU_CG_SR");
+      if (!a.true_residual && a.precond != EGPU_PREC_ILU0 && !(e && e[0] == '0')) {
+        if (a.precond == EGPU_PREC_NONE || a.unit_diag)
+          return offs ? launch_coop(ctx, cg_sr_kernel<TRI_TS, true, true>, a, nullptr, 0)
+                      : launch_coop(ctx, cg_sr_kernel<TRI_TS, false, true>, a, nullptr, 0);
+        return offs ? launch_coop(ctx, cg_sr_kernel<TRI_TS, true, false>, a, nullptr, 0)
+                    : launch_coop(ctx, cg_sr_kernel<TRI_TS, false, false>, a, nullptr, 0);
+      }
+    }
     if (cta) {
       if (offs) return launch_coop(ctx, cg_kernel<VT, TRI_TS, true, true>, a, nullptr, smem);
       return launch_coop(ctx, cg_kernel<VT, TRI_TS, false, true>, a, nullptr, smem);

@@ -464,6 +464,32 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *smem /* >= 32
   __syncthreads();
 }
 
+// NV sums at once: slot k's partials at partials + slot[k] * nb, all loads in flight together
+// (one L2 round trip for all of them); the same fixed order as reduce_partials.
+template <int NV>
+__device__ __forceinline__ void reduce_partials_n(const double *partials, const int (&slot)[NV], int nb,
+                                                  double *smem, double (&out)[NV]) {
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x < 32) {
+    double t[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) t[k] = 0.0;
+    for (int i = lane; i < nb; i += 32)
+#pragma unroll
+      for (int k = 0; k < NV; ++k) t[k] += __ldcg(partials + slot[k] * nb + i);
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) t[k] += __shfl_down_sync(0xffffffffu, t[k], off);
+      if (lane == 0) smem[k] = t[k];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < NV; ++k) out[k] = smem[k];
+  __syncthreads();
+}
+
 // Sum of partials[0..nb) read from L2 in a fixed order (same result in every block).
 __device__ __forceinline__ double reduce_partials(const double *partials, int nb, double *smem) {
   double t = 0.0;
