@@ -36,7 +36,7 @@ class Params(C.Structure):
                 ("scale_system", C.c_int), ("precision", C.c_int), ("refactorize", C.c_int),
                 ("precond_recompute", C.c_int), ("inner_tol", C.c_double), ("inner_max_iter", C.c_int),
                 ("max_refinements", C.c_int), ("ilu_order", C.c_int), ("restart", C.c_int),
-                ("ilut_tol", C.c_double), ("divtol", C.c_double)]
+                ("ilut_tol", C.c_double), ("divtol", C.c_double), ("ilu_sweeps", C.c_int)]
 
 
 class Result(C.Structure):

@@ -95,12 +95,13 @@ __device__ __forceinline__ int batch_locate(const BatchShared &sh, int q) {
   return l;
 }
 
-__device__ __forceinline__ SliceMeta batch_slice_meta(const BatchArgs &ba, const BatchShared &sh, int q, int hi) {
+__device__ __forceinline__ SliceMeta batch_slice_meta(const BatchArgs &ba, const BatchShared &sh, int q, int hi,
+                                                      unsigned run) {
   SliceMeta m{nullptr, nullptr, 0u, 0u};
   if (q >= hi) return m;
   const int a = batch_locate(sh, q);
   const int s = sh.act[a];
-  if (sh.status[s] != ST_RUN) return m;
+  if (!((run >> sh.status[s]) & 1u)) return m;
   const SysDesc &d = ba.sys[s];
   const int sl = q - sh.pre[a];
   if (sl < 0 || sl >= d.nslices) return m;
@@ -130,17 +131,25 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 // flush this block's per-system partials (slots v0/v1 of red) to the global accumulators
-__device__ __forceinline__ void batch_flush(const BatchArgs &a, BatchShared &sh, int slot0, int slot1) {
+__device__ __forceinline__ void batch_flush(const BatchArgs &a, BatchShared &sh, int slot0, int slot1, int slot2 = -1,
+                                            int slot3 = -1) {
   __syncthreads();
+  const int slot[4] = {slot0, slot1, slot2, slot3};
   for (int t = threadIdx.x; t < sh.nact; t += blockDim.x) {
     const int s = sh.act[t];
-    const double v0 = sh.red[2 * t], v1 = sh.red[2 * t + 1];
-    if (v0 != 0.0 && slot0 >= 0) atomicAdd(&a.acc[slot0 * BATCH_MAX_SYS + s], v0);
-    if (v1 != 0.0 && slot1 >= 0) atomicAdd(&a.acc[slot1 * BATCH_MAX_SYS + s], v1);
-    sh.red[2 * t] = 0.0;
-    sh.red[2 * t + 1] = 0.0;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const double x = sh.red[4 * t + v];
+      if (x != 0.0 && slot[v] >= 0) atomicAdd(&a.acc[slot[v] * BATCH_MAX_SYS + s], x);
+      sh.red[4 * t + v] = 0.0;
+    }
   }
   __syncthreads();
+}
+
+// CG accumulator slot v (0 gamma, 1 delta, 2 (r, r), 3 (z, s)) of set `set` (iteration parity)
+__device__ __forceinline__ int cg_slot(int set, int v) {
+  return set ? BA_CG1 + v : (v == 0 ? BA_RHO : v == 1 ? BA_PQ : v == 2 ? BA_RR : BA_SS);
 }
 
 // designated block of system s clears accumulator slots
@@ -203,24 +212,25 @@ __device__ __forceinline__ void slice_spmv2(const SysDesc *d0, int sl0, const fl
 }
 
 // SpMV phase over this block's share of the active slices, one slice per warp at a time;
-// lane 0 prefetches the next one into L2.  src(s): the vector system s multiplies;
-// epi(act_index, s, slice, y): once per running slice, y the lane's row sum.  Slices of
-// systems that do not run are skipped (warp-uniform).
+// lane 0 prefetches the next one into L2.  run: bit mask of the statuses whose systems take
+// part; src(s): the vector system s multiplies; epi(act_index, s, slice, y): once per
+// running slice, y the lane's row sum.  Slices of other systems are skipped (warp-uniform).
 template <typename SRC, typename EPI>
-__device__ __forceinline__ void batch_spmv1(const BatchArgs &ba, const BatchShared &sh, SRC &&src, EPI &&epi) {
+__device__ __forceinline__ void batch_spmv1(const BatchArgs &ba, const BatchShared &sh, unsigned run, SRC &&src,
+                                            EPI &&epi) {
   const int total = sh.total, nb = gridDim.x;
   const int lo = (int)((long long)total * blockIdx.x / nb), hi = (int)((long long)total * (blockIdx.x + 1) / nb);
   const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, lane = threadIdx.x & 31;
-  SliceMeta next = batch_slice_meta(ba, sh, lo + warp + nw, hi);
+  SliceMeta next = batch_slice_meta(ba, sh, lo + warp + nw, hi, run);
   for (int q = lo + warp; q < hi; q += nw) {
     const int a = batch_locate(sh, q);
     if (lane == 0 && next.vbytes) {
       prefetch_l2_bulk(next.vals, next.vbytes);
       prefetch_l2_bulk(next.cols, next.cbytes);
     }
-    next = batch_slice_meta(ba, sh, q + 2 * nw, hi);
+    next = batch_slice_meta(ba, sh, q + 2 * nw, hi, run);
     const int s = sh.act[a];
-    if (sh.status[s] != ST_RUN) continue;
+    if (!((run >> sh.status[s]) & 1u)) continue;
     const int slice = q - sh.pre[a];
     epi(a, s, slice, slice_spmv(ba.sys[s], slice, lane, src(s)));
   }
@@ -228,13 +238,14 @@ __device__ __forceinline__ void batch_spmv1(const BatchArgs &ba, const BatchShar
 
 // The same phase with two slices per warp at a time (slice_spmv2).
 template <typename SRC, typename EPI>
-__device__ __forceinline__ void batch_spmv2(const BatchArgs &ba, const BatchShared &sh, SRC &&src, EPI &&epi) {
+__device__ __forceinline__ void batch_spmv2(const BatchArgs &ba, const BatchShared &sh, unsigned run, SRC &&src,
+                                            EPI &&epi) {
   const int total = sh.total, nb = gridDim.x;
   const int lo = (int)((long long)total * blockIdx.x / nb), hi = (int)((long long)total * (blockIdx.x + 1) / nb);
   const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, lane = threadIdx.x & 31;
   const int g = ba.spw == 2 ? 2 : 1, step = g * nw;  // slices a warp takes at once, and its stride
-  SliceMeta n0 = batch_slice_meta(ba, sh, lo + warp + step, hi),
-            n1 = batch_slice_meta(ba, sh, g == 2 ? lo + warp + step + nw : hi, hi);
+  SliceMeta n0 = batch_slice_meta(ba, sh, lo + warp + step, hi, run),
+            n1 = batch_slice_meta(ba, sh, g == 2 ? lo + warp + step + nw : hi, hi, run);
   for (int q0 = lo + warp; q0 < hi; q0 += step) {
     const int q1 = g == 2 ? q0 + nw : hi;
     if (lane == 0) {
@@ -247,8 +258,8 @@ __device__ __forceinline__ void batch_spmv2(const BatchArgs &ba, const BatchShar
         prefetch_l2_bulk(n1.cols, n1.cbytes);
       }
     }
-    n0 = batch_slice_meta(ba, sh, q0 + 2 * step, hi);
-    n1 = batch_slice_meta(ba, sh, g == 2 ? q1 + 2 * step : hi, hi);
+    n0 = batch_slice_meta(ba, sh, q0 + 2 * step, hi, run);
+    n1 = batch_slice_meta(ba, sh, g == 2 ? q1 + 2 * step : hi, hi, run);
     const int a0 = batch_locate(sh, q0), s0 = sh.act[a0], sl0 = q0 - sh.pre[a0];
     int a1 = -1, s1 = 0, sl1 = 0;
     if (q1 < hi) {
@@ -256,7 +267,7 @@ __device__ __forceinline__ void batch_spmv2(const BatchArgs &ba, const BatchShar
       s1 = sh.act[a1];
       sl1 = q1 - sh.pre[a1];
     }
-    const bool run0 = sh.status[s0] == ST_RUN, run1 = a1 >= 0 && sh.status[s1] == ST_RUN;
+    const bool run0 = (run >> sh.status[s0]) & 1u, run1 = a1 >= 0 && ((run >> sh.status[s1]) & 1u);
     if (!run0 && !run1) continue;
     float y0, y1;
     slice_spmv2(run0 ? &ba.sys[s0] : nullptr, sl0, run0 ? src(s0) : nullptr, run1 ? &ba.sys[s1] : nullptr, sl1,
@@ -269,11 +280,12 @@ __device__ __forceinline__ void batch_spmv2(const BatchArgs &ba, const BatchShar
 // SPW (1 or 2, chosen by the autotuner) slices per warp; each form is its own instantiation of
 // the inner kernel, so neither pays the other's registers
 template <int SPW, typename SRC, typename EPI>
-__device__ __forceinline__ void batch_spmv(const BatchArgs &ba, const BatchShared &sh, SRC &&src, EPI &&epi) {
+__device__ __forceinline__ void batch_spmv(const BatchArgs &ba, const BatchShared &sh, unsigned run, SRC &&src,
+                                           EPI &&epi) {
   if (SPW == 2)
-    batch_spmv2(ba, sh, src, epi);
+    batch_spmv2(ba, sh, run, src, epi);
   else
-    batch_spmv1(ba, sh, src, epi);
+    batch_spmv1(ba, sh, run, src, epi);
 }
 
 // Sync-free ILU0 solves over the systems in RUN state, slots interleaved across systems:
@@ -477,7 +489,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
   const bool bicg = a.method == EGPU_BICGSTAB;
   const bool ilu = a.precond == EGPU_PREC_ILU0;
   const float SENT = Sentinel<float>::value();
-  for (int t = threadIdx.x; t < 2 * BATCH_MAX_SYS; t += blockDim.x) sh.red[t] = 0.0;
+  for (int t = threadIdx.x; t < 4 * BATCH_MAX_SYS; t += blockDim.x) sh.red[t] = 0.0;
   int it = 0;
   for (; it < a.kmax; ++it) {
     const int rd = (parity0 + it) & 1, wr = rd ^ 1;
@@ -489,9 +501,68 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       const int status0 = st.status;
       const double *acc = a.acc;
       float beta = 0.f;
+      float alpha_f = 0.f;
       if (st.status == ST_INIT) {
         st.status = ST_INIT + 10;  // init work this iteration
         st.k = 0;
+      } else if (!bicg) {
+        // single-reduction CG: the sums of the previous iteration's phase A (set rd ^ 1)
+        if (st.status == ST_INIT + 10 || st.status == ST_RUN) {
+          const double g = acc[cg_slot(rd ^ 1, 0) * BATCH_MAX_SYS + s];
+          const double dl = acc[cg_slot(rd ^ 1, 1) * BATCH_MAX_SYS + s];
+          const double rq = a.sys[s].unit_diag ? g : acc[cg_slot(rd ^ 1, 2) * BATCH_MAX_SYS + s];
+          double b = 0.0, eta = dl;
+          bool go = false;
+          if (st.status == ST_INIT + 10) {
+            st.r0norm = sqrt(rq);
+            st.k = 1;
+            st.residual = 1.0;
+            if (!(st.r0norm > 0.0)) {
+              st.status = ST_DONE;
+              st.info = EGPU_HUTI_CONVERGENCE;
+              st.iters = 0;
+              st.residual = 0.0;
+            } else {
+              // resumed: p = z + b P and s = w + b S with the carried P, S; eta formed exactly
+              if (st.resume) {
+                b = g / st.carry_rho;
+                eta = dl + 2.0 * b * acc[cg_slot(rd ^ 1, 3) * BATCH_MAX_SYS + s] + b * b * st.eta;
+              }
+              st.status = ST_RUN;
+              go = true;
+            }
+          } else {
+            st.residual = sqrt(rq) / st.r0norm;
+            if (st.residual <= a.tol) {
+              st.status = ST_DONE;
+              st.info = EGPU_HUTI_CONVERGENCE;
+              st.iters = st.k;
+            } else if (st.k + 1 > a.maxit) {
+              st.status = ST_DONE;
+              st.info = EGPU_HUTI_MAXITER;
+              st.iters = st.k;
+            } else {
+              b = g / st.rho;
+              eta = dl - b * g / st.alpha;
+              st.k += 1;
+              go = true;
+            }
+          }
+          if (go && (g == 0.0 || !(eta != 0.0))) {
+            st.status = ST_DONE;
+            st.info = EGPU_HUTI_CG_RHO;
+            st.iters = st.k;
+            go = false;
+          }
+          if (go) {
+            st.oldrho = st.rho;
+            st.rho = g;
+            st.alpha = g / eta;
+            st.eta = eta;
+            beta = (float)b;
+            alpha_f = (float)st.alpha;
+          }
+        }
       } else if (st.status == ST_INIT + 10) {
         st.rho = acc[BA_RHO * BATCH_MAX_SYS + s];
         st.r0norm = sqrt(acc[BA_RR * BATCH_MAX_SYS + s]);
@@ -543,13 +614,12 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
         }
       }
       if (st.status == ST_DONE && status0 != ST_DONE) sh.any_done = 1;
-      if (st.status == ST_RUN)
-        beta = bicg ? (float)((st.rho * st.alpha) / (st.oldrho * st.omega)) : (float)(st.rho / st.oldrho);
+      if (bicg && st.status == ST_RUN) beta = (float)((st.rho * st.alpha) / (st.oldrho * st.omega));
       sh.status[s] = st.status;
       sh.fresh[s] = st.resume ? 0 : 1;
       sh.kk[s] = st.k;
       sh.sb[s] = beta;
-      sh.sa[s] = (float)st.omega;
+      sh.sa[s] = bicg ? (float)st.omega : alpha_f;
       rho_s[s] = st.rho;
       if (s % gridDim.x == (int)blockIdx.x) a.state[wr * BATCH_MAX_SYS + s] = st;
     }
@@ -560,72 +630,67 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       break;
     }
     if (!bicg) {
-      // ============ CG ============
-      // U: P = Z (k == 1) or Z + beta P;  clear PQ
-      batch_clear(a, BA_PQ);
+      // ============ CG, single reduction (Chronopoulos-Gear; see cg_sr_kernel) ============
+      // layout R Z P W S; this iteration sums into set rd
+      // B: P = Z + beta P; S = W + beta S; X += alpha P; R -= alpha S; Z = M^-1 R
+      //    (init: R = B, X = 0, Z = M^-1 R);  clear set rd
+      for (int v = 0; v < 4; ++v) batch_clear(a, cg_slot(rd, v));
       batch_slices(sh, [&](int, int s, int slice) {
-        if (sh.status[s] != ST_RUN) return;
         const SysDesc &d = a.sys[s];
         const int r = (slice << 5) + lane;
         if (r >= d.n) return;
-        float *Z = d.unit_diag ? d.w : d.w + d.ldw, *P = d.w + 2 * d.ldw;
-        const float z = Z[r];
-        P[r] = (sh.kk[s] == 1 && sh.fresh[s]) ? z : z + sh.sb[s] * P[r];
-      });
-      if (!grid_barrier(a.bar, a.err, epoch)) return;
-      // S: Q = A P; PQ;  clear RHO, RR
-      batch_clear(a, BA_RHO);
-      batch_clear(a, BA_RR);
-      batch_spmv<SPW>(a, sh, [&](int s) -> const float * { return a.sys[s].w + 2 * a.sys[s].ldw; },
-                  [&](int ai, int s, int slice, float q) {
-        const SysDesc &d = a.sys[s];
-        const int r = (slice << 5) + lane;
-        const float *P = d.w + 2 * d.ldw;
-        float *Q = d.w + 3 * d.ldw;
-        double pq = 0.0;
-        if (r < d.n) {
-          Q[r] = q;
-          pq = (double)P[r] * (double)q;
-        }
-        pq = warp_sum(pq);
-        if (lane == 0) batch_acc_add(sh, ai, 0, pq);
-      });
-      batch_flush(a, sh, BA_PQ, -1);
-      if (!grid_barrier(a.bar, a.err, epoch)) return;
-      // C: X += alpha P; R -= alpha Q; Z = M^-1 R; RHO, RR   (init: R = B, X = 0)
-      batch_slices(sh, [&](int ai, int s, int slice) {
-        const SysDesc &d = a.sys[s];
-        const int r = (slice << 5) + lane;
-        float *R = d.w, *Z = d.w + d.ldw, *P = d.w + 2 * d.ldw, *Q = d.w + 3 * d.ldw;
+        float *R = d.w, *Z = d.unit_diag ? d.w : d.w + d.ldw, *P = d.w + 2 * d.ldw, *W = d.w + 3 * d.ldw,
+              *S = d.w + 4 * d.ldw;
         const float *dv = d.w + 13 * d.ldw;
-        double rz = 0.0, rr = 0.0;
-        if (r < d.n) {
-          float rv;
-          if (sh.status[s] == ST_RUN) {
-            const float al = (float)(rho_s[s] / a.acc[BA_PQ * BATCH_MAX_SYS + s]);
-            d.x[r] = d.x[r] + al * P[r];
-            rv = R[r] - al * Q[r];
-          } else {
-            rv = d.b[r];
-            d.x[r] = 0.f;
-          }
-          R[r] = rv;
-          float z = rv;  // the identity on a unit diagonal: Z is R, not stored
-          if (!d.unit_diag) {
-            z = bprec(rv, dv[r], a.precond);
-            Z[r] = z;
-          }
-          rz = (double)rv * (double)z;
-          rr = (double)rv * (double)rv;
+        float rv;
+        if (sh.status[s] == ST_RUN) {
+          const float be = sh.sb[s], al = sh.sa[s];
+          const bool fresh1 = sh.kk[s] == 1 && sh.fresh[s];
+          const float z = Z[r], w = W[r];
+          const float p = fresh1 ? z : z + be * P[r];
+          const float sv = fresh1 ? w : w + be * S[r];
+          P[r] = p;
+          S[r] = sv;
+          d.x[r] = d.x[r] + al * p;
+          rv = (d.unit_diag ? z : R[r]) - al * sv;
+        } else {
+          rv = d.b[r];
+          d.x[r] = 0.f;
         }
-        rz = warp_sum(rz);
-        rr = warp_sum(rr);
+        R[r] = rv;
+        if (!d.unit_diag) Z[r] = bprec(rv, dv[r], a.precond);
+      });
+      if (!grid_barrier(a.bar, a.err, epoch)) return;
+      // A: W = A Z; gamma = (R, Z), delta = (W, Z), (R, R), and (Z, S) for a resumed start
+      batch_spmv<SPW>(a, sh, (1u << ST_RUN) | (1u << (ST_INIT + 10)),
+                      [&](int s) -> const float * { const SysDesc &d = a.sys[s]; return d.unit_diag ? d.w : d.w + d.ldw; },
+                      [&](int ai, int s, int slice, float w) {
+        const SysDesc &d = a.sys[s];
+        const int r = (slice << 5) + lane;
+        const bool resume0 = sh.status[s] != ST_RUN && !sh.fresh[s];
+        double g = 0.0, dl = 0.0, rq = 0.0, ep = 0.0;
+        if (r < d.n) {
+          const float *Z = d.unit_diag ? d.w : d.w + d.ldw;
+          d.w[3 * d.ldw + r] = w;
+          const float z = Z[r];
+          const float rv = d.unit_diag ? z : d.w[r];
+          g = (double)rv * (double)z;
+          dl = (double)w * (double)z;
+          if (!d.unit_diag) rq = (double)rv * (double)rv;
+          if (resume0) ep = (double)z * (double)d.w[4 * d.ldw + r];
+        }
+        g = warp_sum(g);
+        dl = warp_sum(dl);
+        if (!d.unit_diag) rq = warp_sum(rq);
+        if (resume0) ep = warp_sum(ep);
         if (lane == 0) {
-          batch_acc_add(sh, ai, 0, rz);
-          batch_acc_add(sh, ai, 1, rr);
+          batch_acc_add(sh, ai, 0, g);
+          batch_acc_add(sh, ai, 1, dl);
+          if (!d.unit_diag) batch_acc_add(sh, ai, 2, rq);
+          if (resume0) batch_acc_add(sh, ai, 3, ep);
         }
       });
-      batch_flush(a, sh, BA_RHO, BA_RR);
+      batch_flush(a, sh, cg_slot(rd, 0), cg_slot(rd, 1), cg_slot(rd, 2), cg_slot(rd, 3));
       if (!grid_barrier(a.bar, a.err, epoch)) return;
     } else {
       // ============ BiCGStab ============  layout R RT P V T S T1 T2 Y1 Y2
@@ -658,7 +723,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       batch_clear(a, BA_RHO);
       batch_clear(a, BA_RR);
       batch_clear(a, BA_SS);
-      batch_spmv<SPW>(a, sh, [&](int s) -> const float * { return a.sys[s].w + 6 * a.sys[s].ldw; },
+      batch_spmv<SPW>(a, sh, 1u << ST_RUN, [&](int s) -> const float * { return a.sys[s].w + 6 * a.sys[s].ldw; },
                   [&](int ai, int s, int slice, float v) {
         const SysDesc &d = a.sys[s];
         const int r = (slice << 5) + lane;
@@ -688,7 +753,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
           float *R = d.w, *V = d.w + 3 * d.ldw, *S = d.w + 5 * d.ldw;
           const float sv = R[i] - (float)rho_s[s] * V[i];
           S[i] = sv;
-          atomicAdd(&sh.red[2 * ai], (double)sv * (double)sv);
+          atomicAdd(&sh.red[4 * ai], (double)sv * (double)sv);
           return sv;
         }, [&](int, int, const SysDesc &, int, float) {});
         batch_tri_any<false>(a, sh, 9, 7, [&](int, int, const SysDesc &, int) { return 0.f; },
@@ -714,7 +779,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       if (!grid_barrier(a.bar, a.err, epoch)) return;
       // 4: T = A T2; TS, TT;  clear PQ
       batch_clear(a, BA_PQ);
-      batch_spmv<SPW>(a, sh, [&](int s) -> const float * { return a.sys[s].w + 7 * a.sys[s].ldw; },
+      batch_spmv<SPW>(a, sh, 1u << ST_RUN, [&](int s) -> const float * { return a.sys[s].w + 7 * a.sys[s].ldw; },
                   [&](int ai, int s, int slice, float t) {
         const SysDesc &d = a.sys[s];
         const int r = (slice << 5) + lane;

@@ -55,9 +55,13 @@ struct SysState {
   // P, V, RTLD, alpha, omega) with rho_{k-1} = carry_rho (already in the new residual scale)
   int resume, pad;
   double carry_rho;
+  double eta;              // CG: (p, A p) of the last direction (single-reduction recurrence)
 };
 
-enum { BA_BB = 0, BA_RHO, BA_RR, BA_PQ, BA_SS, BA_TS, BA_TT, BA_NSLOT };
+// accumulator slots per system.  CG sums gamma, delta, (r, r) and (z, s) into one of two
+// sets by iteration parity (BA_RHO/BA_PQ/BA_RR/BA_SS or BA_CG1..+3): a set is cleared in the
+// iteration after the one whose top read it, with a grid barrier between.
+enum { BA_BB = 0, BA_RHO, BA_RR, BA_PQ, BA_SS, BA_TS, BA_TT, BA_CG1, BA_NSLOT = BA_CG1 + 4 };
 
 struct BatchArgs {
   int nsys;
@@ -83,13 +87,13 @@ struct BatchShared {
   int status[BATCH_MAX_SYS];     // status decided for this iteration
   int kk[BATCH_MAX_SYS];
   float sa[BATCH_MAX_SYS], sb[BATCH_MAX_SYS];  // per-phase scalars (beta, alpha, omega)
-  double red[BATCH_MAX_SYS * 2];               // per-block per-system accumulators
+  double red[BATCH_MAX_SYS * 4];               // per-block per-system accumulators (4 each)
   int nact, total;
   int any_done;                  // a system finished at this iteration's top
 };
 
 __device__ __forceinline__ void batch_acc_add(BatchShared &sh, int s_local, int v, double x) {
-  atomicAdd(&sh.red[2 * s_local + v], x);
+  atomicAdd(&sh.red[4 * s_local + v], x);
 }
 
 }  // namespace egpu

@@ -86,6 +86,29 @@ __global__ void k_sell_scale(int n, int nslices, const int *__restrict__ rows, c
   }
 }
 
+// CRS-ordered FP32 values into the SELL-32 layout (padding entries 0)
+__global__ void k_sell_gather32(int n, int nslices, const int *__restrict__ rows, const float *__restrict__ vals,
+                                const int *__restrict__ sell_ptr, const int *__restrict__ sell_w,
+                                float *__restrict__ out) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nslices * 32; r += gridDim.x * blockDim.x) {
+    const int sl = r >> 5, lane = r & 31;
+    const int w = sell_w[sl];
+    float *o = out + sell_ptr[sl] + lane;
+    int beg = 0, len = 0;
+    if (r < n) {
+      beg = rows[r];
+      len = rows[r + 1] - beg;
+    }
+    for (int k = 0; k < w; ++k) o[32 * k] = k < len ? vals[beg + k] : 0.f;
+  }
+}
+
+// out[i] = vals[diag[i]]
+__global__ void k_gather_diag32(int n, const int *__restrict__ diag, const float *__restrict__ vals,
+                                float *__restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = vals[diag[i]];
+}
+
 // right-hand side scaling, pass 1: bs = b*D; partials of ||b||^2, ||bs||^2, any x != 0
 __global__ void k_rhs_scale_a(int n, const double *__restrict__ b, const double *__restrict__ D,
                               const double *__restrict__ x, double *__restrict__ bs,
@@ -1067,6 +1090,11 @@ static int run_krylov(egpu_mat *A, const KArgs<VT> &a0, int method, bool offs) {
       return cta ? launch_coop(ctx, bicgstabl_kernel<TRI_TS, true>, a, nullptr, smem)
                  : launch_coop(ctx, bicgstabl_kernel<TRI_TS, false>, a, nullptr, smem);
   }
+  if constexpr (sizeof(VT) == 4) {
+    if (a.sweeps_l > 0 && a.precond == EGPU_PREC_ILU0)
+      return offs ? launch_coop(ctx, bicgstab_kernel<float, TRI_TS, true, false, true>, a, nullptr, 0)
+                  : launch_coop(ctx, bicgstab_kernel<float, TRI_TS, false, false, true>, a, nullptr, 0);
+  }
   if (cta) {
     if (offs) return launch_coop(ctx, bicgstab_kernel<VT, TRI_TS, true, true>, a, nullptr, smem);
     return launch_coop(ctx, bicgstab_kernel<VT, TRI_TS, false, true>, a, nullptr, smem);
@@ -1356,7 +1384,7 @@ __global__ void k_count_not_one(const float *__restrict__ d, int n, unsigned int
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(cnt, c);
 }
 
-static int prepare_fp32(egpu_mat *A, bool with_ilu) {
+static int prepare_fp32(egpu_mat *A, bool with_ilu, bool sweeps) {
   egpu_ctx *ctx = A->ctx;
   const int n = A->n;
   EGPU_CUDA_TRY(ctx, A->work32.alloc((size_t)14 * A->ldw));
@@ -1369,6 +1397,14 @@ static int prepare_fp32(egpu_mat *A, bool with_ilu) {
     EGPU_CUDA_TRY(ctx, A->ilu32.alloc(A->ilu_nnz));
     k_to_f32<<<grid_for(ctx, A->ilu_nnz), 256, 0, ctx->stream>>>(A->ilu.p, A->ilu32.p, A->ilu_nnz);
     ctx->launches++;
+    if (sweeps) {  // ILU0: the factors share the matrix's pattern, hence its SELL layout
+      EGPU_CUDA_TRY(ctx, A->ilu_sell32.alloc(A->sell_nnz));
+      EGPU_CUDA_TRY(ctx, A->ilu_dinv32.alloc(n));
+      k_sell_gather32<<<grid_for(ctx, (long long)A->nslices * 32), 256, 0, ctx->stream>>>(
+          n, A->nslices, A->rows.p, A->ilu32.p, A->sell_ptr.p, A->sell_w.p, A->ilu_sell32.p);
+      k_gather_diag32<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, A->diag.p, A->ilu32.p, A->ilu_dinv32.p);
+      ctx->launches += 2;
+    }
   }
   if (A->max_bandwidth < 32768 && !A->cols16.p) {
     EGPU_CUDA_TRY(ctx, A->cols16.alloc(A->nnz));
@@ -1409,7 +1445,13 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
     rc = precond_factor(A, prm);
     if (rc) return rc;
   }
-  rc = prepare_fp32(A, ilu);
+  // ILU0 by Jacobi sweeps in the FP32 inner BiCGStab (EGPU_ILU_SWEEPS overrides the count)
+  int sweeps = prm->ilu_sweeps;
+  if (const char *e = std::getenv("EGPU_ILU_SWEEPS")) sweeps = std::atoi(e);
+  sweeps = std::max(0, std::min(sweeps, 16));
+  const bool use_sweeps = sweeps > 0 && prm->method == EGPU_BICGSTAB && prm->precond == EGPU_PREC_ILU0 &&
+                          A->ilu_order == 0 && A->ilu_nnz == A->nnz;
+  rc = prepare_fp32(A, ilu, use_sweeps);
   if (rc) return rc;
   float *W32 = A->work32.p;
   float *r32 = W32 + (size_t)10 * ldw, *d32 = W32 + (size_t)11 * ldw, *dv32 = W32 + (size_t)13 * ldw;
@@ -1497,6 +1539,13 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
       a.dvals = dv32;
       a.unit_diag = unit_diag ? 1 : 0;
       set_tri(a, A);
+      if (use_sweeps) {
+        a.sweeps_l = a.sweeps_u = sweeps;
+        a.swr = A->sell_swr.p;
+        a.isvals = A->ilu_sell32.p;
+        a.idinv = A->ilu_dinv32.p;
+        a.tri_cta = 0;
+      }
       a.precond = is_ilu(prm->precond) ? EGPU_PREC_ILU0 : prm->precond;  // ILUT applies like ILU(n)
       a.maxit = std::max(1, std::min(prm->inner_max_iter, prm->max_iter - r.iters));
       a.true_residual = 0;
@@ -1652,7 +1701,7 @@ int rhs_scale(egpu_mat *A, const double *b_dev, const double *x_dev, double *bs,
   return EGPU_OK;
 }
 
-int prepare_fp32_public(egpu_mat *A, bool with_ilu) { return prepare_fp32(A, with_ilu); }
+int prepare_fp32_public(egpu_mat *A, bool with_ilu) { return prepare_fp32(A, with_ilu, false); }
 
 // *unit = 1 when the FP32 copy of the scaled diagonal (work32 vector 13, written by
 // prepare_fp32) is 1.0f in every row; synchronises the stream
@@ -1931,10 +1980,25 @@ extern "C" int egpu_matrix_bind(egpu_ctx *ctx, int n, const int *rows, const int
         }
       }
     }
+    // k ranges of each slice's strictly-lower and strictly-upper entries
+    std::vector<int2> swr(ns);
+    for (int sl = 0; sl < ns; ++sl) {
+      int lo_end = 0, up_beg = sw[sl];
+      for (int r = sl * 32; r < std::min(n, sl * 32 + 32); ++r) {
+        const int beg = rows[r] - 1, len = rows[r + 1] - rows[r];
+        for (int k = 0; k < len; ++k) {
+          const int c = cols[beg + k] - 1;
+          if (c < r) lo_end = std::max(lo_end, k + 1);
+          if (c > r) up_beg = std::min(up_beg, k);
+        }
+      }
+      swr[sl] = make_int2(lo_end, up_beg);
+    }
     A->nslices = ns;
     A->sell_nnz = total;
     A->ldw = ((long long)n + 32 + 63) / 64 * 64;
     if ((e = A->sell_ptr.alloc(ns)) || (e = A->sell_w.alloc(ns)) || (e = A->sell_cols.alloc(total)) ||
+        (e = A->sell_swr.alloc(ns)) ||
         (c16 && (e = A->sell_c16.alloc(total))) || (c16 && (e = A->sell_cptr.alloc(ns))) ||
         (c16 && (e = A->sell_csc.alloc(std::max<size_t>(1, csc.size())))))
       return fail(e);
@@ -1944,6 +2008,7 @@ extern "C" int egpu_matrix_bind(egpu_ctx *ctx, int n, const int *rows, const int
     }
     cudaMemcpy(A->sell_ptr.p, sp.data(), ns * sizeof(int), cudaMemcpyHostToDevice);
     cudaMemcpy(A->sell_w.p, sw.data(), ns * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(A->sell_swr.p, swr.data(), ns * sizeof(int2), cudaMemcpyHostToDevice);
     cudaMemcpy(A->sell_cols.p, sc.data(), total * sizeof(int), cudaMemcpyHostToDevice);
     if (c16) cudaMemcpy(A->sell_c16.p, s16.data(), total * sizeof(int16_t), cudaMemcpyHostToDevice);
   }
@@ -2015,6 +2080,7 @@ extern "C" int egpu_matrix_clone(egpu_mat *proto, egpu_mat **out) {
   A->sell_ptr.view(proto->sell_ptr);
   A->sell_w.view(proto->sell_w);
   A->sell_cols.view(proto->sell_cols);
+  A->sell_swr.view(proto->sell_swr);
   A->sell_c16.view(proto->sell_c16);
   A->sell_cptr.view(proto->sell_cptr);
   A->sell_csc.view(proto->sell_csc);

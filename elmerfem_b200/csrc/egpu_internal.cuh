@@ -223,6 +223,11 @@ struct egpu_mat {
   DevBuf<int16_t> sell_csc;
   DevBuf<double> sell_vals;      // scaled values (FP64)
   DevBuf<float> sell_vals32;     // scaled values (FP32)
+  // per slice: the k range of the strictly-lower entries ([0, x)) and of the strictly-upper
+  // ones ([y, w)); ILU0 factors in the SELL layout (FP32) and the inverted U diagonal in row
+  // order, for the Jacobi-sweep application of the preconditioner
+  DevBuf<int2> sell_swr;
+  DevBuf<float> ilu_sell32, ilu_dinv32;
   // ILU structure: the matrix's own pattern for ILU0, the ILU(n) fill structure otherwise
   // (0-based); the triangular-solve schedules in tri are built on it
   int ilu_order = -1;            // order the structure was built for (-1: not yet, ILU_ORDER_T: ILUT)

@@ -73,6 +73,14 @@ struct KArgs {
   // levels staged cta_pd ahead, ring of cta_rs slots, staging windows of cta_sb entries and
   // cta_sr rows
   int tri_cta, cta_pd, cta_rs, cta_sb, cta_sr, cta_nl, cta_nt;
+  // FP32 inner solves with ILU0: M^-1 by sweeps_l / sweeps_u Jacobi sweeps on the factors
+  // (0: exact triangular solves).  The factors in the matrix's SELL layout (isvals; the
+  // diagonal entries unused), the inverted U diagonal in row order (idinv), and per slice
+  // the k range holding its strictly-lower entries (swr.x: [0, x)) and its strictly-upper
+  // ones (swr.y: [y, w)).
+  int sweeps_l, sweeps_u;
+  const int2 *swr;
+  const VT *isvals, *idinv;
   // inner mode, reliable update: continue the previous segment's recurrences from a replaced
   // residual (B = the new true residual / its norm) instead of restarting.  carry holds
   // the previous segment's scalars (rho_{k-1}, alpha, omega; [3] = 1 when valid) and is
@@ -778,6 +786,105 @@ __device__ __forceinline__ void store_partials(const KArgs<VT> &a, int slot, dou
   if (threadIdx.x == 0) a.partials[slot * gridDim.x + blockIdx.x] = v;
 }
 
+// -------------------------------------------------------------------------------------
+// ILU0 applied by Jacobi sweeps (FP32 inner solves): instead of solving L y = v and U z = y
+// exactly (one dependency level after another), iterate
+//
+//   y_0 = v,            y_{j+1} = v - L_s y_j                  (L unit lower triangular)
+//   z_0 = D^-1 y,       z_{j+1} = D^-1 (y - U_s z_j)           (D^-1 the inverted U diagonal)
+//
+// a fixed number of times (E. Chow and A. Patel, "Fine-grained parallel incomplete LU
+// factorization", SIAM J. Sci. Comput. 37 (2015); H. Anzt, E. Chow and J. Dongarra,
+// "Iterative sparse triangular solves for preconditioning", Euro-Par 2015).  With a fixed
+// count and zero start it is a fixed linear operator, a polynomial in the factors that
+// tends to (LU)^-1, so BiCGStab runs with it unchanged; each sweep is one SELL pass over
+// half the factor entries, fully parallel, instead of a latency-bound level sequence.  The
+// inner solve's result is a correction that the FP64 refinement checks against the true
+// residual, so the preconditioner need not be the reference's exact one there.
+//
+// One sweep over the SELL copy of the factors: lane = row; entries with col < row (LOWER)
+// or col > row (UPPER) of the slice's k range; epi(row, sum of factor * zin[col]).
+template <bool UPPER, bool OFFS, typename F>
+__device__ __forceinline__ void sweep_phase(const KArgs<float> &a, const float *zin, F &&epi) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int nw = (int)(((long long)gridDim.x * blockDim.x) >> 5);
+  for (int s = gw; s < a.nslices; s += nw) {
+    const int r = (s << 5) + lane;
+    const int w = __ldg(a.sell_w + s);
+    const int2 rg = __ldg(a.swr + s);
+    const int k0 = UPPER ? rg.y : 0, k1 = UPPER ? w : rg.x;
+    const int base = __ldg(a.sell_ptr + s) + lane;
+    float sum = 0.f;
+    if (OFFS && a.scolsc) {
+      const int cp = __ldg(a.sell_cptr + s);
+      if (cp < 0) {  // one offset list for the slice: lane k holds offset k of each chunk of 32
+        const int16_t *co = a.scolsc + (-cp - 1);
+        for (int c0 = k0; c0 < k1; c0 += 32) {
+          const int kn = min(32, k1 - c0);
+          const int offl = lane < kn ? (int)__ldg(co + c0 + lane) : 0;
+#pragma unroll 4
+          for (int k = 0; k < kn; ++k) {
+            const int off = __shfl_sync(0xffffffffu, offl, k);
+            const float v = ld_stream(a.isvals + base + ((c0 + k) << 5));
+            const bool take = UPPER ? off > 0 : off < 0;
+            sum = fmaf(take ? v : 0.f, ld_l2(zin + r + off), sum);
+          }
+        }
+      } else {
+        const int16_t *co = a.scolsc + cp + lane;
+#pragma unroll 4
+        for (int k = k0; k < k1; ++k) {
+          const int off = (int)ld_stream(co + (k << 5));
+          const float v = ld_stream(a.isvals + base + (k << 5));
+          const bool take = UPPER ? off > 0 : off < 0;
+          sum = fmaf(take ? v : 0.f, ld_l2(zin + r + off), sum);
+        }
+      }
+    } else {
+#pragma unroll 4
+      for (int k = k0; k < k1; ++k) {
+        const int e = base + (k << 5);
+        const int c = OFFS ? r + (int)ld_stream(a.scols16 + e) : ld_stream(a.scols + e);
+        const float v = ld_stream(a.isvals + e);
+        const bool take = UPPER ? c > r : c < r;
+        sum = fmaf(take ? v : 0.f, ld_l2(zin + c), sum);
+      }
+    }
+    if (r < a.n) epi(r, sum);
+  }
+}
+
+// target = M^-1 vin by sweeps (vin complete in every block; ends without a closing barrier,
+// which the caller's next grid barrier provides).  ya, yb, za: scratch vectors.  Returns
+// false when a grid barrier failed.
+template <bool OFFS>
+__device__ __forceinline__ bool sweep_apply(const KArgs<float> &a, const float *vin, float *target, float *ya,
+                                            float *yb, float *za, unsigned int &epoch) {
+  const int ml = a.sweeps_l, mu = a.sweeps_u;
+  float *z0 = (mu % 2 == 0) ? target : za;  // the U sweeps alternate so the last lands in target
+  const float *yin = vin;
+  for (int j = 1; j <= ml; ++j) {
+    float *yout = (j & 1) ? ya : yb;
+    const bool last = j == ml;
+    sweep_phase<false, OFFS>(a, yin, [&](int i, float sum) {
+      const float y = vin[i] - sum;
+      yout[i] = y;
+      if (last) z0[i] = a.idinv[i] * y;
+    });
+    if (!grid_barrier(a.bar, a.err, epoch)) return false;
+    yin = yout;
+  }
+  const float *y = yin, *zin = z0;
+  for (int j = 1; j <= mu; ++j) {
+    float *zout = ((mu - j) % 2 == 0) ? target : za;
+    sweep_phase<true, OFFS>(a, zin, [&](int i, float sum) { zout[i] = a.idinv[i] * (y[i] - sum); });
+    if (j < mu && !grid_barrier(a.bar, a.err, epoch)) return false;
+    zin = zout;
+  }
+  return true;
+}
+
 // =====================================================================================
 // Every persistent Krylov kernel is instantiated twice: CTA = true carries the
 // level-synchronous triangular solves of block 0 (chosen per matrix when its levels are
@@ -1202,7 +1309,7 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) cg_sr_kernel(KArgs<float> a) {
 // BiCGStab  (huti_dbicgstabsolv, hutiter/src/huti_bicgstab_D.F90:96-284)
 //
 // w layout: R RTLD P V T S T1V T2V Y1 Y2
-template <typename VT, int LPR, bool OFFS, bool CTA>
+template <typename VT, int LPR, bool OFFS, bool CTA, bool SW = false>
 __global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstab_kernel(KArgs<VT> a) {
   if (a.skip && (*a.skip & 2u)) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -1225,6 +1332,10 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstab_kernel(KArgs<VT> a) {
   const bool ilu = a.precond == EGPU_PREC_ILU0;
   const bool jac = a.precond == EGPU_PREC_DIAGONAL;
   const bool cta = CTA && ilu && a.tri_cta;  // block 0 runs the ILU0 solves level-synchronously
+  // FP32 inner solves: ILU0 by Jacobi sweeps (Y1, Y2 and work vector 12 as scratch)
+  constexpr bool sw = SW && sizeof(VT) == 4;
+  const bool syncfree = ilu && !cta && !sw;
+  VT *ZA = a.w + 12 * a.ldw;
   const VT SENT = Sentinel<VT>::value();
   VT *SLO = Y1, *YUP = Y2;           // level-synchronous mode: rhs / y in slot order
   // resumed segment: RTLD, P, V and rho_{k-1}, alpha, omega carry over unchanged (BiCGStab's
@@ -1263,7 +1374,7 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstab_kernel(KArgs<VT> a) {
         vfill<W>(P, i, VT(0));
         vfill<W>(V, i, VT(0));
       }
-      if (ilu && !cta) {
+      if (syncfree) {
         vfill<W>(Y1, i, SENT);
         vfill<W>(Y2, i, SENT);
         vfill<W>(T1, i, SENT);
@@ -1310,7 +1421,22 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstab_kernel(KArgs<VT> a) {
     {
       const VT beta = (VT)((rho * alpha) / (oldrho * omega));
       const VT om = (VT)omega;
-      if (cta) {
+      if (sw && ilu) {
+        vec_loop<VT>(n, [&](int i, auto w) {
+          constexpr int W = decltype(w)::value;
+          VT r[W], p[W], v[W];
+          vld<W>(R, i, r);
+          vld<W>(P, i, p);
+          vld<W>(V, i, v);
+#pragma unroll
+          for (int q = 0; q < W; ++q) p[q] = r[q] + beta * (p[q] - om * v[q]);
+          vst<W>(P, i, p);
+        });
+        if (!grid_barrier(a.bar, a.err, epoch)) return;
+        if constexpr (sw) {
+          if (!sweep_apply<OFFS>(a, P, T1, Y1, Y2, ZA, epoch)) return;
+        }
+      } else if (cta) {
         vec_loop<VT>(n, [&](int i, auto w) {
           constexpr int W = decltype(w)::value;
           VT r[W], p[W], v[W];
@@ -1387,7 +1513,26 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstab_kernel(KArgs<VT> a) {
     {
       const VT al = (VT)alpha;
       double acc[1] = {0.0};
-      if (cta) {
+      if (sw && ilu) {
+        vec_loop<VT>(n, [&](int i, auto w) {
+          constexpr int W = decltype(w)::value;
+          VT r[W], v[W], sv[W];
+          vld<W>(R, i, r);
+          vld<W>(V, i, v);
+#pragma unroll
+          for (int q = 0; q < W; ++q) {
+            sv[q] = row_msub(r[q], al, v[q]);
+            acc[0] += (double)sv[q] * (double)sv[q];
+          }
+          vst<W>(S, i, sv);
+        });
+        block_sum<1>(acc, sm);
+        store_partials(a, SLOT_SS, acc[0]);
+        if (!grid_barrier(a.bar, a.err, epoch)) return;
+        if constexpr (sw) {
+          if (!sweep_apply<OFFS>(a, S, T2, Y1, Y2, ZA, epoch)) return;
+        }
+      } else if (cta) {
         vec_loop<VT>(n, [&](int i, auto w) {
           constexpr int W = decltype(w)::value;
           VT r[W], v[W], sv[W];
@@ -1491,7 +1636,7 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) bicgstab_kernel(KArgs<VT> a) {
         }
         vst<W>(X, i, x);
         vst<W>(R, i, r);
-        if (ilu && !cta) {
+        if (syncfree) {
           vfill<W>(T1, i, SENT);
           vfill<W>(T2, i, SENT);
           vfill<W>(Y1, i, SENT);

@@ -85,6 +85,12 @@ typedef struct {
    * residual ratio exceeds it (IterativeMethods.src:626-629, 817-819, 959-961, 1047-1048);
    * HUTI's CG and BiCGStab do not read it, as in the reference. */
   double divtol;
+  /* mixed precision, BiCGStab + ILU0 (order 0): the FP32 inner solves apply the factors by
+   * this many Jacobi sweeps per triangle (y <- v - L y, z <- D^-1 (y - U z)) instead of
+   * exact triangular solves, trading the solves' dependency levels (latency-bound) for
+   * parallel passes over the factors; the FP64 refinement still stops on the true residual.
+   * 0: exact solves.  The FP64 drop-in always solves exactly, as CRS_LUSolve. */
+  int ilu_sweeps;
 } egpu_params;
 
 typedef struct {
