@@ -109,7 +109,7 @@ def compact_offset_fraction(pat):
     return 1.0 - float((32 * wmax[:full][shared]).sum()) / float(tot)
 
 
-def algorithmic_bytes_per_iter(method, precond, precision, n, nnz, cols16, off_frac=1.0, unit_diag=False):
+def algorithmic_bytes_per_iter(method, precond, precision, n, nnz, cols16, off_frac=1.0, unit_diag=False, sweeps=0):
     """Bytes one Krylov iteration must move (matrix streamed once per SpMV pass, vectors once).
 
     CG+Diagonal, FP32 inner (refinement): SpMV 4z values + 2z·off_frac offsets (int16 column
@@ -129,6 +129,11 @@ def algorithmic_bytes_per_iter(method, precond, precision, n, nnz, cols16, off_f
     if precision == "mixed":
         m = 4 * nnz + cbytes
         tri = (8 * nnz + 16 * n) if precond == 2 else 0
+        if precond == 2 and sweeps > 0:
+            # per application: `sweeps` passes over each triangle's half of the factor entries
+            # (values and offsets), each gathering its input and reading / writing 12n of
+            # vectors, the inverted diagonal (4n) in the upper sweeps, and z0 (4n) once
+            tri = 2 * (2 * sweeps * ((4 * nnz + cbytes) / 2 + 12 * n) + sweeps * 4 * n + 4 * n)
         return 2 * m + tri + 120 * n
     m = 8 * nnz + cbytes
     tri = (12 * nnz + 32 * n) if precond == 2 else 0
@@ -519,8 +524,9 @@ def run_gpu(args, rank, world, local, pg):
         dv = A.values()[pat.diag - 1]
         dsc = 1.0 / np.sqrt(np.abs(dv))
         unit_diag = bool(np.all((dv * dsc * dsc).astype(np.float32) == np.float32(1.0)))
+    sweeps = max((r.get("ilu_sweeps_used", 0) for r in on_path), default=0)
     bpi = algorithmic_bytes_per_iter(solve_kw["method"], solve_kw["precond"], path, n, nnz, cols16, off_frac,
-                                     unit_diag)
+                                     unit_diag, sweeps)
     peak, peak_kind = read_peaks()
     achieved = bpi * iters / sec_k / 1e9
     traffic = read_traffic(cfg["workload"])
@@ -528,8 +534,10 @@ def run_gpu(args, rank, world, local, pg):
     if solve_kw["method"] == eg.CG:
         kernel_name = f"cg_kernel<{ty},LPR,int16 cols> (persistent {what} CG)"
     else:
+        ilu_what = (f"ILU0 by {sweeps} Jacobi sweeps per triangle in the kernel)" if sweeps else
+                    "ILU0 triangular solves in the kernel)")
         kernel_name = (f"bicgstab_kernel<{ty},LPR,int16 cols> (persistent {what} BiCGStab, "
-                       + ("ILU0 triangular solves in the kernel)" if solve_kw["precond"] == eg.PREC_ILU0 else "no ILU)"))
+                       + (ilu_what if solve_kw["precond"] == eg.PREC_ILU0 else "no ILU)"))
 
     # ---- FP64 drop-in on the same system
     t64 = []
@@ -618,7 +626,8 @@ def run_gpu(args, rank, world, local, pg):
                                "fp64": r64["iters"]},
                 # a mixed request runs the FP64 drop-in on values it was measured faster on
                 "path_of_timed_steps": {"mixed": sum(1 for r in results if r.get("precision_used") == 1),
-                                        "fp64": sum(1 for r in results if r.get("precision_used") == 0)},
+                                        "fp64": sum(1 for r in results if r.get("precision_used") == 0),
+                                        "ilu_sweeps": sweeps},
                 "fp64": {"solves_per_s": fp64_rate, "ms_per_solve": 1000 * statistics.median(t64),
                          "krylov_gbs": ach64},
                 "speedup_mixed_vs_fp64": value / world / fp64_rate,

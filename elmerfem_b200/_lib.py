@@ -42,7 +42,7 @@ class Params(C.Structure):
 class Result(C.Structure):
     _fields_ = [("info", C.c_int), ("iters", C.c_int), ("refinements", C.c_int), ("residual", C.c_double),
                 ("seconds", C.c_double), ("seconds_setup", C.c_double), ("seconds_krylov", C.c_double),
-                ("krylov_launches", C.c_int), ("precision_used", C.c_int)]
+                ("krylov_launches", C.c_int), ("precision_used", C.c_int), ("ilu_sweeps_used", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -480,6 +480,75 @@ __device__ __forceinline__ void batch_tri_any(const BatchArgs &a, const BatchSha
 // ------------------------------------------------------------------------------------
 // the kernel
 
+// One Jacobi sweep over the running systems' ILU0 factors (see sweep_phase in
+// egpu_krylov.cuh): a warp per slice, lane = row, the entries with col < row (LOWER) or
+// col > row (UPPER) of the slice's k range.  zin(s): the vector system s multiplies;
+// epi(s, row, sum) for rows < n.
+template <bool UPPER, typename ZIN, typename EPI>
+__device__ __forceinline__ void batch_sweep(const BatchArgs &ba, const BatchShared &sh, ZIN &&zin, EPI &&epi) {
+  const int total = sh.total, nb = gridDim.x;
+  const int lo = (int)((long long)total * blockIdx.x / nb), hi = (int)((long long)total * (blockIdx.x + 1) / nb);
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, lane = threadIdx.x & 31;
+  for (int q = lo + warp; q < hi; q += nw) {
+    const int a = batch_locate(sh, q);
+    const int s = sh.act[a];
+    if (sh.status[s] != ST_RUN) continue;
+    const SysDesc &d = ba.sys[s];
+    const int slice = q - sh.pre[a];
+    const int r = (slice << 5) + lane;
+    const int w = __ldg(d.sell_w + slice);
+    const int2 rg = __ldg(d.swr + slice);
+    const int k0 = UPPER ? rg.y : 0, k1 = UPPER ? w : rg.x;
+    const int base = __ldg(d.sell_ptr + slice) + lane;
+    const float *z = zin(s);
+    float sum = 0.f;
+#pragma unroll 4
+    for (int k = k0; k < k1; ++k) {
+      const int e = base + (k << 5);
+      const int c = d.scols16 ? r + (int)__ldcs(d.scols16 + e) : __ldcs(d.scols + e);
+      const float v = __ldcs(d.isvals + e);
+      const bool take = UPPER ? c > r : c < r;
+      sum = fmaf(take ? v : 0.f, __ldca(z + c), sum);
+    }
+    if (r < d.n) epi(s, r, sum);
+  }
+}
+
+// work vector `tgt` = M^-1 (work vector `src`) of every running system by ba.sweeps sweeps
+// per triangle (src complete; ends without a closing grid barrier).  Scratch: work vectors
+// 8, 9 (y) and 12.  Returns false when a grid barrier failed.
+__device__ __forceinline__ bool batch_sweep_apply(const BatchArgs &a, const BatchShared &sh, int src, int tgt,
+                                                  unsigned int &epoch) {
+  const int m = a.sweeps;
+  const int z0s = (m % 2 == 0) ? tgt : 12;
+  int yin = src;
+  for (int j = 1; j <= m; ++j) {
+    const int yout = (j & 1) ? 8 : 9;
+    const bool last = j == m;
+    batch_sweep<false>(a, sh, [&](int s) -> const float * { return a.sys[s].w + yin * a.sys[s].ldw; },
+                       [&](int s, int r, float sum) {
+      const SysDesc &d = a.sys[s];
+      const float y = d.w[src * d.ldw + r] - sum;
+      d.w[yout * d.ldw + r] = y;
+      if (last) d.w[z0s * d.ldw + r] = d.idinv[r] * y;
+    });
+    if (!grid_barrier(a.bar, a.err, epoch)) return false;
+    yin = yout;
+  }
+  int zin = z0s;
+  for (int j = 1; j <= m; ++j) {
+    const int zout = ((m - j) % 2 == 0) ? tgt : 12;
+    batch_sweep<true>(a, sh, [&](int s) -> const float * { return a.sys[s].w + zin * a.sys[s].ldw; },
+                      [&](int s, int r, float sum) {
+      const SysDesc &d = a.sys[s];
+      d.w[zout * d.ldw + r] = d.idinv[r] * (d.w[yin * d.ldw + r] - sum);
+    });
+    if (j < m && !grid_barrier(a.bar, a.err, epoch)) return false;
+    zin = zout;
+  }
+  return true;
+}
+
 template <int SPW>
 __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int parity0) {
   __shared__ BatchShared sh;
@@ -630,7 +699,16 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       break;
     }
     if (!bicg) {
-      // ============ CG, single reduction (Chronopoulos-Gear; see cg_sr_kernel) ============
+      // ============ CG, single reduction ============
+      // (A. T. Chronopoulos and C. W. Gear, "s-step iterative methods for symmetric linear
+      // systems", J. Comput. Appl. Math. 25 (1989), the s = 1 case.)  The inner solve is a
+      // correction equation that the FP64 refinement checks, so it is not bound to HUTI's
+      // operation order.  With S = A P and W = A Z kept as vectors, both inner products of an
+      // iteration come out of the pass that computes its one SpMV, and the scalars follow as
+      //   beta = gamma / gamma_old,  eta = delta - beta gamma / alpha_old,  alpha = gamma / eta
+      // (gamma = (R, Z), delta = (W, Z)): two phases and two grid barriers per iteration
+      // instead of three.  A resumed segment forms its first eta exactly from the carried P, S:
+      // eta = delta + 2 b (Z, S) + b^2 eta_old, b = gamma / carry_rho (A symmetric).
       // layout R Z P W S; this iteration sums into set rd
       // B: P = Z + beta P; S = W + beta S; X += alpha P; R -= alpha S; Z = M^-1 R
       //    (init: R = B, X = 0, Z = M^-1 R);  clear set rd
@@ -697,7 +775,18 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
       // 1: P = R + beta (P - omega V); T1 = M^-1 P;  clear TS, TT
       batch_clear(a, BA_TS);
       batch_clear(a, BA_TT);
-      if (ilu) {
+      if (ilu && a.sweeps > 0) {
+        batch_slices(sh, [&](int, int s, int slice) {
+          if (sh.status[s] != ST_RUN) return;
+          const SysDesc &d = a.sys[s];
+          const int r = (slice << 5) + lane;
+          if (r >= d.n) return;
+          float *R = d.w, *P = d.w + 2 * d.ldw, *V = d.w + 3 * d.ldw;
+          P[r] = R[r] + sh.sb[s] * (P[r] - sh.sa[s] * V[r]);
+        });
+        if (!grid_barrier(a.bar, a.err, epoch)) return;
+        if (!batch_sweep_apply(a, sh, 2, 6, epoch)) return;
+      } else if (ilu) {
         batch_tri_any<true>(a, sh, 8, 6, [&](int, int s, const SysDesc &d, int i) {
           float *R = d.w, *P = d.w + 2 * d.ldw, *V = d.w + 3 * d.ldw;
           const float p = R[i] + sh.sb[s] * (P[i] - sh.sa[s] * V[i]);
@@ -748,7 +837,25 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
         if (s % gridDim.x == (int)blockIdx.x) a.state[wr * BATCH_MAX_SYS + s].alpha = al;
       }
       __syncthreads();
-      if (ilu) {
+      if (ilu && a.sweeps > 0) {
+        batch_slices(sh, [&](int ai, int s, int slice) {
+          if (sh.status[s] != ST_RUN) return;
+          const SysDesc &d = a.sys[s];
+          const int r = (slice << 5) + lane;
+          double ss = 0.0;
+          if (r < d.n) {
+            float *R = d.w, *V = d.w + 3 * d.ldw, *S = d.w + 5 * d.ldw;
+            const float sv = R[r] - (float)rho_s[s] * V[r];
+            S[r] = sv;
+            ss = (double)sv * (double)sv;
+          }
+          ss = warp_sum(ss);
+          if (lane == 0) batch_acc_add(sh, ai, 0, ss);
+        });
+        batch_flush(a, sh, BA_SS, -1);
+        if (!grid_barrier(a.bar, a.err, epoch)) return;
+        if (!batch_sweep_apply(a, sh, 5, 7, epoch)) return;
+      } else if (ilu) {
         batch_tri_any<true>(a, sh, 9, 7, [&](int ai, int s, const SysDesc &d, int i) {
           float *R = d.w, *V = d.w + 3 * d.ldw, *S = d.w + 5 * d.ldw;
           const float sv = R[i] - (float)rho_s[s] * V[i];
@@ -842,7 +949,7 @@ __global__ void __launch_bounds__(EGPU_BLOCK, 2) k_batch_inner(BatchArgs a, int 
             rt_r = (double)RT[r] * (double)b;
             rr = (double)b * (double)b;
           }
-          if (ilu) {
+          if (ilu && a.sweeps == 0) {
             T1[r] = SENT;
             T2[r] = SENT;
             Y1[r] = SENT;
@@ -1020,6 +1127,7 @@ struct egpu_batch {
   int tri_mult = 2;       // sync-free participants: tri_mult x widest level x running systems
   int bps = 2;            // blocks of the persistent inner kernel per SM (1 or 2)
   int spw = 1;            // SELL slices a warp sums at once in the SpMV phases (1 or 2: 32 or 64 rows)
+  int sweeps = 0;         // BiCGStab + ILU0: Jacobi sweeps per triangle in the inner solves (0: exact)
   bool resume_ok = true;  // reliable updating between segments (EGPU_MIXED_RESTART=1: off)
   bool exit_on_done = false;  // latency mode (egpu_batch_set_latency_mode)
   long long launches = 0;
@@ -1056,6 +1164,9 @@ extern "C" int egpu_batch_create(egpu_ctx *ctx, const egpu_params *prm, egpu_bat
   B->prm = *prm;
   B->prm.precision = EGPU_MIXED;
   if (const char *e = std::getenv("EGPU_MIXED_RESTART")) B->resume_ok = e[0] != '1';
+  B->sweeps = prm->method == EGPU_BICGSTAB ? prm->ilu_sweeps : 0;
+  if (const char *e = std::getenv("EGPU_ILU_SWEEPS")) B->sweeps = prm->method == EGPU_BICGSTAB ? std::atoi(e) : 0;
+  B->sweeps = std::max(0, std::min(B->sweeps, 16));
   if (B->prm.inner_max_iter < 1) B->prm.inner_max_iter = 2000;
   if (B->prm.max_refinements < 1) B->prm.max_refinements = 100;
   *out = B;
@@ -1095,7 +1206,8 @@ static int batch_prepare(egpu_batch *B, int slot, const double *b_dev) {
     rc = ilu_factor(A, B->prm.ilu_order);
     if (rc) return rc;
   }
-  rc = prepare_fp32_public(A, B->prm.precond == EGPU_PREC_ILU0);
+  const bool sweeps = B->sweeps > 0 && B->prm.precond == EGPU_PREC_ILU0 && A->ilu_order == 0 && A->ilu_nnz == A->nnz;
+  rc = prepare_fp32_public(A, B->prm.precond == EGPU_PREC_ILU0, sweeps);
   if (rc) return rc;
   int unit = 0;
   if (B->prm.method == EGPU_CG && B->prm.precond == EGPU_PREC_DIAGONAL) {
@@ -1131,6 +1243,9 @@ static int batch_prepare(egpu_batch *B, int slot, const double *b_dev) {
   d.lo_vals = A->lo_vals32.p;
   d.up_vals = A->up_vals32.p;
   d.up_dinv = A->up_dinv32.p;
+  d.isvals = sweeps ? A->ilu_sell32.p : nullptr;
+  d.idinv = sweeps ? A->ilu_dinv32.p : nullptr;
+  d.swr = A->sell_swr.p;
   d.w = A->work32.p;
   d.ldw = ldw32;
   d.b = A->work32.p + 10 * ldw32;
@@ -1325,6 +1440,7 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
     a.precond = B->prm.precond;
     a.kmax = B->chunk;
     a.spw = B->spw;
+    a.sweeps = B->sweeps;
     a.exit_on_done = B->exit_on_done ? 1 : 0;
     a.tol = inner_tol_of(&B->prm);
     a.maxit = B->prm.inner_max_iter;

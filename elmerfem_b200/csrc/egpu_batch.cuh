@@ -40,6 +40,11 @@ struct SysDesc {
   const int *rows, *cols, *diag, *lower_order, *upper_order;
   const int *lo_ptr, *lo_cols, *up_ptr, *up_cols;   // ILU0 factors packed in solve order
   const float *lo_vals, *up_vals, *up_dinv;
+  // ILU0 by Jacobi sweeps (BatchArgs::sweeps > 0): the factors in the SELL layout, the
+  // inverted U diagonal in row order, per slice the k ranges of the strictly-lower ([0, x))
+  // and strictly-upper ([y, w)) entries
+  const float *isvals, *idinv;
+  const int2 *swr;
   float *w;                // work vectors, stride ldw
   long long ldw;
   const float *b;          // inner right-hand side (r / ||r||)
@@ -75,6 +80,7 @@ struct BatchArgs {
   int tri_warps_per_block;
   int tri_group;            // rows per warp in the sync-free solves (1, 2, 4 or 8)
   int spw;                  // SELL slices (of 32 rows) a warp sums at once in the SpMV phases (1 or 2)
+  int sweeps;               // BiCGStab + ILU0: Jacobi sweeps per triangle (0: sync-free exact solves)
   unsigned int *bar;
   int *err;
   int *it_done;             // iterations run by this launch (written by block 0)

@@ -1064,17 +1064,6 @@ static int run_krylov(egpu_mat *A, const KArgs<VT> &a0, int method, bool offs) {
   // the instantiation with the level-synchronous solves only when this matrix uses them
   const bool cta = a.tri_cta != 0;
   if (method == EGPU_CG) {
-    if constexpr (sizeof(VT) == 4) {
-      // FP32 inner solves without ILU: single-reduction CG (EGPU_CG_SR=0 keeps cg_kernel)
-      const char *e = std::getenv("EGPU_CG_SR");
-      if (!a.true_residual && a.precond != EGPU_PREC_ILU0 && !(e && e[0] == '0')) {
-        if (a.precond == EGPU_PREC_NONE || a.unit_diag)
-          return offs ? launch_coop(ctx, cg_sr_kernel<TRI_TS, true, true>, a, nullptr, 0)
-                      : launch_coop(ctx, cg_sr_kernel<TRI_TS, false, true>, a, nullptr, 0);
-        return offs ? launch_coop(ctx, cg_sr_kernel<TRI_TS, true, false>, a, nullptr, 0)
-                    : launch_coop(ctx, cg_sr_kernel<TRI_TS, false, false>, a, nullptr, 0);
-      }
-    }
     if (cta) {
       if (offs) return launch_coop(ctx, cg_kernel<VT, TRI_TS, true, true>, a, nullptr, smem);
       return launch_coop(ctx, cg_kernel<VT, TRI_TS, false, true>, a, nullptr, smem);
@@ -1445,10 +1434,8 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
     rc = precond_factor(A, prm);
     if (rc) return rc;
   }
-  // ILU0 by Jacobi sweeps in the FP32 inner BiCGStab (EGPU_ILU_SWEEPS overrides the count)
-  int sweeps = prm->ilu_sweeps;
-  if (const char *e = std::getenv("EGPU_ILU_SWEEPS")) sweeps = std::atoi(e);
-  sweeps = std::max(0, std::min(sweeps, 16));
+  // ILU0 by Jacobi sweeps in the FP32 inner BiCGStab (the count egpu_iter_solve_dev chose)
+  const int sweeps = std::max(0, std::min(prm->ilu_sweeps, 16));
   const bool use_sweeps = sweeps > 0 && prm->method == EGPU_BICGSTAB && prm->precond == EGPU_PREC_ILU0 &&
                           A->ilu_order == 0 && A->ilu_nnz == A->nnz;
   rc = prepare_fp32(A, ilu, use_sweeps);
@@ -1701,7 +1688,7 @@ int rhs_scale(egpu_mat *A, const double *b_dev, const double *x_dev, double *bs,
   return EGPU_OK;
 }
 
-int prepare_fp32_public(egpu_mat *A, bool with_ilu) { return prepare_fp32(A, with_ilu, false); }
+int prepare_fp32_public(egpu_mat *A, bool with_ilu, bool sweeps) { return prepare_fp32(A, with_ilu, sweeps); }
 
 // *unit = 1 when the FP32 copy of the scaled diagonal (work32 vector 13, written by
 // prepare_fp32) is 1.0f in every row; synchronises the stream
@@ -1738,6 +1725,7 @@ extern "C" void egpu_params_default(egpu_params *p, int method, int precond) {
   p->inner_tol = 0.0;  // by preconditioner (inner_tol_of)
   p->inner_max_iter = 2000;
   p->max_refinements = 100;
+  p->ilu_sweeps = -1;  // mixed BiCGStab + ILU0: exact or Jacobi-sweep solves, measured
 }
 
 extern "C" int egpu_create(int device, egpu_ctx **out) {
@@ -2164,29 +2152,61 @@ extern "C" int egpu_iter_solve_dev(egpu_mat *A, const double *b_dev, double *x_d
   if (!b_dev) b_dev = A->rhs.p;
   egpu_result r{};
   int rc;
-  // Mixed precision is a request for the faster of the two paths at the same tolerance: on
-  // operators where rounding the scaled matrix to FP32 costs more refinements than the FP32
-  // iterations save (latency-bound triangular solves, stiff elasticity), the FP64 drop-in is
-  // faster.  The library measures both on the matrix itself: the first two mixed requests run
-  // mixed, and while fewer than two FP64 solves have run (the caller's own included) the next
-  // run as the FP64 drop-in; each path's first solve carries one-time set-up and is not
-  // compared.  From then on a mixed request takes FP64 when its latest time is below 0.85 of
-  // the latest mixed one.  Both paths meet the same tolerance.  CG / BiCGStab only (GCR and
-  // BiCGStab(l) are FP64); EGPU_MIXED_AUTO=0 keeps every mixed request mixed.
+  // A mixed request (CG / BiCGStab) asks for the fastest path to the same tolerance.  The
+  // candidates: the mixed solve as requested (exact triangular solves, or ilu_sweeps > 0
+  // Jacobi sweeps), with ilu_sweeps < 0 (BiCGStab + ILU0) also the mixed solve with
+  // AUTO_SWEEPS sweeps, and the FP64 drop-in.  On stiff operators rounding the scaled matrix
+  // to FP32 costs more refinements than FP32 saves, and the sweeps pay only where the
+  // factors are well conditioned, so the library measures: the matrix's first solve is not
+  // timed (one-time set-up), then each candidate runs once, timed, and from then on a mixed
+  // request takes the fastest mixed candidate, or the FP64 drop-in when its time is below
+  // 0.85 of that one.  Each path keeps its latest time.  EGPU_MIXED_AUTO=0 keeps the
+  // requested mixed solve.  GCR and BiCGStab(l) are FP64.
+  constexpr int AUTO_SWEEPS = 2;
   const char *aenv = std::getenv("EGPU_MIXED_AUTO");
   const bool auto_ok = !(aenv && aenv[0] == '0');
   const bool krylov32 = prm->method == EGPU_CG || prm->method == EGPU_BICGSTAB;
-  bool mixed = prm->precision == EGPU_MIXED && krylov32;
-  if (mixed && auto_ok && A->n_mixed >= 2)
-    mixed = A->n_fp64 >= 2 && !(A->t_fp64 < 0.85 * A->t_mixed);
-  if (mixed) {
-    rc = egpu::solve_mixed(A, b_dev, x_dev, prm, &r);
-    r.precision_used = EGPU_MIXED;
-    if (rc > 0 && r.info == EGPU_HUTI_CONVERGENCE && A->n_mixed++ > 0) A->t_mixed = r.seconds;
-  } else {
+  int sweeps_req = prm->ilu_sweeps;
+  if (const char *e = std::getenv("EGPU_ILU_SWEEPS")) sweeps_req = std::atoi(e);
+  const bool sweeps_ok = prm->method == EGPU_BICGSTAB && prm->precond == EGPU_PREC_ILU0 && prm->ilu_order == 0;
+  int path = 0;  // 0 FP64, 1 mixed exact, 2 mixed sweeps
+  if (prm->precision == EGPU_MIXED && krylov32) {
+    const int asked = (sweeps_ok && sweeps_req > 0) ? 2 : 1;
+    path = asked;
+    if (auto_ok) {
+      int cand[3], nc = 0;
+      cand[nc++] = asked;
+      if (sweeps_ok && sweeps_req < 0) cand[nc++] = 2;
+      cand[nc++] = 0;
+      path = -1;
+      if (A->n_solved == 0) path = asked;
+      for (int c = 0; c < nc && path < 0; ++c)
+        if (A->n_path[cand[c]] == 0) path = cand[c];
+      if (path < 0) {
+        int best = asked;
+        for (int c = 0; c < nc; ++c)
+          if (cand[c] != 0 && A->t_path[cand[c]] < A->t_path[best]) best = cand[c];
+        path = A->t_path[0] < 0.85 * A->t_path[best] ? 0 : best;
+      }
+    }
+  }
+  if (path == 0) {
     rc = egpu::solve_fp64(A, b_dev, x_dev, prm, &r);
     r.precision_used = EGPU_FP64;
-    if (krylov32 && rc > 0 && r.info == EGPU_HUTI_CONVERGENCE && A->n_fp64++ > 0) A->t_fp64 = r.seconds;
+  } else {
+    egpu_params p2 = *prm;
+    p2.ilu_sweeps = path == 2 ? (sweeps_req > 0 ? std::min(sweeps_req, 16) : AUTO_SWEEPS) : 0;
+    rc = egpu::solve_mixed(A, b_dev, x_dev, &p2, &r);
+    r.precision_used = EGPU_MIXED;
+    r.ilu_sweeps_used = p2.ilu_sweeps;
+  }
+  // times of converged CG / BiCGStab solves (an FP64 request counts for the FP64 path)
+  if (krylov32 && rc > 0 && r.info == EGPU_HUTI_CONVERGENCE) {
+    if (A->n_solved > 0) {
+      A->t_path[path] = r.seconds;
+      A->n_path[path]++;
+    }
+    A->n_solved++;
   }
   if (res) *res = r;
   return rc;

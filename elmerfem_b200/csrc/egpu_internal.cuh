@@ -191,11 +191,14 @@ struct egpu_mat {
   DevBuf<double> values;         // as bound / assembled (unscaled)
   DevBuf<double> rhs;            // assembled right-hand side
   bool has_values = false, has_rhs = false;
-  // device seconds of the latest FP64 and mixed-precision solves of this matrix after each
-  // path's first (which carries one-time set-up), and the solves of each path so far; they
-  // outlive value updates (a time or nonlinear loop re-assembles the same operator)
-  double t_fp64 = 0.0, t_mixed = 0.0;
-  int n_fp64 = 0, n_mixed = 0;
+  // the library's measured choice of path for mixed requests: per path (0 FP64 drop-in,
+  // 1 mixed with exact triangular solves, 2 mixed with ILU0 by Jacobi sweeps) the device
+  // seconds of its latest timed solve and the number timed; the matrix's first solve (which
+  // carries the one-time set-up) is not timed.  They outlive value updates (a time or
+  // nonlinear loop re-assembles the same operator).
+  double t_path[3] = {0.0, 0.0, 0.0};
+  int n_path[3] = {0, 0, 0};
+  int n_solved = 0;
   int max_row = 0;               // longest row
   int max_bandwidth = 0;         // max |col - row|
   bool sorted_rows = true;       // columns strictly ascending in every row (CRS_SortMatrix); ILU needs it
@@ -466,32 +469,6 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *smem /* >= 32
     for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
     v[k] = __shfl_sync(0xffffffffu, t, 0);
   }
-  __syncthreads();
-}
-
-// NV sums at once: slot k's partials at partials + slot[k] * nb, all loads in flight together
-// (one L2 round trip for all of them); the same fixed order as reduce_partials.
-template <int NV>
-__device__ __forceinline__ void reduce_partials_n(const double *partials, const int (&slot)[NV], int nb,
-                                                  double *smem, double (&out)[NV]) {
-  const int lane = threadIdx.x & 31;
-  if (threadIdx.x < 32) {
-    double t[NV];
-#pragma unroll
-    for (int k = 0; k < NV; ++k) t[k] = 0.0;
-    for (int i = lane; i < nb; i += 32)
-#pragma unroll
-      for (int k = 0; k < NV; ++k) t[k] += __ldcg(partials + slot[k] * nb + i);
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) t[k] += __shfl_down_sync(0xffffffffu, t[k], off);
-      if (lane == 0) smem[k] = t[k];
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < NV; ++k) out[k] = smem[k];
   __syncthreads();
 }
 

@@ -1146,166 +1146,6 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) cg_kernel(KArgs<VT> a) {
 }
 
 // =====================================================================================
-// Single-reduction CG for the FP32 inner solves without ILU (no preconditioner, or Jacobi)
-// (A. T. Chronopoulos and C. W. Gear, "s-step iterative methods for symmetric linear
-// systems", J. Comput. Appl. Math. 25 (1989), the s = 1 case).  The inner solve is a
-// correction equation whose result the FP64 refinement checks, so it is not bound to HUTI's
-// operation order; the FP64 drop-in keeps cg_kernel.  With S = A P and W = A Z kept as
-// vectors, both inner products of an iteration come out of the pass that computes its one
-// SpMV:
-//
-//   phase A:  W = A Z;  gamma = (R, Z), delta = (W, Z), (R, R)          -- grid barrier
-//   scalars:  beta = gamma / gamma_old, eta = delta - beta gamma / alpha_old, alpha = gamma / eta
-//   phase B:  P = Z + beta P;  S = W + beta S;  X += alpha P;  R -= alpha S;  Z = M^-1 R
-//                                                                       -- grid barrier
-//
-// two phases and two grid barriers per iteration instead of three, one combined reduction
-// of the partial sums, and the same 48n bytes of vector traffic on a unit diagonal (Z is R).
-//
-// Reliable updating: a resumed segment continues from the carried P and S (the previous
-// scale; carry = gamma, alpha, eta of the last iteration) with the new residual.  Its first
-// eta is formed exactly, eta = (Z + b P, W + b S) = delta + 2 b (Z, S) + b^2 eta_old with
-// b = gamma / (ru_c gamma_old) (A symmetric), since the replaced residual breaks the
-// orthogonality the recurrence for eta assumes.
-//
-// w layout: R Z P W S.  ZR: M = I (no preconditioner, or Jacobi on a unit diagonal), Z is R.
-template <int LPR, bool OFFS, bool ZR>
-__global__ void __launch_bounds__(EGPU_KBLOCK, 1) cg_sr_kernel(KArgs<float> a) {
-  __shared__ double sm[32 * 4];
-  unsigned int epoch = 0;
-  const int n = a.n, nb = gridDim.x;
-  constexpr bool zr = ZR;
-  float *X = a.x, *R = a.w, *Z = zr ? a.w : a.w + a.ldw, *P = a.w + 2 * a.ldw, *Wv = a.w + 3 * a.ldw,
-        *S = a.w + 4 * a.ldw;
-  const float *B = a.b;
-  const float *D = a.dvals;
-
-  // ---- init: R = B, X = 0, Z = M^-1 R; ||B||^2
-  {
-    double acc[1] = {0.0};
-    vec_loop<float>(n, [&](int i, auto w) {
-      constexpr int W = decltype(w)::value;
-      float b[W], d[W], z[W];
-      vld<W>(B, i, b);
-      vst<W>(R, i, b);
-      vfill<W>(X, i, 0.f);
-      if (!zr) {
-        vld<W>(D, i, d);
-#pragma unroll
-        for (int k = 0; k < W; ++k) z[k] = diag_prec(b[k], d[k]);
-        vst<W>(Z, i, z);
-      }
-#pragma unroll
-      for (int k = 0; k < W; ++k) acc[0] += (double)b[k] * (double)b[k];
-    });
-    block_sum<1>(acc, sm);
-    store_partials(a, SLOT_BB, acc[0]);
-  }
-  if (!grid_barrier(a.bar, a.err, epoch)) return;
-  const double rhsnorm = sqrt(reduce_partials(a.partials + SLOT_BB * nb, nb, sm));
-
-  const bool resumed = a.resume != 0;
-  double gamma_old = resumed ? a.carry[0] * a.ru_c : 1.0, alpha_old = resumed ? a.carry[1] : 1.0,
-         eta_old = resumed ? a.carry[2] : 0.0;
-  int k = 1, info = 0, iters = 0;
-  double residual = 0.0;
-  while (true) {
-    const bool first = k == 1;
-    // ---- phase A: W = A Z; gamma, delta, (R, R); (Z, S) on a resumed first iteration
-    {
-      double acc[4] = {0.0, 0.0, 0.0, 0.0};
-      spmv_phase<float, LPR, OFFS, false>(a, Z, Z, [&](int i, float wv, float) {
-        Wv[i] = wv;
-        const float z = Z[i];
-        const float r = zr ? z : R[i];
-        acc[0] += (double)r * (double)z;
-        acc[1] += (double)wv * (double)z;
-        if (!zr) acc[2] += (double)r * (double)r;
-        if (resumed && first) acc[3] += (double)z * (double)S[i];
-      });
-      block_sum<4>(acc, sm);
-      if (threadIdx.x == 0) {
-        a.partials[SLOT_RHO * nb + blockIdx.x] = acc[0];
-        a.partials[SLOT_PQ * nb + blockIdx.x] = acc[1];
-        a.partials[SLOT_RR2 * nb + blockIdx.x] = acc[2];
-        a.partials[SLOT_TS * nb + blockIdx.x] = acc[3];
-      }
-    }
-    if (!grid_barrier(a.bar, a.err, epoch)) return;
-    double red[4];
-    reduce_partials_n<4>(a.partials, {SLOT_RHO, SLOT_PQ, SLOT_RR2, SLOT_TS}, nb, sm, red);
-    const double gamma = red[0], delta = red[1], rr = zr ? red[0] : red[2];
-    if (k > 1) {  // recursive residual of x_{k-1}
-      residual = sqrt(rr) / rhsnorm;
-      if (residual <= a.tol) { info = EGPU_HUTI_CONVERGENCE; iters = k - 1; break; }
-      if (k > a.maxit) { info = EGPU_HUTI_MAXITER; iters = k - 1; break; }
-    }
-    if (gamma == 0.0) { info = EGPU_HUTI_CG_RHO; iters = k; break; }
-    double beta = 0.0, eta = delta;
-    if (!first) {
-      beta = gamma / gamma_old;
-      eta = delta - beta * gamma / alpha_old;
-    } else if (resumed) {
-      beta = gamma / gamma_old;
-      eta = delta + 2.0 * beta * red[3] + beta * beta * eta_old;
-    }
-    if (!(eta != 0.0)) { info = EGPU_HUTI_CG_RHO; iters = k; break; }
-    const double alpha = gamma / eta;
-    // ---- phase B: P = Z + beta P; S = W + beta S; X += alpha P; R -= alpha S; Z = M^-1 R
-    {
-      const float be = (float)beta, al = (float)alpha;
-      const bool fresh = first && !resumed;
-      vec_loop<float>(n, [&](int i, auto w) {
-        constexpr int W = decltype(w)::value;
-        float z[W], wv[W], p[W], sv[W], x[W], r[W], d[W];
-        vld<W>(Z, i, z);
-        vld<W>(Wv, i, wv);
-        vld<W>(X, i, x);
-        if (!fresh) {
-          vld<W>(P, i, p);
-          vld<W>(S, i, sv);
-        }
-        if (!zr) {
-          vld<W>(R, i, r);
-          vld<W>(D, i, d);
-        }
-#pragma unroll
-        for (int t = 0; t < W; ++t) {
-          p[t] = fresh ? z[t] : z[t] + be * p[t];
-          sv[t] = fresh ? wv[t] : wv[t] + be * sv[t];
-          x[t] = x[t] + al * p[t];
-          const float rt = (zr ? z[t] : r[t]) - al * sv[t];
-          r[t] = rt;
-          if (!zr) z[t] = diag_prec(rt, d[t]);
-        }
-        vst<W>(P, i, p);
-        vst<W>(S, i, sv);
-        vst<W>(X, i, x);
-        vst<W>(R, i, r);
-        if (!zr) vst<W>(Z, i, z);
-      });
-    }
-    if (!grid_barrier(a.bar, a.err, epoch)) return;
-    gamma_old = gamma;
-    alpha_old = alpha;
-    eta_old = eta;
-    ++k;
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    a.out_i[0] = info;
-    a.out_i[1] = iters;
-    a.out_d[0] = residual;
-    a.out_d[1] = rhsnorm;
-    if (a.carry) {  // P, S hold the last iteration's direction and its product with A
-      a.carry[0] = gamma_old;
-      a.carry[1] = alpha_old;
-      a.carry[2] = eta_old;
-      a.carry[3] = (info == EGPU_HUTI_CONVERGENCE && k > 1) ? 1.0 : 0.0;
-    }
-  }
-}
-
-// =====================================================================================
 // BiCGStab  (huti_dbicgstabsolv, hutiter/src/huti_bicgstab_D.F90:96-284)
 //
 // w layout: R RTLD P V T S T1V T2V Y1 Y2

@@ -51,7 +51,7 @@ int krylov_fp64_scaled(egpu_mat *A, const double *bs, double *xs, const egpu_par
 int rhs_scale(egpu_mat *A, const double *b_dev, const double *x_dev, double *bs, double *xs, bool scale_system,
               double *bnorm_s);
 // FP32 SELL values, diagonal and (optionally) ILU0 factors for the inner solver
-int prepare_fp32_public(egpu_mat *A, bool with_ilu);
+int prepare_fp32_public(egpu_mat *A, bool with_ilu, bool sweeps);
 int unit_diagonal_fp32(egpu_mat *A, int *unit);
 
 // level-synchronous single-block ILU0 solves (egpu_tri_cta.cu)

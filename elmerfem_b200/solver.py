@@ -122,8 +122,8 @@ class SolverParams:
     restart: int = 0              # GCR restart (0: max_iter) / BiCGStab(l) degree (0: 2)
     ilut_tol: float = 0.0         # drop tolerance with precond PREC_ILUT (Linear System ILUT Tolerance)
     divtol: float = 0.0           # Linear System Divergence Tolerance (0: none); GCR and BiCGStab(l)
-    ilu_sweeps: int = 0           # mixed BiCGStab + ILU0: Jacobi sweeps per triangle in the FP32 inner
-                                  # solves instead of exact triangular solves (0: exact)
+    ilu_sweeps: int = -1          # mixed BiCGStab + ILU0: Jacobi sweeps per triangle in the FP32 inner
+                                  # solves (0: exact solves; < 0: measured against exact by the library)
 
     def to_c(self) -> _lib.Params:
         return _lib.Params(self.method, self.precond, self.max_iter, self.tol, int(self.scale_system),

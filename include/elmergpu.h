@@ -89,7 +89,9 @@ typedef struct {
    * this many Jacobi sweeps per triangle (y <- v - L y, z <- D^-1 (y - U z)) instead of
    * exact triangular solves, trading the solves' dependency levels (latency-bound) for
    * parallel passes over the factors; the FP64 refinement still stops on the true residual.
-   * 0: exact solves.  The FP64 drop-in always solves exactly, as CRS_LUSolve. */
+   * 0: exact solves; < 0 (egpu_params_default): the library measures exact solves against
+   * two sweeps on the matrix and keeps the faster (see egpu_result.precision_used).  The
+   * FP64 drop-in always solves exactly, as CRS_LUSolve. */
   int ilu_sweeps;
 } egpu_params;
 
@@ -103,12 +105,15 @@ typedef struct {
   double seconds_krylov;  /* device time inside the persistent Krylov kernels */
   int krylov_launches;    /* number of persistent Krylov kernel launches */
   /* the path that ran: EGPU_FP64, or EGPU_MIXED.  A CG / BiCGStab mixed request is a request
-   * for the faster path at the same tolerance: on each matrix the first two mixed requests run
-   * mixed, the next run the FP64 drop-in until two FP64 solves have run (the caller's own
-   * included), and after that the drop-in is taken when its latest time is below 0.85 of the
-   * latest mixed one.  Each path's first solve (one-time set-up) is not compared; the times
-   * outlive value updates.  EGPU_MIXED_AUTO=0 keeps every mixed request mixed. */
+   * for the fastest path at the same tolerance.  The candidates: the mixed solve as asked,
+   * with ilu_sweeps < 0 (BiCGStab + ILU0) also the mixed solve with two Jacobi sweeps, and the
+   * FP64 drop-in.  On each matrix the first solve is not timed (one-time set-up), then every
+   * candidate not yet timed runs once (the caller's own FP64 solves count), and after that a
+   * mixed request takes the fastest mixed candidate, or the FP64 drop-in when its latest time
+   * is below 0.85 of that one.  The times outlive value updates.  EGPU_MIXED_AUTO=0 keeps the
+   * mixed solve as asked. */
   int precision_used;
+  int ilu_sweeps_used;    /* Jacobi sweeps per triangle of the mixed solve that ran (0: exact) */
 } egpu_result;
 
 /* fills p with Elmer's defaults for the given method/preconditioner */

@@ -68,3 +68,29 @@ def test_exact_paths_ignore_sweeps(ctx, monkeypatch):
             assert np.array_equal(x0, x1)
     finally:
         A.free()
+
+
+@pytest.mark.parametrize("sweeps", [1, 2])
+def test_batched_sweeps_against_the_oracle(ctx, sweeps):
+    """egpu_batch with ilu_sweeps > 0: every system of a mixed batch (hex Poisson with
+    log-normal conductivity, and a tet mesh) within 1e-8 of the oracle's exact ILU0 solve."""
+    tol = 1e-11
+    systems = []
+    for i, m in enumerate([6, 11, 8, 5, 9]):
+        mesh = meshgen.hex_cube(m) if i % 2 == 0 else meshgen.tet_cube(m)
+        k = meshgen.lognormal_conductivity(mesh.nelem, 1.0, 20 + i)
+        p, _, _, v, b, _ = poisson_problem(mesh, elem_k=k, load=meshgen.sine_source(mesh.coords))
+        systems.append((p, v, b))
+    prm = eg.SolverParams(method=eg.BICGSTAB, precond=eg.PREC_ILU0, tol=tol, max_iter=5000, ilu_sweeps=sweeps)
+    B = eg.Batch(ctx, prm, chunk=16)
+    try:
+        ids = [B.add(_pat(p), v, b) for p, v, b in systems]
+        B.solve()
+        for sid, (p, v, b) in zip(ids, systems):
+            r = B.result(sid)
+            assert r["info"] == 1, r
+            x_ref, r_ref = oracle.solve(p, v, b, method=oracle.BICGSTAB, precond=oracle.PREC_ILU0, max_iter=5000,
+                                        tol=tol)
+            assert rel(B.solution(sid), x_ref) < 1e-8
+    finally:
+        B.free()

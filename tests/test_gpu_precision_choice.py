@@ -1,102 +1,124 @@
-"""A mixed-precision CG / BiCGStab request runs the faster of the two paths measured on the
-matrix itself: the first two mixed requests run mixed, the next run the FP64 drop-in until two
-FP64 solves have run (the caller's own included), and from then on the drop-in is taken when
-its latest time is below 0.85 of the latest mixed one.  Each path's first solve (one-time
-set-up) is not compared.  The measurements outlive value updates.  Every solution meets 1e-8
-against the oracle; EGPU_MIXED_AUTO=0 keeps the mixed path."""
+"""A mixed-precision CG / BiCGStab request runs the fastest path the library has measured on the
+matrix.  Candidates: the mixed solve as asked; with ilu_sweeps < 0 (BiCGStab + ILU0, the
+default) also the mixed solve with two Jacobi sweeps per triangle; and the FP64 drop-in.  The
+matrix's first solve is not timed (one-time set-up), then every candidate not yet timed runs
+once (the caller's own FP64 solves count), and from then on a mixed request takes the fastest
+mixed candidate, or FP64 when its latest time is below 0.85 of that one.  Each path keeps its
+latest time; the times outlive value updates.  Every solution meets 1e-8 against the oracle;
+EGPU_MIXED_AUTO=0 keeps the mixed solve as asked."""
 import pytest
 
 import elmerfem_b200 as eg
 import oracle
 from elmerfem_b200 import meshgen
-from helpers import elastic_problem, rel
+from helpers import elastic_problem, poisson_problem, rel
 
 pytestmark = pytest.mark.gpu
 
+FP64, EXACT, SWEEPS = 0, 1, 2
 
-def _params(precision, method=eg.BICGSTAB):
-    return eg.SolverParams(method=method, precond=eg.PREC_ILU0, tol=1e-8, max_iter=5000, precision=precision)
+
+def _params(precision, method=eg.BICGSTAB, precond=eg.PREC_ILU0, **kw):
+    return eg.SolverParams(method=method, precond=precond, tol=1e-8, max_iter=5000, precision=precision, **kw)
+
+
+def _path(r):
+    if r["precision_used"] == eg.FP64:
+        return FP64
+    return SWEEPS if r["ilu_sweeps_used"] > 0 else EXACT
 
 
 class Model:
-    """the library's bookkeeping, restated: counts and latest warm times per path"""
+    """the library's bookkeeping, restated"""
 
     def __init__(self):
-        self.n = {eg.FP64: 0, eg.MIXED: 0}
-        self.t = {eg.FP64: 0.0, eg.MIXED: 0.0}
+        self.solved = 0
+        self.n = {FP64: 0, EXACT: 0, SWEEPS: 0}
+        self.t = {FP64: 0.0, EXACT: 0.0, SWEEPS: 0.0}
 
-    def expect(self):
-        if self.n[eg.MIXED] < 2:
-            return eg.MIXED
-        if self.n[eg.FP64] < 2:
-            return eg.FP64
-        return eg.FP64 if self.t[eg.FP64] < 0.85 * self.t[eg.MIXED] else eg.MIXED
+    def expect(self, cands):
+        if self.solved == 0:
+            return cands[0]
+        for c in cands:
+            if self.n[c] == 0:
+                return c
+        best = cands[0]
+        for c in cands:
+            if c != FP64 and self.t[c] < self.t[best]:
+                best = c
+        return FP64 if self.t[FP64] < 0.85 * self.t[best] else best
 
     def record(self, path, r):
         assert r["info"] == 1
-        if self.n[path] > 0:
+        if self.solved > 0:
             self.t[path] = r["seconds"]
-        self.n[path] += 1
+            self.n[path] += 1
+        self.solved += 1
 
 
-def test_mixed_request_takes_the_measured_faster_path(ctx, monkeypatch):
+def test_mixed_request_takes_the_measured_fastest_path(ctx, monkeypatch):
     p, _, _, v, b, _ = elastic_problem(meshgen.hex_cube(8))
     x_orc, r_orc = oracle.solve(p, v, b, method=oracle.BICGSTAB, precond=oracle.PREC_ILU0, tol=1e-8, max_iter=5000)
     A = eg.Matrix(ctx, eg.CRSPattern(p.n, p.nnz, 3, p.perm, p.rows, p.cols, p.diag), v)
     try:
         mod = Model()
+        cands = [EXACT, SWEEPS, FP64]
         seen = []
         for _ in range(7):
-            want = mod.expect()
+            want = mod.expect(cands)
             x, r = A.solve(b, params=_params(eg.MIXED))
-            assert r["precision_used"] == want, (len(seen), mod.n, mod.t)
+            assert _path(r) == want, (len(seen), mod.n, mod.t)
             assert r["info"] == 1 and rel(x, x_orc) < 1e-8
             mod.record(want, r)
             seen.append(want)
-        # two mixed, then two FP64 probes, then the choice
-        assert seen[:4] == [eg.MIXED, eg.MIXED, eg.FP64, eg.FP64]
+        # untimed first solve, then each candidate once
+        assert seen[:4] == [EXACT, EXACT, SWEEPS, FP64]
 
         # an explicit FP64 request is always FP64, and it refreshes the FP64 time
         x, r = A.solve(b, params=_params(eg.FP64))
-        assert r["precision_used"] == eg.FP64 and rel(x, x_orc) < 1e-8
-        mod.record(eg.FP64, r)
+        assert _path(r) == FP64 and rel(x, x_orc) < 1e-8
+        mod.record(FP64, r)
 
         monkeypatch.setenv("EGPU_MIXED_AUTO", "0")
         x, r = A.solve(b, params=_params(eg.MIXED))
-        assert r["precision_used"] == eg.MIXED and rel(x, x_orc) < 1e-8
-        mod.record(eg.MIXED, r)
+        assert _path(r) == EXACT and rel(x, x_orc) < 1e-8
+        mod.record(EXACT, r)
+        x, r = A.solve(b, params=_params(eg.MIXED, ilu_sweeps=3))
+        assert _path(r) == SWEEPS and r["ilu_sweeps_used"] == 3 and rel(x, x_orc) < 1e-8
+        mod.record(SWEEPS, r)
         monkeypatch.delenv("EGPU_MIXED_AUTO")
 
         # new values of the same operator keep the measurements
         A.update_values(v)
-        want = mod.expect()
+        want = mod.expect(cands)
         x, r = A.solve(b, params=_params(eg.MIXED))
-        assert r["precision_used"] == want and rel(x, x_orc) < 1e-8
+        assert _path(r) == want and rel(x, x_orc) < 1e-8
     finally:
         A.free()
 
 
-def test_caller_fp64_solves_count_and_other_methods_stay_fp64(ctx):
-    p, _, _, v, b, _ = elastic_problem(meshgen.hex_cube(6))
-    x_orc, _ = oracle.solve(p, v, b, method=oracle.BICGSTAB, precond=oracle.PREC_ILU0, tol=1e-8, max_iter=5000)
-    A = eg.Matrix(ctx, eg.CRSPattern(p.n, p.nnz, 3, p.perm, p.rows, p.cols, p.diag), v)
+def test_caller_fp64_solves_count_and_cg_has_no_sweeps(ctx):
+    p, _, _, v, b, _ = poisson_problem(meshgen.hex_cube(10))
+    x_orc, _ = oracle.solve(p, v, b, method=oracle.CG, precond=oracle.PREC_DIAGONAL, tol=1e-8, max_iter=5000)
+    A = eg.Matrix(ctx, eg.CRSPattern(p.n, p.nnz, 1, p.perm, p.rows, p.cols, p.diag), v)
     try:
         mod = Model()
-        for _ in range(2):  # the caller's own FP64 solves count: no probe after the two mixed
-            x, r = A.solve(b, params=_params(eg.FP64))
-            assert r["precision_used"] == eg.FP64
-            mod.record(eg.FP64, r)
+        cands = [EXACT, FP64]
+        for _ in range(2):  # the caller's own FP64 solves: the first is untimed, the second counts
+            x, r = A.solve(b, params=_params(eg.FP64, method=eg.CG, precond=eg.PREC_DIAGONAL))
+            assert _path(r) == FP64
+            mod.record(FP64, r)
         for _ in range(3):
-            want = mod.expect()
-            x, r = A.solve(b, params=_params(eg.MIXED))
-            assert r["precision_used"] == want and rel(x, x_orc) < 1e-8
+            want = mod.expect(cands)
+            x, r = A.solve(b, params=_params(eg.MIXED, method=eg.CG, precond=eg.PREC_DIAGONAL))
+            assert _path(r) == want and rel(x, x_orc) < 1e-8
             mod.record(want, r)
         # GCR has no FP32 inner solver: a mixed request runs FP64 and is not timed
-        x, r = A.solve(b, params=eg.SolverParams(method=eg.GCR, precond=eg.PREC_ILU0, tol=1e-8, max_iter=5000,
+        x, r = A.solve(b, params=eg.SolverParams(method=eg.GCR, precond=eg.PREC_DIAGONAL, tol=1e-8, max_iter=5000,
                                                  precision=eg.MIXED))
-        assert r["precision_used"] == eg.FP64 and r["info"] == 1
-        want = mod.expect()
-        x, r = A.solve(b, params=_params(eg.MIXED))
-        assert r["precision_used"] == want
+        assert _path(r) == FP64 and r["info"] == 1
+        want = mod.expect(cands)
+        x, r = A.solve(b, params=_params(eg.MIXED, method=eg.CG, precond=eg.PREC_DIAGONAL))
+        assert _path(r) == want
     finally:
         A.free()
