@@ -867,6 +867,11 @@ def serve_config(args, world, kind):
             "tol": args.tol, "server": kind, "parallelism": f"replicas{world}"}
 
 
+def serve_inner(args):
+    """how the GPU arm's inner solves apply ILU0 (not part of the workload's config)"""
+    return {"ilu_sweeps": args.serve_sweeps, "inner_tol": args.inner_tol or "library default"}
+
+
 def section_serving(args, rank, world, local, pg, nested=False):
     """Poisson-process request streams (200 req/s) of hex Poisson solves, m log-uniform in
     [16, 128], through the native server; the FP64 drop-in serves the first stream one request
@@ -878,7 +883,7 @@ def section_serving(args, rank, world, local, pg, nested=False):
 
     torch.cuda.set_device(local)
     prm = eg.SolverParams(method=eg.BICGSTAB, precond=eg.PREC_ILU0, tol=args.tol, max_iter=20000,
-                          inner_tol=args.inner_tol, abort_not_converged=False)
+                          inner_tol=args.inner_tol, abort_not_converged=False, ilu_sweeps=args.serve_sweeps)
     nstreams = max(1, args.serve_streams)
     streams = [server.poisson_stream(args.requests, rate=args.rate, m_lo=16, m_hi=128,
                                      seed=(1 + rank) if s == 0 else 1000 * (rank + 1) + s, sigma=1.0)
@@ -940,7 +945,8 @@ def section_serving(args, rank, world, local, pg, nested=False):
         med = int(np.argsort(rates)[len(rates) // 2])
         s0 = stats[0]
         out = {"value": rates[med] * world, "unit": UNIT, "streams": len(stats),
-               "config": serve_config(args, world, "native (egpu_server_*)"), "dtype": "f32 inner / f64 refinement",
+               "config": serve_config(args, world, "native (egpu_server_*)"), "inner": serve_inner(args),
+               "dtype": "f32 inner / f64 refinement",
                "latency_ms": {"p50": stats[med]["p50_ms"], "p99": stats[med]["p99_ms"]},
                "per_stream": stats,
                "fp64_one_at_a_time": stats64,
@@ -982,6 +988,8 @@ def main():
     ap.add_argument("--systems", type=int, default=512, help="batched workload: number of systems")
     ap.add_argument("--requests", type=int, default=400, help="serving workload: requests per stream")
     ap.add_argument("--serve-streams", type=int, default=3, help="serving workload: streams (median reported)")
+    ap.add_argument("--serve-sweeps", type=int, default=1,
+                    help="serving workload: Jacobi sweeps per ILU0 triangle in the FP32 inner solves (0: exact)")
     ap.add_argument("--batch-steps", type=int, default=3, help="nested batched section: timed batches")
     ap.add_argument("--cpu-seconds", type=float, default=6.0, help="nested sections: CPU reference sample")
     ap.add_argument("--no-nested", action="store_true", help="headline workload only")

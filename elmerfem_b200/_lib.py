@@ -60,7 +60,7 @@ class ServerStats(C.Structure):
     _fields_ = [("queued", C.c_longlong), ("resident", C.c_longlong), ("done", C.c_longlong),
                 ("steps", C.c_longlong), ("used_bytes", C.c_double), ("seconds_prepare", C.c_double),
                 ("seconds_step", C.c_double), ("seconds_retire", C.c_double), ("kernel_launches", C.c_longlong),
-                ("bytes_h2d", C.c_double), ("bytes_d2h", C.c_double)]
+                ("bytes_h2d", C.c_double), ("bytes_d2h", C.c_double), ("requeues", C.c_longlong)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

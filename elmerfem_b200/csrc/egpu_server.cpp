@@ -92,6 +92,7 @@ struct egpu_server {
   double t_prepare = 0, t_step = 0, t_retire = 0;  // worker wall time per activity (under mu)
   long long launches = 0;                           // kernel launches of ctx (under mu)
   double bytes_h2d = 0, bytes_d2h = 0;              // request inputs uploaded, solutions read back (under mu)
+  long long requeues = 0;                           // admitted requests put back after a failed allocation (under mu)
   bool stop = false;
   std::thread worker;
 };
@@ -262,6 +263,7 @@ void work(egpu_server *S) {
       S->used -= (*it)->footprint;
       S->queue.push_front(*it);
     }
+    S->requeues += (long long)requeue.size();
     S->launches = nl;
     S->bytes_h2d += h2d;
     S->bytes_d2h += d2h;
@@ -461,6 +463,7 @@ extern "C" int egpu_server_info(egpu_server *S, egpu_server_stats *st) {
   st->kernel_launches = S->launches;
   st->bytes_h2d = S->bytes_h2d;
   st->bytes_d2h = S->bytes_d2h;
+  st->requeues = S->requeues;
   return EGPU_OK;
 }
 

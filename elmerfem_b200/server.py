@@ -312,6 +312,7 @@ class NativeSolveServer:
                 "worker_seconds": {k: round(w1[k] - w0[k], 4) for k in ("seconds_prepare", "seconds_step",
                                                                         "seconds_retire")},
                 "kernel_launches": int(w1["kernel_launches"] - w0["kernel_launches"]),
+                "requeues": int(w1["requeues"] - w0["requeues"]),
                 "bytes_h2d": w1["bytes_h2d"] - w0["bytes_h2d"], "bytes_d2h": w1["bytes_d2h"] - w0["bytes_d2h"]}
 
 

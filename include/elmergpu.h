@@ -350,6 +350,9 @@ typedef struct {
    * (Values, RHS, conductivities, loads, Dirichlet rows) and solutions device -> host, bytes */
   long long kernel_launches;
   double bytes_h2d, bytes_d2h;
+  /* admitted requests put back in the queue because a device allocation failed while others
+   * were resident (each is prepared again when admitted again) */
+  long long requeues;
 } egpu_server_stats;
 int egpu_server_create(int device, const egpu_params *prm, double hbm_budget_bytes, int chunk_iters,
                        int max_resident, egpu_server **out);
