@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstddef>
 #include <map>
 #include <mutex>
@@ -18,15 +19,18 @@ namespace egpu {
 // stay in a process-wide cache, by device, and are handed out again to requests of a size
 // between the block's half and its full size.  A release first synchronises the device,
 // as cudaFree does implicitly, so no queued kernel can still use a block when it is reused.
-// At most DEVCACHE_MAX bytes are kept; an allocation that fails empties the device's cache
-// and retries.
+// At most devcache_cap(dev) bytes are kept (24 GB, or 40% of the device's memory when that
+// is more: a serving stream of large meshes frees and re-allocates tens of GB per second, and
+// every block past the cap costs a cudaFree and a cudaMalloc); an allocation that fails
+// empties the device's cache and retries.  egpu_release_cached_memory gives the blocks back.
 constexpr size_t DEVCACHE_GRAIN = (size_t)1 << 16;   // blocks are multiples of 64 KB
-constexpr size_t DEVCACHE_MAX = (size_t)24 << 30;    // bytes kept in the cache per device
+constexpr size_t DEVCACHE_MIN_CAP = (size_t)24 << 30;
 
 struct DevCache {
   std::mutex mu;
   std::map<int, std::multimap<size_t, void *>> free_blocks;  // device -> size -> block
   std::map<int, size_t> cached;                                 // device -> bytes held
+  std::map<int, size_t> cap;                                    // device -> bytes kept at most
 };
 inline DevCache &devcache() {
   static DevCache *c = new DevCache;  // never destroyed: blocks go back with the process
@@ -77,7 +81,14 @@ inline void dev_free(void *p, size_t cap, int dev) {
   bool keep = false;
   {
     std::lock_guard<std::mutex> g(c.mu);
-    if (c.cached[dev] + cap <= DEVCACHE_MAX) {
+    auto ci = c.cap.find(dev);
+    if (ci == c.cap.end()) {
+      size_t fr = 0, tot = 0;
+      const size_t cp = cudaMemGetInfo(&fr, &tot) == cudaSuccess ? std::max(DEVCACHE_MIN_CAP, tot / 10 * 4)
+                                                                 : DEVCACHE_MIN_CAP;
+      ci = c.cap.emplace(dev, cp).first;
+    }
+    if (c.cached[dev] + cap <= ci->second) {
       c.free_blocks[dev].emplace(cap, p);
       c.cached[dev] += cap;
       keep = true;
