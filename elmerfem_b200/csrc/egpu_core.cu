@@ -1525,10 +1525,6 @@ int solve_mixed(egpu_mat *A, const double *b_dev, double *x_dev, const egpu_para
       a.ilu = A->ilu32.p;
       a.dvals = dv32;
       a.unit_diag = unit_diag ? 1 : 0;
-      {  // CG: direction update inside the SpMV (EGPU_CG_FUSE=0: separate pass)
-        const char *e = std::getenv("EGPU_CG_FUSE");
-        a.fuse_p = !(e && e[0] == '0');
-      }
       set_tri(a, A);
       if (use_sweeps) {
         a.sweeps_l = a.sweeps_u = sweeps;

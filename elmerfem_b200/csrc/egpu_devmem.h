@@ -3,8 +3,8 @@
 
 #include <cuda_runtime.h>
 
-#include <algorithm>
 #include <cstddef>
+#include <iterator>
 #include <map>
 #include <mutex>
 
@@ -19,18 +19,17 @@ namespace egpu {
 // stay in a process-wide cache, by device, and are handed out again to requests of a size
 // between the block's half and its full size.  A release first synchronises the device,
 // as cudaFree does implicitly, so no queued kernel can still use a block when it is reused.
-// At most devcache_cap(dev) bytes are kept (24 GB, or 40% of the device's memory when that
-// is more: a serving stream of large meshes frees and re-allocates tens of GB per second, and
-// every block past the cap costs a cudaFree and a cudaMalloc); an allocation that fails
-// empties the device's cache and retries.  egpu_release_cached_memory gives the blocks back.
+// At most DEVCACHE_MAX bytes are kept.  An allocation that fails gives cached blocks back to
+// the driver, largest first, until the freed bytes cover the request, and retries; only when
+// that is not enough does it empty the device's cache.  (Emptying it on every failure cost
+// seconds of cudaFree per serving stream once the cache was large.)
 constexpr size_t DEVCACHE_GRAIN = (size_t)1 << 16;   // blocks are multiples of 64 KB
-constexpr size_t DEVCACHE_MIN_CAP = (size_t)24 << 30;
+constexpr size_t DEVCACHE_MAX = (size_t)24 << 30;    // bytes kept in the cache per device
 
 struct DevCache {
   std::mutex mu;
   std::map<int, std::multimap<size_t, void *>> free_blocks;  // device -> size -> block
   std::map<int, size_t> cached;                                 // device -> bytes held
-  std::map<int, size_t> cap;                                    // device -> bytes kept at most
 };
 inline DevCache &devcache() {
   static DevCache *c = new DevCache;  // never destroyed: blocks go back with the process
@@ -58,13 +57,26 @@ inline cudaError_t dev_alloc(void **p, size_t bytes, size_t *cap, int *dev) {
   }
   e = cudaMalloc(p, want);
   if (e == cudaErrorMemoryAllocation) {
-    cudaGetLastError();  // clear the sticky-free allocation error before retrying
+    cudaGetLastError();  // clear the non-sticky allocation error before retrying
     std::lock_guard<std::mutex> g(c.mu);
     auto &fb = c.free_blocks[*dev];
-    for (auto &kv : fb) cudaFree(kv.second);
-    fb.clear();
-    c.cached[*dev] = 0;
+    // largest blocks first, until the bytes given back cover the request; then everything
+    size_t given = 0;
+    while (!fb.empty() && given < want) {
+      auto last = std::prev(fb.end());
+      cudaFree(last->second);
+      given += last->first;
+      c.cached[*dev] -= last->first;
+      fb.erase(last);
+    }
     e = cudaMalloc(p, want);
+    if (e == cudaErrorMemoryAllocation && !fb.empty()) {
+      cudaGetLastError();
+      for (auto &kv : fb) cudaFree(kv.second);
+      fb.clear();
+      c.cached[*dev] = 0;
+      e = cudaMalloc(p, want);
+    }
   }
   if (e == cudaSuccess) *cap = want;
   return e;
@@ -81,14 +93,7 @@ inline void dev_free(void *p, size_t cap, int dev) {
   bool keep = false;
   {
     std::lock_guard<std::mutex> g(c.mu);
-    auto ci = c.cap.find(dev);
-    if (ci == c.cap.end()) {
-      size_t fr = 0, tot = 0;
-      const size_t cp = cudaMemGetInfo(&fr, &tot) == cudaSuccess ? std::max(DEVCACHE_MIN_CAP, tot / 10 * 4)
-                                                                 : DEVCACHE_MIN_CAP;
-      ci = c.cap.emplace(dev, cp).first;
-    }
-    if (c.cached[dev] + cap <= ci->second) {
+    if (c.cached[dev] + cap <= DEVCACHE_MAX) {
       c.free_blocks[dev].emplace(cap, p);
       c.cached[dev] += cap;
       keep = true;

@@ -59,7 +59,6 @@ struct KArgs {
   int tri_bs;                     // rows per sync-free slot group (node blocks; 1 = row per slot)
   int unit_diag;                  // FP32 inner CG: every diagonal of the scaled matrix is 1.0f, so the
                                   // Jacobi step is the identity (Z is R, no diagonal loads)
-  int fuse_p;                     // FP32 inner CG without ILU: direction update inside the SpMV
   // ILU0 factors packed in solve order (see TriSchedule)
   const int *lo_ptr, *lo_cols, *up_ptr, *up_cols;
   const VT *lo_vals, *up_vals, *up_dinv;
@@ -244,76 +243,6 @@ __device__ __forceinline__ void spmv_phase(const KArgs<VT> &a, const VT *x0, con
     if (lane == 0 && s2 < a.nslices && nw_w > 0)
       prefetch_l2_bulk(a.svals + nw_p, (unsigned)(32 * nw_w * (int)sizeof(VT)));
     if (r < a.n) epi(r, s0, s1);
-  }
-}
-
-// The FP32 inner CG's SpMV with the direction update folded in: Q = A P_new where
-// P_new = Z + beta P_old is formed at every gathered column from Z and P_old (fmaf, the same
-// rounding as the separate update pass), so the update needs no pass and no grid barrier of
-// its own and the iterates are bit-identical to the unfused form.  first: P_new = Z.  Each
-// lane writes its own row's P_new to pnew (a different vector from pold, which other warps
-// still gather).  epi(row, (A P_new)_row, P_new_row).
-template <bool OFFS, typename F>
-__device__ __forceinline__ void spmv_phase_pz(const KArgs<float> &a, const float *z, const float *pold, float *pnew,
-                                              float beta, bool first, F &&epi) {
-  const int lane = threadIdx.x & 31;
-  const int gw = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int nw = (int)(((long long)gridDim.x * blockDim.x) >> 5);
-  auto px = [&](int c) { return first ? ld_l2(z + c) : fmaf(beta, ld_l2(pold + c), ld_l2(z + c)); };
-  int nw_w = 0, nw_p = 0;
-  if (gw < a.nslices) {
-    nw_w = __ldg(a.sell_w + gw);
-    nw_p = __ldg(a.sell_ptr + gw);
-  }
-  for (int s = gw; s < a.nslices; s += nw) {
-    const int r = (s << 5) + lane;
-    const int w = nw_w;
-    const int base = nw_p + lane;
-    const int s2 = s + nw;
-    if (s2 < a.nslices) {
-      nw_w = __ldg(a.sell_w + s2);
-      nw_p = __ldg(a.sell_ptr + s2);
-    }
-    float s0 = 0.f;
-    if (OFFS && a.scolsc) {
-      const int cp = __ldg(a.sell_cptr + s);
-      if (cp < 0) {
-        const int16_t *co = a.scolsc + (-cp - 1);
-        for (int k0 = 0; k0 < w; k0 += 32) {
-          const int kn = min(32, w - k0);
-          const int offl = lane < kn ? (int)__ldg(co + k0 + lane) : 0;
-#pragma unroll 8
-          for (int k = 0; k < kn; ++k) {
-            const float v = ld_stream(a.svals + base + ((k0 + k) << 5));
-            const int c = r + __shfl_sync(0xffffffffu, offl, k);
-            s0 = fmaf(v, px(c), s0);
-          }
-        }
-      } else {
-        const int16_t *co = a.scolsc + cp + lane;
-#pragma unroll 8
-        for (int k = 0; k < w; ++k) {
-          const float v = ld_stream(a.svals + base + (k << 5));
-          const int c = r + (int)ld_stream(co + (k << 5));
-          s0 = fmaf(v, px(c), s0);
-        }
-      }
-    } else {
-#pragma unroll 8
-      for (int k = 0; k < w; ++k) {
-        const int e = base + (k << 5);
-        const float v = ld_stream(a.svals + e);
-        const int c = OFFS ? r + (int)ld_stream(a.scols16 + e) : ld_stream(a.scols + e);
-        s0 = fmaf(v, px(c), s0);
-      }
-    }
-    if (lane == 0 && s2 < a.nslices && nw_w > 0)
-      prefetch_l2_bulk(a.svals + nw_p, (unsigned)(32 * nw_w * (int)sizeof(float)));
-    if (r < a.n) {
-      const float pn = px(r);
-      pnew[r] = pn;
-      epi(r, s0, pn);
-    }
   }
 }
 
@@ -1071,16 +1000,6 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) cg_kernel(KArgs<VT> a) {
   // scale (rho is quadratic in the residual's scale, P linear)
   const bool resumed = a.resume && !a.true_residual;
   if (resumed) oldrho = a.carry[0] * a.ru_c;
-  // FP32 inner solve without ILU: the direction update rides in the SpMV (spmv_phase_pz), P
-  // alternating between work vectors 2 and 4; carry[2] says which holds the carried P
-  constexpr bool fz = sizeof(VT) == 4;
-  const bool fuse = fz && !a.true_residual && !ilu && a.fuse_p;
-  VT *Palt = a.w + 4 * a.ldw;
-  if (fuse && resumed && a.carry[2] == 1.0) {
-    VT *t = P;
-    P = Palt;
-    Palt = t;
-  }
   while (true) {
     rho = reduce_partials(a.partials + SLOT_RHO * nb, nb, sm);
     if (!a.true_residual && k > 1) {
@@ -1089,8 +1008,8 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) cg_kernel(KArgs<VT> a) {
       if (residual <= a.tol) { info = EGPU_HUTI_CONVERGENCE; iters = k - 1; break; }
       if (k > a.maxit) { info = EGPU_HUTI_MAXITER; iters = k - 1; break; }
     }
-    // ---- P = Z (first iteration) or Z + beta P   (fused: in the SpMV below)
-    if (!fuse) {
+    // ---- P = Z (first iteration) or Z + beta P
+    {
       const VT beta = (VT)(rho / oldrho);
       const bool first = k == 1 && !resumed;
       vec_loop<VT>(n, [&](int i, auto w) {
@@ -1106,24 +1025,12 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) cg_kernel(KArgs<VT> a) {
           vfill<W>(Y, i, SENT);
         }
       });
-      if (!grid_barrier(a.bar, a.err, epoch)) return;
     }
+    if (!grid_barrier(a.bar, a.err, epoch)) return;
     // ---- Q = A P  (+ A x_{k-1} for the stopping test of iterate k-1)
     {
       double acc[2] = {0.0, 0.0};
-      if constexpr (fz) {
-        if (fuse) {
-          spmv_phase_pz<OFFS>(a, Z, P, Palt, (float)(rho / oldrho), k == 1 && !resumed, [&](int i, float s0, float pn) {
-            Q[i] = s0;
-            acc[0] += (double)pn * (double)s0;
-          });
-          VT *t = P;
-          P = Palt;
-          Palt = t;
-        }
-      }
-      if (fuse) {
-      } else if (a.true_residual && k > 1) {
+      if (a.true_residual && k > 1) {
         spmv_phase<VT, LPR, OFFS, true>(a, P, X, [&](int i, VT s0, VT s1) {
           Q[i] = s0;
           acc[0] += (double)P[i] * (double)s0;
@@ -1233,7 +1140,6 @@ __global__ void __launch_bounds__(EGPU_KBLOCK, 1) cg_kernel(KArgs<VT> a) {
     a.out_d[1] = rhsnorm;
     if (a.carry) {  // state for the next segment: P was built with oldrho
       a.carry[0] = oldrho;
-      a.carry[2] = (fuse && P != a.w + 2 * a.ldw) ? 1.0 : 0.0;
       a.carry[3] = (!a.true_residual && info == EGPU_HUTI_CONVERGENCE && k > 1) ? 1.0 : 0.0;
     }
   }
