@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <cstdlib>
 #include <iterator>
 #include <map>
 #include <mutex>
@@ -19,12 +20,21 @@ namespace egpu {
 // stay in a process-wide cache, by device, and are handed out again to requests of a size
 // between the block's half and its full size.  A release first synchronises the device,
 // as cudaFree does implicitly, so no queued kernel can still use a block when it is reused.
-// At most DEVCACHE_MAX bytes are kept.  An allocation that fails gives cached blocks back to
+// At most devcache_max() bytes are kept.  An allocation that fails gives cached blocks back to
 // the driver, largest first, until the freed bytes cover the request, and retries; only when
 // that is not enough does it empty the device's cache.  (Emptying it on every failure cost
 // seconds of cudaFree per serving stream once the cache was large.)
 constexpr size_t DEVCACHE_GRAIN = (size_t)1 << 16;   // blocks are multiples of 64 KB
-constexpr size_t DEVCACHE_MAX = (size_t)24 << 30;    // bytes kept in the cache per device
+
+// bytes kept in the cache per device: 24 GB, or EGPU_DEVCACHE_GB
+inline size_t devcache_max() {
+  static const size_t v = [] {
+    const char *e = std::getenv("EGPU_DEVCACHE_GB");
+    const double gb = e ? std::atof(e) : 24.0;
+    return (size_t)((gb > 0 ? gb : 0.0) * (double)(1ull << 30));
+  }();
+  return v;
+}
 
 struct DevCache {
   std::mutex mu;
@@ -93,7 +103,7 @@ inline void dev_free(void *p, size_t cap, int dev) {
   bool keep = false;
   {
     std::lock_guard<std::mutex> g(c.mu);
-    if (c.cached[dev] + cap <= DEVCACHE_MAX) {
+    if (c.cached[dev] + cap <= devcache_max()) {
       c.free_blocks[dev].emplace(cap, p);
       c.cached[dev] += cap;
       keep = true;
