@@ -988,7 +988,7 @@ def main():
     ap.add_argument("--systems", type=int, default=512, help="batched workload: number of systems")
     ap.add_argument("--requests", type=int, default=400, help="serving workload: requests per stream")
     ap.add_argument("--serve-streams", type=int, default=3, help="serving workload: streams (median reported)")
-    ap.add_argument("--serve-sweeps", type=int, default=1,
+    ap.add_argument("--serve-sweeps", type=int, default=2,
                     help="serving workload: Jacobi sweeps per ILU0 triangle in the FP32 inner solves (0: exact)")
     ap.add_argument("--batch-steps", type=int, default=3, help="nested batched section: timed batches")
     ap.add_argument("--cpu-seconds", type=float, default=6.0, help="nested sections: CPU reference sample")

@@ -2124,8 +2124,12 @@ extern "C" long long egpu_matrix_footprint(const egpu_mat *A, int precond) {
   b += 8 * z + 8 * zs + 4 * zs;             // scaled CRS, SELL FP64, SELL FP32
   b += 8 * n + 13 * 8 * l + 14 * 4 * l;     // DiagScaling, work vectors
   const long long zi = std::max(z, A->ilu_nnz);   // ILU structure (ILU(n) fill included once built)
-  if (is_ilu(precond)) b += 8 * zi + 4 * zi + 4 * n + (zi > z ? 8 * zi : 0);  // factors, flags, scatter
-  if (is_ilu(precond)) b += 12 * (A->tri.cta_lo.nent + A->tri.cta_up.nent);  // single-block layout
+  if (is_ilu(precond)) {
+    b += 8 * zi + 4 * zi + 4 * n + (zi > z ? 8 * zi : 0);  // factors FP64 / FP32, flags, scatter
+    b += 12 * zi + 12 * n;                                 // factors packed in solve order, FP64 + FP32
+    b += 4 * zs + 4 * n;                                   // FP32 factors in SELL order (Jacobi sweeps)
+    b += 12 * (A->tri.cta_lo.nent + A->tri.cta_up.nent);   // single-block layout
+  }
   return b + 8 * n;                         // back-scaled solution
 }
 

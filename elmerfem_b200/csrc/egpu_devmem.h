@@ -18,7 +18,7 @@ namespace egpu {
 // cost milliseconds each and vary with the driver's state (measured on B200: 1 to 5 s of
 // allocation and free per 48-request serving stream, varying from run to run).  Freed blocks therefore
 // stay in a process-wide cache, by device, and are handed out again to requests of a size
-// between the block's half and its full size.  A release first synchronises the device,
+// between two thirds of the block's size and its full size.  A release first synchronises the device,
 // as cudaFree does implicitly, so no queued kernel can still use a block when it is reused.
 // At most devcache_max() bytes are kept.  An allocation that fails gives cached blocks back to
 // the driver, largest first, until the freed bytes cover the request, and retries; only when
@@ -57,7 +57,7 @@ inline cudaError_t dev_alloc(void **p, size_t bytes, size_t *cap, int *dev) {
     std::lock_guard<std::mutex> g(c.mu);
     auto &fb = c.free_blocks[*dev];
     auto it = fb.lower_bound(want);
-    if (it != fb.end() && it->first <= 2 * want) {
+    if (it != fb.end() && it->first <= want + want / 2) {
       *p = it->second;
       *cap = it->first;
       c.cached[*dev] -= it->first;
