@@ -731,7 +731,7 @@ def section_batched(args, rank, world, local, pg, nested=False):
     launches0 = ctx.kernel_launches
     barrier(pg, dev)
     torch.cuda.synchronize()
-    times, allres = [], None
+    times, kms, allres = [], [], None
     with ClockSampler(local) as clk:
         for _ in range(steps):
             e0.record(ext)
@@ -739,6 +739,7 @@ def section_batched(args, rank, world, local, pg, nested=False):
             e1.record(ext)
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1) / 1000.0)
+            kms.append(B.last_launch_ms())
             if allres is None:
                 allres = res
                 xs_b = [B.solution(i) for i in ids]
@@ -801,6 +802,10 @@ def section_batched(args, rank, world, local, pg, nested=False):
     units = [unit_diag_of(A) for A in mats]
     bpi = sum(algorithmic_bytes_per_iter(1, 1, "mixed", A.n, A.nnz, True, 1.0, u) * r["iters"]
               for A, r, u in zip(mats, allres, units))
+    # device time of the batched launch (the team solver runs every solve in one launch; on the
+    # stepwise path this is the last chunk only, and the whole step is the honest figure)
+    teams = os.environ.get("EGPU_BATCH_TEAMS", "1") != "0"
+    kt = float(np.mean(kms)) / 1000.0 if teams and kms and min(kms) > 0 else t / steps
     # against the FP64 oracle: a seeded sample of systems (the smallest six and two more)
     out = None
     if rank == 0:
@@ -833,9 +838,13 @@ def section_batched(args, rank, world, local, pg, nested=False):
                "rel_err_vs_oracle": {"systems": [int(j) for j in pick], "m": [int(ms[j]) for j in pick],
                                      "mixed_max": max(eo), "fp64_max": max(e64o), "bound": 1e-8},
                "iterations": {"inner_total": inner_iters},
-               "roofline": {"bound": "hbm", "achieved": bpi / (t / steps) / 1e9, "peak": peak,
-                            "unit": "GB/s", "frac": bpi / (t / steps) / 1e9 / peak, "traffic": None,
-                            "peak_kind": peak_kind, "kernel": "k_batch_inner (whole step incl. refinement)",
+               "roofline": {"bound": "hbm", "achieved": bpi / kt / 1e9, "peak": peak,
+                            "unit": "GB/s", "frac": bpi / kt / 1e9 / peak, "traffic": None,
+                            "peak_kind": peak_kind,
+                            "kernel": "k_batch_team (one cooperative launch: every system's whole mixed solve, "
+                                      "FP64 residuals included)",
+                            "kernel_ms": 1000 * kt,
+                            "whole_step_achieved": bpi / (t / steps) / 1e9,
                             "unit_diagonal_systems": int(sum(units))},
                "e2e": {"value": world * nsys * steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * ndofs,
                        "d2h_bytes_per_step": 8 * ndofs, "max_rel_diff_vs_device_timed": e2e_err},

@@ -128,6 +128,7 @@ PROTOTYPES = {
     "egpu_batch_step": (C.c_int, [_vp, _vp, C.POINTER(C.c_int)]),
     "egpu_batch_pending": (C.c_int, [_vp]),
     "egpu_batch_solve": (C.c_int, [_vp, _vp]),
+    "egpu_batch_last_launch": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "egpu_batch_result": (C.c_int, [_vp, C.c_int, C.POINTER(Result)]),
     "egpu_batch_solution": (C.c_int, [_vp, C.c_int, _f64p]),
     "egpu_batch_remove": (C.c_int, [_vp, C.c_int]),

@@ -1090,6 +1090,310 @@ __global__ void k_batch_backscale(int nsel, const int *sel, const RefDesc *rd, c
   }
 }
 
+// ------------------------------------------------------------------------------------
+// Team solver (CG with M = I or Jacobi, egpu_batch_solve).  The systems are independent, so
+// none needs to wait for another: each system's whole mixed-precision solve (FP64 residual,
+// FP32 inner CG segments with reliable updating, FP64 update; the same sequence as
+// egpu_batch_step's) runs on a team of CTAs of one cooperative launch.  A small system's team
+// is one CTA, synchronised by block barriers only; a large one's is several CTAs that split
+// its SELL slices and meet at a barrier of their own (one counter per system).  CTAs take
+// (system, member) tasks from a queue ordered largest team first, so every team is formed
+// from CTAs that are free at once and the small systems fill in behind.  Dot products: block
+// sums, one partial per member, summed in member order by every member (same value in all).
+
+constexpr int TEAM_MAX = 16;
+constexpr int TEAM_BLOCK = EGPU_KBLOCK;  // threads of a team CTA
+constexpr int TEAM_PER_SM = 65536 / (TEAM_BLOCK * 64);  // CTAs per SM at 64 registers a thread
+enum { TS_BB = 0, TS_RHO0, TS_PQ, TS_RHO, TS_RR, TS_RES, TS_NSLOT };
+
+struct TeamSys {
+  int n, nslices, team;
+  int zr;                  // Z is R: no preconditioner, or Jacobi on a diagonal that is 1.0f everywhere
+  const int *sell_ptr, *sell_w;
+  const int16_t *scols16;  // col - row (FP32 SpMV), or null: scols
+  const int *scols;        // absolute columns
+  const float *svals32, *dvals32;
+  float *w32;              // R Z P Q D(inner solution), stride ldw
+  long long ldw;
+  const double *svals64;   // scaled FP64 values, SELL order
+  const double *bs;        // scaled right-hand side
+  double *xs, *r64;        // scaled solution, FP64 residual
+  double bnorm_s;          // ||bs|| (1 when the right-hand side was normalised)
+  unsigned int *bar;       // the team's barrier counter
+  double *part;            // TS_NSLOT x team partial sums
+};
+
+struct TeamOut {
+  int info, iters, refinements, pad;
+  double residual;
+};
+
+struct TeamTask {
+  int sys, rank;
+};
+
+struct TeamArgs {
+  int ntasks;
+  const TeamTask *tasks;
+  unsigned int *next;      // queue position
+  const TeamSys *sys;
+  TeamOut *out;
+  double tol, inner_tol;
+  int inner_maxit, max_iter, max_ref, resume_ok;
+  int *err;
+};
+
+// barrier of one team (T CTAs; a block barrier when T = 1), bounded like grid_barrier.  The
+// error word is read once, by thread 0, and broadcast, so the whole block takes the same way out.
+__device__ __forceinline__ bool team_sync(unsigned int *cnt, int team, unsigned int &epoch, int *err) {
+  __shared__ int ok_s;
+  __syncthreads();
+  if (team > 1) {
+    epoch += 1;
+    if (threadIdx.x == 0) {
+      const unsigned int target = epoch * (unsigned int)team;
+      red_release_add_u32(cnt, 1u);
+      if (ld_acquire_u32(cnt) < target) {
+        const unsigned long long t0 = egpu_globaltimer(), lim = egpu_wait_limit(err);
+        unsigned int spins = 0;
+        while (ld_acquire_u32(cnt) < target) {
+          if ((++spins & 63u) == 0) {
+            if (*(volatile int *)err) break;
+            if (egpu_globaltimer() - t0 > lim) {
+              atomicCAS(err, 0, (int)EGPU_ERR_TIMEOUT);
+              break;
+            }
+          }
+        }
+      }
+      __threadfence();
+    }
+  }
+  if (threadIdx.x == 0) ok_s = *(volatile int *)err == 0;
+  __syncthreads();
+  return ok_s != 0;
+}
+
+// NV team-wide sums: the block's sums of v, one partial per member in slots [slot, slot + NV),
+// then every member adds the team's partials in member order
+template <int NV>
+__device__ __forceinline__ bool team_sum(const TeamSys &S, int rank, int slot, double (&v)[NV], double *sm,
+                                         unsigned int &epoch, int *err) {
+  block_sum<NV>(v, sm);
+  if (S.team == 1) return team_sync(S.bar, 1, epoch, err);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) S.part[(slot + k) * S.team + rank] = v[k];
+  if (!team_sync(S.bar, S.team, epoch, err)) return false;
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    double t = 0.0;
+    for (int q = 0; q < S.team; ++q) t += __ldcg(S.part + (slot + k) * S.team + q);
+    v[k] = t;
+  }
+  return true;
+}
+
+// f(i, VW<W>) over this member's rows [r0, r1): 16-byte groups (r0 is a multiple of 32 and the
+// work vectors are 256-byte aligned with a stride of a multiple of 64), then a scalar tail;
+// unrolled so each thread keeps several groups' loads in flight
+template <typename F>
+__device__ __forceinline__ void team_vec(int r0, int r1, F &&f) {
+  const int q0 = r0 >> 2, q1 = r1 >> 2;
+#pragma unroll 4
+  for (int q = q0 + (int)threadIdx.x; q < q1; q += blockDim.x) f(q << 2, VW<4>{});
+  for (int i = (q1 << 2) + (int)threadIdx.x; i < r1; i += blockDim.x) f(i, VW<1>{});
+}
+
+// one member's whole solve of system S; false on a recorded error
+__device__ bool team_solve(const TeamArgs &a, const TeamSys &S, int rank, TeamOut &o, double *sm) {
+  const int n = S.n, T = S.team;
+  const int per = (S.nslices + T - 1) / T;
+  const int sb = min(S.nslices, rank * per), se = min(S.nslices, sb + per);
+  const int r0 = sb << 5, r1 = min(n, se << 5);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  float *R = S.w32, *Z = S.zr ? S.w32 : S.w32 + S.ldw, *P = S.w32 + 2 * S.ldw, *Q = S.w32 + 3 * S.ldw,
+        *Dd = S.w32 + 4 * S.ldw;
+  unsigned int epoch = 0;
+  int refinements = 0, inner_total = 0, info = 0, last_info = 0;
+  double residual = 0.0, rnorm = 1.0, rnorm_prev = 1.0, carry_rho = 0.0;
+  while (true) {
+    // ---- FP64 residual r = bs - A xs on this member's rows (as k_batch_residual)
+    double acc[2] = {0.0, 0.0};
+    for (int s = sb + warp; s < se; s += nwarp) {
+      const int r = (s << 5) + lane;
+      const int w = S.sell_w[s];
+      const int base = S.sell_ptr[s] + lane;
+      double t = 0.0;
+      for (int k = 0; k < w; ++k) {
+        const int e = base + (k << 5);
+        t = __dadd_rn(t, __dmul_rn(S.svals64[e], S.xs[S.scols[e]]));
+      }
+      if (r < n) {
+        const double ri = S.bs[r] - t;
+        S.r64[r] = ri;
+        acc[0] += ri * ri;
+      }
+    }
+    double rr1[1] = {acc[0]};
+    if (!team_sum<1>(S, rank, TS_RES, rr1, sm, epoch, a.err)) return false;
+    residual = sqrt(rr1[0]) / S.bnorm_s;
+    if (residual < a.tol) {
+      info = EGPU_HUTI_CONVERGENCE;
+      break;
+    }
+    if (refinements >= a.max_ref || inner_total >= a.max_iter) {
+      info = EGPU_HUTI_MAXITER;
+      break;
+    }
+    rnorm_prev = rnorm;
+    rnorm = sqrt(rr1[0]);
+    // ---- inner FP32 CG on A d = r / ||r||, d0 = 0 (huti_cg_D.F90:158-240, recursive residual);
+    // reliable updating: a segment after a converged one keeps P and continues with
+    // rho_{k-1} scaled to the new residual (rho is quadratic in the scale, P linear)
+    const bool resume = a.resume_ok && refinements > 0 && last_info == EGPU_HUTI_CONVERGENCE;
+    double oldrho = resume ? carry_rho * (rnorm_prev / rnorm) : 1.0;
+    acc[0] = acc[1] = 0.0;
+    team_vec(r0, r1, [&](int i, auto vw) {
+      constexpr int W = decltype(vw)::value;
+      float r[W], z[W], d[W];
+#pragma unroll
+      for (int t = 0; t < W; ++t) r[t] = (float)(S.r64[i + t] / rnorm);
+      if (!S.zr) vld<W>(S.dvals32, i, d);
+#pragma unroll
+      for (int t = 0; t < W; ++t) {
+        z[t] = S.zr ? r[t] : diag_prec(r[t], d[t]);
+        acc[0] += (double)r[t] * (double)r[t];
+        acc[1] += (double)r[t] * (double)z[t];
+      }
+      vst<W>(R, i, r);
+      vfill<W>(Dd, i, 0.f);
+      if (!S.zr) vst<W>(Z, i, z);
+    });
+    if (!team_sum<2>(S, rank, TS_BB, acc, sm, epoch, a.err)) return false;
+    const double rhsnorm = sqrt(acc[0]);
+    double rho = acc[1], rr_prev = 0.0;
+    int k = 1, iters = 0, iinfo = 0;
+    while (true) {
+      if (k > 1) {
+        const double res_in = sqrt(rr_prev) / rhsnorm;
+        if (res_in <= a.inner_tol) { iinfo = EGPU_HUTI_CONVERGENCE; iters = k - 1; break; }
+        if (k > a.inner_maxit) { iinfo = EGPU_HUTI_MAXITER; iters = k - 1; break; }
+      }
+      // P = Z (first direction) or Z + beta P
+      const float beta = (float)(rho / oldrho);
+      const bool first = k == 1 && !resume;
+      team_vec(r0, r1, [&](int i, auto vw) {
+        constexpr int W = decltype(vw)::value;
+        float z[W], p[W];
+        vld<W>(Z, i, z);
+        if (!first) vld<W>(P, i, p);
+#pragma unroll
+        for (int t = 0; t < W; ++t) p[t] = first ? z[t] : z[t] + beta * p[t];
+        vst<W>(P, i, p);
+      });
+      if (!team_sync(S.bar, T, epoch, a.err)) return false;
+      // Q = A P on this member's slices, (P, Q)
+      double pq[1] = {0.0};
+      for (int s = sb + warp; s < se; s += nwarp) {
+        const int r = (s << 5) + lane;
+        const int w = S.sell_w[s];
+        const int base = S.sell_ptr[s] + lane;
+        const int s2 = s + nwarp;
+        if (lane == 0 && s2 < se) {
+          const int w2 = S.sell_w[s2], p2 = S.sell_ptr[s2];
+          prefetch_l2_bulk(S.svals32 + p2, (unsigned)(128 * w2));
+          if (S.scols16) prefetch_l2_bulk(S.scols16 + p2, (unsigned)(64 * w2));
+        }
+        float t = 0.f;
+        if (S.scols16) {
+#pragma unroll 16
+          for (int kk = 0; kk < w; ++kk) {
+            const int e = base + (kk << 5);
+            t = fmaf(__ldcs(S.svals32 + e), __ldca(P + r + (int)__ldcs(S.scols16 + e)), t);
+          }
+        } else {
+#pragma unroll 8
+          for (int kk = 0; kk < w; ++kk) {
+            const int e = base + (kk << 5);
+            t = fmaf(__ldcs(S.svals32 + e), __ldca(P + __ldcs(S.scols + e)), t);
+          }
+        }
+        if (r < n) {
+          Q[r] = t;
+          pq[0] += (double)P[r] * (double)t;
+        }
+      }
+      if (!team_sum<1>(S, rank, TS_PQ, pq, sm, epoch, a.err)) return false;
+      if (rho == 0.0) { iinfo = EGPU_HUTI_CG_RHO; iters = k; break; }
+      const double alpha_d = rho / pq[0];
+      const float alpha = (float)alpha_d;
+      // D += alpha P, R -= alpha Q, Z = M^-1 R, (R, Z), (R, R)
+      acc[0] = acc[1] = 0.0;
+      team_vec(r0, r1, [&](int i, auto vw) {
+        constexpr int W = decltype(vw)::value;
+        float d[W], p[W], r[W], q[W], g[W], z[W];
+        vld<W>(Dd, i, d);
+        vld<W>(P, i, p);
+        vld<W>(R, i, r);
+        vld<W>(Q, i, q);
+        if (!S.zr) vld<W>(S.dvals32, i, g);
+#pragma unroll
+        for (int t = 0; t < W; ++t) {
+          d[t] = d[t] + alpha * p[t];
+          r[t] = r[t] - alpha * q[t];
+          z[t] = S.zr ? r[t] : diag_prec(r[t], g[t]);
+          acc[0] += (double)r[t] * (double)z[t];
+          acc[1] += (double)r[t] * (double)r[t];
+        }
+        vst<W>(Dd, i, d);
+        vst<W>(R, i, r);
+        if (!S.zr) vst<W>(Z, i, z);
+      });
+      if (!team_sum<2>(S, rank, TS_RHO, acc, sm, epoch, a.err)) return false;
+      rr_prev = acc[1];
+      oldrho = rho;
+      rho = acc[0];
+      ++k;
+    }
+    inner_total += max(1, iters);
+    last_info = iinfo;
+    carry_rho = oldrho;  // P was built with it
+    // xs += ||r|| d on this member's rows; the next residual gathers them
+    team_vec(r0, r1, [&](int i, auto vw) {
+      constexpr int W = decltype(vw)::value;
+#pragma unroll
+      for (int t = 0; t < W; ++t) S.xs[i + t] += rnorm * (double)Dd[i + t];
+    });
+    ++refinements;
+    if (!team_sync(S.bar, T, epoch, a.err)) return false;
+  }
+  o.info = info;
+  o.iters = inner_total;
+  o.refinements = refinements;
+  o.residual = residual;
+  return true;
+}
+
+__global__ void __launch_bounds__(TEAM_BLOCK, TEAM_PER_SM) k_batch_team(TeamArgs a) {
+  __shared__ double sm[32 * 2];
+  __shared__ int task;
+  __shared__ TeamSys S;  // the system's descriptor, read by every thread (never aliased by the vectors)
+  while (true) {
+    __syncthreads();
+    if (threadIdx.x == 0) task = *(volatile int *)a.err ? a.ntasks : (int)atomicAdd(a.next, 1u);
+    __syncthreads();
+    const int t = task;
+    if (t >= a.ntasks) return;
+    const TeamTask tk = a.tasks[t];
+    if (threadIdx.x == 0) S = a.sys[tk.sys];
+    __syncthreads();
+    TeamOut o{};
+    if (!team_solve(a, S, tk.rank, o, sm)) return;
+    if (tk.rank == 0 && threadIdx.x == 0) a.out[tk.sys] = o;
+  }
+}
+
 }  // namespace egpu
 
 // =====================================================================================
@@ -1135,6 +1439,13 @@ struct egpu_batch {
   float last_ms = 0.f;
   int last_iters = 0;
   long long last_nnz = 0;
+  // team solver (egpu_batch_solve with CG): descriptors, task queue, results, team barriers,
+  // partial sums
+  DevBuf<TeamSys> d_team;
+  DevBuf<TeamTask> d_tasks;
+  DevBuf<TeamOut> d_tout;
+  DevBuf<unsigned int> d_tbar;
+  DevBuf<double> d_part;
 };
 
 static int slot_of(egpu_batch *B) {
@@ -1321,6 +1632,23 @@ static int upload_selection(egpu_batch *B, const std::vector<int> &sel, int *tot
   return EGPU_OK;
 }
 
+// the per-system descriptor tables, uploaded when systems were admitted or removed
+static int upload_desc(egpu_batch *B) {
+  const int ns = (int)B->sys.size();
+  if (!B->desc_dirty || ns == 0) return EGPU_OK;
+  std::vector<SysDesc> d(ns);
+  std::vector<RefDesc> r(ns);
+  for (int i = 0; i < ns; ++i)
+    if (B->sys[i] && i < (int)B->h_desc.size()) {
+      d[i] = B->h_desc[i];
+      r[i] = B->h_ref[i];
+    }
+  EGPU_CUDA_TRY(B->ctx, cudaMemcpy(B->d_desc.p, d.data(), ns * sizeof(SysDesc), cudaMemcpyHostToDevice));
+  EGPU_CUDA_TRY(B->ctx, cudaMemcpy(B->d_ref.p, r.data(), ns * sizeof(RefDesc), cudaMemcpyHostToDevice));
+  B->desc_dirty = false;
+  return EGPU_OK;
+}
+
 // One server step: FP64 residuals + decisions for systems that need them, then one chunk
 // of the batched inner solver.  finished[] receives slots completed in this step.
 extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
@@ -1329,18 +1657,8 @@ extern "C" int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished) {
   cudaSetDevice(ctx->device);
   const int ns = (int)B->sys.size();
   int nf = 0;
-  if (B->desc_dirty && ns > 0) {
-    std::vector<SysDesc> d(ns);
-    std::vector<RefDesc> r(ns);
-    for (int i = 0; i < ns; ++i)
-      if (B->sys[i] && i < (int)B->h_desc.size()) {
-        d[i] = B->h_desc[i];
-        r[i] = B->h_ref[i];
-      }
-    EGPU_CUDA_TRY(ctx, cudaMemcpy(B->d_desc.p, d.data(), ns * sizeof(SysDesc), cudaMemcpyHostToDevice));
-    EGPU_CUDA_TRY(ctx, cudaMemcpy(B->d_ref.p, r.data(), ns * sizeof(RefDesc), cudaMemcpyHostToDevice));
-    B->desc_dirty = false;
-  }
+  int rc0 = upload_desc(B);
+  if (rc0) return rc0;
   // systems that finished while nobody collected the list (egpu_batch_tune) are listed now
   if (finished)
     for (int i = 0; i < ns; ++i)
@@ -1563,6 +1881,12 @@ extern "C" int egpu_batch_set_chunk(egpu_batch *B, int chunk_iters) {
   return EGPU_OK;
 }
 
+extern "C" int egpu_batch_last_launch(egpu_batch *B, double *ms) {
+  if (!B || !ms) return EGPU_ERR_ARG;
+  *ms = B->last_ms;
+  return EGPU_OK;
+}
+
 extern "C" int egpu_batch_result(egpu_batch *B, int sys, egpu_result *res) {
   if (!B || sys < 0 || sys >= (int)B->sys.size() || !B->sys[sys] || !res) return EGPU_ERR_ARG;
   const BatchSys *S = B->sys[sys];
@@ -1605,12 +1929,153 @@ extern "C" int egpu_batch_pending(egpu_batch *B) {
   return k;
 }
 
+// egpu_batch_solve on the team solver (k_batch_team): CG with M = I or Jacobi, when every
+// resident system still waits for its first residual (none is inside an inner solve).  Returns
+// 1 when it solved them, 0 when the batch does not qualify (EGPU_BATCH_TEAMS=0 turns it off),
+// < 0 on an error.
+static int batch_solve_teams(egpu_batch *B) {
+  if (B->prm.method != EGPU_CG || B->prm.precond == EGPU_PREC_ILU0) return 0;
+  if (const char *e = std::getenv("EGPU_BATCH_TEAMS"))
+    if (e[0] == '0') return 0;
+  egpu_ctx *ctx = B->ctx;
+  const int ns = (int)B->sys.size();
+  std::vector<int> sel;
+  for (int i = 0; i < ns; ++i)
+    if (B->sys[i]) {
+      if (B->sys[i]->phase == 2) return 0;
+      if (B->sys[i]->phase == 1) sel.push_back(i);
+    }
+  if (sel.empty()) return 0;
+  int rc = upload_desc(B);
+  if (rc) return rc;
+  int bps = 0;
+  EGPU_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_batch_team, TEAM_BLOCK, 0));
+  if (bps < 1) return 0;
+  bps = std::min(bps, TEAM_PER_SM);
+  const int G = ctx->num_sms * bps;
+  // team sizes from a work estimate (nonzeros x n^(1/3): CG's iteration count grows with the
+  // mesh's linear size), at least 64 slices a member; the largest teams take the queue first
+  const size_t m = sel.size();
+  std::vector<double> wk(m);
+  double tot = 0.0;
+  for (size_t j = 0; j < m; ++j) {
+    const egpu_mat *A = B->sys[sel[j]]->A;
+    wk[j] = (double)A->nnz * std::cbrt((double)A->n);
+    tot += wk[j];
+  }
+  const double fair = tot / G;
+  std::vector<int> team(m), ord(m);
+  for (size_t j = 0; j < m; ++j) {
+    const int cap = std::max(1, std::min(TEAM_MAX, B->sys[sel[j]]->A->nslices / 64));
+    team[j] = std::max(1, std::min(cap, (int)std::ceil(wk[j] / fair)));
+    ord[j] = (int)j;
+  }
+  std::sort(ord.begin(), ord.end(), [&](int x, int y) { return team[x] != team[y] ? team[x] > team[y] : wk[x] > wk[y]; });
+  std::vector<TeamSys> ts(ns);
+  std::vector<TeamTask> tasks;
+  EGPU_CUDA_TRY(ctx, B->d_team.alloc(BATCH_MAX_SYS));
+  EGPU_CUDA_TRY(ctx, B->d_tout.alloc(BATCH_MAX_SYS));
+  EGPU_CUDA_TRY(ctx, B->d_tbar.alloc(BATCH_MAX_SYS));
+  EGPU_CUDA_TRY(ctx, B->d_part.alloc((size_t)BATCH_MAX_SYS * TS_NSLOT * TEAM_MAX));
+  for (size_t j = 0; j < m; ++j) {
+    const int i = sel[j];
+    const SysDesc &d = B->h_desc[i];
+    const RefDesc &r = B->h_ref[i];
+    TeamSys t{};
+    t.n = d.n;
+    t.nslices = d.nslices;
+    t.team = team[j];
+    t.zr = (B->prm.precond == EGPU_PREC_NONE || d.unit_diag) ? 1 : 0;
+    t.sell_ptr = d.sell_ptr;
+    t.sell_w = d.sell_w;
+    t.scols16 = d.scols16;
+    t.scols = r.scols;
+    t.svals32 = d.svals;
+    t.dvals32 = d.dvals;
+    t.w32 = d.w;
+    t.ldw = d.ldw;
+    t.svals64 = r.svals;
+    t.bs = r.bs;
+    t.xs = r.xs;
+    t.r64 = r.r;
+    t.bnorm_s = B->sys[i]->bnorm_s;
+    t.bar = B->d_tbar.p + i;
+    t.part = B->d_part.p + (size_t)i * TS_NSLOT * TEAM_MAX;
+    ts[i] = t;
+  }
+  for (int j : ord)
+    for (int q = 0; q < team[j]; ++q) tasks.push_back(TeamTask{sel[j], q});
+  EGPU_CUDA_TRY(ctx, B->d_tasks.alloc(std::max<size_t>(tasks.size(), 1)));
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(B->d_team.p, ts.data(), ns * sizeof(TeamSys), cudaMemcpyHostToDevice, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(B->d_tasks.p, tasks.data(), tasks.size() * sizeof(TeamTask),
+                                     cudaMemcpyHostToDevice, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaMemsetAsync(B->d_tbar.p, 0, BATCH_MAX_SYS * sizeof(unsigned int), ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaMemsetAsync(B->d_tout.p, 0, BATCH_MAX_SYS * sizeof(TeamOut), ctx->stream));
+  // queue position (sync word 0) and error word
+  EGPU_CUDA_TRY(ctx, cudaMemsetAsync(ctx->sync.p, 0, 2 * sizeof(unsigned int), ctx->stream));
+  TeamArgs a{};
+  a.ntasks = (int)tasks.size();
+  a.tasks = B->d_tasks.p;
+  a.next = ctx->sync.p;
+  a.sys = B->d_team.p;
+  a.out = B->d_tout.p;
+  a.tol = B->prm.tol;
+  a.inner_tol = inner_tol_of(&B->prm);
+  a.inner_maxit = B->prm.inner_max_iter;
+  a.max_iter = B->prm.max_iter;
+  a.max_ref = B->prm.max_refinements;
+  a.resume_ok = B->resume_ok ? 1 : 0;
+  a.err = (int *)(ctx->sync.p + 1);
+  void *args[] = {&a};
+  EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ek0, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaLaunchCooperativeKernel((const void *)k_batch_team, dim3(G), dim3(TEAM_BLOCK), args, 0,
+                                                 ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaEventRecord(ctx->ek1, ctx->stream));
+  ctx->launches++;
+  B->launches++;
+  std::vector<TeamOut> out(ns);
+  unsigned int herr[2] = {0, 0};
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(out.data(), B->d_tout.p, ns * sizeof(TeamOut), cudaMemcpyDeviceToHost, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaMemcpyAsync(herr, ctx->sync.p, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
+  EGPU_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (herr[1]) {
+    egpu_set_error(ctx, egpu_device_status_text((int)herr[1]) + " in the batched team solver");
+    return (int)herr[1];
+  }
+  cudaEventElapsedTime(&B->last_ms, ctx->ek0, ctx->ek1);
+  B->last_nnz = 0;
+  B->last_iters = 0;
+  for (int i : sel) {
+    BatchSys *S = B->sys[i];
+    S->info = out[i].info;
+    S->inner_iters = out[i].iters;
+    S->refinements = out[i].refinements;
+    S->residual = out[i].residual;
+    S->phase = 3;
+    B->last_nnz += S->A->nnz;
+    B->last_iters = std::max(B->last_iters, out[i].iters);
+  }
+  int total = 0;
+  rc = upload_selection(B, sel, &total);
+  if (rc) return rc;
+  const int grid3 = std::max(1, std::min((total + 7) / 8, ctx->num_sms * 8));
+  k_batch_backscale<<<grid3, 256, 0, ctx->stream>>>((int)sel.size(), B->d_sel.p, B->d_ref.p, B->d_pre.p);
+  ctx->launches++;
+  B->launches++;
+  EGPU_CUDA_TRY(ctx, cudaGetLastError());
+  return 1;
+}
+
 // Runs every resident system to completion; per_system (optional) receives one result per
 // slot (slots that are free get info 0).
 extern "C" int egpu_batch_solve(egpu_batch *B, egpu_result *per_system) {
   if (!B) return EGPU_ERR_ARG;
   cudaSetDevice(B->ctx->device);
   EGPU_CUDA_TRY(B->ctx, cudaEventRecord(B->ctx->ev0, B->ctx->stream));
+  {
+    const int rt = batch_solve_teams(B);
+    if (rt < 0) return rt;
+  }
   int guard = 0;
   while (egpu_batch_pending(B) > 0) {
     int rc = egpu_batch_step(B, nullptr, nullptr);

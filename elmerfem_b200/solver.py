@@ -459,6 +459,12 @@ class Batch:
     def solve(self):
         check(lib().egpu_batch_solve(self._h, None), self.ctx.handle, "egpu_batch_solve")
 
+    def last_launch_ms(self) -> float:
+        """Device milliseconds of the latest batched launch (the team solver's, or the last chunk's)."""
+        ms = C.c_double(0.0)
+        check(lib().egpu_batch_last_launch(self._h, C.byref(ms)), self.ctx.handle, "egpu_batch_last_launch")
+        return ms.value
+
     def result(self, sid: int) -> dict:
         r = _lib.Result()
         check(lib().egpu_batch_result(self._h, sid, C.byref(r)), self.ctx.handle, "egpu_batch_result")

@@ -283,7 +283,14 @@ int egpu_cg_noalloc(int device, int n, const int *rows_dev, const int *cols_dev,
  *   egpu_batch_add      host Matrix_t arrays + rhs; the batch owns the device copy
  *   egpu_batch_add_matrix  a bound/assembled matrix (b_dev NULL: its assembled rhs); borrowed
  *   egpu_batch_step     one refinement check + one chunk; lists the systems that finished
- *   egpu_batch_solve    steps until every resident system has finished
+ *   egpu_batch_solve    steps until every resident system has finished.  With CG and no
+ *                       preconditioner or Diagonal, when no system is inside an inner solve,
+ *                       it runs every system's whole solve in one cooperative launch instead:
+ *                       each system on a team of CTAs of its own (one CTA when small), with
+ *                       team barriers, no grid barrier and no host round trip between
+ *                       refinements (EGPU_BATCH_TEAMS=0 keeps the stepwise path)
+ *   egpu_batch_last_launch  device milliseconds of the latest batched launch (the team
+ *                       solver's one launch, or the latest chunk of egpu_batch_step)
  *   egpu_batch_remove   frees a finished system's slot
  * Returns the slot id (>= 0) from the add calls, EGPU_ERR_BUDGET when all slots are used. */
 typedef struct egpu_batch egpu_batch;
@@ -298,6 +305,7 @@ int egpu_batch_set_latency_mode(egpu_batch *B, int on);
 int egpu_batch_step(egpu_batch *B, int *finished, int *nfinished);
 int egpu_batch_pending(egpu_batch *B);
 int egpu_batch_solve(egpu_batch *B, egpu_result *per_system);
+int egpu_batch_last_launch(egpu_batch *B, double *ms);
 int egpu_batch_result(egpu_batch *B, int sys, egpu_result *res);
 int egpu_batch_solution(egpu_batch *B, int sys, double *x);
 int egpu_batch_remove(egpu_batch *B, int sys);
