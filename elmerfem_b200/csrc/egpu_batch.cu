@@ -1218,6 +1218,9 @@ __device__ bool team_solve(const TeamArgs &a, const TeamSys &S, int rank, TeamOu
   int refinements = 0, inner_total = 0, info = 0, last_info = 0;
   double residual = 0.0, rnorm = 1.0, rnorm_prev = 1.0, carry_rho = 0.0;
   while (true) {
+    // cancellation: the host-mapped abort word, read once per refinement (the barrier of the
+    // residual's sum below then takes every member out)
+    if (threadIdx.x == 0) egpu_poll_abort(a.err);
     // ---- FP64 residual r = bs - A xs on this member's rows (as k_batch_residual)
     double acc[2] = {0.0, 0.0};
     for (int s = sb + warp; s < se; s += nwarp) {
@@ -1381,7 +1384,10 @@ __global__ void __launch_bounds__(TEAM_BLOCK, TEAM_PER_SM) k_batch_team(TeamArgs
   __shared__ TeamSys S;  // the system's descriptor, read by every thread (never aliased by the vectors)
   while (true) {
     __syncthreads();
-    if (threadIdx.x == 0) task = *(volatile int *)a.err ? a.ntasks : (int)atomicAdd(a.next, 1u);
+    if (threadIdx.x == 0) {
+      egpu_poll_abort(a.err);
+      task = *(volatile int *)a.err ? a.ntasks : (int)atomicAdd(a.next, 1u);
+    }
     __syncthreads();
     const int t = task;
     if (t >= a.ntasks) return;

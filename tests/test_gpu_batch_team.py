@@ -96,3 +96,47 @@ def test_many_systems_every_result_reported(ctx, monkeypatch):
         x_ref, _ = oracle.solve(p, v, b, method=oracle.CG, precond=oracle.PREC_DIAGONAL, max_iter=5000, tol=TOL)
         assert rel(xs[j], x_ref) < 1e-8, j
     assert all(r["info"] == 1 for r in res)
+
+
+def test_abort_word_cancels_the_team_solver(ctx, monkeypatch):
+    """A batched solve that would run for seconds (tolerance 1e-300; it ends by itself at 200,000
+    inner iterations a system) is cancelled from another host thread: it returns EGPU_ERR_ABORT
+    promptly, and once the word is cleared the context solves a batch as the oracle does."""
+    import threading
+    import time
+
+    from elmerfem_b200 import _lib
+
+    monkeypatch.setenv("EGPU_BATCH_TEAMS", "1")
+    systems = [_tet_system(m, 60 + i) for i, m in enumerate([20, 24, 6, 9])]
+    prm = eg.SolverParams(method=eg.CG, precond=eg.PREC_DIAGONAL, tol=1e-300, max_iter=200000,
+                          max_refinements=1000000, inner_tol=3e-4)
+    B = eg.Batch(ctx, prm)
+    out = {}
+
+    def run():
+        try:
+            B.solve()
+            out["rc"] = "returned"
+        except _lib.LibError as e:
+            out["rc"] = e.code
+
+    try:
+        for p, v, b in systems:
+            B.add(_pat(p), v, b)
+        th = threading.Thread(target=run)
+        th.start()
+        time.sleep(0.3)
+        t_abort = time.perf_counter()
+        ctx.abort(True)
+        th.join(timeout=60)
+        assert not th.is_alive()
+        assert out["rc"] == -7, out  # EGPU_ERR_ABORT
+        assert time.perf_counter() - t_abort < 2.0
+    finally:
+        ctx.abort(False)
+        B.free()
+    res, xs = _run(ctx, monkeypatch, systems, True)
+    for (p, v, b), r, x in zip(systems, res, xs):
+        x_ref, _ = oracle.solve(p, v, b, method=oracle.CG, precond=oracle.PREC_DIAGONAL, max_iter=5000, tol=TOL)
+        assert r["info"] == 1 and rel(x, x_ref) < 1e-8
