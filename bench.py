@@ -830,7 +830,12 @@ def section_batched(args, rank, world, local, pg, nested=False):
                    "sample": f"the first {cn} systems in seeded order, whole FP64 oracle solves one at a time "
                              f"({ct:.1f} s)"}
         out = {"value": value, "unit": UNIT, "steps": steps, "ms_per_step": 1000 * t / steps,
-               "config": dict(batch_config(args, world), dofs_total=ndofs, nnz_total=nnz, autotuned=tuned or None),
+               "config": dict(batch_config(args, world), dofs_total=ndofs, nnz_total=nnz,
+                              solver=("team (k_batch_team: one launch, a team of CTAs per system)" if teams
+                                      else "stepwise (k_batch_inner chunks)"),
+                              # the autotuner sets up the stepwise kernel (the first warm-up batch
+                              # runs on it); the team solver sizes its teams from the systems
+                              autotuned_stepwise=tuned or None),
                "dtype": "f32 inner / f64 refinement",
                "fp64_one_at_a_time": {"solves_per_s": nsys / t64, "seconds": t64, "iters_total": it64},
                "speedup_vs_fp64": value / world / (nsys / t64),
